@@ -1,0 +1,286 @@
+/*
+ * vxp.h — C ABI of the B200 voxel contact-generation + TGS-soft solver library.
+ *
+ * This header is the drop-in boundary for the per-step hot path of the Zig
+ * engine nitanmarcel/zig-voxel-physics.  In that engine the seams are two
+ * concrete structs held by value in VoxelPhysicsSystem (src/system.zig:195-198):
+ *
+ *   narrow_phase: NarrowPhase   — beginFrame / processPair / getContactManager
+ *   solver:       ContactSolver — clear / addBody / setContactManager /
+ *                                 addManifold / solve
+ *
+ * and the frame entry VoxelPhysicsSystem.step (src/system.zig:537-555), which
+ * runs narrowPhase() (src/system.zig:586-655), solve() (src/system.zig:670-783)
+ * and updateSleepStates() (src/system.zig:786-792) once per fixed step.  The
+ * entry points below replace those calls; the broad phase stays with the host
+ * and hands its pair list across (BodyPair, src/broad_phase.zig:17-39).
+ *
+ * Conventions
+ *   - Every function returns an int status: VXP_OK (0) or a negative VXP_ERR_*.
+ *     vxp_last_error() gives a one-line message for the last failing call.
+ *   - The context owns all device memory.  Host buffers are borrowed for the
+ *     duration of the call only.
+ *   - One host thread and one CUDA stream per context.
+ *   - All layouts are plain C structs with fixed-width fields (no padding
+ *     surprises: every struct is a multiple of 4 bytes and only the manifold
+ *     contact carries a u64, placed 8-byte aligned).
+ */
+#ifndef VXP_H
+#define VXP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VXP_ABI_VERSION 1
+
+/* ---- status codes (Zig error unions swallowed by `catch {}` in the
+ *      reference become explicit codes here; src/system.zig:577,610,637,...) */
+#define VXP_OK            0
+#define VXP_ERR_ARG      -1  /* bad argument, unknown id, size mismatch      */
+#define VXP_ERR_OOM      -2  /* device or host allocation failed             */
+#define VXP_ERR_CUDA     -3  /* a CUDA runtime call failed                   */
+#define VXP_ERR_TIMEOUT  -4  /* a bounded device-side wait ran out           */
+#define VXP_ERR_CAP      -5  /* a configured capacity was exceeded           */
+#define VXP_ERR_STATE    -6  /* call out of order (e.g. no colliders)        */
+
+/* ---- body types (BodyType, src/body.zig:29-48) */
+#define VXP_BODY_STATIC    0u
+#define VXP_BODY_KINEMATIC 1u
+#define VXP_BODY_DYNAMIC   2u
+
+/* ---- solver constraint ordering.  The reference sweeps manifolds in
+ *      ContactManager hash-map order (src/solver.zig:733); a parallel sweep
+ *      needs colour batches.  Both modes order the sweep colour-major.      */
+#define VXP_COLOUR_PROJECT   0u  /* greedy over writable (dynamic, awake) bodies,
+                                    Jones-Plassmann priorities              */
+#define VXP_COLOUR_REFERENCE 1u  /* GraphColoring.build (src/islands.zig:668-736):
+                                    first-fit in manifold order, every body a node */
+
+/* One 8x8x8 brick of CollisionVoxel bytes (CollisionBrick.voxels,
+ * src/collider.zig:44-46): index x + 8*y + 64*z; bits 0-2 = VoxelType,
+ * bits 3-7 = NORMAL_LUT index (packed struct, src/collision_voxel.zig:133-140). */
+typedef struct {
+    int32_t pos[3];        /* brick position in brick coordinates */
+    uint8_t voxels[512];
+} vxp_brick;               /* 524 bytes */
+
+/* VoxelBody (src/body.zig:177-203) flattened: BodyMotionState + BodyProperties
+ * + sleep fields + the collider it references. */
+typedef struct {
+    uint32_t id;                 /* unique, > 0; the smaller id is body A   */
+    uint32_t body_type;          /* VXP_BODY_*                              */
+    uint32_t collider_id;        /* as passed to vxp_collider_upload        */
+    uint32_t is_sleeping;        /* 0/1                                     */
+    float position[3];
+    float rotation[4];           /* quaternion x, y, z, w                   */
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float inv_mass;
+    float inv_inertia_local[9];  /* Mat3 m[i][j] row-major                  */
+    float friction;
+    float restitution;
+    float linear_damping;
+    float angular_damping;
+    float sleep_timer;
+} vxp_body;                      /* 32 x 4 = 128 bytes */
+
+/* BodyPair (src/broad_phase.zig:17-28); body_a < body_b. */
+typedef struct {
+    uint32_t body_a;
+    uint32_t body_b;
+} vxp_pair;
+
+/* ContactPoint (src/narrow_phase.zig:336-393) in field order. */
+typedef struct {
+    float point[3];
+    float normal[3];
+    float penetration;
+    float local_anchor_a[3];
+    float local_anchor_b[3];
+    float normal_impulse;
+    float tangent_impulse[2];
+    float normal_mass;
+    float tangent_mass[2];
+    uint32_t _pad;
+    uint64_t feature_id;
+} vxp_contact;                   /* 88 bytes */
+
+/* ContactManifold (src/narrow_phase.zig:416-448); friction_anchor is never
+ * set by the reference and is omitted. */
+typedef struct {
+    uint32_t body_a_id;
+    uint32_t body_b_id;
+    uint32_t contact_count;
+    float friction;
+    float restitution;
+    uint32_t _pad;
+    vxp_contact contacts[4];
+} vxp_manifold;                  /* 24 + 352 = 376 bytes */
+
+/* PhysicsConfig (src/system.zig:47-88) + SolverConfig (src/solver.zig:75-119)
+ * + NarrowPhaseConfig (src/narrow_phase.zig:1325-1343) + the two documented
+ * deviation flags.  vxp_config_default() fills the reference defaults. */
+typedef struct {
+    /* PhysicsConfig */
+    float gravity[3];
+    float fixed_timestep;
+    uint32_t enable_sleeping;
+    uint32_t enable_warm_starting;
+    /* SolverConfig */
+    uint32_t substeps;
+    uint32_t velocity_iterations;
+    uint32_t position_iterations;
+    uint32_t disable_rotation;
+    float hertz;
+    float damping_ratio;
+    float position_correction_rate;
+    float max_position_correction;
+    float slop;
+    uint32_t warm_starting;
+    float warm_start_scale;
+    uint32_t enable_friction;
+    uint32_t enable_restitution;
+    /* NarrowPhaseConfig */
+    uint32_t use_brick_sat;
+    uint32_t use_brick_pair_cache;
+    uint32_t brick_pair_cache_size;
+    /* deviation flags */
+    uint32_t reference_caps;     /* 1: keep the reference's 512-pair cap
+                                    (src/system.zig:594,612); 0: uncapped   */
+    uint32_t colouring;          /* VXP_COLOUR_*                           */
+    /* capacities (device buffers are sized from these; 0 = grow on demand) */
+    uint32_t max_bodies;
+    uint32_t max_pairs;
+} vxp_config;
+
+/* Per-step counters: NarrowPhase.stats (src/narrow_phase.zig:1355-1366) and
+ * SolverStats (src/solver.zig:381-392), plus device-side extras. */
+typedef struct {
+    uint32_t pairs_in;               /* pairs handed in                      */
+    uint32_t pairs_tested;           /* processPair calls                    */
+    uint32_t pairs_colliding;
+    uint32_t voxels_checked;
+    uint32_t contacts_generated;
+    uint32_t pairs_skipped_sleeping; /* system-level + narrow-phase skips    */
+    uint32_t manifolds_preserved;
+    uint32_t cache_hits;
+    uint32_t cache_misses;
+    uint32_t cache_evictions;
+    uint32_t manifolds;              /* manifolds in the ContactManager      */
+    uint32_t constraints;            /* manifolds handed to the solver       */
+    uint32_t contact_points;         /* points in the solver's constraint set*/
+    uint32_t colours;                /* colour batches used by the sweep     */
+    uint32_t position_iterations_run;
+    uint32_t step_skipped;           /* 1 when every dynamic body slept      */
+    float max_penetration;
+    uint32_t candidates;             /* distance-passing voxel pairs         */
+} vxp_stats;
+
+/* One candidate voxel pair of the narrow phase, for parity checks of the
+ * candidate set (checkNeighborhood, src/narrow_phase.zig:796-857). */
+typedef struct {
+    uint32_t pair_index;   /* index into the pair list handed in            */
+    int32_t a[3];          /* voxel of body A                               */
+    int32_t b[3];          /* voxel of body B                               */
+    uint32_t passed;       /* 1: dist^2 < speculative threshold             */
+    float dist_sq;
+} vxp_candidate;           /* 36 bytes */
+
+typedef struct vxp_ctx vxp_ctx;
+
+/* ---------------------------------------------------------------------------
+ * Context
+ * ------------------------------------------------------------------------- */
+
+/* Reference defaults: PhysicsConfig{} + SolverConfig{} + NarrowPhaseConfig{}. */
+void vxp_config_default(vxp_config* cfg);
+
+/* Replaces VoxelPhysicsSystem.init's NarrowPhase.init / ContactSolver.init
+ * (src/system.zig:248-249).  device = CUDA ordinal. */
+int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out);
+void vxp_destroy(vxp_ctx* ctx);
+int vxp_last_error(const vxp_ctx* ctx, char* buf, size_t n);
+int vxp_abi_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Colliders and bodies
+ * ------------------------------------------------------------------------- */
+
+/* Uploads one VoxelCollider (src/collider.zig:144-409): its bricks and voxel
+ * size.  Bounds, local AABB and solid count are recomputed as
+ * VoxelCollider.recomputeMetadata does (src/collider.zig:283-333).
+ * Bricks whose hashBrickPos collide (src/collider.zig:187-192) are rejected. */
+int vxp_collider_upload(vxp_ctx* ctx, uint32_t collider_id, float voxel_size,
+                        const vxp_brick* bricks, uint32_t n_bricks);
+
+/* Replaces the per-slot body state that step() reads and writes.  Bodies are
+ * kept in the order given (the solver's addBody order, src/system.zig:677-681). */
+int vxp_bodies_set(vxp_ctx* ctx, const vxp_body* bodies, uint32_t n);
+int vxp_bodies_get(vxp_ctx* ctx, vxp_body* bodies, uint32_t n);
+
+/* Host-side computeMassProperties (src/body.zig:462-519) over a brick list in
+ * the order given; the inertia sum runs brick by brick, voxel index order. */
+int vxp_mass_properties(float voxel_size, const vxp_brick* bricks, uint32_t n_bricks,
+                        float density, float* inv_mass, float inv_inertia[9]);
+
+/* ---------------------------------------------------------------------------
+ * The per-step hot path
+ * ------------------------------------------------------------------------- */
+
+/* One VoxelPhysicsSystem.step (src/system.zig:537-555) with the broad-phase
+ * pairs given: narrowPhase + solve + updateSleepStates, all on the device. */
+int vxp_step(vxp_ctx* ctx, float dt, const vxp_pair* pairs, uint32_t n_pairs);
+
+/* Same step, with the pair list produced on the device from inflated world
+ * AABBs (margin in metres) instead of handed in. */
+int vxp_step_device_pairs(vxp_ctx* ctx, float dt, float margin);
+
+/* The two halves of the step, for tests: narrowPhase() then solve()+sleep. */
+int vxp_narrow_phase(vxp_ctx* ctx, const vxp_pair* pairs, uint32_t n_pairs);
+int vxp_solve(vxp_ctx* ctx, float dt);
+
+/* ContactManager.manifolds after the last narrow phase, in manifold order
+ * (pair order).  *n_out = number written (<= cap). */
+int vxp_manifolds_get(vxp_ctx* ctx, vxp_manifold* out, uint32_t cap, uint32_t* n_out);
+
+/* Every type-filter-passing voxel pair of the last narrow phase (debug mode:
+ * enable with vxp_set_candidate_dump before vxp_narrow_phase). */
+int vxp_set_candidate_dump(vxp_ctx* ctx, uint32_t capacity);
+int vxp_candidates_get(vxp_ctx* ctx, vxp_candidate* out, uint32_t cap, uint32_t* n_out);
+
+int vxp_stats_get(vxp_ctx* ctx, vxp_stats* out);
+
+/* Colours of the last solve, indexed like the constraint list. */
+int vxp_colours_get(vxp_ctx* ctx, uint32_t* colours, uint32_t cap, uint32_t* n_out);
+
+/* Pair source used by tests, the bench and vxp_step_device_pairs: every
+ * (min id, max id) pair, not both static, whose world AABBs inflated by
+ * margin overlap, sorted by (body_a, body_b).  Computed on the device from the
+ * current body state. */
+int vxp_pairs_from_bodies(vxp_ctx* ctx, float margin, vxp_pair* out, uint32_t cap,
+                          uint32_t* n_out);
+
+/* Device-side timing of the last step's kernels (ms): [narrow, solve, total]. */
+int vxp_last_step_ms(vxp_ctx* ctx, float out[3]);
+
+/* Step calls queue work on the context's stream and return; a call that
+ * returns data (bodies, manifolds, stats, colours, candidates) waits for it.
+ * vxp_synchronize waits without copying and reports any device-side error
+ * (VXP_ERR_TIMEOUT, VXP_ERR_CAP) of the steps queued since the last wait.
+ * VXP_ERR_CAP from a step means the step left all state untouched: grow the
+ * capacity (vxp_config.max_pairs) and run it again. */
+int vxp_synchronize(vxp_ctx* ctx);
+
+/* -1: choose per step (default); 0: one CTA steps the world; 1: the world is
+ * stepped by a cooperative grid over every SM. */
+int vxp_set_launch_mode(vxp_ctx* ctx, int mode);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VXP_H */

@@ -1,0 +1,1008 @@
+// vxp_lib.cu — C ABI of the B200 voxel contact + TGS-soft solver library.
+//
+// Host side: context and device-memory management, collider upload, the pair
+// source, kernel launches.  Device side: the step kernels over the phases of
+// vxp_step.cuh.  Built with
+//   nvcc -gencode arch=compute_100a,code=sm_100a --fmad=false
+//        -prec-div=true -prec-sqrt=true -ftz=false
+// so that every float operation rounds like the reference's strict f32 code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/vxp.h"
+#include "vxp_math.cuh"
+#include "vxp_step.cuh"
+#include "vxp_world.cuh"
+
+using namespace vxp;
+
+// ===========================================================================
+// Kernels
+// ===========================================================================
+
+// One world per CTA.
+__global__ void __launch_bounds__(512) k_step_block(WorldDev* worlds, ColliderSet cs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpManifold* wsm = reinterpret_cast<WarpManifold*>(smem_raw);
+    WorldDev w = worlds[blockIdx.x];
+    BlockGroup g;
+    world_step(g, w, cs, wsm);
+}
+
+// One world over a cooperative grid.
+__global__ void __launch_bounds__(512) k_step_grid(const WorldDev* world, ColliderSet cs, GridBar* bar,
+                                                   unsigned long long timeout_ns) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpManifold* wsm = reinterpret_cast<WarpManifold*>(smem_raw);
+    WorldDev w = *world;
+    GridGroup g{bar, &w.ctr[C_ERROR], timeout_ns};
+    world_step(g, w, cs, wsm);
+}
+
+// Pair source: world AABB of each body's collider (AABB.transform,
+// math.zig:686-693) inflated by margin.
+__global__ void k_body_aabbs(const DBody* body, const DBodyProp* prop, uint32_t n, ColliderSet cs, float margin,
+                             float4* mn, float4* mx) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DBody b = body[i];
+    const F3 x = f3of(b.p);
+    const Qt q = qof(b.q);
+    F3 lo, hi;
+    if (prop[i].collider < cs.n) {
+        const DCollider& c = cs.c[prop[i].collider];
+        const float inf = __int_as_float(0x7f800000);
+        lo = F3{inf, inf, inf};
+        hi = F3{-inf, -inf, -inf};
+        for (int k = 0; k < 8; ++k) {
+            const F3 corner{(k & 1) ? c.aabb_max[0] : c.aabb_min[0], (k & 2) ? c.aabb_max[1] : c.aabb_min[1],
+                            (k & 4) ? c.aabb_max[2] : c.aabb_min[2]};
+            const F3 p = transform_point(x, q, corner);
+            lo = min3(lo, p);
+            hi = max3(hi, p);
+        }
+    } else {
+        lo = x;
+        hi = x;
+    }
+    lo = lo - F3{margin, margin, margin};
+    hi = hi + F3{margin, margin, margin};
+    mn[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    mx[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
+}
+
+// Pairs (i < j in id order) whose inflated AABBs overlap and that are not both
+// static.  Pass 0 counts per i, pass 1 writes at the scanned offsets.
+__global__ void k_pairs(const uint2* ids, const DBodyProp* prop, uint32_t n, const float4* mn, const float4* mx,
+                        uint32_t* counts, const uint32_t* offsets, uint2* out, uint32_t cap, int pass) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t i = ids[s].y;
+    const float4 a0 = mn[i], a1 = mx[i];
+    const bool si = prop[i].type == 0u;
+    uint32_t cnt = 0;
+    uint32_t o = pass ? offsets[s] : 0u;
+    for (uint32_t t = s + 1; t < n; ++t) {
+        const uint32_t j = ids[t].y;
+        if (si && prop[j].type == 0u) continue;
+        const float4 b0 = mn[j], b1 = mx[j];
+        if (a0.x <= b1.x && a1.x >= b0.x && a0.y <= b1.y && a1.y >= b0.y && a0.z <= b1.z && a1.z >= b0.z) {
+            if (pass) {
+                if (o < cap) out[o] = make_uint2(ids[s].x, ids[t].x);
+                ++o;
+            }
+            ++cnt;
+        }
+    }
+    if (!pass) counts[s] = cnt;
+}
+
+// Exclusive scan of counts (single block, n arbitrary); writes total to *total.
+__global__ void __launch_bounds__(1024) k_scan1(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total) {
+    uint32_t carry = 0;
+    for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
+        const uint32_t i = t0 + threadIdx.x;
+        const uint32_t v = i < n ? in[i] : 0u;
+        uint32_t tile;
+        const uint32_t ex = block_excl_scan(v, &tile);
+        if (i < n) out[i] = carry + ex;
+        carry += tile;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// Rebuild a manifold hash table after the manifold buffers were re-allocated.
+__global__ void k_rehash(const ManifoldRec* man, uint32_t n, HashSlot* ht, uint32_t cap) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (man[p].n > 0u) ht_insert(ht, cap, pair_key(man[p].a, man[p].b), p);
+}
+
+// ===========================================================================
+// Host side
+// ===========================================================================
+namespace {
+
+struct HostCollider {
+    uint32_t id;
+    float vs;
+    std::vector<int32_t> pos;     // 3 per brick
+    std::vector<uint8_t> vox;     // 512 per brick
+    int32_t min_bound[3], max_bound[3];
+    float aabb_min[3], aabb_max[3];
+    uint32_t solid;
+};
+
+template <class T> struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t reserve(size_t k, bool keep = false) {
+        if (k <= n && p) return cudaSuccess;
+        T* q = nullptr;
+        const size_t bytes = std::max<size_t>(k, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&q, bytes);
+        if (e != cudaSuccess) return e;
+        cudaMemset(q, 0, bytes);
+        if (keep && p && n) cudaMemcpy(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice);
+        if (p) cudaFree(p);
+        p = q;
+        n = std::max<size_t>(k, 1);
+        return cudaSuccess;
+    }
+};
+
+uint32_t next_pow2(uint32_t x) {
+    uint32_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+}  // namespace
+
+struct vxp_ctx {
+    vxp_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int sm_count = 148;
+    // colliders
+    std::vector<HostCollider> colliders;
+    std::unordered_map<uint32_t, uint32_t> collider_index;
+    bool colliders_dirty = true;
+    DBuf<DCollider> d_col;
+    DBuf<int32_t> d_grid;
+    DBuf<uint8_t> d_vox;
+    uint32_t n_col_dev = 0;
+    // bodies
+    uint32_t n_bodies = 0;
+    std::vector<uint32_t> body_collider_public;  // public collider id per body
+    DBuf<DBody> body;
+    DBuf<DBodyProp> prop;
+    DBuf<float4> p0, qn, aabb_mn, aabb_mx;
+    DBuf<uint2> ids;
+    DBuf<uint32_t> pair_counts, pair_offsets;
+    // pairs and everything sized by pair_cap
+    uint32_t pair_cap = 0, ht_cap = 0;
+    DBuf<uint2> pairs;
+    DBuf<uint32_t> n_pairs_dev;
+    DBuf<PairInfo> pinfo;
+    DBuf<ManifoldRec> man0, man1;
+    DBuf<HashSlot> ht0, ht1;
+    DBuf<uint32_t> frame;
+    DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag;
+    DBuf<float> cp;
+    DBuf<uint4> cm;
+    DBuf<float2> cfr;
+    // body-sized
+    DBuf<uint32_t> adj_off, adj_cur, bmask;
+    // fixed
+    DBuf<uint32_t> colour_cnt, colour_cur, scan, ctr, cwriter;
+    DBuf<CacheKeyRec> ckey;
+    DBuf<CacheValRec> cval;
+    DBuf<unsigned long long> cframe;
+    DBuf<WorldDev> d_world;
+    DBuf<GridBar> bar;
+    DBuf<WorldDev::Cand> dump;
+    uint32_t dump_cap = 0;
+    uint32_t body_cap = 0;
+    uint32_t grid_blocks = 0;
+    uint32_t last_pairs = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms[3] = {0, 0, 0};
+    int use_grid = -1;  // -1 auto, 0 block, 1 grid
+};
+
+namespace {
+
+int fail(vxp_ctx* c, int code, const char* fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return fail(ctx, VXP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr uint32_t kBlockThreads = 512;
+constexpr size_t kWarpSmem = sizeof(WarpManifold) * (kBlockThreads / 32);
+
+uint64_t hash_brick_pos(int32_t x, int32_t y, int32_t z) {  // collider.zig:187-192
+    const uint64_t ux = (uint64_t)(int64_t)x, uy = (uint64_t)(int64_t)y, uz = (uint64_t)(int64_t)z;
+    return ux ^ (uy * 0x517cc1b727220a95ull) ^ (uz * 0x9e3779b97f4a7c15ull);
+}
+
+// VoxelCollider.recomputeMetadata (collider.zig:283-333), bricks in the order given.
+void collider_metadata(HostCollider& h) {
+    h.solid = 0;
+    for (int k = 0; k < 3; ++k) {
+        h.min_bound[k] = INT32_MAX;
+        h.max_bound[k] = INT32_MIN;
+    }
+    const float inf = __builtin_inff();
+    float amn[3] = {inf, inf, inf}, amx[3] = {-inf, -inf, -inf};
+    const size_t nb = h.pos.size() / 3;
+    for (size_t b = 0; b < nb; ++b) {
+        const int32_t* bp = &h.pos[b * 3];
+        const uint8_t* v = &h.vox[b * 512];
+        uint32_t solid = 0;
+        float bmn[3] = {inf, inf, inf}, bmx[3] = {-inf, -inf, -inf};
+        for (int i = 0; i < 512; ++i) {
+            if ((v[i] & 7u) == 0u) continue;
+            ++solid;
+            const int c[3] = {i % 8, (i / 8) % 8, i / 64};
+            for (int k = 0; k < 3; ++k) {
+                const float lp = ((float)bp[k] * 8.0f + (float)c[k]) * h.vs;
+                bmn[k] = std::fmin(bmn[k], lp);
+                bmx[k] = std::fmax(bmx[k], lp + h.vs);
+                const int32_t vc = bp[k] * 8 + c[k];
+                h.min_bound[k] = std::min(h.min_bound[k], vc);
+                h.max_bound[k] = std::max(h.max_bound[k], vc + 1);
+            }
+        }
+        if (solid == 0) continue;
+        h.solid += solid;
+        for (int k = 0; k < 3; ++k) {
+            amn[k] = std::fmin(amn[k], bmn[k]);
+            amx[k] = std::fmax(amx[k], bmx[k]);
+        }
+    }
+    if (h.solid == 0)
+        for (int k = 0; k < 3; ++k) h.min_bound[k] = h.max_bound[k] = 0;
+    for (int k = 0; k < 3; ++k) {
+        h.aabb_min[k] = amn[k];
+        h.aabb_max[k] = amx[k];
+    }
+}
+
+int sync_colliders(vxp_ctx* ctx) {
+    if (!ctx->colliders_dirty) return VXP_OK;
+    std::vector<DCollider> dc(ctx->colliders.size());
+    std::vector<int32_t> grid;
+    std::vector<uint8_t> vox;
+    uint32_t brick_total = 0;
+    for (size_t ci = 0; ci < ctx->colliders.size(); ++ci) {
+        const HostCollider& h = ctx->colliders[ci];
+        DCollider& d = dc[ci];
+        std::memset(&d, 0, sizeof(d));
+        d.vs = h.vs;
+        for (int k = 0; k < 3; ++k) {
+            d.min_bound[k] = h.min_bound[k];
+            d.max_bound[k] = h.max_bound[k];
+            d.aabb_min[k] = h.aabb_min[k];
+            d.aabb_max[k] = h.aabb_max[k];
+        }
+        d.solid_count = h.solid;
+        const size_t nb = h.pos.size() / 3;
+        // The reference finds a brick through hashBrickPos (collider.zig:187-192,
+        // 241-248), and distinct positions can share a hash.  Every voxel the
+        // step looks up lies in [min_bound, max_bound] (the overlap region is
+        // clamped to the bounds, inclusive; B probes pass isValidCoord), so
+        // the grid covers those bricks and resolves each cell by its hash.
+        std::unordered_map<uint64_t, int32_t> by_hash;
+        for (size_t b = 0; b < nb; ++b)
+            by_hash.emplace(hash_brick_pos(h.pos[b * 3], h.pos[b * 3 + 1], h.pos[b * 3 + 2]), (int32_t)b);
+        int32_t lo[3], hi[3];
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = h.min_bound[k] >> 3;
+            hi[k] = h.max_bound[k] >> 3;
+            d.bmin[k] = lo[k];
+            d.bdim[k] = hi[k] - lo[k] + 1;
+        }
+        d.grid_off = (uint32_t)grid.size();
+        d.brick_off = brick_total;
+        d.n_bricks = (uint32_t)nb;
+        const size_t cells = (size_t)d.bdim[0] * d.bdim[1] * d.bdim[2];
+        if (cells > (size_t)1 << 28) return fail(ctx, VXP_ERR_CAP, "collider %u brick grid too large", h.id);
+        grid.resize(grid.size() + cells, -1);
+        for (int32_t bz = lo[2]; bz <= hi[2]; ++bz)
+            for (int32_t by = lo[1]; by <= hi[1]; ++by)
+                for (int32_t bx = lo[0]; bx <= hi[0]; ++bx) {
+                    auto it = by_hash.find(hash_brick_pos(bx, by, bz));
+                    if (it == by_hash.end()) continue;
+                    grid[d.grid_off + (size_t)(bx - lo[0]) +
+                         (size_t)d.bdim[0] * ((size_t)(by - lo[1]) + (size_t)d.bdim[1] * (size_t)(bz - lo[2]))] =
+                        it->second;
+                }
+        vox.insert(vox.end(), h.vox.begin(), h.vox.end());
+        brick_total += (uint32_t)nb;
+    }
+    if (ctx->d_col.reserve(dc.size()) != cudaSuccess || ctx->d_grid.reserve(grid.size()) != cudaSuccess ||
+        ctx->d_vox.reserve(vox.size()) != cudaSuccess)
+        return fail(ctx, VXP_ERR_OOM, "collider upload: device allocation failed");
+    if (!dc.empty()) CK(cudaMemcpy(ctx->d_col.p, dc.data(), dc.size() * sizeof(DCollider), cudaMemcpyHostToDevice));
+    if (!grid.empty()) CK(cudaMemcpy(ctx->d_grid.p, grid.data(), grid.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    if (!vox.empty()) CK(cudaMemcpy(ctx->d_vox.p, vox.data(), vox.size(), cudaMemcpyHostToDevice));
+    ctx->n_col_dev = (uint32_t)dc.size();
+    ctx->colliders_dirty = false;
+    return VXP_OK;
+}
+
+ColliderSet collider_set(vxp_ctx* ctx) {
+    return ColliderSet{ctx->d_col.p, ctx->d_grid.p, ctx->d_vox.p, ctx->n_col_dev};
+}
+
+// Grows every pair-sized buffer to hold cap pairs; keeps the previous frame's
+// manifolds and rebuilds their hash table.
+int ensure_pair_cap(vxp_ctx* ctx, uint32_t need) {
+    if (need <= ctx->pair_cap && ctx->pair_cap) return VXP_OK;
+    uint32_t cap = std::max<uint32_t>(1024, ctx->pair_cap);
+    while (cap < need) cap *= 2;
+    const uint32_t old_cap = ctx->pair_cap;
+    const uint32_t ht_cap = next_pow2(cap * 2);
+    bool ok = true;
+    ok &= ctx->pairs.reserve(cap) == cudaSuccess;
+    ok &= ctx->pinfo.reserve(cap) == cudaSuccess;
+    ok &= ctx->man0.reserve(cap, true) == cudaSuccess;
+    ok &= ctx->man1.reserve(cap, true) == cudaSuccess;
+    ok &= ctx->cons.reserve(cap) == cudaSuccess;
+    ok &= ctx->colour.reserve(cap) == cudaSuccess;
+    ok &= ctx->pos_of.reserve(cap) == cudaSuccess;
+    ok &= ctx->packed_pair.reserve(cap) == cudaSuccess;
+    ok &= ctx->adj.reserve((size_t)2 * cap) == cudaSuccess;
+    ok &= ctx->flag.reserve(cap) == cudaSuccess;
+    ok &= ctx->cp.reserve((size_t)CP_NFIELDS * 4 * cap) == cudaSuccess;
+    ok &= ctx->cm.reserve(cap) == cudaSuccess;
+    ok &= ctx->cfr.reserve(cap) == cudaSuccess;
+    if (!ok) return fail(ctx, VXP_ERR_OOM, "pair buffers: device allocation of %u pairs failed", cap);
+    if (ht_cap != ctx->ht_cap) {
+        // frame parity decides which table is "previous": rebuild both
+        DBuf<HashSlot> n0, n1;
+        if (n0.reserve(ht_cap) != cudaSuccess || n1.reserve(ht_cap) != cudaSuccess)
+            return fail(ctx, VXP_ERR_OOM, "hash tables: allocation failed");
+        std::swap(ctx->ht0.p, n0.p);
+        std::swap(ctx->ht0.n, n0.n);
+        std::swap(ctx->ht1.p, n1.p);
+        std::swap(ctx->ht1.n, n1.n);
+        ctx->ht_cap = ht_cap;
+        if (old_cap) {
+            uint32_t fr[2] = {0, 0};
+            CK(cudaMemcpy(fr, ctx->frame.p, sizeof(fr), cudaMemcpyDeviceToHost));
+            const uint32_t prev_n = fr[1];
+            const uint32_t prev_slot = fr[0] & 1u;  // the latest manifolds: next step's "previous"
+            if (prev_n) {
+                ManifoldRec* m = prev_slot ? ctx->man1.p : ctx->man0.p;
+                HashSlot* h = prev_slot ? ctx->ht1.p : ctx->ht0.p;
+                k_rehash<<<(prev_n + 255) / 256, 256>>>(m, prev_n, h, ht_cap);
+                CK(cudaGetLastError());
+                CK(cudaDeviceSynchronize());
+            }
+        }
+    }
+    ctx->pair_cap = cap;
+    return VXP_OK;
+}
+
+int ensure_body_cap(vxp_ctx* ctx, uint32_t n) {
+    if (n <= ctx->body_cap && ctx->body_cap) return VXP_OK;
+    uint32_t cap = std::max<uint32_t>(256, ctx->body_cap);
+    while (cap < n) cap *= 2;
+    bool ok = true;
+    ok &= ctx->body.reserve(cap) == cudaSuccess;
+    ok &= ctx->prop.reserve(cap) == cudaSuccess;
+    ok &= ctx->p0.reserve(cap) == cudaSuccess;
+    ok &= ctx->qn.reserve(cap) == cudaSuccess;
+    ok &= ctx->aabb_mn.reserve(cap) == cudaSuccess;
+    ok &= ctx->aabb_mx.reserve(cap) == cudaSuccess;
+    ok &= ctx->ids.reserve(cap) == cudaSuccess;
+    ok &= ctx->pair_counts.reserve(cap) == cudaSuccess;
+    ok &= ctx->pair_offsets.reserve(cap) == cudaSuccess;
+    ok &= ctx->adj_off.reserve((size_t)cap + 1) == cudaSuccess;
+    ok &= ctx->adj_cur.reserve(cap) == cudaSuccess;
+    ok &= ctx->bmask.reserve((size_t)cap * 8) == cudaSuccess;
+    if (!ok) return fail(ctx, VXP_ERR_OOM, "body buffers: device allocation of %u bodies failed", cap);
+    ctx->body_cap = cap;
+    return VXP_OK;
+}
+
+StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) {
+    StepCfg s;
+    s.phases = phases;
+    for (int i = 0; i < 3; ++i) s.gravity[i] = c.gravity[i];
+    s.dt = dt;
+    s.substeps = c.substeps;
+    s.vel_iters = c.velocity_iterations;
+    s.pos_iters = c.position_iterations;
+    s.disable_rotation = c.disable_rotation;
+    s.hertz = c.hertz;
+    s.damping_ratio = c.damping_ratio;
+    s.pos_rate = c.position_correction_rate;
+    s.max_pos_corr = c.max_position_correction;
+    s.slop = c.slop;
+    s.warm_starting = c.warm_starting;
+    s.warm_scale = c.warm_start_scale;
+    s.friction_on = c.enable_friction;
+    s.restitution_on = c.enable_restitution;
+    s.sleeping_on = c.enable_sleeping;
+    s.warm_store_on = c.enable_warm_starting;
+    s.use_sat = c.use_brick_sat;
+    s.use_cache = c.use_brick_pair_cache;
+    s.reference_caps = c.reference_caps;
+    s.colouring = c.colouring;
+    s.dump_candidates = dump;
+    return s;
+}
+
+WorldDev make_world(vxp_ctx* ctx, float dt, uint32_t phases) {
+    WorldDev w;
+    std::memset(&w, 0, sizeof(w));
+    w.cfg = step_cfg(ctx->cfg, dt, ctx->dump_cap ? 1u : 0u, phases);
+    w.n_bodies = ctx->n_bodies;
+    w.n_pairs = 0;
+    w.n_pairs_dev = ctx->n_pairs_dev.p;
+    w.pair_cap = ctx->pair_cap;
+    w.ht_cap = ctx->ht_cap;
+    w.cache_cap = ctx->cfg.brick_pair_cache_size ? ctx->cfg.brick_pair_cache_size : 1024u;
+    w.dump_cap = ctx->dump_cap;
+    w.body = ctx->body.p;
+    w.prop = ctx->prop.p;
+    w.p0 = ctx->p0.p;
+    w.qn = ctx->qn.p;
+    w.ids = ctx->ids.p;
+    w.pairs = ctx->pairs.p;
+    w.pinfo = ctx->pinfo.p;
+    w.man[0] = ctx->man0.p;
+    w.man[1] = ctx->man1.p;
+    w.ht[0] = ctx->ht0.p;
+    w.ht[1] = ctx->ht1.p;
+    w.frame = ctx->frame.p;
+    w.ckey = ctx->ckey.p;
+    w.cval = ctx->cval.p;
+    w.cwriter = ctx->cwriter.p;
+    w.cframe = ctx->cframe.p;
+    w.cons = ctx->cons.p;
+    w.colour = ctx->colour.p;
+    w.pos_of = ctx->pos_of.p;
+    w.packed_pair = ctx->packed_pair.p;
+    w.adj_off = ctx->adj_off.p;
+    w.adj = ctx->adj.p;
+    w.adj_cur = ctx->adj_cur.p;
+    w.colour_cnt = ctx->colour_cnt.p;
+    w.colour_cur = ctx->colour_cur.p;
+    w.bmask = ctx->bmask.p;
+    w.cp = ctx->cp.p;
+    w.cm = ctx->cm.p;
+    w.cfr = ctx->cfr.p;
+    w.scan = ctx->scan.p;
+    w.flag = ctx->flag.p;
+    w.ctr = ctx->ctr.p;
+    w.dump = ctx->dump.p;
+    return w;
+}
+
+// Runs the step kernel for the pairs already in ctx->pairs / n_pairs_dev.
+int launch_step(vxp_ctx* ctx, float dt, uint32_t n_pairs_hint, uint32_t phases) {
+    if (int rc = sync_colliders(ctx)) return rc;
+    WorldDev w = make_world(ctx, dt, phases);
+    CK(cudaMemcpyAsync(ctx->d_world.p, &w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->ctr.p, 0, sizeof(uint32_t) * C_ERROR, ctx->stream));
+    const ColliderSet cs = collider_set(ctx);
+    bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && (n_pairs_hint > 1024 || ctx->n_bodies > 2048));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (grid) {
+        CK(cudaMemsetAsync(ctx->bar.p, 0, sizeof(GridBar), ctx->stream));
+        const WorldDev* wp = ctx->d_world.p;
+        GridBar* bp = ctx->bar.p;
+        unsigned long long timeout = 10ull * 1000ull * 1000ull * 1000ull;  // 10 s per barrier wait
+        void* args[] = {(void*)&wp, (void*)&cs, (void*)&bp, (void*)&timeout};
+        CK(cudaLaunchCooperativeKernel((const void*)k_step_grid, dim3(ctx->grid_blocks), dim3(kBlockThreads), args,
+                                       kWarpSmem, ctx->stream));
+    } else {
+        k_step_block<<<1, kBlockThreads, kWarpSmem, ctx->stream>>>(ctx->d_world.p, cs);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    return VXP_OK;
+}
+
+int check_device_error(vxp_ctx* ctx) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    uint32_t e = 0;
+    CK(cudaMemcpy(&e, ctx->ctr.p + C_ERROR, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) {
+        const uint32_t z = 0;
+        cudaMemcpy(ctx->ctr.p + C_ERROR, &z, sizeof(z), cudaMemcpyHostToDevice);
+        if (e & ERR_TIMEOUT) return fail(ctx, VXP_ERR_TIMEOUT, "a grid barrier wait ran out (error bits 0x%x)", e);
+        if (e & ERR_CAP) return fail(ctx, VXP_ERR_CAP, "pair list exceeded the device capacity (error bits 0x%x)", e);
+        if (e & ERR_COLOURS) return fail(ctx, VXP_ERR_CAP, "more than 255 colours needed (error bits 0x%x)", e);
+        return fail(ctx, VXP_ERR_STATE, "device error bits 0x%x", e);
+    }
+    return VXP_OK;
+}
+
+int compute_device_pairs(vxp_ctx* ctx, float margin, uint32_t* n_out) {
+    if (int rc = sync_colliders(ctx)) return rc;
+    const uint32_t n = ctx->n_bodies;
+    const ColliderSet cs = collider_set(ctx);
+    if (n == 0) {
+        *n_out = 0;
+        CK(cudaMemsetAsync(ctx->n_pairs_dev.p, 0, sizeof(uint32_t), ctx->stream));
+        return VXP_OK;
+    }
+    const uint32_t tb = 256, nb = (n + tb - 1) / tb;
+    k_body_aabbs<<<nb, tb, 0, ctx->stream>>>(ctx->body.p, ctx->prop.p, n, cs, margin, ctx->aabb_mn.p, ctx->aabb_mx.p);
+    k_pairs<<<nb, tb, 0, ctx->stream>>>(ctx->ids.p, ctx->prop.p, n, ctx->aabb_mn.p, ctx->aabb_mx.p,
+                                        ctx->pair_counts.p, nullptr, nullptr, 0, 0);
+    k_scan1<<<1, 1024, 0, ctx->stream>>>(ctx->pair_counts.p, ctx->pair_offsets.p, n, ctx->n_pairs_dev.p);
+    CK(cudaGetLastError());
+    uint32_t total = 0;
+    CK(cudaMemcpyAsync(&total, ctx->n_pairs_dev.p, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (int rc = ensure_pair_cap(ctx, total)) return rc;
+    k_pairs<<<nb, tb, 0, ctx->stream>>>(ctx->ids.p, ctx->prop.p, n, ctx->aabb_mn.p, ctx->aabb_mx.p, nullptr,
+                                        ctx->pair_offsets.p, ctx->pairs.p, ctx->pair_cap, 1);
+    CK(cudaGetLastError());
+    *n_out = total;
+    return VXP_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int vxp_abi_version(void) { return VXP_ABI_VERSION; }
+
+void vxp_config_default(vxp_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->gravity[0] = 0.0f;
+    c->gravity[1] = -9.81f;
+    c->gravity[2] = 0.0f;
+    c->fixed_timestep = 1.0f / 60.0f;
+    c->enable_sleeping = 1;
+    c->enable_warm_starting = 1;
+    c->substeps = 4;
+    c->velocity_iterations = 1;
+    c->position_iterations = 2;
+    c->disable_rotation = 0;
+    c->hertz = 30.0f;
+    c->damping_ratio = 1.0f;
+    c->position_correction_rate = 0.2f;
+    c->max_position_correction = 0.04f;
+    c->slop = 0.005f;
+    c->warm_starting = 1;
+    c->warm_start_scale = 0.8f;
+    c->enable_friction = 1;
+    c->enable_restitution = 1;
+    c->use_brick_sat = 1;
+    c->use_brick_pair_cache = 1;
+    c->brick_pair_cache_size = 1024;
+    c->reference_caps = 0;
+    c->colouring = VXP_COLOUR_PROJECT;
+    c->max_bodies = 0;
+    c->max_pairs = 0;
+}
+
+int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
+    if (!cfg || !out) return VXP_ERR_ARG;
+    *out = nullptr;
+    if (cfg->substeps == 0) return VXP_ERR_ARG;
+    if (cfg->position_iterations > 16) return VXP_ERR_ARG;
+    vxp_ctx* ctx = new vxp_ctx;
+    ctx->cfg = *cfg;
+    ctx->device = device;
+    auto bail = [&](int rc) {
+        vxp_destroy(ctx);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(VXP_ERR_CUDA);
+    int smc = 0;
+    if (cudaDeviceGetAttribute(&smc, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return bail(VXP_ERR_CUDA);
+    ctx->sm_count = smc;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(VXP_ERR_CUDA);
+    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+        return bail(VXP_ERR_CUDA);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads, kWarpSmem) != cudaSuccess ||
+        per_sm < 1)
+        return bail(VXP_ERR_CUDA);
+    ctx->grid_blocks = (uint32_t)(smc * std::min(per_sm, 2));
+    const uint32_t cache_cap = cfg->brick_pair_cache_size ? cfg->brick_pair_cache_size : 1024u;
+    bool ok = true;
+    ok &= ctx->n_pairs_dev.reserve(1) == cudaSuccess;
+    ok &= ctx->frame.reserve(2) == cudaSuccess;
+    ok &= ctx->colour_cnt.reserve(257) == cudaSuccess;
+    ok &= ctx->colour_cur.reserve(256) == cudaSuccess;
+    ok &= ctx->scan.reserve(ctx->grid_blocks + 64) == cudaSuccess;
+    ok &= ctx->ctr.reserve(C_NCTR) == cudaSuccess;
+    ok &= ctx->ckey.reserve(cache_cap) == cudaSuccess;
+    ok &= ctx->cval.reserve(cache_cap) == cudaSuccess;
+    ok &= ctx->cwriter.reserve(cache_cap) == cudaSuccess;
+    ok &= ctx->cframe.reserve(1) == cudaSuccess;
+    ok &= ctx->d_world.reserve(1) == cudaSuccess;
+    ok &= ctx->bar.reserve(1) == cudaSuccess;
+    if (!ok) return bail(VXP_ERR_OOM);
+    if (cudaFuncSetAttribute(k_step_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWarpSmem) !=
+        cudaSuccess)
+        return bail(VXP_ERR_CUDA);
+    if (ensure_pair_cap(ctx, std::max<uint32_t>(cfg->max_pairs, 1024)) != VXP_OK) return bail(VXP_ERR_OOM);
+    if (ensure_body_cap(ctx, std::max<uint32_t>(cfg->max_bodies, 256)) != VXP_OK) return bail(VXP_ERR_OOM);
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(VXP_ERR_CUDA);
+    *out = ctx;
+    return VXP_OK;
+}
+
+void vxp_destroy(vxp_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int vxp_last_error(const vxp_ctx* ctx, char* buf, size_t n) {
+    if (!ctx || !buf || n == 0) return VXP_ERR_ARG;
+    std::snprintf(buf, n, "%s", ctx->err.c_str());
+    return VXP_OK;
+}
+
+int vxp_collider_upload(vxp_ctx* ctx, uint32_t collider_id, float voxel_size, const vxp_brick* bricks,
+                        uint32_t n_bricks) {
+    if (!ctx || (!bricks && n_bricks)) return fail(ctx, VXP_ERR_ARG, "null argument");
+    if (!(voxel_size > 0.0f)) return fail(ctx, VXP_ERR_ARG, "voxel_size must be positive");
+    HostCollider h;
+    h.id = collider_id;
+    h.vs = voxel_size;
+    h.pos.resize((size_t)n_bricks * 3);
+    h.vox.resize((size_t)n_bricks * 512);
+    std::unordered_map<uint64_t, uint32_t> seen;
+    for (uint32_t i = 0; i < n_bricks; ++i) {
+        for (int k = 0; k < 3; ++k) h.pos[(size_t)i * 3 + k] = bricks[i].pos[k];
+        std::memcpy(&h.vox[(size_t)i * 512], bricks[i].voxels, 512);
+        if (!seen.emplace(hash_brick_pos(bricks[i].pos[0], bricks[i].pos[1], bricks[i].pos[2]), i).second)
+            return fail(ctx, VXP_ERR_ARG, "collider %u: bricks %u and %u share a hashBrickPos value", collider_id,
+                        seen[hash_brick_pos(bricks[i].pos[0], bricks[i].pos[1], bricks[i].pos[2])], i);
+    }
+    collider_metadata(h);
+    auto it = ctx->collider_index.find(collider_id);
+    if (it != ctx->collider_index.end()) ctx->colliders[it->second] = std::move(h);
+    else {
+        ctx->collider_index[collider_id] = (uint32_t)ctx->colliders.size();
+        ctx->colliders.push_back(std::move(h));
+    }
+    ctx->colliders_dirty = true;
+    return VXP_OK;
+}
+
+int vxp_bodies_set(vxp_ctx* ctx, const vxp_body* b, uint32_t n) {
+    if (!ctx || (!b && n)) return fail(ctx, VXP_ERR_ARG, "null argument");
+    if (int rc = ensure_body_cap(ctx, n)) return rc;
+    std::vector<DBody> db(n);
+    std::vector<DBodyProp> dp(n);
+    std::vector<uint2> ids(n);
+    ctx->body_collider_public.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const vxp_body& s = b[i];
+        if (s.body_type > 2u) return fail(ctx, VXP_ERR_ARG, "body %u: bad body_type %u", i, s.body_type);
+        DBody& d = db[i];
+        d.p = make_float4(s.position[0], s.position[1], s.position[2], s.inv_mass);
+        d.q = make_float4(s.rotation[0], s.rotation[1], s.rotation[2], s.rotation[3]);
+        d.v = make_float4(s.linear_velocity[0], s.linear_velocity[1], s.linear_velocity[2], 0.f);
+        d.w = make_float4(s.angular_velocity[0], s.angular_velocity[1], s.angular_velocity[2], 0.f);
+        d.i0 = d.i1 = d.i2 = make_float4(0.f, 0.f, 0.f, 0.f);
+        DBodyProp& p = dp[i];
+        for (int k = 0; k < 9; ++k) p.il[k] = s.inv_inertia_local[k];
+        p.friction = s.friction;
+        p.restitution = s.restitution;
+        p.lin_damp = s.linear_damping;
+        p.ang_damp = s.angular_damping;
+        p.sleep_timer = s.sleep_timer;
+        p.id = s.id;
+        p.type = s.body_type;
+        auto it = ctx->collider_index.find(s.collider_id);
+        p.collider = it == ctx->collider_index.end() ? 0xFFFFFFFFu : it->second;
+        p.sleeping = s.is_sleeping ? 1u : 0u;
+        ctx->body_collider_public[i] = s.collider_id;
+        ids[i] = make_uint2(s.id, i);
+    }
+    std::sort(ids.begin(), ids.end(), [](const uint2& x, const uint2& y) { return x.x < y.x; });
+    for (uint32_t i = 1; i < n; ++i)
+        if (ids[i].x == ids[i - 1].x) return fail(ctx, VXP_ERR_ARG, "duplicate body id %u", ids[i].x);
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (n) {
+        CK(cudaMemcpy(ctx->body.p, db.data(), n * sizeof(DBody), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->prop.p, dp.data(), n * sizeof(DBodyProp), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->ids.p, ids.data(), n * sizeof(uint2), cudaMemcpyHostToDevice));
+    }
+    ctx->n_bodies = n;
+    return VXP_OK;
+}
+
+int vxp_bodies_get(vxp_ctx* ctx, vxp_body* b, uint32_t n) {
+    if (!ctx || (!b && n)) return fail(ctx, VXP_ERR_ARG, "null argument");
+    if (n != ctx->n_bodies) return fail(ctx, VXP_ERR_ARG, "expected %u bodies, got %u", ctx->n_bodies, n);
+    if (int rc = check_device_error(ctx)) return rc;
+    std::vector<DBody> db(n);
+    std::vector<DBodyProp> dp(n);
+    if (n) {
+        CK(cudaMemcpy(db.data(), ctx->body.p, n * sizeof(DBody), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(dp.data(), ctx->prop.p, n * sizeof(DBodyProp), cudaMemcpyDeviceToHost));
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        vxp_body& s = b[i];
+        const DBody& d = db[i];
+        const DBodyProp& p = dp[i];
+        s.id = p.id;
+        s.body_type = p.type;
+        s.collider_id = ctx->body_collider_public[i];
+        s.is_sleeping = p.sleeping;
+        s.position[0] = d.p.x; s.position[1] = d.p.y; s.position[2] = d.p.z;
+        s.rotation[0] = d.q.x; s.rotation[1] = d.q.y; s.rotation[2] = d.q.z; s.rotation[3] = d.q.w;
+        s.linear_velocity[0] = d.v.x; s.linear_velocity[1] = d.v.y; s.linear_velocity[2] = d.v.z;
+        s.angular_velocity[0] = d.w.x; s.angular_velocity[1] = d.w.y; s.angular_velocity[2] = d.w.z;
+        s.inv_mass = d.p.w;
+        for (int k = 0; k < 9; ++k) s.inv_inertia_local[k] = p.il[k];
+        s.friction = p.friction;
+        s.restitution = p.restitution;
+        s.linear_damping = p.lin_damp;
+        s.angular_damping = p.ang_damp;
+        s.sleep_timer = p.sleep_timer;
+    }
+    return VXP_OK;
+}
+
+int vxp_mass_properties(float vs, const vxp_brick* bricks, uint32_t n, float density, float* inv_mass,
+                        float inv_inertia[9]) {
+    if ((!bricks && n) || !inv_mass || !inv_inertia) return VXP_ERR_ARG;
+    HostCollider h;
+    h.vs = vs;
+    h.pos.resize((size_t)n * 3);
+    h.vox.resize((size_t)n * 512);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (int k = 0; k < 3; ++k) h.pos[(size_t)i * 3 + k] = bricks[i].pos[k];
+        std::memcpy(&h.vox[(size_t)i * 512], bricks[i].voxels, 512);
+    }
+    collider_metadata(h);
+    if (h.solid == 0) {
+        *inv_mass = 0.0f;
+        for (int k = 0; k < 9; ++k) inv_inertia[k] = 0.0f;
+        return VXP_OK;
+    }
+    // body.zig:473-519 with getCenterOfMass (collider.zig:376-403)
+    const float vv = vs * vs * vs;
+    const float vm = vv * density;
+    const float total = vm * (float)h.solid;
+    float sum[3] = {0.f, 0.f, 0.f};
+    uint32_t count = 0;
+    const float half = vs * 0.5f;
+    for (uint32_t b = 0; b < n; ++b)
+        for (int i = 0; i < 512; ++i) {
+            if ((h.vox[(size_t)b * 512 + i] & 7u) == 0u) continue;
+            const int c[3] = {i % 8, (i / 8) % 8, i / 64};
+            for (int k = 0; k < 3; ++k) {
+                const float p = ((float)(h.pos[(size_t)b * 3 + k] * 8 + c[k]) * vs + half) + vs * 0.5f;
+                sum[k] = sum[k] + p;
+            }
+            ++count;
+        }
+    const float inv_count = 1.0f / (float)count;
+    const float com[3] = {sum[0] * inv_count, sum[1] * inv_count, sum[2] * inv_count};
+    vxp::M33 I;
+    for (int k = 0; k < 9; ++k) I.m[k] = 0.0f;
+    for (uint32_t b = 0; b < n; ++b)
+        for (int i = 0; i < 512; ++i) {
+            if ((h.vox[(size_t)b * 512 + i] & 7u) == 0u) continue;
+            const int c[3] = {i % 8, (i / 8) % 8, i / 64};
+            float r[3];
+            for (int k = 0; k < 3; ++k) {
+                const float p = ((float)(h.pos[(size_t)b * 3 + k] * 8 + c[k]) * vs + half) + vs * 0.5f;
+                r[k] = p - com[k];
+            }
+            const float r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+            I.m[0] += vm * (r2 - r[0] * r[0]);
+            I.m[4] += vm * (r2 - r[1] * r[1]);
+            I.m[8] += vm * (r2 - r[2] * r[2]);
+            I.m[1] -= vm * r[0] * r[1];
+            I.m[2] -= vm * r[0] * r[2];
+            I.m[5] -= vm * r[1] * r[2];
+        }
+    I.m[3] = I.m[1];
+    I.m[6] = I.m[2];
+    I.m[7] = I.m[5];
+    *inv_mass = 1.0f / total;
+    const vxp::M33 inv = vxp::mat3_inverse(I);
+    for (int k = 0; k < 9; ++k) inv_inertia[k] = inv.m[k];
+    return VXP_OK;
+}
+
+int vxp_narrow_phase(vxp_ctx* ctx, const vxp_pair* pairs, uint32_t n_pairs);
+
+int vxp_step(vxp_ctx* ctx, float dt, const vxp_pair* pairs, uint32_t n_pairs) {
+    if (!ctx || (!pairs && n_pairs)) return fail(ctx, VXP_ERR_ARG, "null argument");
+    if (int rc = ensure_pair_cap(ctx, n_pairs)) return rc;
+    if (n_pairs) CK(cudaMemcpyAsync(ctx->pairs.p, pairs, n_pairs * sizeof(vxp_pair), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->n_pairs_dev.p, &n_pairs, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->last_pairs = n_pairs;
+    return launch_step(ctx, dt, n_pairs, PH_STEP);
+}
+
+int vxp_step_device_pairs(vxp_ctx* ctx, float dt, float margin) {
+    if (!ctx) return VXP_ERR_ARG;
+    uint32_t n = 0;
+    if (int rc = compute_device_pairs(ctx, margin, &n)) return rc;
+    ctx->last_pairs = n;
+    return launch_step(ctx, dt, n, PH_STEP);
+}
+
+// system.narrowPhase() alone: no all-sleeping early return (that test is
+// VoxelPhysicsSystem.step's).
+int vxp_narrow_phase(vxp_ctx* ctx, const vxp_pair* pairs, uint32_t n_pairs) {
+    if (!ctx || (!pairs && n_pairs)) return fail(ctx, VXP_ERR_ARG, "null argument");
+    if (int rc = ensure_pair_cap(ctx, n_pairs)) return rc;
+    if (n_pairs) CK(cudaMemcpyAsync(ctx->pairs.p, pairs, n_pairs * sizeof(vxp_pair), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->n_pairs_dev.p, &n_pairs, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->last_pairs = n_pairs;
+    return launch_step(ctx, 0.0f, n_pairs, PH_NARROW);
+}
+
+// system.solve() + updateSleepStates on the manifolds of the last narrow phase.
+int vxp_solve(vxp_ctx* ctx, float dt) {
+    if (!ctx) return VXP_ERR_ARG;
+    return launch_step(ctx, dt, ctx->last_pairs, PH_SOLVE);
+}
+
+int vxp_manifolds_get(vxp_ctx* ctx, vxp_manifold* out, uint32_t cap, uint32_t* n_out) {
+    if (!ctx || !n_out) return VXP_ERR_ARG;
+    if (int rc = check_device_error(ctx)) return rc;
+    uint32_t fr[2];
+    CK(cudaMemcpy(fr, ctx->frame.p, sizeof(fr), cudaMemcpyDeviceToHost));
+    // the latest narrow phase wrote man[frame & 1] with fr[1] slots
+    const uint32_t slot = fr[0] & 1u;
+    const ManifoldRec* m = slot ? ctx->man1.p : ctx->man0.p;
+    const uint32_t P = fr[1];
+    std::vector<ManifoldRec> hm(P);
+    if (P) CK(cudaMemcpy(hm.data(), m, P * sizeof(ManifoldRec), cudaMemcpyDeviceToHost));
+    uint32_t k = 0;
+    for (uint32_t p = 0; p < P; ++p) {
+        if (hm[p].n == 0u) continue;
+        if (k < cap && out) {
+            // slots past contact_count hold stale data on the device
+            ManifoldRec m = hm[p];
+            m._pad = 0u;
+            for (uint32_t i = m.n; i < 4u; ++i) std::memset(&m.c[i], 0, sizeof(ContactRec));
+            for (uint32_t i = 0; i < m.n; ++i) m.c[i]._pad = 0u;
+            std::memcpy(&out[k], &m, sizeof(vxp_manifold));
+        }
+        ++k;
+    }
+    *n_out = k;
+    return VXP_OK;
+}
+
+int vxp_set_candidate_dump(vxp_ctx* ctx, uint32_t capacity) {
+    if (!ctx) return VXP_ERR_ARG;
+    if (capacity && ctx->dump.reserve(capacity) != cudaSuccess) return fail(ctx, VXP_ERR_OOM, "dump buffer");
+    ctx->dump_cap = capacity;
+    return VXP_OK;
+}
+
+int vxp_candidates_get(vxp_ctx* ctx, vxp_candidate* out, uint32_t cap, uint32_t* n_out) {
+    if (!ctx || !n_out) return VXP_ERR_ARG;
+    if (int rc = check_device_error(ctx)) return rc;
+    uint32_t n = 0;
+    CK(cudaMemcpy(&n, ctx->ctr.p + C_DUMP_N, sizeof(n), cudaMemcpyDeviceToHost));
+    *n_out = n;
+    const uint32_t k = std::min(std::min(n, cap), ctx->dump_cap);
+    if (k && out) {
+        static_assert(sizeof(WorldDev::Cand) == sizeof(vxp_candidate), "candidate layout");
+        CK(cudaMemcpy(out, ctx->dump.p, k * sizeof(vxp_candidate), cudaMemcpyDeviceToHost));
+    }
+    if (n > ctx->dump_cap) return fail(ctx, VXP_ERR_CAP, "candidate dump overflow: %u > %u", n, ctx->dump_cap);
+    return VXP_OK;
+}
+
+int vxp_stats_get(vxp_ctx* ctx, vxp_stats* s) {
+    if (!ctx || !s) return VXP_ERR_ARG;
+    if (int rc = check_device_error(ctx)) return rc;
+    uint32_t c[C_NCTR];
+    CK(cudaMemcpy(c, ctx->ctr.p, sizeof(c), cudaMemcpyDeviceToHost));
+    std::memset(s, 0, sizeof(*s));
+    s->pairs_in = ctx->last_pairs;
+    s->pairs_tested = c[C_PAIRS_TESTED];
+    s->pairs_colliding = c[C_PAIRS_COLLIDING];
+    s->voxels_checked = c[C_VOXELS_CHECKED];
+    s->contacts_generated = c[C_CONTACTS];
+    s->pairs_skipped_sleeping = c[C_SKIPPED_SLEEPING];
+    s->manifolds_preserved = c[C_PRESERVED];
+    s->cache_hits = c[C_CACHE_HITS];
+    s->cache_misses = c[C_CACHE_MISSES];
+    s->cache_evictions = c[C_CACHE_EVICTIONS];
+    s->manifolds = c[C_MANIFOLDS];
+    s->constraints = c[C_CONSTRAINTS];
+    s->contact_points = c[C_POINTS];
+    s->colours = c[C_COLOURS];
+    s->position_iterations_run = c[C_POS_ITERS];
+    s->step_skipped = c[C_STEP_SKIPPED];
+    const int32_t k = (int32_t)c[C_MAX_PEN_KEY];
+    int32_t bits = k >= 0 ? k : (k ^ 0x7FFFFFFF);
+    std::memcpy(&s->max_penetration, &bits, 4);
+    s->candidates = c[C_CANDIDATES];
+    return VXP_OK;
+}
+
+int vxp_colours_get(vxp_ctx* ctx, uint32_t* colours, uint32_t cap, uint32_t* n_out) {
+    if (!ctx || !n_out) return VXP_ERR_ARG;
+    if (int rc = check_device_error(ctx)) return rc;
+    uint32_t M = 0;
+    CK(cudaMemcpy(&M, ctx->ctr.p + C_CONSTRAINTS, sizeof(M), cudaMemcpyDeviceToHost));
+    *n_out = M;
+    const uint32_t k = std::min(M, cap);
+    if (k && colours) CK(cudaMemcpy(colours, ctx->colour.p, k * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return VXP_OK;
+}
+
+int vxp_pairs_from_bodies(vxp_ctx* ctx, float margin, vxp_pair* out, uint32_t cap, uint32_t* n_out) {
+    if (!ctx || !n_out) return VXP_ERR_ARG;
+    uint32_t n = 0;
+    if (int rc = compute_device_pairs(ctx, margin, &n)) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    *n_out = n;
+    const uint32_t k = std::min(n, cap);
+    if (k && out) CK(cudaMemcpy(out, ctx->pairs.p, k * sizeof(vxp_pair), cudaMemcpyDeviceToHost));
+    return n > cap ? fail(ctx, VXP_ERR_CAP, "pair output holds %u, need %u", cap, n) : VXP_OK;
+}
+
+int vxp_last_step_ms(vxp_ctx* ctx, float out[3]) {
+    if (!ctx || !out) return VXP_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    out[0] = 0.f;
+    out[1] = 0.f;
+    out[2] = ms;
+    return VXP_OK;
+}
+
+// Extensions beyond the reference seams (declared in vxp.h).
+int vxp_synchronize(vxp_ctx* ctx) {
+    if (!ctx) return VXP_ERR_ARG;
+    return check_device_error(ctx);
+}
+
+int vxp_set_launch_mode(vxp_ctx* ctx, int mode) {
+    if (!ctx || mode < -1 || mode > 1) return VXP_ERR_ARG;
+    ctx->use_grid = mode;
+    return VXP_OK;
+}
+
+}  // extern "C"

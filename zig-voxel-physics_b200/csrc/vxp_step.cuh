@@ -1,0 +1,1790 @@
+// vxp_step.cuh — the phases of one physics step on the device.
+//
+// Included by vxp_lib.cu only.  See vxp_world.cuh for the layouts and the
+// phase map.  Float expressions keep the reference's operation order (the
+// library is compiled with --fmad=false and IEEE div/sqrt).
+#pragma once
+
+#include <cstdint>
+
+#include "vxp_math.cuh"
+#include "vxp_world.cuh"
+
+namespace vxp {
+
+__device__ __forceinline__ F3 f3of(float4 a) { return F3{a.x, a.y, a.z}; }
+__device__ __forceinline__ Qt qof(float4 a) { return Qt{a.x, a.y, a.z, a.w}; }
+__device__ __forceinline__ float4 f4of(F3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+__device__ __forceinline__ float4 f4of(Qt a) { return make_float4(a.x, a.y, a.z, a.w); }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Ordered-int key of a float: min/max of keys == min/max of the floats.
+__device__ __forceinline__ int32_t fkey(float f) {
+    const int32_t i = __float_as_int(f);
+    return i >= 0 ? i : (i ^ 0x7FFFFFFF);
+}
+__device__ __forceinline__ float fkey_inv(int32_t k) {
+    return __int_as_float(k >= 0 ? k : (k ^ 0x7FFFFFFF));
+}
+
+// ---------------------------------------------------------------------------
+// Groups
+// ---------------------------------------------------------------------------
+struct BlockGroup {
+    __device__ uint32_t rank() const { return threadIdx.x; }
+    __device__ uint32_t size() const { return blockDim.x; }
+    __device__ uint32_t block() const { return 0; }
+    __device__ uint32_t nblocks() const { return 1; }
+    __device__ bool sync() {
+        __syncthreads();
+        return true;
+    }
+};
+
+struct GridBar {
+    unsigned int count;
+    unsigned int gen;
+};
+
+struct GridGroup {
+    GridBar* bar;
+    uint32_t* err;
+    unsigned long long timeout_ns;
+    __device__ uint32_t rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+    __device__ uint32_t size() const { return gridDim.x * blockDim.x; }
+    __device__ uint32_t block() const { return blockIdx.x; }
+    __device__ uint32_t nblocks() const { return gridDim.x; }
+    // Bounded grid barrier: a waiting block gives up after timeout_ns, sets
+    // ERR_TIMEOUT and every later sync() of every block returns false.
+    __device__ bool sync() {
+        __shared__ int s_ok;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            volatile unsigned int* vgen = &bar->gen;
+            const unsigned int g = *vgen;
+            __threadfence();
+            const unsigned int arrived = atomicAdd(&bar->count, 1u);
+            if (arrived == gridDim.x - 1) {
+                atomicExch(&bar->count, 0u);
+                __threadfence();
+                atomicAdd(&bar->gen, 1u);
+            } else {
+                const unsigned long long t0 = global_ns();
+                while (*vgen == g) {
+                    __nanosleep(64);
+                    if (global_ns() - t0 > timeout_ns) {
+                        atomicOr(err, ERR_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+            __threadfence();
+            if (*(volatile uint32_t*)err & ERR_TIMEOUT) ok = 0;
+            s_ok = ok;
+        }
+        __syncthreads();
+        return s_ok != 0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Block-level primitives (blockDim.x <= 1024, multiple of 32)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+    const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= (uint32_t)d) v += o;
+    }
+    return v;
+}
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    return v;
+}
+// Exclusive block scan; *total receives the block sum (all threads).
+__device__ uint32_t block_excl_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t s_w[33];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t inc = warp_incl_scan(v);
+    if (lane == 31) s_w[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        const uint32_t x = lane < nw ? s_w[lane] : 0u;
+        const uint32_t xi = warp_incl_scan(x);
+        if (lane < nw) s_w[lane] = xi - x;
+        if (lane == 31) s_w[32] = xi;
+    }
+    __syncthreads();
+    const uint32_t r = s_w[wid] + inc - v;
+    *total = s_w[32];
+    __syncthreads();
+    return r;
+}
+__device__ uint32_t block_sum(uint32_t v) {
+    uint32_t t;
+    block_excl_scan(v, &t);
+    return t;
+}
+
+// Exclusive scan over the group of f(i), i in [0, n).  write(i, prefix) is
+// called for every i; returns the total.  Uses scratch[nblocks].
+template <class G, class F, class W>
+__device__ bool group_scan(G& g, uint32_t n, F f, W write, uint32_t* scratch, uint32_t* total_out) {
+    const uint32_t nb = g.nblocks(), b = g.block();
+    const uint32_t seg = (n + nb - 1) / nb;
+    const uint32_t lo = min(n, b * seg), hi = min(n, lo + seg);
+    uint32_t part = 0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) part += f(i);
+    part = block_sum(part);
+    if (threadIdx.x == 0) scratch[b] = part;
+    if (!g.sync()) return false;
+    uint32_t base = 0, tot = 0;
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        const uint32_t x = *(volatile uint32_t*)&scratch[j];
+        tot += x;
+        if (j < b) base += x;
+    }
+    base = block_sum(base);
+    tot = block_sum(tot);
+    uint32_t carry = base;
+    for (uint32_t t0 = lo; t0 < hi; t0 += blockDim.x) {
+        const uint32_t i = t0 + threadIdx.x;
+        const uint32_t v = i < hi ? f(i) : 0u;
+        uint32_t tile;
+        const uint32_t ex = block_excl_scan(v, &tile);
+        if (i < hi) write(i, carry + ex);
+        carry += tile;
+    }
+    *total_out = tot;
+    return g.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Collider access
+// ---------------------------------------------------------------------------
+struct ColliderSet {
+    const DCollider* c;
+    const int32_t* grid;
+    const uint8_t* vox;
+    uint32_t n;
+};
+
+__device__ __forceinline__ uint32_t voxel_at(const ColliderSet& cs, const DCollider& c, int32_t x, int32_t y,
+                                             int32_t z) {
+    const int32_t bx = (x >> 3) - c.bmin[0], by = (y >> 3) - c.bmin[1], bz = (z >> 3) - c.bmin[2];
+    if ((uint32_t)bx >= (uint32_t)c.bdim[0] || (uint32_t)by >= (uint32_t)c.bdim[1] ||
+        (uint32_t)bz >= (uint32_t)c.bdim[2])
+        return 0u;
+    const int32_t slot = __ldg(&cs.grid[c.grid_off + (uint32_t)(bx + c.bdim[0] * (by + c.bdim[1] * bz))]);
+    if (slot < 0) return 0u;
+    return (uint32_t)__ldg(&cs.vox[(size_t)(c.brick_off + (uint32_t)slot) * 512u + (uint32_t)((x & 7) + 8 * (y & 7) +
+                                                                                                 64 * (z & 7))]);
+}
+__device__ __forceinline__ F3 voxel_to_local(float vs, int32_t x, int32_t y, int32_t z) {
+    const float half = vs * 0.5f;
+    return F3{(float)x * vs + half, (float)y * vs + half, (float)z * vs + half};
+}
+__device__ __forceinline__ I3 local_to_voxel(float vs, F3 p) {
+    return I3{(int32_t)floorf(p.x / vs), (int32_t)floorf(p.y / vs), (int32_t)floorf(p.z / vs)};
+}
+__device__ __forceinline__ bool valid_coord(const DCollider& c, int32_t x, int32_t y, int32_t z) {
+    return x >= c.min_bound[0] && x < c.max_bound[0] && y >= c.min_bound[1] && y < c.max_bound[1] &&
+           z >= c.min_bound[2] && z < c.max_bound[2];
+}
+
+// NORMAL_LUT (collision_voxel.zig:47-76) as getNormalVec3 would return it.
+__device__ __forceinline__ F3 lut_normal(uint32_t idx) {
+    if (idx >= 26u) return F3{0.f, 0.f, 0.f};
+    // component codes: 0 -> 0, 1 -> +1, 2 -> -1, packed 2 bits per axis
+    const uint32_t kCode[26] = {0x01, 0x02, 0x04, 0x08, 0x10, 0x20, 0x05, 0x09, 0x06, 0x0A, 0x11, 0x21, 0x12,
+                                0x22, 0x14, 0x24, 0x18, 0x28, 0x15, 0x25, 0x19, 0x29, 0x16, 0x26, 0x1A, 0x2A};
+    const uint32_t c = kCode[idx];
+    const float x = (c & 3u) == 1u ? 1.f : ((c & 3u) == 2u ? -1.f : 0.f);
+    const float y = ((c >> 2) & 3u) == 1u ? 1.f : (((c >> 2) & 3u) == 2u ? -1.f : 0.f);
+    const float z = ((c >> 4) & 3u) == 1u ? 1.f : (((c >> 4) & 3u) == 2u ? -1.f : 0.f);
+    return normalize3(F3{x, y, z});
+}
+
+// ---------------------------------------------------------------------------
+// OBB helpers (math.zig:715-747) and SAT (narrow_phase.zig:505-569)
+// ---------------------------------------------------------------------------
+struct Obb {
+    F3 c, h;
+    Qt q;
+};
+__device__ __forceinline__ Obb obb_from(const DCollider& col, F3 pos, Qt q) {
+    const F3 mn{col.aabb_min[0], col.aabb_min[1], col.aabb_min[2]};
+    const F3 mx{col.aabb_max[0], col.aabb_max[1], col.aabb_max[2]};
+    const F3 center = (mn + mx) * 0.5f;
+    const F3 ext = (mx - mn) * 0.5f;
+    return Obb{transform_point(pos, q, center), ext, q};
+}
+__device__ __forceinline__ void obb_axes(const Obb& o, F3 ax[3]) {
+    ax[0] = qrotate(o.q, F3{1.f, 0.f, 0.f});
+    ax[1] = qrotate(o.q, F3{0.f, 1.f, 0.f});
+    ax[2] = qrotate(o.q, F3{0.f, 0.f, 1.f});
+}
+__device__ __forceinline__ void obb_verts(const Obb& o, F3 v[8]) {
+    F3 ax[3];
+    obb_axes(o, ax);
+    const F3 ex = ax[0] * o.h.x, ey = ax[1] * o.h.y, ez = ax[2] * o.h.z;
+    v[0] = ((o.c - ex) - ey) - ez;
+    v[1] = ((o.c + ex) - ey) - ez;
+    v[2] = ((o.c - ex) + ey) - ez;
+    v[3] = ((o.c + ex) + ey) - ez;
+    v[4] = ((o.c - ex) - ey) + ez;
+    v[5] = ((o.c + ex) - ey) + ez;
+    v[6] = ((o.c - ex) + ey) + ez;
+    v[7] = ((o.c + ex) + ey) + ez;
+}
+__device__ __forceinline__ void project8(const F3 v[8], F3 axis, float* mn, float* mx) {
+    float lo = __int_as_float(0x7f800000), hi = -__int_as_float(0x7f800000);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float p = dot3(v[i], axis);
+        lo = fminf(lo, p);
+        hi = fmaxf(hi, p);
+    }
+    *mn = lo;
+    *mx = hi;
+}
+__device__ bool sat_separated(const Obb& a, const Obb& b) {
+    F3 aa[3], ab[3], va[8], vb[8];
+    obb_axes(a, aa);
+    obb_axes(b, ab);
+    obb_verts(a, va);
+    obb_verts(b, vb);
+    float p0, p1, q0, q1;
+    for (int i = 0; i < 3; ++i) {
+        project8(va, aa[i], &p0, &p1);
+        project8(vb, aa[i], &q0, &q1);
+        if (p1 < q0 || q1 < p0) return true;
+    }
+    for (int i = 0; i < 3; ++i) {
+        project8(va, ab[i], &p0, &p1);
+        project8(vb, ab[i], &q0, &q1);
+        if (p1 < q0 || q1 < p0) return true;
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const F3 cr = cross3(aa[i], ab[j]);
+            const float l = len3(cr);
+            if (l < 0.001f) continue;
+            const F3 ax = cr * (1.0f / l);
+            project8(va, ax, &p0, &p1);
+            project8(vb, ax, &q0, &q1);
+            if (p1 < q0 || q1 < p0) return true;
+        }
+    return false;
+}
+
+// getOverlapRegion (narrow_phase.zig:644-698).  Returns false when empty.
+__device__ bool overlap_region(const DCollider& ca, F3 pa, Qt qa, const DCollider& cb, F3 pb, Qt qb, I3* rmin,
+                               I3* rmax) {
+    const Obb ob = obb_from(cb, pb, qb);
+    F3 vb[8];
+    obb_verts(ob, vb);
+    const Qt inv = qconj(qa);
+    const float inf = __int_as_float(0x7f800000);
+    F3 tmn{inf, inf, inf}, tmx{-inf, -inf, -inf};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const F3 rel = qrotate(inv, vb[i] - pa);
+        tmn = min3(tmn, rel);
+        tmx = max3(tmx, rel);
+    }
+    const float vs = ca.vs;
+    tmn = tmn - F3{vs, vs, vs};
+    tmx = tmx + F3{vs, vs, vs};
+    const F3 lo{ca.aabb_min[0], ca.aabb_min[1], ca.aabb_min[2]};
+    const F3 hi{ca.aabb_max[0], ca.aabb_max[1], ca.aabb_max[2]};
+    const F3 mnc = clamp3(tmn, lo, hi), mxc = clamp3(tmx, lo, hi);
+    if (mnc.x >= mxc.x || mnc.y >= mxc.y || mnc.z >= mxc.z) return false;
+    const I3 a = local_to_voxel(vs, mnc), b = local_to_voxel(vs, mxc);
+    *rmin = I3{max(a.x, ca.min_bound[0]), max(a.y, ca.min_bound[1]), max(a.z, ca.min_bound[2])};
+    *rmax = I3{min(b.x, ca.max_bound[0]), min(b.y, ca.max_bound[1]), min(b.z, ca.max_bound[2])};
+    return true;
+}
+
+// BrickPairKey.hash with zero brick positions, and computeTransformHash
+// (narrow_phase.zig:118-169).
+__device__ __forceinline__ unsigned long long cache_transform_hash(F3 rp, Qt rr) {
+    const int32_t qx = (int32_t)(rp.x * 100.0f), qy = (int32_t)(rp.y * 100.0f), qz = (int32_t)(rp.z * 100.0f);
+    const int16_t rw = (int16_t)(int32_t)clampf_ref(rr.w * 1000.0f, -32767.0f, 32767.0f);
+    const int16_t rx = (int16_t)(int32_t)clampf_ref(rr.x * 1000.0f, -32767.0f, 32767.0f);
+    const int16_t ry = (int16_t)(int32_t)clampf_ref(rr.y * 1000.0f, -32767.0f, 32767.0f);
+    const int16_t rz = (int16_t)(int32_t)clampf_ref(rr.z * 1000.0f, -32767.0f, 32767.0f);
+    unsigned long long h = 0;
+    h = h * 31ull + (unsigned long long)(uint32_t)qx;
+    h = h * 31ull + (unsigned long long)(uint32_t)qy;
+    h = h * 31ull + (unsigned long long)(uint32_t)qz;
+    h = h * 31ull + (unsigned long long)(uint16_t)rw;
+    h = h * 31ull + (unsigned long long)(uint16_t)rx;
+    h = h * 31ull + (unsigned long long)(uint16_t)ry;
+    h = h * 31ull + (unsigned long long)(uint16_t)rz;
+    return h;
+}
+__device__ __forceinline__ unsigned long long cache_key_hash(uint32_t a, uint32_t b, unsigned long long th) {
+    unsigned long long h = 0;
+    h = h * 31ull + (unsigned long long)a;
+    h = h * 31ull + (unsigned long long)b;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) h = h * 31ull;  // brick positions (0,0,0), (0,0,0)
+    h = h * 31ull + th;
+    return h;
+}
+
+// Hash table of pair keys (open addressing).
+__device__ __forceinline__ uint32_t ht_hash(unsigned long long k, uint32_t cap) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return (uint32_t)k & (cap - 1u);
+}
+__device__ void ht_insert(HashSlot* t, uint32_t cap, unsigned long long key, uint32_t idx) {
+    uint32_t s = ht_hash(key, cap);
+    for (uint32_t i = 0; i < cap; ++i) {
+        const unsigned long long prev = atomicCAS(&t[s].key, 0ull, key);
+        if (prev == 0ull || prev == key) {
+            t[s].idx = idx;
+            return;
+        }
+        s = (s + 1u) & (cap - 1u);
+    }
+}
+__device__ uint32_t ht_find(const HashSlot* t, uint32_t cap, unsigned long long key) {
+    uint32_t s = ht_hash(key, cap);
+    for (uint32_t i = 0; i < cap; ++i) {
+        const unsigned long long k = t[s].key;
+        if (k == key) return t[s].idx;
+        if (k == 0ull) return 0xFFFFFFFFu;
+        s = (s + 1u) & (cap - 1u);
+    }
+    return 0xFFFFFFFFu;
+}
+
+__device__ __forceinline__ uint32_t find_body(const uint2* ids, uint32_t n, uint32_t id) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t v = ids[mid].x;
+        if (v < id) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && ids[lo].x == id) ? ids[lo].y : 0xFFFFFFFFu;
+}
+
+// ---------------------------------------------------------------------------
+// Phase: begin (sleep skip test, per-body step-start state)
+// ---------------------------------------------------------------------------
+template <class G>
+__device__ bool phase_begin(G& g, WorldDev& w, bool skip_test, bool* skipped) {
+    // counters (not the sticky error word) are zeroed by the host/graph memset.
+    for (uint32_t i = g.rank(); i < w.n_bodies; i += g.size()) {
+        const DBodyProp& pr = w.prop[i];
+        if (pr.type == 2u && !pr.sleeping) atomicAdd(&w.ctr[C_AWAKE], 1u);
+    }
+    if (!g.sync()) return false;
+    const uint32_t awake = *(volatile uint32_t*)&w.ctr[C_AWAKE];
+    // VoxelPhysicsSystem.step returns early when every dynamic body sleeps
+    // (system.zig:538-544)
+    if (skip_test && w.cfg.sleeping_on && awake == 0u) {
+        *skipped = true;
+        if (g.rank() == 0) w.ctr[C_STEP_SKIPPED] = 1u;
+        return true;
+    }
+    *skipped = false;
+    // BodyState.fromBody: world inverse inertia from the current rotation.
+    for (uint32_t i = g.rank(); i < w.n_bodies; i += g.size()) {
+        DBody& b = w.body[i];
+        const DBodyProp& pr = w.prop[i];
+        const Qt q = qof(b.q);
+        w.qn[i] = f4of(qnormalize(q));
+        w.p0[i] = b.p;
+        if (b.p.w == 0.0f) {
+            b.i0 = b.i1 = b.i2 = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+            M33 il;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) il.m[k] = pr.il[k];
+            const M33 m = world_inv_inertia(q, il);
+            b.i0 = make_float4(m.m[0], m.m[1], m.m[2], 0.f);
+            b.i1 = make_float4(m.m[3], m.m[4], m.m[5], 0.f);
+            b.i2 = make_float4(m.m[6], m.m[7], m.m[8], 0.f);
+        }
+    }
+    return g.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Phase: pairs (system.narrowPhase filter + processPair head)
+// ---------------------------------------------------------------------------
+template <class G>
+__device__ bool phase_pairs(G& g, WorldDev& w, const ColliderSet& cs, uint32_t cur) {
+    const uint32_t P = w.n_pairs;
+    if (g.rank() == 0) {
+        w.ctr[C_PAIRS_IN] = P;
+        w.cframe[0] += 1ull;  // BrickPairCache.beginFrame
+    }
+    for (uint32_t i = g.rank(); i < w.ht_cap; i += g.size()) {
+        w.ht[cur][i].key = 0ull;
+        w.ht[cur][i].idx = 0xFFFFFFFFu;
+    }
+    for (uint32_t p = g.rank(); p < P; p += g.size()) {
+        const uint2 pr = w.pairs[p];
+        const uint32_t ia = find_body(w.ids, w.n_bodies, pr.x), ib = find_body(w.ids, w.n_bodies, pr.y);
+        uint32_t fl = 0;
+        if (ia == 0xFFFFFFFFu || ib == 0xFFFFFFFFu) fl |= PF_INVALID;
+        const bool as = ia != 0xFFFFFFFFu ? w.prop[ia].sleeping != 0u : false;
+        const bool bs = ib != 0xFFFFFFFFu ? w.prop[ib].sleeping != 0u : false;
+        if (as && bs) fl |= PF_CARRY;
+        PairInfo& pi = w.pinfo[p];
+        pi.ia = ia;
+        pi.ib = ib;
+        pi.flags = fl;
+        pi.voxels_checked = 0;
+        pi.candidates = 0;
+        pi.cache_slot = 0xFFFFFFFFu;
+        w.flag[p] = (fl & PF_CARRY) ? 0u : 1u;
+    }
+    if (!g.sync()) return false;
+    if (w.cfg.reference_caps) {
+        uint32_t tot;
+        if (!group_scan(
+                g, P, [&](uint32_t i) { return w.flag[i]; },
+                [&](uint32_t i, uint32_t pre) {
+                    if (w.flag[i] && pre >= 512u) w.pinfo[i].flags |= PF_DROPPED;
+                },
+                w.scan, &tot))
+            return false;
+    }
+    uint32_t tested = 0;
+    for (uint32_t p = g.rank(); p < P; p += g.size()) {
+        PairInfo& pi = w.pinfo[p];
+        uint32_t fl = pi.flags;
+        if (fl & (PF_CARRY | PF_DROPPED | PF_INVALID)) continue;
+        fl |= PF_TESTED;
+        ++tested;
+        const DBody& A = w.body[pi.ia];
+        const DBody& B = w.body[pi.ib];
+        const DBodyProp& pa = w.prop[pi.ia];
+        const DBodyProp& pb = w.prop[pi.ib];
+        if (pa.collider >= cs.n || pb.collider >= cs.n) {
+            pi.flags = fl | PF_NOCOLL;
+            continue;
+        }
+        const DCollider& ca = cs.c[pa.collider];
+        const DCollider& cb = cs.c[pb.collider];
+        const F3 xa = f3of(A.p), xb = f3of(B.p);
+        const Qt qa = qof(A.q), qb = qof(B.q);
+        if (w.cfg.use_sat) {
+            if (sat_separated(obb_from(ca, xa, qa), obb_from(cb, xb, qb))) {
+                pi.flags = fl | PF_SEPARATED;
+                continue;
+            }
+        }
+        const bool use_cache =
+            w.cfg.use_cache && (pa.type == 0u || pb.type == 0u || pa.sleeping != 0u || pb.sleeping != 0u);
+        if (use_cache) {
+            fl |= PF_CACHE;
+            const F3 rp = xb - xa;
+            const Qt rr = qmul(qconj(qa), qb);
+            const bool af = pa.id < pb.id;
+            pi.key_a = af ? pa.id : pb.id;
+            pi.key_b = af ? pb.id : pa.id;
+            pi.th = cache_transform_hash(rp, rr);
+        } else {
+            fl |= PF_DETECT;
+        }
+        I3 rmin, rmax;
+        if (overlap_region(ca, xa, qa, cb, xb, qb, &rmin, &rmax)) {
+            if (rmin.x <= rmax.x && rmin.y <= rmax.y && rmin.z <= rmax.z) fl |= PF_REGION;
+            pi.rmin[0] = rmin.x; pi.rmin[1] = rmin.y; pi.rmin[2] = rmin.z;
+            pi.rmax[0] = rmax.x; pi.rmax[1] = rmax.y; pi.rmax[2] = rmax.z;
+        }
+        pi.flags = fl;
+    }
+    tested = warp_sum(tested);
+    if ((threadIdx.x & 31) == 0 && tested) atomicAdd(&w.ctr[C_PAIRS_TESTED], tested);
+    return g.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Phase: brick-pair cache replay (one warp, pairs in order)
+// ---------------------------------------------------------------------------
+template <class G>
+__device__ bool phase_cache(G& g, WorldDev& w) {
+    if (w.cfg.use_cache && g.rank() < 32u) {
+        const uint32_t lane = threadIdx.x & 31;
+        const unsigned long long frame = w.cframe[0];
+        const uint32_t cap = w.cache_cap;
+        const uint32_t maxp = cap < 16u ? cap : 16u;
+        uint32_t hits = 0, misses = 0, evictions = 0;
+        for (uint32_t base = 0; base < w.n_pairs; base += 32u) {
+            const uint32_t p0 = base + lane;
+            const bool is_c = p0 < w.n_pairs && (w.pinfo[p0].flags & PF_CACHE) && !(w.pinfo[p0].flags & PF_NOCOLL);
+            uint32_t m = __ballot_sync(0xffffffffu, is_c);
+            while (m) {
+                const uint32_t bit = __ffs(m) - 1;
+                m &= m - 1;
+                const uint32_t p = base + bit;
+                PairInfo& pi = w.pinfo[p];
+                const uint32_t ka = pi.key_a, kb = pi.key_b;
+                const unsigned long long th = pi.th;
+                const uint32_t start = (uint32_t)(cache_key_hash(ka, kb, th) % (unsigned long long)cap);
+                const uint32_t slot = (start + lane) % cap;
+                bool valid = false, match = false;
+                unsigned long long lu = ~0ull;
+                if (lane < maxp) {
+                    const volatile CacheKeyRec* e = &w.ckey[slot];
+                    valid = e->valid != 0u;
+                    match = valid && e->a == ka && e->b == kb && e->th == th;
+                    lu = e->last_used;
+                }
+                const uint32_t inv_m = __ballot_sync(0xffffffffu, lane < maxp && !valid);
+                const uint32_t mat_m = __ballot_sync(0xffffffffu, match);
+                const uint32_t fi = inv_m ? (uint32_t)(__ffs(inv_m) - 1) : 32u;
+                const uint32_t fm = mat_m ? (uint32_t)(__ffs(mat_m) - 1) : 32u;
+                uint32_t target;
+                bool hit = false;
+                if (fm < fi) {
+                    hit = true;
+                    target = (start + fm) % cap;
+                } else if (fi < 32u) {
+                    target = (start + fi) % cap;
+                } else {
+                    // evict the first least-recently-used entry of the window
+                    unsigned long long best = lane < maxp ? lu : ~0ull;
+                    uint32_t bl = lane < maxp ? lane : 32u;
+#pragma unroll
+                    for (int d = 16; d > 0; d >>= 1) {
+                        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, best, d);
+                        const uint32_t ol = __shfl_xor_sync(0xffffffffu, bl, d);
+                        if (ob < best || (ob == best && ol < bl)) {
+                            best = ob;
+                            bl = ol;
+                        }
+                    }
+                    target = (start + bl) % cap;
+                    ++evictions;
+                }
+                if (lane == 0) {
+                    if (hit) {
+                        w.ckey[target].last_used = frame;
+                        pi.flags |= PF_HIT;
+                        ++hits;
+                    } else {
+                        CacheKeyRec k;
+                        k.a = ka;
+                        k.b = kb;
+                        k.th = th;
+                        k.last_used = frame;
+                        k.valid = 1u;
+                        k._pad = 0u;
+                        w.ckey[target] = k;
+                        w.cwriter[target] = p;
+                        pi.flags |= PF_DETECT;
+                        ++misses;
+                    }
+                    pi.cache_slot = target;
+                }
+                __syncwarp();
+            }
+        }
+        if (lane == 0) {
+            w.ctr[C_CACHE_HITS] += hits;
+            w.ctr[C_CACHE_MISSES] += misses;
+            w.ctr[C_CACHE_EVICTIONS] += evictions;
+        }
+    }
+    return g.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Phase: probe (detectVoxelCollisions + checkNeighborhood + addContact)
+// ---------------------------------------------------------------------------
+// Top-4 multiset of penetrations, sorted descending, -inf padded.
+struct Top4 {
+    float v[4];
+};
+__device__ __forceinline__ Top4 top4_empty() {
+    const float ni = -__int_as_float(0x7f800000);
+    return Top4{{ni, ni, ni, ni}};
+}
+__device__ __forceinline__ void cswap_desc(float& a, float& b) {
+    const float hi = fmaxf(a, b), lo = fminf(a, b);
+    a = hi;
+    b = lo;
+}
+// Top four of the union of two descending multisets.
+__device__ __forceinline__ Top4 top4_merge(const Top4& a, const Top4& b) {
+    Top4 c{{fmaxf(a.v[0], b.v[3]), fmaxf(a.v[1], b.v[2]), fmaxf(a.v[2], b.v[1]), fmaxf(a.v[3], b.v[0])}};
+    cswap_desc(c.v[0], c.v[2]);
+    cswap_desc(c.v[1], c.v[3]);
+    cswap_desc(c.v[0], c.v[1]);
+    cswap_desc(c.v[2], c.v[3]);
+    return c;
+}
+__device__ __forceinline__ void top4_insert(Top4& t, float x) {
+    if (!(x > t.v[3])) return;
+    t.v[3] = x;
+    cswap_desc(t.v[2], t.v[3]);
+    cswap_desc(t.v[1], t.v[2]);
+    cswap_desc(t.v[0], t.v[1]);
+}
+__device__ __forceinline__ Top4 top4_shfl_up(const Top4& t, int d) {
+    Top4 r;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r.v[i] = __shfl_up_sync(0xffffffffu, t.v[i], d);
+    return r;
+}
+
+struct ProbeCtx {
+    const DCollider* ca;
+    const DCollider* cb;
+    F3 pa, pb;
+    Qt qa, qb, qna, qnb;
+    float vs_a, vs_b, spec;
+};
+
+// The 27 neighbour offsets in checkNeighborhood order: dz, dy, dx in {-1,0,1}.
+__device__ __forceinline__ I3 probe_offset(uint32_t k) {
+    return I3{(int32_t)(k % 3u) - 1, (int32_t)((k / 3u) % 3u) - 1, (int32_t)(k / 9u) - 1};
+}
+
+// Penetration of a distance-passing candidate (generateContact).
+__device__ __forceinline__ float cand_pen(float vs_a, uint32_t ta, uint32_t tb, float d2) {
+    float pen = vs_a - sqrtf(d2);
+    if (ta == kInside || tb == kInside) pen = fmaxf(pen, vs_a);
+    return pen;
+}
+
+// generateContact (narrow_phase.zig:860-922).
+__device__ void generate_contact(const ProbeCtx& c, uint32_t va, I3 ia, F3 wa, uint32_t vb, I3 ib, F3 wb,
+                                 ContactRec* out) {
+    const F3 diff = wb - wa;
+    const float d2 = lensq3(diff);
+    const float dist = sqrtf(d2);
+    const F3 cp = (wa + wb) * 0.5f;
+    float pen = c.vs_a - dist;
+    const F3 na = qrotate(c.qa, lut_normal(vnormal(va)));
+    const F3 nb = qrotate(c.qb, lut_normal(vnormal(vb)));
+    F3 n;
+    if (vtype(va) == kFace) {
+        n = na;
+    } else if (vtype(vb) == kFace) {
+        n = -nb;
+    } else if (dist > 0.001f) {
+        const F3 dn = diff * (1.0f / dist);
+        if (dot3(dn, na) > 0.3f) n = na;
+        else if (dot3(dn, -nb) > 0.3f) n = -nb;
+        else n = dn;
+    } else {
+        n = na;
+    }
+    if (vtype(va) == kInside || vtype(vb) == kInside) pen = fmaxf(pen, c.vs_a);
+    const F3 la = inverse_transform_point(c.pa, c.qa, cp);
+    const F3 lb = inverse_transform_point(c.pb, c.qb, cp);
+    out->point[0] = cp.x; out->point[1] = cp.y; out->point[2] = cp.z;
+    out->normal[0] = n.x; out->normal[1] = n.y; out->normal[2] = n.z;
+    out->penetration = pen;
+    out->la[0] = la.x; out->la[1] = la.y; out->la[2] = la.z;
+    out->lb[0] = lb.x; out->lb[1] = lb.y; out->lb[2] = lb.z;
+    out->normal_impulse = 0.f;
+    out->tangent_impulse[0] = 0.f;
+    out->tangent_impulse[1] = 0.f;
+    out->normal_mass = 0.f;
+    out->tangent_mass[0] = 0.f;
+    out->tangent_mass[1] = 0.f;
+    out->_pad = 0u;
+    out->feature_id = feature_id(ia, ib);
+}
+
+// Per-warp shared state of phase_probe.
+struct WarpManifold {
+    ContactRec c[4];
+    ContactRec stage;
+    float pens[4];
+    uint32_t n;
+    uint32_t pad[3];
+};
+
+// ContactManifold.addContact (narrow_phase.zig:451-481), executed by one lane.
+__device__ __forceinline__ void add_contact(WarpManifold& m, const ContactRec& k) {
+    for (uint32_t i = 0; i < m.n; ++i) {
+        if (m.c[i].feature_id == k.feature_id) {
+            const float ni = m.c[i].normal_impulse, t0 = m.c[i].tangent_impulse[0], t1 = m.c[i].tangent_impulse[1];
+            m.c[i] = k;
+            m.c[i].normal_impulse = ni;
+            m.c[i].tangent_impulse[0] = t0;
+            m.c[i].tangent_impulse[1] = t1;
+            return;
+        }
+    }
+    if (m.n < 4u) {
+        m.c[m.n] = k;
+        m.n += 1u;
+        return;
+    }
+    float mp = k.penetration;
+    int mi = -1;
+    for (uint32_t i = 0; i < m.n; ++i) {
+        if (m.c[i].penetration < mp) {
+            mp = m.c[i].penetration;
+            mi = (int)i;
+        }
+    }
+    if (mi >= 0) m.c[mi] = k;
+}
+
+// One warp runs detectVoxelCollisions for pair p.  The inclusive z, y, x loop
+// over the overlap region is cut into groups of 32 consecutive voxels, one per
+// lane; each lane runs the 27 probes of its voxel.  The manifold reduction is
+// order dependent, so it is reproduced exactly: a candidate can only enter the
+// 4-slot manifold if its penetration beats the 4th largest penetration of all
+// candidates before it (the multiset of penetrations held by the manifold is
+// always the top four of the prefix).  A warp scan of top-4 multisets gives
+// every lane that prefix, seeded with the manifold's state; only the entering
+// candidates are replayed, in order, through addContact.
+__device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uint32_t p, WarpManifold& sm) {
+    const uint32_t lane = threadIdx.x & 31;
+    PairInfo& pi = w.pinfo[p];
+    const uint32_t ia = pi.ia, ib = pi.ib;
+    const DBody& A = w.body[ia];
+    const DBody& B = w.body[ib];
+    const DBodyProp& prA = w.prop[ia];
+    const DBodyProp& prB = w.prop[ib];
+    ProbeCtx c;
+    c.ca = &cs.c[prA.collider];
+    c.cb = &cs.c[prB.collider];
+    c.pa = f3of(A.p);
+    c.pb = f3of(B.p);
+    c.qa = qof(A.q);
+    c.qb = qof(B.q);
+    c.qna = qof(w.qn[ia]);
+    c.qnb = qof(w.qn[ib]);
+    c.vs_a = c.ca->vs;
+    c.vs_b = c.cb->vs;
+    {
+        const float cds = c.vs_a * c.vs_a * 1.0f * 1.0f;
+        c.spec = cds + 0.02f * 0.02f + 2.0f * sqrtf(cds) * 0.02f;
+    }
+    const DCollider& ca = *c.ca;
+    const DCollider& cb = *c.cb;
+    const int32_t nx = pi.rmax[0] - pi.rmin[0] + 1, ny = pi.rmax[1] - pi.rmin[1] + 1,
+                  nz = pi.rmax[2] - pi.rmin[2] + 1;
+    const unsigned long long V = (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
+    if (lane == 0) sm.n = 0u;
+    Top4 state = top4_empty();
+    uint32_t checked = 0, ncand = 0;
+    __syncwarp();
+    for (unsigned long long base = 0; base < V; base += 32ull) {
+        const unsigned long long l = base + lane;
+        uint32_t va = 0u;
+        int32_t x = 0, y = 0, z = 0;
+        if (l < V) {
+            const uint32_t li = (uint32_t)l;
+            x = pi.rmin[0] + (int32_t)(li % (uint32_t)nx);
+            y = pi.rmin[1] + (int32_t)((li / (uint32_t)nx) % (uint32_t)ny);
+            z = pi.rmin[2] + (int32_t)(li / ((uint32_t)nx * (uint32_t)ny));
+            va = voxel_at(cs, ca, x, y, z);
+        }
+        uint32_t mask = 0u;
+        Top4 t = top4_empty();
+        F3 wa{0.f, 0.f, 0.f};
+        I3 cbv{0, 0, 0};
+        const uint32_t ta = vtype(va);
+        if (ta != kEmpty) {
+            wa = transform_point_n(c.pa, c.qna, voxel_to_local(c.vs_a, x, y, z));
+            cbv = local_to_voxel(c.vs_b, inverse_transform_point(c.pb, c.qb, wa));
+            for (uint32_t k = 0; k < 27u; ++k) {
+                const I3 o = probe_offset(k);
+                const int32_t bx = cbv.x + o.x, by = cbv.y + o.y, bz = cbv.z + o.z;
+                if (!valid_coord(cb, bx, by, bz)) continue;
+                const uint32_t vb = voxel_at(cs, cb, bx, by, bz);
+                const uint32_t tb = vtype(vb);
+                if (tb == kEmpty) continue;
+                ++checked;
+                if (!type_filter(ta, tb)) continue;
+                const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, bx, by, bz));
+                const F3 diff = wb - wa;
+                const float d2 = lensq3(diff);
+                const bool pass = d2 < c.spec;
+                if (w.cfg.dump_candidates) {
+                    const uint32_t slot = atomicAdd(&w.ctr[C_DUMP_N], 1u);
+                    if (slot < w.dump_cap) {
+                        WorldDev::Cand& r = w.dump[slot];
+                        r.pair_index = p;
+                        r.a[0] = x; r.a[1] = y; r.a[2] = z;
+                        r.b[0] = bx; r.b[1] = by; r.b[2] = bz;
+                        r.passed = pass ? 1u : 0u;
+                        r.dist_sq = d2;
+                    }
+                }
+                if (pass) {
+                    mask |= 1u << k;
+                    top4_insert(t, cand_pen(c.vs_a, ta, tb, d2));
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, mask != 0u) == 0u) continue;
+        ncand += __popc(mask);
+        // exclusive warp scan of the lanes' top-4 multisets
+        Top4 inc = t;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const Top4 o = top4_shfl_up(inc, d);
+            if ((int)lane >= d) inc = top4_merge(o, inc);
+        }
+        Top4 ex = top4_shfl_up(inc, 1);
+        if (lane == 0) ex = top4_empty();
+        Top4 run = top4_merge(state, ex);
+        // candidates of this lane that enter the manifold
+        uint32_t enter = 0u;
+        for (uint32_t mm = mask; mm; mm &= mm - 1u) {
+            const uint32_t k = __ffs(mm) - 1;
+            const I3 o = probe_offset(k);
+            const int32_t bx = cbv.x + o.x, by = cbv.y + o.y, bz = cbv.z + o.z;
+            const uint32_t vb = voxel_at(cs, cb, bx, by, bz);
+            const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, bx, by, bz));
+            const float d2 = lensq3(wb - wa);
+            const float pen = cand_pen(c.vs_a, ta, vtype(vb), d2);
+            if (pen > run.v[3]) {
+                enter |= 1u << k;
+                top4_insert(run, pen);
+            }
+        }
+        // replay entering candidates in canonical order
+        uint32_t lanes = __ballot_sync(0xffffffffu, enter != 0u);
+        while (lanes) {
+            const uint32_t L = __ffs(lanes) - 1;
+            lanes &= lanes - 1u;
+            uint32_t em = __shfl_sync(0xffffffffu, enter, L);
+            while (em) {
+                const uint32_t k = __ffs(em) - 1;
+                em &= em - 1u;
+                if (lane == L) {
+                    const I3 o = probe_offset(k);
+                    const I3 ibv{cbv.x + o.x, cbv.y + o.y, cbv.z + o.z};
+                    const uint32_t vb = voxel_at(cs, cb, ibv.x, ibv.y, ibv.z);
+                    const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
+                    generate_contact(c, va, I3{x, y, z}, wa, vb, ibv, wb, &sm.stage);
+                }
+                __syncwarp();
+                if (lane == 0) add_contact(sm, sm.stage);
+                __syncwarp();
+            }
+        }
+        // manifold penetration multiset -> state (at most four finite values,
+        // so every insert lands)
+        if (lane == 0) {
+            Top4 s = top4_empty();
+            for (uint32_t i = 0; i < sm.n; ++i) top4_insert(s, sm.c[i].penetration);
+            sm.pens[0] = s.v[0];
+            sm.pens[1] = s.v[1];
+            sm.pens[2] = s.v[2];
+            sm.pens[3] = s.v[3];
+        }
+        __syncwarp();
+        state.v[0] = sm.pens[0];
+        state.v[1] = sm.pens[1];
+        state.v[2] = sm.pens[2];
+        state.v[3] = sm.pens[3];
+    }
+    checked = warp_sum(checked);
+    ncand = warp_sum(ncand);
+    ManifoldRec& out = w.man[cur][p];
+    if (lane == 0) {
+        pi.voxels_checked = checked;
+        pi.candidates = ncand;
+        out.a = prA.id;
+        out.b = prB.id;
+        out.n = sm.n;
+        out.friction = sqrtf(prA.friction * prB.friction);
+        out.restitution = fmaxf(prA.restitution, prB.restitution);
+        out._pad = 0u;
+    }
+    __syncwarp();
+    // copy the contacts (one lane per 4-byte word)
+    const uint32_t words = sm.n * (uint32_t)(sizeof(ContactRec) / 4);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(sm.c);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(out.c);
+    for (uint32_t i = lane; i < words; i += 32u) dst[i] = src[i];
+    __syncwarp();
+}
+
+template <class G>
+__device__ bool phase_probe(G& g, WorldDev& w, const ColliderSet& cs, uint32_t cur, WarpManifold* warp_sm) {
+    const uint32_t lane = threadIdx.x & 31;
+    WarpManifold& sm = warp_sm[threadIdx.x >> 5];
+    for (;;) {
+        uint32_t p = 0;
+        if (lane == 0) p = atomicAdd(&w.ctr[C_WORK], 1u);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= w.n_pairs) break;
+        const uint32_t fl = w.pinfo[p].flags;
+        if ((fl & PF_DETECT) && (fl & PF_REGION)) probe_pair(w, cs, cur, p, sm);
+    }
+    return g.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Phase: finalize (cache hits, carries, ContactManager.addManifold warm start)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void warm_from_prev(const WorldDev& w, uint32_t prev, ManifoldRec& m) {
+    const uint32_t idx = ht_find(w.ht[prev], w.ht_cap, pair_key(m.a, m.b));
+    if (idx == 0xFFFFFFFFu) return;
+    const ManifoldRec& o = w.man[prev][idx];
+    for (uint32_t i = 0; i < m.n; ++i)
+        for (uint32_t j = 0; j < o.n; ++j)
+            if (m.c[i].feature_id == o.c[j].feature_id) {
+                m.c[i].normal_impulse = o.c[j].normal_impulse;
+                m.c[i].tangent_impulse[0] = o.c[j].tangent_impulse[0];
+                m.c[i].tangent_impulse[1] = o.c[j].tangent_impulse[1];
+                break;
+            }
+}
+
+template <class G>
+__device__ bool phase_finalize(G& g, WorldDev& w, uint32_t cur, uint32_t prev) {
+    uint32_t skipped = 0, colliding = 0, contacts = 0, voxels = 0, manifolds = 0, cands = 0;
+    for (uint32_t p = g.rank(); p < w.n_pairs; p += g.size()) {
+        const PairInfo& pi = w.pinfo[p];
+        const uint32_t fl = pi.flags;
+        ManifoldRec& m = w.man[cur][p];
+        if (fl & PF_CARRY) {
+            ++skipped;
+            const uint2 pr = w.pairs[p];
+            const uint32_t idx = ht_find(w.ht[prev], w.ht_cap, pair_key(pr.x, pr.y));
+            if (idx != 0xFFFFFFFFu) m = w.man[prev][idx];
+            else m.n = 0u;
+        } else if (!(fl & PF_TESTED) || (fl & (PF_NOCOLL | PF_SEPARATED))) {
+            m.n = 0u;
+        } else if (fl & PF_HIT) {
+            const CacheValRec& v = w.cval[pi.cache_slot];
+            if (v.has_collision) {
+                const DBodyProp& a = w.prop[pi.ia];
+                const DBodyProp& b = w.prop[pi.ib];
+                m.a = a.id;
+                m.b = b.id;
+                m.friction = sqrtf(a.friction * b.friction);
+                m.restitution = fmaxf(a.restitution, b.restitution);
+                m._pad = 0u;
+                // ContactManifold.addContact from empty: feature ids are unique
+                m.n = 0u;
+                for (uint32_t i = 0; i < v.n; ++i) {
+                    bool dup = false;
+                    for (uint32_t j = 0; j < m.n; ++j)
+                        if (m.c[j].feature_id == v.c[i].feature_id) {
+                            const float ni = m.c[j].normal_impulse, t0 = m.c[j].tangent_impulse[0],
+                                        t1 = m.c[j].tangent_impulse[1];
+                            m.c[j] = v.c[i];
+                            m.c[j].normal_impulse = ni;
+                            m.c[j].tangent_impulse[0] = t0;
+                            m.c[j].tangent_impulse[1] = t1;
+                            dup = true;
+                            break;
+                        }
+                    if (!dup && m.n < 4u) m.c[m.n++] = v.c[i];
+                }
+                ++colliding;
+                contacts += v.n;
+                voxels += v.voxels_checked;
+                warm_from_prev(w, prev, m);
+            } else {
+                m.n = 0u;
+            }
+        } else if (fl & PF_DETECT) {
+            if (!(fl & PF_REGION)) {
+                const DBodyProp& a = w.prop[pi.ia];
+                const DBodyProp& b = w.prop[pi.ib];
+                m.a = a.id;
+                m.b = b.id;
+                m.n = 0u;
+                m.friction = sqrtf(a.friction * b.friction);
+                m.restitution = fmaxf(a.restitution, b.restitution);
+            }
+            voxels += pi.voxels_checked;
+            cands += pi.candidates;
+            if (m.n > 0u) {
+                ++colliding;
+                contacts += m.n;
+                warm_from_prev(w, prev, m);
+            }
+        } else {
+            m.n = 0u;
+        }
+        if (m.n > 0u) {
+            ++manifolds;
+            ht_insert(w.ht[cur], w.ht_cap, pair_key(m.a, m.b), p);
+        }
+    }
+    skipped = warp_sum(skipped);
+    colliding = warp_sum(colliding);
+    contacts = warp_sum(contacts);
+    voxels = warp_sum(voxels);
+    manifolds = warp_sum(manifolds);
+    cands = warp_sum(cands);
+    if ((threadIdx.x & 31) == 0) {
+        if (skipped) atomicAdd(&w.ctr[C_SKIPPED_SLEEPING], skipped);
+        if (colliding) atomicAdd(&w.ctr[C_PAIRS_COLLIDING], colliding);
+        if (contacts) atomicAdd(&w.ctr[C_CONTACTS], contacts);
+        if (voxels) atomicAdd(&w.ctr[C_VOXELS_CHECKED], voxels);
+        if (manifolds) atomicAdd(&w.ctr[C_MANIFOLDS], manifolds);
+        if (cands) atomicAdd(&w.ctr[C_CANDIDATES], cands);
+    }
+    if (!g.sync()) return false;
+    // BrickPairCache.put values of this frame's misses (last writer wins)
+    if (w.cfg.use_cache) {
+        for (uint32_t p = g.rank(); p < w.n_pairs; p += g.size()) {
+            const PairInfo& pi = w.pinfo[p];
+            if (!(pi.flags & PF_CACHE) || (pi.flags & PF_HIT) || !(pi.flags & PF_DETECT)) continue;
+            if (pi.flags & (PF_NOCOLL | PF_SEPARATED)) continue;
+            const uint32_t s = pi.cache_slot;
+            if (s == 0xFFFFFFFFu || w.cwriter[s] != p) continue;
+            const ManifoldRec& m = w.man[cur][p];
+            CacheValRec& v = w.cval[s];
+            const uint32_t n = m.n < 4u ? m.n : 4u;
+            v.n = n;
+            v.has_collision = n > 0u ? 1u : 0u;
+            v.voxels_checked = pi.voxels_checked;
+            for (uint32_t i = 0; i < n; ++i) {
+                v.c[i] = m.c[i];
+                v.c[i].normal_impulse = 0.f;
+                v.c[i].tangent_impulse[0] = 0.f;
+                v.c[i].tangent_impulse[1] = 0.f;
+                v.c[i].normal_mass = 0.f;
+                v.c[i].tangent_mass[0] = 0.f;
+                v.c[i].tangent_mass[1] = 0.f;
+            }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Phase: constraints (system.solve assembly, colouring, ContactSolver.addManifold)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool writable(const DBodyProp& p) { return p.type == 2u && p.sleeping == 0u; }
+
+// Jones-Plassmann priority; the oracle colours greedily in the same order.
+__device__ __forceinline__ uint32_t jp_priority(uint32_t k) {
+    uint32_t h = k * 0x9E3779B1u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+__device__ __forceinline__ bool jp_before(uint32_t i, uint32_t j) {
+    const uint32_t pi = jp_priority(i), pj = jp_priority(j);
+    return pi != pj ? pi > pj : i < j;
+}
+
+__device__ __forceinline__ size_t cpi(const WorldDev& w, uint32_t field, uint32_t slot, uint32_t pos) {
+    return ((size_t)(field * 4u + slot)) * w.pair_cap + pos;
+}
+
+template <class G>
+__device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_out, uint32_t* ncol_out) {
+    const uint32_t P = w.n_pairs, N = w.n_bodies;
+    // 1. solver constraint list: manifolds that are not both-sleeping, pair order
+    for (uint32_t p = g.rank(); p < P; p += g.size()) {
+        const ManifoldRec& m = w.man[cur][p];
+        uint32_t f = 0;
+        if (m.n > 0u) {
+            const PairInfo& pi = w.pinfo[p];
+            const bool as = pi.ia != 0xFFFFFFFFu ? w.prop[pi.ia].sleeping != 0u : true;
+            const bool bs = pi.ib != 0xFFFFFFFFu ? w.prop[pi.ib].sleeping != 0u : true;
+            f = (as && bs) ? 0u : 1u;
+        }
+        w.flag[p] = f;
+    }
+    for (uint32_t i = g.rank(); i <= N; i += g.size()) {
+        w.adj_off[i] = 0u;
+        if (i < N) w.adj_cur[i] = 0u;
+    }
+    for (uint32_t i = g.rank(); i < 257u; i += g.size()) {
+        w.colour_cnt[i] = 0u;
+        if (i < 256u) w.colour_cur[i] = 0u;
+    }
+    // colouring round counters (3) and position-sweep min separations (16)
+    // live after the per-block scan partials
+    if (g.rank() < 20u) w.scan[g.nblocks() + g.rank()] = 0u;
+    if (!g.sync()) return false;
+    uint32_t M = 0;
+    if (!group_scan(
+            g, P, [&](uint32_t i) { return w.flag[i]; },
+            [&](uint32_t i, uint32_t pre) {
+                if (w.flag[i]) w.cons[pre] = i;
+            },
+            w.scan, &M))
+        return false;
+    *M_out = M;
+    uint32_t pts = 0;
+    for (uint32_t k = g.rank(); k < M; k += g.size()) pts += w.man[cur][w.cons[k]].n;
+    pts = warp_sum(pts);
+    if ((threadIdx.x & 31) == 0 && pts) atomicAdd(&w.ctr[C_POINTS], pts);
+    if (g.rank() == 0) w.ctr[C_CONSTRAINTS] = M;
+
+    // 2. colouring
+    if (w.cfg.colouring == 1u) {
+        // GraphColoring.build (islands.zig:668-736) over every manifold in
+        // pair order, all bodies as nodes; one thread.
+        for (uint32_t i = g.rank(); i < N * 8u; i += g.size()) w.bmask[i] = 0u;
+        if (!g.sync()) return false;
+        if (g.rank() == 0) {
+            for (uint32_t p = 0; p < P; ++p) {
+                const ManifoldRec& m = w.man[cur][p];
+                if (m.n == 0u) continue;
+                const PairInfo& pi = w.pinfo[p];
+                uint32_t* ma = &w.bmask[pi.ia * 8u];
+                uint32_t* mb = &w.bmask[pi.ib * 8u];
+                uint32_t c = 0;
+                while (c < 255u && (((ma[c >> 5] | mb[c >> 5]) >> (c & 31)) & 1u)) ++c;
+                if (c == 255u) atomicOr(&w.ctr[C_ERROR], ERR_COLOURS);
+                ma[c >> 5] |= 1u << (c & 31);
+                mb[c >> 5] |= 1u << (c & 31);
+                w.flag[p] = c;
+            }
+        }
+        if (!g.sync()) return false;
+        for (uint32_t k = g.rank(); k < M; k += g.size()) w.colour[k] = w.flag[w.cons[k]];
+        if (!g.sync()) return false;
+    } else {
+        // Jones-Plassmann over writable bodies == greedy in priority order.
+        for (uint32_t k = g.rank(); k < M; k += g.size()) {
+            const PairInfo& pi = w.pinfo[w.cons[k]];
+            if (writable(w.prop[pi.ia])) atomicAdd(&w.adj_off[pi.ia], 1u);
+            if (writable(w.prop[pi.ib])) atomicAdd(&w.adj_off[pi.ib], 1u);
+            w.colour[k] = 0xFFFFFFFFu;
+        }
+        if (!g.sync()) return false;
+        uint32_t tot;
+        // in-place exclusive scan: read counts into adj_cur, write offsets
+        for (uint32_t i = g.rank(); i < N; i += g.size()) w.adj_cur[i] = w.adj_off[i];
+        if (!g.sync()) return false;
+        if (!group_scan(
+                g, N, [&](uint32_t i) { return w.adj_cur[i]; }, [&](uint32_t i, uint32_t pre) { w.adj_off[i] = pre; },
+                w.scan, &tot))
+            return false;
+        if (g.rank() == 0) w.adj_off[N] = tot;
+        for (uint32_t i = g.rank(); i < N; i += g.size()) w.adj_cur[i] = 0u;
+        if (!g.sync()) return false;
+        for (uint32_t k = g.rank(); k < M; k += g.size()) {
+            const PairInfo& pi = w.pinfo[w.cons[k]];
+            if (writable(w.prop[pi.ia])) w.adj[w.adj_off[pi.ia] + atomicAdd(&w.adj_cur[pi.ia], 1u)] = k;
+            if (writable(w.prop[pi.ib])) w.adj[w.adj_off[pi.ib] + atomicAdd(&w.adj_cur[pi.ib], 1u)] = k;
+        }
+        if (!g.sync()) return false;
+        // rounds; three rotating counters at scan[nblocks .. nblocks+3)
+        uint32_t* rem = w.scan + g.nblocks();
+        for (uint32_t round = 0;; ++round) {
+            if (round > M + 1u) {
+                if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_COLOURS);
+                break;
+            }
+            if (g.rank() == 0) rem[(round + 1u) % 3u] = 0u;
+            uint32_t left = 0;
+            for (uint32_t k = g.rank(); k < M; k += g.size()) {
+                volatile uint32_t* vc = w.colour;
+                if (vc[k] != 0xFFFFFFFFu) continue;
+                const PairInfo& pi = w.pinfo[w.cons[k]];
+                uint32_t used[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                bool ready = true;
+                const uint32_t bodies[2] = {pi.ia, pi.ib};
+                for (int s = 0; s < 2 && ready; ++s) {
+                    const uint32_t b = bodies[s];
+                    if (!writable(w.prop[b])) continue;
+                    for (uint32_t e = w.adj_off[b]; e < w.adj_off[b + 1u]; ++e) {
+                        const uint32_t j = w.adj[e];
+                        if (j == k) continue;
+                        const uint32_t cj = vc[j];
+                        if (cj == 0xFFFFFFFFu) {
+                            if (jp_before(j, k)) {
+                                ready = false;
+                                break;
+                            }
+                        } else if (cj < 256u) {
+                            used[cj >> 5] |= 1u << (cj & 31);
+                        }
+                    }
+                }
+                if (!ready) {
+                    ++left;
+                    continue;
+                }
+                uint32_t c = 256u;
+                for (uint32_t wd = 0; wd < 8u; ++wd)
+                    if (used[wd] != 0xFFFFFFFFu) {
+                        c = wd * 32u + (uint32_t)(__ffs(~used[wd]) - 1);
+                        break;
+                    }
+                if (c >= 256u) {
+                    atomicOr(&w.ctr[C_ERROR], ERR_COLOURS);
+                    c = 255u;
+                }
+                vc[k] = c;
+            }
+            left = warp_sum(left);
+            if ((threadIdx.x & 31) == 0 && left) atomicAdd(&rem[round % 3u], left);
+            if (!g.sync()) return false;
+            const uint32_t r = *(volatile uint32_t*)&rem[round % 3u];
+            if (r == 0u) break;
+        }
+    }
+    // 3. colour-major packing + ContactSolver.addManifold (solver.zig:449-491)
+    for (uint32_t k = g.rank(); k < M; k += g.size()) {
+        if (w.colour[k] > 255u) w.colour[k] = 255u;  // only after ERR_COLOURS
+        atomicAdd(&w.colour_cnt[w.colour[k]], 1u);
+    }
+    if (!g.sync()) return false;
+    if (g.rank() < 32u) {
+        const uint32_t lane = threadIdx.x & 31;
+        uint32_t carry = 0, last = 0;
+        for (uint32_t c0 = 0; c0 < 256u; c0 += 32u) {
+            const uint32_t v = w.colour_cnt[c0 + lane];
+            const uint32_t inc = warp_incl_scan(v);
+            const uint32_t nz = __ballot_sync(0xffffffffu, v != 0u);
+            if (nz) last = c0 + 32u - __clz(nz);
+            __syncwarp();
+            w.colour_cnt[c0 + lane] = carry + inc - v;
+            carry += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        if (lane == 0) {
+            w.colour_cnt[256] = carry;
+            w.ctr[C_COLOURS] = last;
+        }
+    }
+    if (!g.sync()) return false;
+    *ncol_out = *(volatile uint32_t*)&w.ctr[C_COLOURS];
+    for (uint32_t k = g.rank(); k < M; k += g.size()) {
+        const uint32_t c = w.colour[k];
+        const uint32_t pos = w.colour_cnt[c] + atomicAdd(&w.colour_cur[c], 1u);
+        const uint32_t p = w.cons[k];
+        w.pos_of[k] = pos;
+        w.packed_pair[pos] = p;
+        const PairInfo& pi = w.pinfo[p];
+        const ManifoldRec& m = w.man[cur][p];
+        w.cm[pos] = make_uint4(pi.ia, pi.ib, m.n, p);
+        w.cfr[pos] = make_float2(m.friction, m.restitution);
+        const DBody& A = w.body[pi.ia];
+        const DBody& B = w.body[pi.ib];
+        const F3 pa = f3of(A.p), pb = f3of(B.p);
+        const Qt qa = qof(A.q), qb = qof(B.q);
+        for (uint32_t i = 0; i < m.n; ++i) {
+            const ContactRec& ct = m.c[i];
+            const F3 la{ct.la[0], ct.la[1], ct.la[2]}, lb{ct.lb[0], ct.lb[1], ct.lb[2]};
+            const F3 nn{ct.normal[0], ct.normal[1], ct.normal[2]};
+            const F3 wa = qrotate(qa, la) + pa;
+            const F3 wb = qrotate(qb, lb) + pb;
+            const F3 ad = wb - wa;
+            const float base = -ct.penetration - dot3(ad, nn);
+            const F3 ra = wa - pa, rb = wb - pb;
+            float* cp = w.cp;
+            cp[cpi(w, CP_NX, i, pos)] = nn.x; cp[cpi(w, CP_NY, i, pos)] = nn.y; cp[cpi(w, CP_NZ, i, pos)] = nn.z;
+            cp[cpi(w, CP_LAX, i, pos)] = la.x; cp[cpi(w, CP_LAY, i, pos)] = la.y; cp[cpi(w, CP_LAZ, i, pos)] = la.z;
+            cp[cpi(w, CP_LBX, i, pos)] = lb.x; cp[cpi(w, CP_LBY, i, pos)] = lb.y; cp[cpi(w, CP_LBZ, i, pos)] = lb.z;
+            cp[cpi(w, CP_PX, i, pos)] = ct.point[0]; cp[cpi(w, CP_PY, i, pos)] = ct.point[1];
+            cp[cpi(w, CP_PZ, i, pos)] = ct.point[2];
+            cp[cpi(w, CP_RAX, i, pos)] = ra.x; cp[cpi(w, CP_RAY, i, pos)] = ra.y; cp[cpi(w, CP_RAZ, i, pos)] = ra.z;
+            cp[cpi(w, CP_RBX, i, pos)] = rb.x; cp[cpi(w, CP_RBY, i, pos)] = rb.y; cp[cpi(w, CP_RBZ, i, pos)] = rb.z;
+            cp[cpi(w, CP_BASE, i, pos)] = base;
+            cp[cpi(w, CP_NM, i, pos)] = 0.f; cp[cpi(w, CP_TM0, i, pos)] = 0.f; cp[cpi(w, CP_TM1, i, pos)] = 0.f;
+            cp[cpi(w, CP_T1X, i, pos)] = 0.f; cp[cpi(w, CP_T1Y, i, pos)] = 0.f; cp[cpi(w, CP_T1Z, i, pos)] = 0.f;
+            cp[cpi(w, CP_T2X, i, pos)] = 0.f; cp[cpi(w, CP_T2Y, i, pos)] = 0.f; cp[cpi(w, CP_T2Z, i, pos)] = 0.f;
+            cp[cpi(w, CP_BIAS, i, pos)] = 0.f;
+            cp[cpi(w, CP_NI, i, pos)] = ct.normal_impulse;
+            cp[cpi(w, CP_TI0, i, pos)] = ct.tangent_impulse[0];
+            cp[cpi(w, CP_TI1, i, pos)] = ct.tangent_impulse[1];
+        }
+    }
+    return g.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Solver building blocks (solver.zig:564-1005)
+// ---------------------------------------------------------------------------
+struct Soft {
+    float bias_rate, mass_coeff, impulse_coeff;
+};
+__device__ __forceinline__ Soft soft_params(float hz, float zeta, float h) {  // solver.zig:57-72
+    if (hz <= 0.0f) return Soft{0.f, 1.f, 1.f};
+    const float pi = 3.14159274101257324f;
+    const float omega = 2.0f * pi * hz;
+    const float a1 = 2.0f * zeta + omega * h;
+    const float a2 = h * omega * a1;
+    const float a3 = 1.0f / (1.0f + a2);
+    return Soft{omega / a1, a2 * a3, a3};
+}
+__device__ __forceinline__ F3 compute_orthogonal(F3 v) {  // solver.zig:967-981
+    if (fabsf(v.x) < fabsf(v.y)) {
+        if (fabsf(v.x) < fabsf(v.z)) return normalize_or_zero3(F3{0.f, -v.z, v.y});
+        return normalize_or_zero3(F3{-v.y, v.x, 0.f});
+    }
+    if (fabsf(v.y) < fabsf(v.z)) return normalize_or_zero3(F3{-v.z, 0.f, v.x});
+    return normalize_or_zero3(F3{-v.y, v.x, 0.f});
+}
+__device__ __forceinline__ Qt integrate_rotation_small(Qt r, F3 d) {  // solver.zig:984-1005
+    const Qt h{d.x * 0.5f, d.y * 0.5f, d.z * 0.5f, 0.f};
+    const Qt dq{h.w * r.x + h.x * r.w + h.y * r.z - h.z * r.y, h.w * r.y - h.x * r.z + h.y * r.w + h.z * r.x,
+                h.w * r.z + h.x * r.y - h.y * r.x + h.z * r.w, h.w * r.w - h.x * r.x - h.y * r.y - h.z * r.z};
+    return qnormalize(Qt{r.x + dq.x, r.y + dq.y, r.z + dq.z, r.w + dq.w});
+}
+
+// Local copy of one body's velocity state for a manifold sweep.
+struct BV {
+    F3 p, v, w;
+    float im;
+    M33 I;
+    bool wr;
+};
+__device__ __forceinline__ BV load_bv(const WorldDev& w, uint32_t i) {
+    const DBody& b = w.body[i];
+    BV r;
+    const float4 p = b.p, v = b.v, ww = b.w, i0 = b.i0, i1 = b.i1, i2 = b.i2;
+    r.p = f3of(p);
+    r.im = p.w;
+    r.v = f3of(v);
+    r.w = f3of(ww);
+    r.I.m[0] = i0.x; r.I.m[1] = i0.y; r.I.m[2] = i0.z;
+    r.I.m[3] = i1.x; r.I.m[4] = i1.y; r.I.m[5] = i1.z;
+    r.I.m[6] = i2.x; r.I.m[7] = i2.y; r.I.m[8] = i2.z;
+    r.wr = writable(w.prop[i]);
+    return r;
+}
+__device__ __forceinline__ F3 point_vel(const BV& b, F3 wp) { return b.v + cross3(b.w, wp - b.p); }
+__device__ __forceinline__ void apply_impulse(BV& b, F3 imp, F3 r) {  // BodyState.applyImpulseAtPoint
+    if (!b.wr) return;
+    b.v = b.v + imp * b.im;
+    b.w = b.w + mat3_mul_vec(b.I, cross3(r, imp));
+}
+__device__ __forceinline__ void store_bv(WorldDev& w, uint32_t i, const BV& b) {
+    if (!b.wr) return;
+    w.body[i].v = make_float4(b.v.x, b.v.y, b.v.z, 0.f);
+    w.body[i].w = make_float4(b.w.x, b.w.y, b.w.z, 0.f);
+}
+__device__ __forceinline__ F3 ld3(const WorldDev& w, uint32_t f, uint32_t s, uint32_t pos) {
+    return F3{w.cp[cpi(w, f, s, pos)], w.cp[cpi(w, f + 1, s, pos)], w.cp[cpi(w, f + 2, s, pos)]};
+}
+__device__ __forceinline__ void st3(WorldDev& w, uint32_t f, uint32_t s, uint32_t pos, F3 v) {
+    w.cp[cpi(w, f, s, pos)] = v.x;
+    w.cp[cpi(w, f + 1, s, pos)] = v.y;
+    w.cp[cpi(w, f + 2, s, pos)] = v.z;
+}
+
+// prepareConstraints for one point (solver.zig:608-699).
+__device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft& soft, float hinv) {
+    const uint4 cmv = w.cm[pos];
+    const BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
+    const Qt qa = qof(w.body[cmv.x].q), qb = qof(w.body[cmv.y].q);
+    const F3 n = ld3(w, CP_NX, i, pos);
+    const F3 wa = qrotate(qa, ld3(w, CP_LAX, i, pos)) + a.p;
+    const F3 wb = qrotate(qb, ld3(w, CP_LBX, i, pos)) + b.p;
+    const F3 ra = wa - a.p, rb = wb - b.p;
+    const F3 pt = (wa + wb) * 0.5f;
+    const F3 ad = wb - wa;
+    const float sep = w.cp[cpi(w, CP_BASE, i, pos)] + dot3(ad, n);
+    const F3 rna = cross3(ra, n), rnb = cross3(rb, n);
+    float k = a.im + b.im;
+    k += dot3(rna, mat3_mul_vec(a.I, rna));
+    k += dot3(rnb, mat3_mul_vec(b.I, rnb));
+    const float nm = k > kEpsilon ? 1.0f / k : 0.0f;
+    const F3 rv = point_vel(b, pt) - point_vel(a, pt);
+    const float vn = dot3(rv, n);
+    float bias;
+    if (sep > 0.0f) bias = sep * hinv;
+    else bias = fmaxf(soft.bias_rate * sep, -0.2f);
+    if (w.cfg.restitution_on && vn < -1.0f) bias = fmaxf(bias, -w.cfr[pos].y * vn);
+    st3(w, CP_RAX, i, pos, ra);
+    st3(w, CP_RBX, i, pos, rb);
+    st3(w, CP_PX, i, pos, pt);
+    w.cp[cpi(w, CP_NM, i, pos)] = nm;
+    w.cp[cpi(w, CP_BIAS, i, pos)] = bias;
+    if (w.cfg.friction_on) {
+        const F3 t1 = compute_orthogonal(n);
+        const F3 t2 = cross3(n, t1);
+        const F3 r1a = cross3(ra, t1), r1b = cross3(rb, t1);
+        float k1 = a.im + b.im;
+        k1 += dot3(r1a, mat3_mul_vec(a.I, r1a));
+        k1 += dot3(r1b, mat3_mul_vec(b.I, r1b));
+        const F3 r2a = cross3(ra, t2), r2b = cross3(rb, t2);
+        float k2 = a.im + b.im;
+        k2 += dot3(r2a, mat3_mul_vec(a.I, r2a));
+        k2 += dot3(r2b, mat3_mul_vec(b.I, r2b));
+        st3(w, CP_T1X, i, pos, t1);
+        st3(w, CP_T2X, i, pos, t2);
+        w.cp[cpi(w, CP_TM0, i, pos)] = k1 > kEpsilon ? 1.0f / k1 : 0.0f;
+        w.cp[cpi(w, CP_TM1, i, pos)] = k2 > kEpsilon ? 1.0f / k2 : 0.0f;
+    }
+}
+
+// warmStart for one manifold (solver.zig:702-729).
+__device__ void warm_manifold(WorldDev& w, uint32_t pos, float scale) {
+    const uint4 cmv = w.cm[pos];
+    BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
+    for (uint32_t i = 0; i < cmv.z; ++i) {
+        const float sn = w.cp[cpi(w, CP_NI, i, pos)] * scale;
+        const float s1 = w.cp[cpi(w, CP_TI0, i, pos)] * scale;
+        const float s2 = w.cp[cpi(w, CP_TI1, i, pos)] * scale;
+        const F3 imp = (ld3(w, CP_NX, i, pos) * sn + ld3(w, CP_T1X, i, pos) * s1) + ld3(w, CP_T2X, i, pos) * s2;
+        apply_impulse(a, -imp, ld3(w, CP_RAX, i, pos));
+        apply_impulse(b, imp, ld3(w, CP_RBX, i, pos));
+        w.cp[cpi(w, CP_NI, i, pos)] = sn;
+        w.cp[cpi(w, CP_TI0, i, pos)] = s1;
+        w.cp[cpi(w, CP_TI1, i, pos)] = s2;
+    }
+    store_bv(w, cmv.x, a);
+    store_bv(w, cmv.y, b);
+}
+
+// solveVelocityConstraints + solveFriction for one manifold (solver.zig:732-838).
+__device__ void velocity_manifold(WorldDev& w, uint32_t pos, const Soft& soft, bool use_bias) {
+    const uint4 cmv = w.cm[pos];
+    const float fr = w.cfr[pos].x;
+    BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
+    for (uint32_t i = 0; i < cmv.z; ++i) {
+        const F3 pt = ld3(w, CP_PX, i, pos);
+        const F3 n = ld3(w, CP_NX, i, pos);
+        const F3 ra = ld3(w, CP_RAX, i, pos), rb = ld3(w, CP_RBX, i, pos);
+        const float nm = w.cp[cpi(w, CP_NM, i, pos)];
+        float ni = w.cp[cpi(w, CP_NI, i, pos)];
+        const F3 rv = point_vel(b, pt) - point_vel(a, pt);
+        const float vn = dot3(rv, n);
+        float imp;
+        if (use_bias)
+            imp = -soft.mass_coeff * nm * (vn + w.cp[cpi(w, CP_BIAS, i, pos)]) - soft.impulse_coeff * ni;
+        else
+            imp = -nm * vn;
+        const float nn = fmaxf(ni + imp, 0.0f);
+        imp = nn - ni;
+        ni = nn;
+        w.cp[cpi(w, CP_NI, i, pos)] = ni;
+        const F3 P = n * imp;
+        apply_impulse(a, -P, ra);
+        apply_impulse(b, P, rb);
+        if (w.cfg.friction_on && fr > 0.0f) {
+            const F3 t1 = ld3(w, CP_T1X, i, pos), t2 = ld3(w, CP_T2X, i, pos);
+            const float mf = fr * ni;
+            {
+                const F3 rv1 = point_vel(b, pt) - point_vel(a, pt);
+                const float vt1 = dot3(rv1, t1);
+                float f1 = -w.cp[cpi(w, CP_TM0, i, pos)] * vt1;
+                const float o1 = w.cp[cpi(w, CP_TI0, i, pos)];
+                const float t = clampf_ref(o1 + f1, -mf, mf);
+                w.cp[cpi(w, CP_TI0, i, pos)] = t;
+                f1 = t - o1;
+                const F3 I1 = t1 * f1;
+                apply_impulse(a, -I1, ra);
+                apply_impulse(b, I1, rb);
+            }
+            {
+                const F3 rv2 = point_vel(b, pt) - point_vel(a, pt);
+                const float vt2 = dot3(rv2, t2);
+                float f2 = -w.cp[cpi(w, CP_TM1, i, pos)] * vt2;
+                const float o2 = w.cp[cpi(w, CP_TI1, i, pos)];
+                const float t = clampf_ref(o2 + f2, -mf, mf);
+                w.cp[cpi(w, CP_TI1, i, pos)] = t;
+                f2 = t - o2;
+                const F3 I2 = t2 * f2;
+                apply_impulse(a, -I2, ra);
+                apply_impulse(b, I2, rb);
+            }
+        }
+    }
+    store_bv(w, cmv.x, a);
+    store_bv(w, cmv.y, b);
+}
+
+// solvePositionConstraints for one manifold (solver.zig:860-923).
+__device__ void position_manifold(WorldDev& w, uint32_t pos, float* min_sep, float* max_pen) {
+    const uint4 cmv = w.cm[pos];
+    const DBodyProp& pa = w.prop[cmv.x];
+    const DBodyProp& pb = w.prop[cmv.y];
+    if (pa.type == 0u && pb.type == 0u) return;
+    DBody& A = w.body[cmv.x];
+    DBody& B = w.body[cmv.y];
+    F3 xa = f3of(A.p), xb = f3of(B.p);
+    Qt qa = qof(A.q), qb = qof(B.q);
+    const float ima = A.p.w, imb = B.p.w;
+    M33 Ia, Ib;
+    Ia.m[0] = A.i0.x; Ia.m[1] = A.i0.y; Ia.m[2] = A.i0.z; Ia.m[3] = A.i1.x; Ia.m[4] = A.i1.y;
+    Ia.m[5] = A.i1.z; Ia.m[6] = A.i2.x; Ia.m[7] = A.i2.y; Ia.m[8] = A.i2.z;
+    Ib.m[0] = B.i0.x; Ib.m[1] = B.i0.y; Ib.m[2] = B.i0.z; Ib.m[3] = B.i1.x; Ib.m[4] = B.i1.y;
+    Ib.m[5] = B.i1.z; Ib.m[6] = B.i2.x; Ib.m[7] = B.i2.y; Ib.m[8] = B.i2.z;
+    const bool wa_ = writable(pa), wb_ = writable(pb);
+    const float slop = w.cfg.slop;
+    for (uint32_t i = 0; i < cmv.z; ++i) {
+        const F3 n = ld3(w, CP_NX, i, pos);
+        const F3 wa = qrotate(qa, ld3(w, CP_LAX, i, pos)) + xa;
+        const F3 wb = qrotate(qb, ld3(w, CP_LBX, i, pos)) + xb;
+        const F3 ad = wb - wa;
+        const float sep = w.cp[cpi(w, CP_BASE, i, pos)] + dot3(ad, n);
+        *min_sep = fminf(*min_sep, sep);
+        *max_pen = fmaxf(*max_pen, -sep);
+        if (sep >= -slop) continue;
+        const float corr = fmaxf(w.cfg.pos_rate * (sep + slop), -w.cfg.max_pos_corr);
+        const F3 ra = wa - xa, rb = wb - xb;
+        const F3 rna = cross3(ra, n), rnb = cross3(rb, n);
+        float k = ima + imb;
+        k += dot3(rna, mat3_mul_vec(Ia, rna));
+        k += dot3(rnb, mat3_mul_vec(Ib, rnb));
+        if (k < kEpsilon) continue;
+        const F3 pimp = n * (-corr / k);
+        if (wa_) {
+            xa = xa - pimp * ima;
+            qa = integrate_rotation_small(qa, mat3_mul_vec(Ia, cross3(ra, -pimp)));
+        }
+        if (wb_) {
+            xb = xb + pimp * imb;
+            qb = integrate_rotation_small(qb, mat3_mul_vec(Ib, cross3(rb, pimp)));
+        }
+    }
+    if (wa_) {
+        A.p = make_float4(xa.x, xa.y, xa.z, ima);
+        A.q = f4of(qa);
+    }
+    if (wb_) {
+        B.p = make_float4(xb.x, xb.y, xb.z, imb);
+        B.q = f4of(qb);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase: solve (ContactSolver.solve, solver.zig:494-561)
+// ---------------------------------------------------------------------------
+template <class G>
+__device__ bool phase_solve(G& g, WorldDev& w, uint32_t M, uint32_t ncol) {
+    const StepCfg& cf = w.cfg;
+    const float dt = cf.dt;
+    const bool has = M > 0u;
+    const float h = dt / (float)cf.substeps;
+    const Soft soft = soft_params(cf.hertz, cf.damping_ratio, h);
+    const float hinv = h > kEpsilon ? 1.0f / h : 0.0f;
+    const Soft hard{0.f, 1.f, 1.f};
+    const F3 grav{cf.gravity[0], cf.gravity[1], cf.gravity[2]};
+    const uint32_t N = w.n_bodies;
+    for (uint32_t s = 0; s < cf.substeps; ++s) {
+        // applyGravity (solver.zig:564-605)
+        for (uint32_t i = g.rank(); i < N; i += g.size()) {
+            const DBodyProp& pr = w.prop[i];
+            if (!(pr.type == 2u && pr.sleeping == 0u)) continue;
+            DBody& b = w.body[i];
+            F3 v = f3of(b.v), av = f3of(b.w);
+            v = v + grav * h;
+            float ld = pr.lin_damp, adp = pr.ang_damp;
+            const float ls = len3(v), as = len3(av);
+            if (ls < 0.5f) ld += 5.0f * (1.0f - (ls / 0.5f));
+            if (as < 0.5f) adp += 5.0f * (1.0f - (as / 0.5f));
+            const float ldec = fmaxf(0.0f, 1.0f - ld * h), adec = fmaxf(0.0f, 1.0f - adp * h);
+            v = v * ldec;
+            av = av * adec;
+            if (lensq3(v) < 0.001f * 0.001f) v = F3{0.f, 0.f, 0.f};
+            if (lensq3(av) < 0.001f * 0.001f) av = F3{0.f, 0.f, 0.f};
+            b.v = make_float4(v.x, v.y, v.z, 0.f);
+            b.w = make_float4(av.x, av.y, av.z, 0.f);
+        }
+        if (!g.sync()) return false;
+        if (has) {
+            for (uint32_t it = g.rank(); it < 4u * M; it += g.size()) {
+                const uint32_t slot = it / M, pos = it - slot * M;
+                if (slot < w.cm[pos].z) prepare_point(w, pos, slot, soft, hinv);
+            }
+            if (!g.sync()) return false;
+            if (cf.warm_starting && s == 0u) {
+                for (uint32_t c = 0; c < ncol; ++c) {
+                    const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
+                    for (uint32_t pos = lo + g.rank(); pos < hi; pos += g.size()) warm_manifold(w, pos, cf.warm_scale);
+                    if (!g.sync()) return false;
+                }
+            }
+            for (uint32_t vi = 0; vi < cf.vel_iters; ++vi) {
+                for (uint32_t c = 0; c < ncol; ++c) {
+                    const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
+                    for (uint32_t pos = lo + g.rank(); pos < hi; pos += g.size()) velocity_manifold(w, pos, soft, true);
+                    if (!g.sync()) return false;
+                }
+            }
+        }
+        // integratePositions (solver.zig:841-845, 341-356)
+        for (uint32_t i = g.rank(); i < N; i += g.size()) {
+            const DBodyProp& pr = w.prop[i];
+            if (pr.type == 0u || pr.sleeping) continue;
+            DBody& b = w.body[i];
+            const F3 x = f3of(b.p) + f3of(b.v) * h;
+            Qt q = qof(b.q);
+            if (!cf.disable_rotation) q = integrate_rotation(q, f3of(b.w), h);
+            b.p = make_float4(x.x, x.y, x.z, b.p.w);
+            b.q = f4of(q);
+            if (pr.type == 2u) {
+                M33 il;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) il.m[k] = pr.il[k];
+                const M33 m = world_inv_inertia(q, il);
+                b.i0 = make_float4(m.m[0], m.m[1], m.m[2], 0.f);
+                b.i1 = make_float4(m.m[3], m.m[4], m.m[5], 0.f);
+                b.i2 = make_float4(m.m[6], m.m[7], m.m[8], 0.f);
+            }
+        }
+        if (!g.sync()) return false;
+        if (has) {
+            for (uint32_t c = 0; c < ncol; ++c) {
+                const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
+                for (uint32_t pos = lo + g.rank(); pos < hi; pos += g.size()) velocity_manifold(w, pos, hard, false);
+                if (!g.sync()) return false;
+            }
+        }
+    }
+    if (has) {
+        for (uint32_t it = 0; it < cf.pos_iters; ++it) {
+            float mn = 0.0f, mx = -__int_as_float(0x7f800000);
+            for (uint32_t c = 0; c < ncol; ++c) {
+                const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
+                for (uint32_t pos = lo + g.rank(); pos < hi; pos += g.size()) position_manifold(w, pos, &mn, &mx);
+                if (!g.sync()) return false;
+            }
+            // reduce min separation / max penetration of this sweep
+            int32_t kmn = fkey(mn), kmx = fkey(mx);
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                kmn = min(kmn, __shfl_xor_sync(0xffffffffu, kmn, d));
+                kmx = max(kmx, __shfl_xor_sync(0xffffffffu, kmx, d));
+            }
+            int32_t* minsep = reinterpret_cast<int32_t*>(w.scan + g.nblocks() + 4u);  // 16 slots
+            if ((threadIdx.x & 31) == 0) {
+                atomicMin(&minsep[it & 15u], kmn);
+                atomicMax(reinterpret_cast<int32_t*>(&w.ctr[C_MAX_PEN_KEY]), kmx);
+            }
+            if (g.rank() == 0) w.ctr[C_POS_ITERS] += 1u;
+            if (!g.sync()) return false;
+            const float ms = fkey_inv(*(volatile int32_t*)&minsep[it & 15u]);
+            if (ms >= -3.0f * cf.slop) break;
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Phase: store (writeBack, storeImpulses, updateSleepStates)
+// ---------------------------------------------------------------------------
+template <class G>
+__device__ bool phase_store(G& g, WorldDev& w, uint32_t cur, uint32_t M, bool solved) {
+    const StepCfg& cf = w.cfg;
+    for (uint32_t i = g.rank(); i < w.n_bodies; i += g.size()) {
+        DBodyProp& pr = w.prop[i];
+        if (pr.type == 0u) continue;
+        DBody& b = w.body[i];
+        F3 x = f3of(b.p), v = f3of(b.v), av = f3of(b.w);
+        Qt q = qof(b.q);
+        // BodyState.writeBack (solver.zig:246-296); skipped with the rest of
+        // ContactSolver.solve when dt <= 0 (solver.zig:495)
+        const bool qf = isfinite(q.x) && isfinite(q.y) && isfinite(q.z) && isfinite(q.w);
+        if (solved && (!finite3(x) || !qf)) {
+            const F3 x0 = f3of(w.p0[i]);
+            x = finite3(x0) ? x0 : F3{0.f, 2.f, 0.f};
+            q = Qt{0.f, 0.f, 0.f, 1.f};
+            v = F3{0.f, 0.f, 0.f};
+            av = F3{0.f, 0.f, 0.f};
+        }
+        if (solved) {
+            if (!finite3(v)) v = F3{0.f, 0.f, 0.f};
+            if (!finite3(av)) av = F3{0.f, 0.f, 0.f};
+            const float ls2 = lensq3(v), as2 = lensq3(av);
+            if (ls2 > 50.0f * 50.0f) v = v * (50.0f / sqrtf(ls2));
+            if (as2 > 30.0f * 30.0f) av = av * (30.0f / sqrtf(as2));
+            if (ls2 < 0.002f) v = F3{0.f, 0.f, 0.f};
+            if (as2 < 0.002f) av = F3{0.f, 0.f, 0.f};
+            q = qnormalize(q);
+        }
+        // VoxelBody.updateSleepState (body.zig:415-427) for awake dynamic bodies
+        if (cf.sleeping_on && pr.type == 2u && !pr.sleeping) {
+            if (len3(v) < 0.1f && len3(av) < 0.1f) {
+                pr.sleep_timer += cf.dt;
+                if (pr.sleep_timer >= 0.5f) {
+                    pr.sleeping = 1u;
+                    v = F3{0.f, 0.f, 0.f};
+                    av = F3{0.f, 0.f, 0.f};
+                }
+            } else {
+                pr.sleep_timer = 0.0f;
+            }
+        }
+        b.p = make_float4(x.x, x.y, x.z, b.p.w);
+        b.q = f4of(q);
+        b.v = make_float4(v.x, v.y, v.z, 0.f);
+        b.w = make_float4(av.x, av.y, av.z, 0.f);
+    }
+    // storeImpulses (solver.zig:933-958)
+    if (solved && cf.warm_store_on) {
+        for (uint32_t pos = g.rank(); pos < M; pos += g.size()) {
+            const uint4 cmv = w.cm[pos];
+            ManifoldRec& m = w.man[cur][cmv.w];
+            const uint32_t n = cmv.z < m.n ? cmv.z : m.n;
+            for (uint32_t i = 0; i < n; ++i) {
+                m.c[i].normal_impulse = w.cp[cpi(w, CP_NI, i, pos)];
+                m.c[i].tangent_impulse[0] = w.cp[cpi(w, CP_TI0, i, pos)];
+                m.c[i].tangent_impulse[1] = w.cp[cpi(w, CP_TI1, i, pos)];
+                m.c[i].normal_mass = w.cp[cpi(w, CP_NM, i, pos)];
+                m.c[i].tangent_mass[0] = w.cp[cpi(w, CP_TM0, i, pos)];
+                m.c[i].tangent_mass[1] = w.cp[cpi(w, CP_TM1, i, pos)];
+            }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// One whole step (VoxelPhysicsSystem.step with the pairs given)
+// ---------------------------------------------------------------------------
+template <class G>
+__device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifold* warp_sm) {
+    const uint32_t ph = w.cfg.phases;
+    const uint32_t f0 = *(volatile uint32_t*)&w.frame[0];
+    w.n_pairs = *w.n_pairs_dev;
+    if ((ph & PH_NARROW) && w.n_pairs > w.pair_cap) {
+        // the pair list did not fit: leave every state untouched, the host
+        // grows the buffers and runs the step again
+        if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_CAP);
+        return;
+    }
+    bool skipped = false;
+    if (!phase_begin(g, w, (ph & PH_SKIP_TEST) != 0u, &skipped)) return;
+    if (skipped) return;
+    // ContactManager.beginFrame (narrow_phase.zig:1003-1008): the previous
+    // "current" manifolds become "previous"
+    const uint32_t cur = (ph & PH_NARROW) ? ((f0 + 1u) & 1u) : (f0 & 1u), prev = cur ^ 1u;
+    if (ph & PH_NARROW) {
+        if (g.rank() == 0) {
+            w.frame[0] = f0 + 1u;
+            w.frame[1] = w.n_pairs;
+        }
+        if (!phase_pairs(g, w, cs, cur)) return;
+        if (!phase_cache(g, w)) return;
+        if (!phase_probe(g, w, cs, cur, warp_sm)) return;
+        if (!phase_finalize(g, w, cur, prev)) return;
+        if (!g.sync()) return;
+    }
+    if (ph & PH_SOLVE) {
+        uint32_t M = 0, ncol = 0;
+        if (!phase_constraints(g, w, cur, &M, &ncol)) return;
+        const bool solved = w.cfg.dt > 0.0f && w.n_bodies > 0u;
+        if (solved && !phase_solve(g, w, M, ncol)) return;
+        if (!g.sync()) return;
+        if (!phase_store(g, w, cur, M, solved)) return;
+    }
+}
+
+}  // namespace vxp

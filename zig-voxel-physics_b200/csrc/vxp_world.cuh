@@ -1,0 +1,240 @@
+// vxp_world.cuh — device data layout of one simulated world and the phases of
+// one VoxelPhysicsSystem.step (src/system.zig:537-555) on the GPU.
+//
+// One world is stepped by a "group": either one CTA (BlockGroup; many small
+// worlds run side by side, one per CTA) or a whole cooperative grid
+// (GridGroup; one large world).  Each phase below is written once against the
+// group interface: rank()/size() for thread-parallel loops, warp_id()/nwarps()
+// for warp-parallel loops, sync() between phases.  GridGroup.sync() is a
+// bounded grid barrier that reports VXP_ERR_TIMEOUT instead of spinning
+// forever.
+//
+// Phase map (reference file:line → phase)
+//   system.narrowPhase filter        system.zig:586-655      phase_pairs
+//   NarrowPhase.processPair head     narrow_phase.zig:1414-1469 phase_pairs
+//   BrickPairCache.get/put           narrow_phase.zig:228-302 phase_cache
+//   detectVoxelCollisions            narrow_phase.zig:722-857 phase_probe
+//   ContactManifold.addContact       narrow_phase.zig:451-481 phase_probe (replay)
+//   ContactManager.addManifold       narrow_phase.zig:1011-1059 phase_finalize
+//   system.solve / ContactSolver     solver.zig:449-958      phase_constraints..phase_store
+//   updateSleepStates                system.zig:786-792      phase_store
+#pragma once
+
+#include <cstdint>
+
+#include "vxp_math.cuh"
+
+namespace vxp {
+
+// ---------------------------------------------------------------------------
+// Layouts
+// ---------------------------------------------------------------------------
+
+// A collider on the device: the reference's hash map of bricks becomes a dense
+// brick-coordinate grid of slots into one voxel pool.
+struct DCollider {
+    float vs;
+    int32_t min_bound[3], max_bound[3];   // voxel coords, max exclusive
+    float aabb_min[3], aabb_max[3];       // local AABB (recomputeMetadata)
+    int32_t bmin[3];                      // brick grid origin
+    int32_t bdim[3];                      // brick grid extent
+    uint32_t grid_off;                    // into the slot grid
+    uint32_t brick_off;                   // first brick in the voxel pool
+    uint32_t n_bricks;
+    uint32_t solid_count;
+};
+
+// Solver / narrow-phase state of one body (BodyState, solver.zig:203-229).
+struct __align__(16) DBody {
+    float4 p;             // position, w = inv_mass
+    float4 q;             // rotation
+    float4 v;             // linear velocity
+    float4 w;             // angular velocity
+    float4 i0, i1, i2;    // world inverse inertia rows (w unused)
+};
+
+// Per-body properties that the step reads (BodyProperties, body.zig:103-174)
+// and the sleep fields it updates.
+struct DBodyProp {
+    float il[9];          // inverse inertia, local
+    float friction, restitution, lin_damp, ang_damp;
+    float sleep_timer;
+    uint32_t id, type, collider, sleeping;
+};
+
+// Flags of a pair after phase_pairs / phase_cache.
+enum : uint32_t {
+    PF_INVALID = 1u << 0,   // a body id not found
+    PF_CARRY = 1u << 1,     // both sleeping: previous manifold carried over
+    PF_DROPPED = 1u << 2,   // beyond the reference's 512-pair cap
+    PF_NOCOLL = 1u << 3,    // a body without collider
+    PF_SEPARATED = 1u << 4, // SAT early-out
+    PF_CACHE = 1u << 5,     // brick-pair cache consulted
+    PF_HIT = 1u << 6,       // cache hit
+    PF_DETECT = 1u << 7,    // detectVoxelCollisions runs
+    PF_REGION = 1u << 8,    // overlap region non-empty
+    PF_TESTED = 1u << 9,    // processPair was called
+};
+
+struct PairInfo {
+    uint32_t ia, ib;
+    uint32_t flags;
+    uint32_t cache_slot;    // hit: entry read; miss: entry written
+    int32_t rmin[3], rmax[3];
+    uint32_t voxels_checked;
+    uint32_t candidates;
+    uint32_t key_a, key_b;
+    unsigned long long th; // transform hash of the cache key
+};
+
+// Brick-pair cache entry (BrickPairCacheEntry, narrow_phase.zig:172-177); the
+// brick positions of every key the reference builds are (0,0,0).
+struct CacheKeyRec {
+    uint32_t a, b;
+    unsigned long long th;
+    unsigned long long last_used;
+    uint32_t valid, _pad;
+};
+struct ContactRec {          // same field order as vxp_contact
+    float point[3], normal[3], penetration, la[3], lb[3];
+    float normal_impulse, tangent_impulse[2], normal_mass, tangent_mass[2];
+    uint32_t _pad;
+    unsigned long long feature_id;
+};
+struct ManifoldRec {         // same layout as vxp_manifold
+    uint32_t a, b, n;
+    float friction, restitution;
+    uint32_t _pad;
+    ContactRec c[4];
+};
+struct CacheValRec {
+    ContactRec c[4];
+    uint32_t n, has_collision, voxels_checked, _pad;
+};
+
+struct HashSlot {            // pairKey -> manifold index
+    unsigned long long key;  // 0 = empty (pair keys are never 0: ids > 0)
+    uint32_t idx, _pad;
+};
+
+// Step configuration (vxp_config distilled).
+struct StepCfg {
+    float gravity[3];
+    float dt;
+    uint32_t substeps, vel_iters, pos_iters;
+    uint32_t disable_rotation;
+    float hertz, damping_ratio, pos_rate, max_pos_corr, slop;
+    uint32_t warm_starting;
+    float warm_scale;
+    uint32_t friction_on, restitution_on;
+    uint32_t sleeping_on, warm_store_on;
+    uint32_t use_sat, use_cache;
+    uint32_t reference_caps;
+    uint32_t colouring;
+    uint32_t dump_candidates;
+    uint32_t phases;          // PH_* bits
+};
+enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
+
+// Per-world counters and flags (device).  Indices of WorldDev::ctr.
+enum : uint32_t {
+    C_PAIRS_IN = 0,
+    C_PAIRS_TESTED,
+    C_PAIRS_COLLIDING,
+    C_VOXELS_CHECKED,
+    C_CONTACTS,
+    C_SKIPPED_SLEEPING,
+    C_PRESERVED,
+    C_CACHE_HITS,
+    C_CACHE_MISSES,
+    C_CACHE_EVICTIONS,
+    C_MANIFOLDS,
+    C_CONSTRAINTS,
+    C_POINTS,
+    C_COLOURS,
+    C_POS_ITERS,
+    C_STEP_SKIPPED,
+    C_MAX_PEN_KEY,   // ordered-int key of max penetration
+    C_CANDIDATES,
+    C_WORK,          // work counter of phase_probe
+    C_DUMP_N,        // candidates dumped
+    C_AWAKE,         // dynamic awake bodies seen by the sleep check
+    C_ERROR = 31,    // sticky error bits (not cleared per step)
+    C_NCTR = 32
+};
+enum : uint32_t { ERR_TIMEOUT = 1u, ERR_CAP = 2u, ERR_COLOURS = 4u, ERR_OVERFLOW = 8u };
+
+struct WorldDev {
+    StepCfg cfg;
+    uint32_t n_bodies;
+    uint32_t n_pairs;             // set from *n_pairs_dev at kernel start
+    const uint32_t* n_pairs_dev;  // pair count of this step (device)
+    uint32_t pair_cap;
+    uint32_t ht_cap;              // power of two >= 2 * pair_cap
+    uint32_t cache_cap;
+    uint32_t dump_cap;
+    // bodies
+    DBody* body;
+    DBodyProp* prop;
+    float4* p0;                   // position at step start (writeBack NaN reset)
+    float4* qn;                   // normalised rotation per body (transformPoint)
+    uint2* ids;                   // (id, index) sorted by id
+    // pairs
+    uint2* pairs;                 // (body_a id, body_b id)
+    PairInfo* pinfo;
+    // contact manager: two manifold arrays / hash tables, flipped per frame
+    ManifoldRec* man[2];
+    HashSlot* ht[2];
+    uint32_t* frame;              // [0] = frame counter (man[frame & 1] is the latest),
+                                  // [1] = pair count of the latest manifold array
+    // brick-pair cache
+    CacheKeyRec* ckey;
+    CacheValRec* cval;
+    uint32_t* cwriter;            // last pair writing each slot this frame
+    unsigned long long* cframe;   // cache frame counter
+    // constraints
+    uint32_t* cons;               // constraint -> pair index (pair order)
+    uint32_t* colour;             // per constraint (constraint order)
+    uint32_t* pos_of;             // constraint -> packed position (colour-major)
+    uint32_t* packed_pair;        // packed position -> pair index
+    uint32_t* adj_off;            // body -> adjacency offset (n_bodies + 1)
+    uint32_t* adj;                // constraint ids, 2 per constraint at most
+    uint32_t* adj_cur;            // fill cursors (n_bodies)
+    uint32_t* colour_cnt;         // 257: counts, then offsets
+    uint32_t* colour_cur;         // 256 cursors
+    uint32_t* bmask;              // reference colouring: 8 words per body
+    // packed constraint data, slot-major [slot][M]; see CP_* field ids
+    float* cp;                    // CP_NFIELDS * 4 * pair_cap floats
+    uint4* cm;                    // per packed manifold: ia, ib, n, pair
+    float2* cfr;                  // per packed manifold: friction, restitution
+    // scratch
+    uint32_t* scan;               // per-block partials for group scans
+    uint32_t* flag;               // per-pair scratch flags (n_pairs)
+    uint32_t* ctr;                // C_NCTR counters
+    // debug dump
+    struct Cand {
+        uint32_t pair_index;
+        int32_t a[3], b[3];
+        uint32_t passed;
+        float dist_sq;
+    } * dump;
+};
+
+// Packed constraint-point fields (ConstraintPoint, solver.zig:122-168).
+enum : uint32_t {
+    CP_NX, CP_NY, CP_NZ,            // normal
+    CP_LAX, CP_LAY, CP_LAZ,         // local anchor a
+    CP_LBX, CP_LBY, CP_LBZ,         // local anchor b
+    CP_PX, CP_PY, CP_PZ,            // point
+    CP_RAX, CP_RAY, CP_RAZ,         // r_a
+    CP_RBX, CP_RBY, CP_RBZ,         // r_b
+    CP_BASE,                        // base separation
+    CP_NM, CP_TM0, CP_TM1,          // effective masses
+    CP_T1X, CP_T1Y, CP_T1Z,         // tangent1
+    CP_T2X, CP_T2Y, CP_T2Z,         // tangent2
+    CP_BIAS,                        // velocity bias
+    CP_NI, CP_TI0, CP_TI1,          // accumulated impulses
+    CP_NFIELDS
+};
+
+}  // namespace vxp

@@ -1,0 +1,177 @@
+"""Host-side mirror of the reference's VoxelPhysicsSystem seams over the C ABI.
+
+The reference drives its hot path from VoxelPhysicsSystem.step
+(src/system.zig:537-555): narrowPhase() then solve() then
+updateSleepStates().  This module keeps that call shape:
+
+    sys = VoxelPhysicsSystem(PhysicsConfig)      # NarrowPhase.init / ContactSolver.init
+    sys.add_collider(id, voxel_size, bricks)     # VoxelCollider (recomputeMetadata)
+    sys.set_bodies(table)                        # the body slots (VoxelBody)
+    sys.update(dt)                               # accumulator loop -> step(fixed_timestep)
+    sys.step(dt, pairs)                          # one VoxelPhysicsSystem.step
+    sys.narrow_phase(pairs); sys.solve(dt)       # the two halves, for tests
+
+Every call goes to libvxp.so; there is no CPU path.  Errors raise VxpError
+with the library's message (the reference swallows most errors with
+`catch {}`; here they surface).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import abi
+
+
+class VxpError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"vxp error {code}: {msg}")
+        self.code = code
+
+
+class VoxelPhysicsSystem:
+    """One simulated world on one GPU."""
+
+    def __init__(self, config: abi.Config | None = None, device: int = 0, pair_margin: float = 0.1, **overrides):
+        self.lib = abi.load()
+        self.config = config if config is not None else abi.default_config(**overrides)
+        h = ctypes.c_void_p()
+        rc = self.lib.vxp_create(ctypes.byref(self.config), device, ctypes.byref(h))
+        if rc != 0 or not h.value:
+            raise VxpError(rc, "vxp_create failed")
+        self.ctx = h
+        self.pair_margin = float(pair_margin)
+        self.accumulated_time = np.float32(0.0)
+        self.n_bodies = 0
+        self._last_pairs = 0
+
+    # ------------------------------------------------------------------ utils
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.vxp_last_error(self.ctx, buf, len(buf))
+            raise VxpError(rc, buf.value.decode(errors="replace"))
+
+    def close(self) -> None:
+        if getattr(self, "ctx", None) is not None and self.ctx.value:
+            self.lib.vxp_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------- scene building
+    def add_collider(self, collider_id: int, voxel_size: float, bricks: np.ndarray) -> None:
+        bricks = np.ascontiguousarray(bricks, dtype=abi.BRICK_DTYPE)
+        self._check(self.lib.vxp_collider_upload(self.ctx, int(collider_id), np.float32(voxel_size),
+                                                 abi.ptr(bricks), len(bricks)))
+
+    def set_bodies(self, bodies: np.ndarray) -> None:
+        bodies = np.ascontiguousarray(bodies, dtype=abi.BODY_DTYPE)
+        self._check(self.lib.vxp_bodies_set(self.ctx, abi.ptr(bodies), len(bodies)))
+        self.n_bodies = len(bodies)
+
+    def get_bodies(self) -> np.ndarray:
+        out = np.zeros(self.n_bodies, dtype=abi.BODY_DTYPE)
+        self._check(self.lib.vxp_bodies_get(self.ctx, abi.ptr(out), self.n_bodies))
+        return out
+
+    def load_scene(self, scene) -> None:
+        for c in scene.colliders:
+            self.add_collider(c.id, c.voxel_size, c.bricks)
+        self.set_bodies(scene.bodies)
+
+    # ------------------------------------------------------------- stepping
+    def step(self, dt: float, pairs: np.ndarray | None = None) -> None:
+        """One VoxelPhysicsSystem.step.  With pairs=None the pair list is built on
+        the device from the bodies' inflated AABBs."""
+        if pairs is None:
+            self._check(self.lib.vxp_step_device_pairs(self.ctx, np.float32(dt), np.float32(self.pair_margin)))
+        else:
+            pairs = np.ascontiguousarray(pairs, dtype=abi.PAIR_DTYPE)
+            self._check(self.lib.vxp_step(self.ctx, np.float32(dt), abi.ptr(pairs), len(pairs)))
+            self._last_pairs = len(pairs)
+
+    def update(self, dt: float, pairs_fn=None) -> int:
+        """VoxelPhysicsSystem.update (src/system.zig:508-534): fixed-timestep
+        accumulator in f32, at most max_substeps (8) steps per call."""
+        fixed = np.float32(self.config.fixed_timestep)
+        self.accumulated_time = np.float32(self.accumulated_time + np.float32(dt))
+        n = 0
+        while self.accumulated_time >= fixed and n < 8:
+            self.step(fixed, None if pairs_fn is None else pairs_fn())
+            self.accumulated_time = np.float32(self.accumulated_time - fixed)
+            n += 1
+        if self.accumulated_time > np.float32(fixed * np.float32(8)):
+            self.accumulated_time = fixed
+        return n
+
+    def narrow_phase(self, pairs: np.ndarray) -> None:
+        pairs = np.ascontiguousarray(pairs, dtype=abi.PAIR_DTYPE)
+        self._check(self.lib.vxp_narrow_phase(self.ctx, abi.ptr(pairs), len(pairs)))
+
+    def solve(self, dt: float) -> None:
+        self._check(self.lib.vxp_solve(self.ctx, np.float32(dt)))
+
+    def synchronize(self) -> None:
+        self._check(self.lib.vxp_synchronize(self.ctx))
+
+    def set_launch_mode(self, mode: int) -> None:
+        self._check(self.lib.vxp_set_launch_mode(self.ctx, int(mode)))
+
+    # -------------------------------------------------------------- outputs
+    def pairs(self, margin: float | None = None) -> np.ndarray:
+        m = self.pair_margin if margin is None else margin
+        n = ctypes.c_uint32(0)
+        rc = self.lib.vxp_pairs_from_bodies(self.ctx, np.float32(m), None, 0, ctypes.byref(n))
+        if rc not in (0, abi.VXP_ERR_CAP):
+            self._check(rc)
+        out = np.zeros(n.value, dtype=abi.PAIR_DTYPE)
+        self._check(self.lib.vxp_pairs_from_bodies(self.ctx, np.float32(m), abi.ptr(out), len(out), ctypes.byref(n)))
+        return out
+
+    def manifolds(self) -> np.ndarray:
+        n = ctypes.c_uint32(0)
+        self._check(self.lib.vxp_manifolds_get(self.ctx, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=abi.MANIFOLD_DTYPE)
+        self._check(self.lib.vxp_manifolds_get(self.ctx, abi.ptr(out), len(out), ctypes.byref(n)))
+        return out
+
+    def stats(self) -> dict:
+        s = abi.Stats()
+        self._check(self.lib.vxp_stats_get(self.ctx, ctypes.byref(s)))
+        return s.as_dict()
+
+    def colours(self) -> np.ndarray:
+        n = ctypes.c_uint32(0)
+        self._check(self.lib.vxp_colours_get(self.ctx, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=np.uint32)
+        self._check(self.lib.vxp_colours_get(self.ctx, abi.ptr(out), len(out), ctypes.byref(n)))
+        return out
+
+    def set_candidate_dump(self, capacity: int) -> None:
+        self._check(self.lib.vxp_set_candidate_dump(self.ctx, int(capacity)))
+
+    def candidates(self) -> np.ndarray:
+        n = ctypes.c_uint32(0)
+        rc = self.lib.vxp_candidates_get(self.ctx, None, 0, ctypes.byref(n))
+        if rc not in (0, abi.VXP_ERR_CAP):
+            self._check(rc)
+        out = np.zeros(n.value, dtype=abi.CANDIDATE_DTYPE)
+        self._check(self.lib.vxp_candidates_get(self.ctx, abi.ptr(out), len(out), ctypes.byref(n)))
+        return out
+
+    def last_step_ms(self) -> float:
+        out = np.zeros(3, dtype=np.float32)
+        self._check(self.lib.vxp_last_step_ms(self.ctx, abi.ptr(out)))
+        return float(out[2])
