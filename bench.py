@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark: body-substeps/s of the voxel contact + TGS-soft step on B200.
+
+Workload (N=1): the 4096-body pile (seeded random boxes, per-axis extents
+2..16 voxels at 0.1 m, dropped from a 16^3 lattice into a walled bin on a
+ground slab; dt 1/120, 8 substeps).  The scene is first advanced `--settle`
+steps (default 360: the lower layers have landed and the pile holds ~2x10^4
+contact points), then `--warmup` steps, then `--steps` timed steps.  A "step"
+is one VoxelPhysicsSystem.step: the device pair source, the narrow phase and
+the solver with its 8 substeps.
+
+value: device time (CUDA events on the library's stream) of each step with
+its inputs resident; the L2 is flushed (a 256 MiB write) between timed steps.
+e2e: the same steps through the public C ABI with host buffers in pinned
+memory: every step copies the pair list host->device (vxp_step) and reads the
+pair list and the body table back (vxp_pairs_from_bodies, vxp_bodies_get),
+timed by the host clock.
+
+--impl reference times the reference's CPU path (the CPU restatement of the
+reference, with its thread-pooled narrow phase on every host core and the
+single-threaded solver) on the same scene.
+
+Multi-GPU: a single world does not shard; N ranks run N independent replicas
+("replicas only", weak scaling) and value is the sum of their work over the
+slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20
+SOLVER_V, SOLVER_Q = 1, 2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--settle", type=int, default=360)
+    ap.add_argument("--n-side", type=int, default=16)
+    ap.add_argument("--cpu-sample-s", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--launch-mode", type=int, default=-1)
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def alg_bytes(st: dict, substeps: int, n_dyn_awake: int, n_nonstatic: int) -> tuple:
+    """Algorithmic bytes of one step, counting each f32 or byte field the
+    reference reads or writes once per operation: narrow phase per pair
+    2x28 + 2x8, per brick touched 512, per contact 60, per manifold 16;
+    solver per contact point prepare 308 x S, velocity sweep 316 x V x S,
+    relax 316 x S, warm start 248, position sweep 232 x Q, storeImpulses 20;
+    per dynamic body gravity + integrate 208 x S, write-back 104."""
+    narrow = st["pairs_tested"] * 72 + st["bricks_touched"] * 512 + st["contacts_generated"] * 60 + st["manifolds"] * 16
+    pts = st["contact_points"]
+    solver = pts * (308 * substeps + 316 * SOLVER_V * substeps + 316 * substeps + 248 +
+                    232 * max(1, st["position_iterations_run"]) + 20)
+    solver += n_dyn_awake * 208 * substeps + n_nonstatic * 104
+    return narrow, solver
+
+
+def peaks() -> tuple:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+def run_cpu(scene, oracle, args, body_state=None, steps=None, budget_s=None, threads=None):
+    """Times the reference's CPU step (threaded narrow phase on every host core,
+    single-threaded solver).  Returns (body_substeps_per_s, steps_timed, threads, per-step s)."""
+    threads = threads or os.cpu_count() or 1
+    w = oracle.OracleWorld(substeps=8, fixed_timestep=np.float32(1.0 / 120.0))
+    w.load_scene(scene)
+    if body_state is not None:
+        w.set_bodies(body_state)
+    dt = np.float32(scene.dt)
+    n_dyn = scene.dynamic_count
+    times = []
+    t_start = time.perf_counter()
+    k = 0
+    while True:
+        pairs = w.pairs()
+        t0 = time.perf_counter()
+        w.step_threaded(dt, pairs, threads)
+        times.append(time.perf_counter() - t0)
+        k += 1
+        if steps is not None and k >= steps:
+            break
+        if budget_s is not None and time.perf_counter() - t_start > budget_s and k >= 2:
+            break
+    w.close()
+    return n_dyn * 8 * k / sum(times), k, threads, times
+
+
+def reference_arm(args):
+    ws, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return 0
+    vxp = importlib.import_module("zig-voxel-physics_b200")
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api
+
+    scene = vxp.scenes.config2(mass_fn=oracle_api.mass_fn, n_side=args.n_side)
+    threads = os.cpu_count() or 1
+    w = oracle_api.OracleWorld(substeps=8, fixed_timestep=np.float32(1.0 / 120.0))
+    w.load_scene(scene)
+    dt = np.float32(scene.dt)
+    for _ in range(args.settle + args.warmup):
+        w.step_threaded(dt, w.pairs(), threads)
+    times = []
+    for _ in range(args.steps):
+        pairs = w.pairs()
+        t0 = time.perf_counter()
+        w.step_threaded(dt, pairs, threads)
+        times.append(time.perf_counter() - t0)
+    n_dyn = scene.dynamic_count
+    value = n_dyn * 8 * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": "body_substeps_per_s", "value": value, "unit": "body-substeps/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"config2_pile_{n_dyn}", "bodies": n_dyn, "substeps": 8, "dt": "1/120",
+                   "settle_steps": args.settle},
+        "cpu_baseline": {"value": value, "unit": "body-substeps/s", "cores": threads, "kind": "port",
+                         "sample": f"{len(times)} steps after {args.settle + args.warmup} settle/warm-up steps; "
+                                   "threaded narrow phase (reference partitioning) + single-threaded solver"},
+        "e2e": {"value": value, "unit": "body-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+def ours(args):
+    ws, rank, local, pg = dist_setup(args)
+    import torch
+
+    torch.cuda.set_device(local)
+    vxp = importlib.import_module("zig-voxel-physics_b200")
+    abi = vxp.abi
+    scene = vxp.scenes.config2(n_side=args.n_side)
+    n_dyn = scene.dynamic_count
+    n_nonstatic = int((scene.bodies["body_type"] != abi.BODY_STATIC).sum())
+    sysm = vxp.VoxelPhysicsSystem(device=local, substeps=8, fixed_timestep=np.float32(1.0 / 120.0),
+                                  max_pairs=max(65536, 16 * n_dyn), max_bodies=len(scene.bodies))
+    sysm.load_scene(scene)
+    sysm.set_launch_mode(args.launch_mode)
+    dt = np.float32(scene.dt)
+    for i in range(args.settle):
+        sysm.step(dt)
+        if i % 32 == 31:
+            sysm.synchronize()
+    sysm.synchronize()
+    for _ in range(args.warmup):
+        sysm.step(dt)
+        sysm.synchronize()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    clocks = Clocks(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms, kern_ms, pair_ms, stats = [], [], [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        sysm.step(dt)
+        out = np.zeros(3, dtype=np.float32)
+        sysm._check(sysm.lib.vxp_last_step_ms(sysm.ctx, abi.ptr(out)))
+        pair_ms.append(float(out[0]))
+        kern_ms.append(float(out[1]))
+        step_ms.append(float(out[2]))
+        stats.append(sysm.stats())
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_s = sum(step_ms) / 1e3
+    if pg:
+        t = torch.tensor([total_s], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_s = float(t.item())
+    value = ws * n_dyn * 8 * args.steps / total_s
+    pts = [s["contact_points"] for s in stats]
+    contacts_per_s = ws * sum(pts) * 8 / total_s
+    bodies = sysm.get_bodies()
+    n_dyn_awake = int(((bodies["body_type"] == abi.BODY_DYNAMIC) & (bodies["is_sleeping"] == 0)).sum())
+    nb = [sum(alg_bytes(s, 8, n_dyn_awake, n_nonstatic)) for s in stats]
+    peak, peak_kind = peaks()
+    achieved = sum(nb) / (sum(kern_ms) / 1e3) / 1e9
+
+    # ---- e2e through the public API with pinned host buffers
+    cap = max(65536, 16 * n_dyn)
+    pin_pairs = torch.empty(cap * 8, dtype=torch.uint8).pin_memory().numpy().view(abi.PAIR_DTYPE)
+    pin_bodies = torch.empty(len(scene.bodies) * 128, dtype=torch.uint8).pin_memory().numpy().view(abi.BODY_DTYPE)
+    h2d = d2h = 0
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        n = ctypes.c_uint32(0)
+        sysm._check(sysm.lib.vxp_pairs_from_bodies(sysm.ctx, np.float32(sysm.pair_margin), abi.ptr(pin_pairs), cap,
+                                                    ctypes.byref(n)))
+        sysm._check(sysm.lib.vxp_step(sysm.ctx, dt, abi.ptr(pin_pairs), n.value))
+        sysm._check(sysm.lib.vxp_bodies_get(sysm.ctx, abi.ptr(pin_bodies), len(pin_bodies)))
+        h2d += 8 * n.value
+        d2h += 8 * n.value + 128 * len(pin_bodies)
+    e2e_s = time.perf_counter() - t0
+    if pg:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = ws * n_dyn * 8 * args.steps / e2e_s
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_api
+
+        state = sysm.get_bodies()
+        v, k, threads, _ = run_cpu(scene, oracle_api, args, body_state=state, budget_s=args.cpu_sample_s)
+        cpu = {"value": v, "unit": "body-substeps/s", "cores": threads, "kind": "port",
+               "sample": f"{k} steps of the same pile from the GPU's state after {args.settle + args.warmup + 2 * args.steps} "
+                         "steps; threaded narrow phase (reference partitioning) + single-threaded solver"}
+    sysm.close()
+    if rank == 0:
+        ms = statistics.mean(step_ms)
+        line = {
+            "metric": "body_substeps_per_s", "value": value, "unit": "body-substeps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"config2_pile_{n_dyn}", "bodies": n_dyn, "substeps": 8, "dt": "1/120",
+                       "settle_steps": args.settle, "l2": "flushed (256 MiB write) between timed steps",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single world",
+                       "contact_points_mean": statistics.mean(pts), "pairs_mean": statistics.mean(
+                           [s["pairs_tested"] for s in stats])},
+            "contacts_per_s": contacts_per_s,
+            "step_latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                                "kernel_mean": statistics.mean(kern_ms), "pairs_mean": statistics.mean(pair_ms)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "k_step_grid" if n_dyn >= 512 else "k_step_block",
+                         "alg_bytes_per_launch": statistics.mean(nb)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "body-substeps/s", "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps},
+            "clocks": clk,
+            "gpu_launches": 5 * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

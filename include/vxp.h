@@ -178,6 +178,9 @@ typedef struct {
     uint32_t step_skipped;           /* 1 when every dynamic body slept      */
     float max_penetration;
     uint32_t candidates;             /* distance-passing voxel pairs         */
+    uint32_t bricks_touched;         /* bricks of A inside the overlap region
+                                        plus bricks of B inside B's, summed over
+                                        the pairs detected (traffic accounting) */
 } vxp_stats;
 
 /* One candidate voxel pair of the narrow phase, for parity checks of the
@@ -264,7 +267,8 @@ int vxp_colours_get(vxp_ctx* ctx, uint32_t* colours, uint32_t cap, uint32_t* n_o
 int vxp_pairs_from_bodies(vxp_ctx* ctx, float margin, vxp_pair* out, uint32_t cap,
                           uint32_t* n_out);
 
-/* Device-side timing of the last step's kernels (ms): [narrow, solve, total]. */
+/* Device time of the last step call (ms, CUDA events on the context's
+ * stream): [pair source and copies, step kernel, whole call]. */
 int vxp_last_step_ms(vxp_ctx* ctx, float out[3]);
 
 /* Step calls queue work on the context's stream and return; a call that

@@ -326,45 +326,81 @@ int vxo_pairs_find(void* p, float margin, vxp_pair* out, uint32_t cap, uint32_t*
 }
 
 // Multi-threaded narrow phase with the reference's partitioning: T contiguous
-// ranges of ceil(P/T) pairs, each processed by one thread, results merged in
-// thread order (narrow_phase.zig:1538-1632).  f32 worlds only; the cache is
-// read-only on this path, as in ParallelNarrowPhaseContext (narrow_phase.zig:1249).
-// Returns the number of contacts generated.
-int vxo_narrow_phase_threaded(void* p, const vxp_pair* pairs, uint32_t n, int threads) {
-    if (prec(p) != 32) return VXP_ERR_ARG;
-    Handle<float>* h = H<float>(p);
-    World<float>& w = h->w;
+// ranges of ceil(P/T) pairs, each processed by one thread into its own buffer,
+// buffers merged in thread order (narrow_phase.zig:1538-1632).  As in
+// ParallelNarrowPhaseContext, the brick-pair cache is read (hits replay) but
+// never written (narrow_phase.zig:1231-1270).  f32 worlds only.  Returns the
+// number of contacts generated.
+static int narrow_threaded(World<float>& w, const vxp_pair* pairs, uint32_t n, int threads) {
     w.cm.beginFrame();
     w.cache.beginFrame();
     std::vector<uint32_t> filt;
     for (uint32_t i = 0; i < n; ++i) {
         Body<float>* a = w.find(pairs[i].body_a);
         Body<float>* b = w.find(pairs[i].body_b);
-        if (!a || !b) continue;
-        if (a->sleeping && b->sleeping) {
-            const uint64_t key = pairKey(a->id, b->id);
+        const bool as = a ? a->sleeping : false, bs = b ? b->sleeping : false;
+        if (as && bs) {
+            const uint64_t key = pairKey(pairs[i].body_a, pairs[i].body_b);
             if (const Manifold<float>* pm = w.cm.prevGet(key)) w.cm.put(key, *pm);
             continue;
         }
-        filt.push_back(i);
+        if (w.wcfg.reference_caps && filt.size() >= 512) continue;
+        if (a && b) filt.push_back(i);
     }
-    const int T = std::max(1, std::min(threads, 64));
+    const int T = std::max(1, std::min(threads, 256));
     const size_t per = (filt.size() + (size_t)T - 1) / (size_t)T;
     std::vector<std::vector<Manifold<float>>> out((size_t)T);
     std::vector<std::thread> th;
+    std::atomic<uint64_t> hits{0}, misses{0};
     for (int t = 0; t < T; ++t) {
-        const size_t s = (size_t)t * per, e = std::min(filt.size(), s + per);
-        if (s >= e) break;
-        th.emplace_back([&, t, s, e]() {
-            for (size_t k = s; k < e; ++k) {
+        const size_t s0 = (size_t)t * per, e = std::min(filt.size(), s0 + per);
+        if (s0 >= e) break;
+        th.emplace_back([&, t, s0, e]() {
+            for (size_t k = s0; k < e; ++k) {
                 const Body<float>& a = *w.find(pairs[filt[k]].body_a);
                 const Body<float>& b = *w.find(pairs[filt[k]].body_b);
                 if (a.collider < 0 || b.collider < 0) continue;
                 const Collider<float>& ca = w.colliders[(size_t)a.collider];
                 const Collider<float>& cb = w.colliders[(size_t)b.collider];
+                const Xf<float> ta = a.xf(), tb = b.xf();
                 if (w.wcfg.use_brick_sat &&
-                    satEarlyOut(obbFromAabb(ca.local_aabb, a.xf()), obbFromAabb(cb.local_aabb, b.xf())))
+                    satEarlyOut(obbFromAabb(ca.local_aabb, ta), obbFromAabb(cb.local_aabb, tb)))
                     continue;
+                const bool use_cache = w.wcfg.use_brick_pair_cache &&
+                                       (a.type == B_STATIC || b.type == B_STATIC || a.sleeping || b.sleeping);
+                if (use_cache) {
+                    // read-only lookup without touching LRU state (the
+                    // reference mutates last_used_frame from several threads)
+                    const V3<float> rp = sub(tb.p, ta.p);
+                    const Q<float> rr = qmul(qconj(ta.q), tb.q);
+                    const CacheKey key = makeCacheKey(a.id, b.id, IV3{0, 0, 0}, IV3{0, 0, 0}, rp, rr);
+                    const size_t cap = w.cache.e.size();
+                    size_t idx = (size_t)(key.hash() % cap);
+                    const CacheValue<float>* hit = nullptr;
+                    for (size_t p = 0; p < std::min<size_t>(cap, 16); ++p) {
+                        const auto& en = w.cache.e[idx];
+                        if (!en.valid) break;
+                        if (en.key == key) {
+                            hit = &en.value;
+                            break;
+                        }
+                        idx = (idx + 1) % cap;
+                    }
+                    if (hit) {
+                        hits++;
+                        if (hit->has_collision) {
+                            Manifold<float> m;
+                            m.a = a.id;
+                            m.b = b.id;
+                            m.friction = std::sqrt(a.friction * b.friction);
+                            m.restitution = fmx(a.restitution, b.restitution);
+                            for (uint32_t i = 0; i < hit->n; ++i) m.addContact(hit->c[i]);
+                            out[(size_t)t].push_back(m);
+                        }
+                        continue;
+                    }
+                    misses++;
+                }
                 DetectResult<float> r = detectVoxelCollisions(a, ca, b, cb, nullptr, 0);
                 if (r.has_collision) out[(size_t)t].push_back(r.m);
             }
@@ -377,7 +413,34 @@ int vxo_narrow_phase_threaded(void* p, const vxp_pair* pairs, uint32_t n, int th
             contacts += (int)m.n;
             w.cm.addManifold(m);
         }
+    w.stats.cache_hits = (uint32_t)hits.load();
+    w.stats.cache_misses = (uint32_t)misses.load();
+    w.stats.manifolds = (uint32_t)w.cm.cur.size();
     return contacts;
+}
+
+int vxo_narrow_phase_threaded(void* p, const vxp_pair* pairs, uint32_t n, int threads) {
+    if (prec(p) != 32) return VXP_ERR_ARG;
+    return narrow_threaded(H<float>(p)->w, pairs, n, threads);
+}
+
+// One VoxelPhysicsSystem.step with enable_threading: threaded narrow phase,
+// then the (single-threaded) solve and the sleep update.
+int vxo_step_threaded(void* p, float dt, const vxp_pair* pairs, uint32_t n, int threads) {
+    if (prec(p) != 32) return VXP_ERR_ARG;
+    World<float>& w = H<float>(p)->w;
+    w.stats = Stats{};
+    w.stats.pairs_in = n;
+    if (w.wcfg.enable_sleeping && w.allDynamicSleeping()) {
+        w.stats.step_skipped = 1;
+        return 0;
+    }
+    narrow_threaded(w, pairs, n, threads);
+    w.solve(dt);
+    if (w.wcfg.enable_sleeping)
+        for (auto& b : w.bodies)
+            if (b.type == B_DYNAMIC && !b.sleeping) b.updateSleepState(dt);
+    return 0;
 }
 
 int vxo_mass_properties(float vs, const vxp_brick* bricks, uint32_t n, float density, float* inv_mass,

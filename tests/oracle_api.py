@@ -44,6 +44,7 @@ for name, res, args in [
     ("vxo_candidates_get", _I, [_VP, _VP, _U32, _PU32]),
     ("vxo_pairs_find", _I, [_VP, _F, _VP, _U32, _PU32]),
     ("vxo_narrow_phase_threaded", _I, [_VP, _VP, _U32, _I]),
+    ("vxo_step_threaded", _I, [_VP, _F, _VP, _U32, _I]),
     ("vxo_mass_properties", _I, [_F, _VP, _U32, _F, ctypes.POINTER(_F), _VP]),
     ("vxo_collider_metadata", _I, [_F, _VP, _U32, _VP, _VP, _PU32]),
     ("vxo_classify", ctypes.c_uint8, [_I, ctypes.c_uint8]),
@@ -157,6 +158,10 @@ class OracleWorld:
     def narrow_phase_threaded(self, pairs, threads):
         pairs = np.ascontiguousarray(pairs, dtype=abi.PAIR_DTYPE)
         return L.vxo_narrow_phase_threaded(self.h, abi.ptr(pairs), len(pairs), int(threads))
+
+    def step_threaded(self, dt, pairs, threads):
+        pairs = np.ascontiguousarray(pairs, dtype=abi.PAIR_DTYPE)
+        assert L.vxo_step_threaded(self.h, np.float32(dt), abi.ptr(pairs), len(pairs), int(threads)) == 0
 
     def solve(self, dt):
         assert L.vxo_solve(self.h, np.float32(dt)) == 0

@@ -36,7 +36,7 @@ def test_struct_sizes(vxp):
     assert a.MANIFOLD_DTYPE.itemsize == 376
     assert a.CONTACT_DTYPE.itemsize == 88
     assert ctypes.sizeof(a.Config) == 4 * 26
-    assert ctypes.sizeof(a.Stats) == 4 * 18
+    assert ctypes.sizeof(a.Stats) == 4 * 19
 
 
 def test_classification_matches_reference(vxp):

@@ -138,6 +138,7 @@ class Stats(ctypes.Structure):
         ("step_skipped", ctypes.c_uint32),
         ("max_penetration", ctypes.c_float),
         ("candidates", ctypes.c_uint32),
+        ("bricks_touched", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:

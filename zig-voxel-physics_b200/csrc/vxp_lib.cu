@@ -78,30 +78,40 @@ __global__ void k_body_aabbs(const DBody* body, const DBodyProp* prop, uint32_t 
     mx[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
 }
 
-// Pairs (i < j in id order) whose inflated AABBs overlap and that are not both
-// static.  Pass 0 counts per i, pass 1 writes at the scanned offsets.
+// Pairs (s < t in id order) whose inflated AABBs overlap and that are not
+// both static.  One warp per row s; lanes sweep t in strides of 32 and a
+// ballot keeps the row's pairs in t order.  Pass 0 counts per row, pass 1
+// writes at the scanned offsets (clamped to cap).
 __global__ void k_pairs(const uint2* ids, const DBodyProp* prop, uint32_t n, const float4* mn, const float4* mx,
                         uint32_t* counts, const uint32_t* offsets, uint2* out, uint32_t cap, int pass) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
     if (s >= n) return;
-    const uint32_t i = ids[s].y;
-    const float4 a0 = mn[i], a1 = mx[i];
-    const bool si = prop[i].type == 0u;
-    uint32_t cnt = 0;
+    const uint2 is = ids[s];
+    const float4 a0 = mn[is.y], a1 = mx[is.y];
+    const bool si = prop[is.y].type == 0u;
     uint32_t o = pass ? offsets[s] : 0u;
-    for (uint32_t t = s + 1; t < n; ++t) {
-        const uint32_t j = ids[t].y;
-        if (si && prop[j].type == 0u) continue;
-        const float4 b0 = mn[j], b1 = mx[j];
-        if (a0.x <= b1.x && a1.x >= b0.x && a0.y <= b1.y && a1.y >= b0.y && a0.z <= b1.z && a1.z >= b0.z) {
-            if (pass) {
-                if (o < cap) out[o] = make_uint2(ids[s].x, ids[t].x);
-                ++o;
+    uint32_t cnt = 0;
+    for (uint32_t t0 = s + 1; t0 < n; t0 += 32u) {
+        const uint32_t t = t0 + lane;
+        bool hit = false;
+        uint2 it = make_uint2(0u, 0u);
+        if (t < n) {
+            it = ids[t];
+            if (!(si && prop[it.y].type == 0u)) {
+                const float4 b0 = mn[it.y], b1 = mx[it.y];
+                hit = a0.x <= b1.x && a1.x >= b0.x && a0.y <= b1.y && a1.y >= b0.y && a0.z <= b1.z && a1.z >= b0.z;
             }
-            ++cnt;
         }
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (pass && hit) {
+            const uint32_t slot = o + __popc(m & ((1u << lane) - 1u));
+            if (slot < cap) out[slot] = make_uint2(is.x, it.x);
+        }
+        o += __popc(m);
+        cnt += __popc(m);
     }
-    if (!pass) counts[s] = cnt;
+    if (!pass && lane == 0) counts[s] = cnt;
 }
 
 // Exclusive scan of counts (single block, n arbitrary); writes total to *total.
@@ -217,7 +227,9 @@ struct vxp_ctx {
     uint32_t body_cap = 0;
     uint32_t grid_blocks = 0;
     uint32_t last_pairs = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_start = nullptr, ev0 = nullptr, ev1 = nullptr, ev_count = nullptr;
+    uint32_t* h_count = nullptr;  // pinned mirror of the device pair count
+    bool count_pending = false;
     float last_ms[3] = {0, 0, 0};
     int use_grid = -1;  // -1 auto, 0 block, 1 grid
 };
@@ -514,7 +526,8 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t n_pairs_hint, uint32_t phases) 
     CK(cudaMemcpyAsync(ctx->d_world.p, &w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(ctx->ctr.p, 0, sizeof(uint32_t) * C_ERROR, ctx->stream));
     const ColliderSet cs = collider_set(ctx);
-    bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && (n_pairs_hint > 1024 || ctx->n_bodies > 2048));
+    (void)n_pairs_hint;
+    bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->n_bodies >= 512);
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (grid) {
         CK(cudaMemsetAsync(ctx->bar.p, 0, sizeof(GridBar), ctx->stream));
@@ -547,29 +560,50 @@ int check_device_error(vxp_ctx* ctx) {
     return VXP_OK;
 }
 
-int compute_device_pairs(vxp_ctx* ctx, float margin, uint32_t* n_out) {
+// The pair source on the device.  With wait_count the pair count is read back
+// (growing the buffers and rewriting when it did not fit); without, nothing
+// waits: the step kernel refuses a list that overflowed (VXP_ERR_CAP at the
+// next wait, state untouched) and the buffers grow ahead of need from the
+// count of an earlier step, copied back asynchronously.
+int compute_device_pairs(vxp_ctx* ctx, float margin, bool wait_count, uint32_t* n_out) {
     if (int rc = sync_colliders(ctx)) return rc;
     const uint32_t n = ctx->n_bodies;
     const ColliderSet cs = collider_set(ctx);
+    if (!wait_count && ctx->count_pending && cudaEventQuery(ctx->ev_count) == cudaSuccess) {
+        ctx->count_pending = false;
+        const uint32_t seen = *ctx->h_count;
+        if (seen > ctx->pair_cap - ctx->pair_cap / 4u) {
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (int rc = ensure_pair_cap(ctx, seen + seen / 2u + 1024u)) return rc;
+        }
+    }
     if (n == 0) {
         *n_out = 0;
         CK(cudaMemsetAsync(ctx->n_pairs_dev.p, 0, sizeof(uint32_t), ctx->stream));
         return VXP_OK;
     }
     const uint32_t tb = 256, nb = (n + tb - 1) / tb;
+    const uint32_t wb = (n * 32u + tb - 1) / tb;
     k_body_aabbs<<<nb, tb, 0, ctx->stream>>>(ctx->body.p, ctx->prop.p, n, cs, margin, ctx->aabb_mn.p, ctx->aabb_mx.p);
-    k_pairs<<<nb, tb, 0, ctx->stream>>>(ctx->ids.p, ctx->prop.p, n, ctx->aabb_mn.p, ctx->aabb_mx.p,
+    k_pairs<<<wb, tb, 0, ctx->stream>>>(ctx->ids.p, ctx->prop.p, n, ctx->aabb_mn.p, ctx->aabb_mx.p,
                                         ctx->pair_counts.p, nullptr, nullptr, 0, 0);
     k_scan1<<<1, 1024, 0, ctx->stream>>>(ctx->pair_counts.p, ctx->pair_offsets.p, n, ctx->n_pairs_dev.p);
     CK(cudaGetLastError());
     uint32_t total = 0;
-    CK(cudaMemcpyAsync(&total, ctx->n_pairs_dev.p, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    if (int rc = ensure_pair_cap(ctx, total)) return rc;
-    k_pairs<<<nb, tb, 0, ctx->stream>>>(ctx->ids.p, ctx->prop.p, n, ctx->aabb_mn.p, ctx->aabb_mx.p, nullptr,
+    if (wait_count) {
+        CK(cudaMemcpyAsync(&total, ctx->n_pairs_dev.p, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (int rc = ensure_pair_cap(ctx, total)) return rc;
+    }
+    k_pairs<<<wb, tb, 0, ctx->stream>>>(ctx->ids.p, ctx->prop.p, n, ctx->aabb_mn.p, ctx->aabb_mx.p, nullptr,
                                         ctx->pair_offsets.p, ctx->pairs.p, ctx->pair_cap, 1);
     CK(cudaGetLastError());
-    *n_out = total;
+    if (!wait_count && !ctx->count_pending) {
+        CK(cudaMemcpyAsync(ctx->h_count, ctx->n_pairs_dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaEventRecord(ctx->ev_count, ctx->stream));
+        ctx->count_pending = true;
+    }
+    *n_out = wait_count ? total : ctx->pair_cap;
     return VXP_OK;
 }
 
@@ -629,8 +663,12 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     if (cudaDeviceGetAttribute(&smc, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return bail(VXP_ERR_CUDA);
     ctx->sm_count = smc;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(VXP_ERR_CUDA);
-    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+    if (cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev0) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_count, cudaEventDisableTiming) != cudaSuccess)
         return bail(VXP_ERR_CUDA);
+    if (cudaMallocHost(&ctx->h_count, sizeof(uint32_t)) != cudaSuccess) return bail(VXP_ERR_OOM);
+    *ctx->h_count = 0;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads, kWarpSmem) != cudaSuccess ||
         per_sm < 1)
@@ -664,8 +702,11 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
 void vxp_destroy(vxp_ctx* ctx) {
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->ev_count) cudaEventDestroy(ctx->ev_count);
+    if (ctx->h_count) cudaFreeHost(ctx->h_count);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -850,6 +891,7 @@ int vxp_narrow_phase(vxp_ctx* ctx, const vxp_pair* pairs, uint32_t n_pairs);
 int vxp_step(vxp_ctx* ctx, float dt, const vxp_pair* pairs, uint32_t n_pairs) {
     if (!ctx || (!pairs && n_pairs)) return fail(ctx, VXP_ERR_ARG, "null argument");
     if (int rc = ensure_pair_cap(ctx, n_pairs)) return rc;
+    CK(cudaEventRecord(ctx->ev_start, ctx->stream));
     if (n_pairs) CK(cudaMemcpyAsync(ctx->pairs.p, pairs, n_pairs * sizeof(vxp_pair), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->n_pairs_dev.p, &n_pairs, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     ctx->last_pairs = n_pairs;
@@ -859,7 +901,8 @@ int vxp_step(vxp_ctx* ctx, float dt, const vxp_pair* pairs, uint32_t n_pairs) {
 int vxp_step_device_pairs(vxp_ctx* ctx, float dt, float margin) {
     if (!ctx) return VXP_ERR_ARG;
     uint32_t n = 0;
-    if (int rc = compute_device_pairs(ctx, margin, &n)) return rc;
+    CK(cudaEventRecord(ctx->ev_start, ctx->stream));
+    if (int rc = compute_device_pairs(ctx, margin, false, &n)) return rc;
     ctx->last_pairs = n;
     return launch_step(ctx, dt, n, PH_STEP);
 }
@@ -869,6 +912,7 @@ int vxp_step_device_pairs(vxp_ctx* ctx, float dt, float margin) {
 int vxp_narrow_phase(vxp_ctx* ctx, const vxp_pair* pairs, uint32_t n_pairs) {
     if (!ctx || (!pairs && n_pairs)) return fail(ctx, VXP_ERR_ARG, "null argument");
     if (int rc = ensure_pair_cap(ctx, n_pairs)) return rc;
+    CK(cudaEventRecord(ctx->ev_start, ctx->stream));
     if (n_pairs) CK(cudaMemcpyAsync(ctx->pairs.p, pairs, n_pairs * sizeof(vxp_pair), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->n_pairs_dev.p, &n_pairs, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     ctx->last_pairs = n_pairs;
@@ -878,6 +922,7 @@ int vxp_narrow_phase(vxp_ctx* ctx, const vxp_pair* pairs, uint32_t n_pairs) {
 // system.solve() + updateSleepStates on the manifolds of the last narrow phase.
 int vxp_solve(vxp_ctx* ctx, float dt) {
     if (!ctx) return VXP_ERR_ARG;
+    CK(cudaEventRecord(ctx->ev_start, ctx->stream));
     return launch_step(ctx, dt, ctx->last_pairs, PH_SOLVE);
 }
 
@@ -957,6 +1002,7 @@ int vxp_stats_get(vxp_ctx* ctx, vxp_stats* s) {
     int32_t bits = k >= 0 ? k : (k ^ 0x7FFFFFFF);
     std::memcpy(&s->max_penetration, &bits, 4);
     s->candidates = c[C_CANDIDATES];
+    s->bricks_touched = c[C_BRICKS];
     return VXP_OK;
 }
 
@@ -974,7 +1020,7 @@ int vxp_colours_get(vxp_ctx* ctx, uint32_t* colours, uint32_t cap, uint32_t* n_o
 int vxp_pairs_from_bodies(vxp_ctx* ctx, float margin, vxp_pair* out, uint32_t cap, uint32_t* n_out) {
     if (!ctx || !n_out) return VXP_ERR_ARG;
     uint32_t n = 0;
-    if (int rc = compute_device_pairs(ctx, margin, &n)) return rc;
+    if (int rc = compute_device_pairs(ctx, margin, true, &n)) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     *n_out = n;
     const uint32_t k = std::min(n, cap);
@@ -985,11 +1031,13 @@ int vxp_pairs_from_bodies(vxp_ctx* ctx, float margin, vxp_pair* out, uint32_t ca
 int vxp_last_step_ms(vxp_ctx* ctx, float out[3]) {
     if (!ctx || !out) return VXP_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    out[0] = 0.f;
-    out[1] = 0.f;
-    out[2] = ms;
+    float a = 0.f, b = 0.f, c = 0.f;
+    CK(cudaEventElapsedTime(&a, ctx->ev_start, ctx->ev0));
+    CK(cudaEventElapsedTime(&b, ctx->ev0, ctx->ev1));
+    CK(cudaEventElapsedTime(&c, ctx->ev_start, ctx->ev1));
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
     return VXP_OK;
 }
 

@@ -190,6 +190,34 @@ __device__ __forceinline__ uint32_t voxel_at(const ColliderSet& cs, const DColli
     return (uint32_t)__ldg(&cs.vox[(size_t)(c.brick_off + (uint32_t)slot) * 512u + (uint32_t)((x & 7) + 8 * (y & 7) +
                                                                                                  64 * (z & 7))]);
 }
+// Slot of the brick at brick coordinates (bx, by, bz), or -1.
+__device__ __forceinline__ int32_t brick_slot(const ColliderSet& cs, const DCollider& c, int32_t bx, int32_t by,
+                                              int32_t bz) {
+    bx -= c.bmin[0];
+    by -= c.bmin[1];
+    bz -= c.bmin[2];
+    if ((uint32_t)bx >= (uint32_t)c.bdim[0] || (uint32_t)by >= (uint32_t)c.bdim[1] ||
+        (uint32_t)bz >= (uint32_t)c.bdim[2])
+        return -1;
+    return __ldg(&cs.grid[c.grid_off + (uint32_t)(bx + c.bdim[0] * (by + c.bdim[1] * bz))]);
+}
+// Bricks holding voxels inside the inclusive voxel box [lo, hi], counted by
+// the lanes of a warp (result in every lane).
+__device__ uint32_t warp_count_bricks(const ColliderSet& cs, const DCollider& c, I3 lo, I3 hi) {
+    const int32_t x0 = lo.x >> 3, y0 = lo.y >> 3, z0 = lo.z >> 3;
+    const int32_t nx = (hi.x >> 3) - x0 + 1, ny = (hi.y >> 3) - y0 + 1, nz = (hi.z >> 3) - z0 + 1;
+    uint32_t cnt = 0;
+    if (nx > 0 && ny > 0 && nz > 0) {
+        const uint32_t cells = (uint32_t)(nx * ny * nz);
+        for (uint32_t i = threadIdx.x & 31; i < cells; i += 32u) {
+            const int32_t bx = x0 + (int32_t)(i % (uint32_t)nx), by = y0 + (int32_t)((i / (uint32_t)nx) % (uint32_t)ny),
+                          bz = z0 + (int32_t)(i / ((uint32_t)nx * (uint32_t)ny));
+            if (brick_slot(cs, c, bx, by, bz) >= 0) ++cnt;
+        }
+    }
+    return warp_sum(cnt);
+}
+
 __device__ __forceinline__ F3 voxel_to_local(float vs, int32_t x, int32_t y, int32_t z) {
     const float half = vs * 0.5f;
     return F3{(float)x * vs + half, (float)y * vs + half, (float)z * vs + half};
@@ -789,6 +817,14 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
     if (lane == 0) sm.n = 0u;
     Top4 state = top4_empty();
     uint32_t checked = 0, ncand = 0;
+    {
+        // traffic accounting: A bricks in the region, B bricks in B's region
+        uint32_t nb = warp_count_bricks(cs, ca, I3{pi.rmin[0], pi.rmin[1], pi.rmin[2]},
+                                        I3{pi.rmax[0], pi.rmax[1], pi.rmax[2]});
+        I3 blo, bhi;
+        if (overlap_region(cb, c.pb, c.qb, ca, c.pa, c.qa, &blo, &bhi)) nb += warp_count_bricks(cs, cb, blo, bhi);
+        if (lane == 0) atomicAdd(&w.ctr[C_BRICKS], nb);
+    }
     __syncwarp();
     for (unsigned long long base = 0; base < V; base += 32ull) {
         const unsigned long long l = base + lane;

@@ -159,6 +159,7 @@ enum : uint32_t {
     C_WORK,          // work counter of phase_probe
     C_DUMP_N,        // candidates dumped
     C_AWAKE,         // dynamic awake bodies seen by the sleep check
+    C_BRICKS,        // bricks of A in the overlap region + bricks of B in B's
     C_ERROR = 31,    // sticky error bits (not cleared per step)
     C_NCTR = 32
 };
