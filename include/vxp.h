@@ -283,6 +283,15 @@ int vxp_synchronize(vxp_ctx* ctx);
  * stepped by a cooperative grid over every SM. */
 int vxp_set_launch_mode(vxp_ctx* ctx, int mode);
 
+/* Grid launch tuning: after the narrow phase, the solver runs on
+ * ceil(manifolds / div) blocks (at least 2); default div 128. */
+int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div);
+
+/* Diagnostics: ns from the start of the last step kernel to the end of each
+ * of its phases: [start, begin, pairs, cache, probe, finalize, constraints,
+ * solve, end]. */
+int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -214,6 +214,8 @@ SIGNATURES = {
     "vxp_last_step_ms": (_I, [_VP, _VP]),
     "vxp_synchronize": (_I, [_VP]),
     "vxp_set_launch_mode": (_I, [_VP, _I]),
+    "vxp_phase_times": (_I, [_VP, _VP, _U32]),
+    "vxp_set_solver_blocks_divisor": (_I, [_VP, _U32]),
 }
 
 _LIB = None

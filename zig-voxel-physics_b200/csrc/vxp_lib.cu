@@ -27,13 +27,24 @@ using namespace vxp;
 // Kernels
 // ===========================================================================
 
+// Dynamic shared memory: one WarpManifold per warp, then the cache table.
+__device__ __forceinline__ CacheSmem cache_smem(unsigned char* raw, uint32_t nwarps, uint32_t cap) {
+    unsigned char* p = raw + sizeof(WarpManifold) * nwarps;
+    CacheSmem c;
+    c.ab = reinterpret_cast<uint2*>(p);
+    c.th = reinterpret_cast<unsigned long long*>(p + sizeof(uint2) * cap);
+    c.lu = reinterpret_cast<uint32_t*>(p + (sizeof(uint2) + sizeof(unsigned long long)) * cap);
+    return c;
+}
+
 // One world per CTA.
 __global__ void __launch_bounds__(512) k_step_block(WorldDev* worlds, ColliderSet cs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WarpManifold* wsm = reinterpret_cast<WarpManifold*>(smem_raw);
     WorldDev w = worlds[blockIdx.x];
+    const CacheSmem csm = cache_smem(smem_raw, blockDim.x / 32u, w.cache_cap);
     BlockGroup g;
-    world_step(g, w, cs, wsm);
+    world_step(g, w, cs, wsm, csm);
 }
 
 // One world over a cooperative grid.
@@ -42,8 +53,9 @@ __global__ void __launch_bounds__(512) k_step_grid(const WorldDev* world, Collid
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WarpManifold* wsm = reinterpret_cast<WarpManifold*>(smem_raw);
     WorldDev w = *world;
-    GridGroup g{bar, &w.ctr[C_ERROR], timeout_ns};
-    world_step(g, w, cs, wsm);
+    const CacheSmem csm = cache_smem(smem_raw, blockDim.x / 32u, w.cache_cap);
+    GridGroup g{bar, &w.ctr[C_ERROR], timeout_ns, gridDim.x};
+    world_step(g, w, cs, wsm, csm);
 }
 
 // Pair source: world AABB of each body's collider (AABB.transform,
@@ -209,7 +221,7 @@ struct vxp_ctx {
     DBuf<ManifoldRec> man0, man1;
     DBuf<HashSlot> ht0, ht1;
     DBuf<uint32_t> frame;
-    DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag;
+    DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag, clist;
     DBuf<float> cp;
     DBuf<uint4> cm;
     DBuf<float2> cfr;
@@ -217,6 +229,7 @@ struct vxp_ctx {
     DBuf<uint32_t> adj_off, adj_cur, bmask;
     // fixed
     DBuf<uint32_t> colour_cnt, colour_cur, scan, ctr, cwriter;
+    DBuf<unsigned long long> ts;
     DBuf<CacheKeyRec> ckey;
     DBuf<CacheValRec> cval;
     DBuf<unsigned long long> cframe;
@@ -232,6 +245,7 @@ struct vxp_ctx {
     bool count_pending = false;
     float last_ms[3] = {0, 0, 0};
     int use_grid = -1;  // -1 auto, 0 block, 1 grid
+    uint32_t solver_div = 128;
 };
 
 namespace {
@@ -255,6 +269,9 @@ int fail(vxp_ctx* c, int code, const char* fmt, ...) {
 
 constexpr uint32_t kBlockThreads = 512;
 constexpr size_t kWarpSmem = sizeof(WarpManifold) * (kBlockThreads / 32);
+size_t step_smem(uint32_t cache_cap) {
+    return kWarpSmem + (size_t)cache_cap * (sizeof(uint2) + sizeof(unsigned long long) + sizeof(uint32_t));
+}
 
 uint64_t hash_brick_pos(int32_t x, int32_t y, int32_t z) {  // collider.zig:187-192
     const uint64_t ux = (uint64_t)(int64_t)x, uy = (uint64_t)(int64_t)y, uz = (uint64_t)(int64_t)z;
@@ -390,6 +407,7 @@ int ensure_pair_cap(vxp_ctx* ctx, uint32_t need) {
     ok &= ctx->packed_pair.reserve(cap) == cudaSuccess;
     ok &= ctx->adj.reserve((size_t)2 * cap) == cudaSuccess;
     ok &= ctx->flag.reserve(cap) == cudaSuccess;
+    ok &= ctx->clist.reserve(cap) == cudaSuccess;
     ok &= ctx->cp.reserve((size_t)CP_NFIELDS * 4 * cap) == cudaSuccess;
     ok &= ctx->cm.reserve(cap) == cudaSuccess;
     ok &= ctx->cfr.reserve(cap) == cudaSuccess;
@@ -447,6 +465,7 @@ int ensure_body_cap(vxp_ctx* ctx, uint32_t n) {
 StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) {
     StepCfg s;
     s.phases = phases;
+    s.solver_div = 128;
     for (int i = 0; i < 3; ++i) s.gravity[i] = c.gravity[i];
     s.dt = dt;
     s.substeps = c.substeps;
@@ -476,6 +495,7 @@ WorldDev make_world(vxp_ctx* ctx, float dt, uint32_t phases) {
     WorldDev w;
     std::memset(&w, 0, sizeof(w));
     w.cfg = step_cfg(ctx->cfg, dt, ctx->dump_cap ? 1u : 0u, phases);
+    w.cfg.solver_div = ctx->solver_div;
     w.n_bodies = ctx->n_bodies;
     w.n_pairs = 0;
     w.n_pairs_dev = ctx->n_pairs_dev.p;
@@ -498,6 +518,7 @@ WorldDev make_world(vxp_ctx* ctx, float dt, uint32_t phases) {
     w.ckey = ctx->ckey.p;
     w.cval = ctx->cval.p;
     w.cwriter = ctx->cwriter.p;
+    w.clist = ctx->clist.p;
     w.cframe = ctx->cframe.p;
     w.cons = ctx->cons.p;
     w.colour = ctx->colour.p;
@@ -515,6 +536,7 @@ WorldDev make_world(vxp_ctx* ctx, float dt, uint32_t phases) {
     w.scan = ctx->scan.p;
     w.flag = ctx->flag.p;
     w.ctr = ctx->ctr.p;
+    w.ts = ctx->ts.p;
     w.dump = ctx->dump.p;
     return w;
 }
@@ -530,15 +552,15 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t n_pairs_hint, uint32_t phases) 
     bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->n_bodies >= 512);
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (grid) {
-        CK(cudaMemsetAsync(ctx->bar.p, 0, sizeof(GridBar), ctx->stream));
+        CK(cudaMemsetAsync(ctx->bar.p, 0, 2 * sizeof(GridBar), ctx->stream));
         const WorldDev* wp = ctx->d_world.p;
         GridBar* bp = ctx->bar.p;
         unsigned long long timeout = 10ull * 1000ull * 1000ull * 1000ull;  // 10 s per barrier wait
         void* args[] = {(void*)&wp, (void*)&cs, (void*)&bp, (void*)&timeout};
         CK(cudaLaunchCooperativeKernel((const void*)k_step_grid, dim3(ctx->grid_blocks), dim3(kBlockThreads), args,
-                                       kWarpSmem, ctx->stream));
+                                       step_smem(w.cache_cap), ctx->stream));
     } else {
-        k_step_block<<<1, kBlockThreads, kWarpSmem, ctx->stream>>>(ctx->d_world.p, cs);
+        k_step_block<<<1, kBlockThreads, step_smem(w.cache_cap), ctx->stream>>>(ctx->d_world.p, cs);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -651,6 +673,7 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     *out = nullptr;
     if (cfg->substeps == 0) return VXP_ERR_ARG;
     if (cfg->position_iterations > 16) return VXP_ERR_ARG;
+    if (cfg->brick_pair_cache_size > kMaxCacheSmem) return VXP_ERR_ARG;
     vxp_ctx* ctx = new vxp_ctx;
     ctx->cfg = *cfg;
     ctx->device = device;
@@ -669,12 +692,18 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
         return bail(VXP_ERR_CUDA);
     if (cudaMallocHost(&ctx->h_count, sizeof(uint32_t)) != cudaSuccess) return bail(VXP_ERR_OOM);
     *ctx->h_count = 0;
+    const uint32_t cache_cap = cfg->brick_pair_cache_size ? cfg->brick_pair_cache_size : 1024u;
+    if (cudaFuncSetAttribute(k_step_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)step_smem(cache_cap)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_step_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)step_smem(cache_cap)) !=
+            cudaSuccess)
+        return bail(VXP_ERR_CUDA);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads, kWarpSmem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads, step_smem(cache_cap)) !=
+            cudaSuccess ||
         per_sm < 1)
         return bail(VXP_ERR_CUDA);
     ctx->grid_blocks = (uint32_t)(smc * std::min(per_sm, 2));
-    const uint32_t cache_cap = cfg->brick_pair_cache_size ? cfg->brick_pair_cache_size : 1024u;
     bool ok = true;
     ok &= ctx->n_pairs_dev.reserve(1) == cudaSuccess;
     ok &= ctx->frame.reserve(2) == cudaSuccess;
@@ -682,16 +711,14 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     ok &= ctx->colour_cur.reserve(256) == cudaSuccess;
     ok &= ctx->scan.reserve(ctx->grid_blocks + 64) == cudaSuccess;
     ok &= ctx->ctr.reserve(C_NCTR) == cudaSuccess;
+    ok &= ctx->ts.reserve(TS_N) == cudaSuccess;
     ok &= ctx->ckey.reserve(cache_cap) == cudaSuccess;
     ok &= ctx->cval.reserve(cache_cap) == cudaSuccess;
     ok &= ctx->cwriter.reserve(cache_cap) == cudaSuccess;
     ok &= ctx->cframe.reserve(1) == cudaSuccess;
     ok &= ctx->d_world.reserve(1) == cudaSuccess;
-    ok &= ctx->bar.reserve(1) == cudaSuccess;
+    ok &= ctx->bar.reserve(2) == cudaSuccess;
     if (!ok) return bail(VXP_ERR_OOM);
-    if (cudaFuncSetAttribute(k_step_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWarpSmem) !=
-        cudaSuccess)
-        return bail(VXP_ERR_CUDA);
     if (ensure_pair_cap(ctx, std::max<uint32_t>(cfg->max_pairs, 1024)) != VXP_OK) return bail(VXP_ERR_OOM);
     if (ensure_body_cap(ctx, std::max<uint32_t>(cfg->max_bodies, 256)) != VXP_OK) return bail(VXP_ERR_OOM);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(VXP_ERR_CUDA);
@@ -967,12 +994,24 @@ int vxp_candidates_get(vxp_ctx* ctx, vxp_candidate* out, uint32_t cap, uint32_t*
     uint32_t n = 0;
     CK(cudaMemcpy(&n, ctx->ctr.p + C_DUMP_N, sizeof(n), cudaMemcpyDeviceToHost));
     *n_out = n;
-    const uint32_t k = std::min(std::min(n, cap), ctx->dump_cap);
-    if (k && out) {
-        static_assert(sizeof(WorldDev::Cand) == sizeof(vxp_candidate), "candidate layout");
-        CK(cudaMemcpy(out, ctx->dump.p, k * sizeof(vxp_candidate), cudaMemcpyDeviceToHost));
-    }
     if (n > ctx->dump_cap) return fail(ctx, VXP_ERR_CAP, "candidate dump overflow: %u > %u", n, ctx->dump_cap);
+    // cache-consulting pairs are detected speculatively while the cache is
+    // replayed; the records of the pairs that hit are not part of the step
+    static_assert(sizeof(WorldDev::Cand) == sizeof(vxp_candidate), "candidate layout");
+    std::vector<vxp_candidate> all(n);
+    if (n) CK(cudaMemcpy(all.data(), ctx->dump.p, n * sizeof(vxp_candidate), cudaMemcpyDeviceToHost));
+    uint32_t P = 0;
+    CK(cudaMemcpy(&P, ctx->frame.p + 1, sizeof(P), cudaMemcpyDeviceToHost));
+    std::vector<PairInfo> pi(P);
+    if (P) CK(cudaMemcpy(pi.data(), ctx->pinfo.p, P * sizeof(PairInfo), cudaMemcpyDeviceToHost));
+    uint32_t k = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t p = all[i].pair_index;
+        if (p < P && (pi[p].flags & PF_CACHE) && pi[p].hit == 1u) continue;
+        if (out && k < cap) out[k] = all[i];
+        ++k;
+    }
+    *n_out = k;
     return VXP_OK;
 }
 
@@ -1041,6 +1080,16 @@ int vxp_last_step_ms(vxp_ctx* ctx, float out[3]) {
     return VXP_OK;
 }
 
+// Phase boundaries of the last step, ns since its start (diagnostics).
+int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n) {
+    if (!ctx || !out) return VXP_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long t[TS_N];
+    CK(cudaMemcpy(t, ctx->ts.p, sizeof(t), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n && i < TS_N; ++i) out[i] = t[i] >= t[0] ? (uint64_t)(t[i] - t[0]) : 0u;
+    return VXP_OK;
+}
+
 // Extensions beyond the reference seams (declared in vxp.h).
 int vxp_synchronize(vxp_ctx* ctx) {
     if (!ctx) return VXP_ERR_ARG;
@@ -1050,6 +1099,13 @@ int vxp_synchronize(vxp_ctx* ctx) {
 int vxp_set_launch_mode(vxp_ctx* ctx, int mode) {
     if (!ctx || mode < -1 || mode > 1) return VXP_ERR_ARG;
     ctx->use_grid = mode;
+    return VXP_OK;
+}
+
+// Tuning: manifolds per solver block in the grid launch.
+int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div) {
+    if (!ctx || div == 0) return VXP_ERR_ARG;
+    ctx->solver_div = div;
     return VXP_OK;
 }
 

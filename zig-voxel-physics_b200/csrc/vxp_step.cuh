@@ -44,6 +44,9 @@ struct BlockGroup {
         __syncthreads();
         return true;
     }
+    // The solver runs on the same CTA.
+    __device__ BlockGroup subgroup(uint32_t) const { return *this; }
+    __device__ bool member() const { return true; }
 };
 
 struct GridBar {
@@ -55,10 +58,16 @@ struct GridGroup {
     GridBar* bar;
     uint32_t* err;
     unsigned long long timeout_ns;
+    uint32_t nb;  // participating blocks: 0 .. nb-1
     __device__ uint32_t rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
-    __device__ uint32_t size() const { return gridDim.x * blockDim.x; }
+    __device__ uint32_t size() const { return nb * blockDim.x; }
     __device__ uint32_t block() const { return blockIdx.x; }
-    __device__ uint32_t nblocks() const { return gridDim.x; }
+    __device__ uint32_t nblocks() const { return nb; }
+    __device__ bool member() const { return blockIdx.x < nb; }
+    // The first k blocks, with their own barrier word (bar + 1): the solver's
+    // colour batches are small, and a barrier over a few blocks costs far less
+    // than one over the whole grid.  The other blocks leave the kernel.
+    __device__ GridGroup subgroup(uint32_t k) const { return GridGroup{bar + 1, err, timeout_ns, k}; }
     // Bounded grid barrier: a waiting block gives up after timeout_ns, sets
     // ERR_TIMEOUT and every later sync() of every block returns false.
     __device__ bool sync() {
@@ -70,7 +79,7 @@ struct GridGroup {
             const unsigned int g = *vgen;
             __threadfence();
             const unsigned int arrived = atomicAdd(&bar->count, 1u);
-            if (arrived == gridDim.x - 1) {
+            if (arrived == nb - 1) {
                 atomicExch(&bar->count, 0u);
                 __threadfence();
                 atomicAdd(&bar->gen, 1u);
@@ -484,6 +493,7 @@ __device__ bool phase_pairs(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
         pi.flags = fl;
         pi.voxels_checked = 0;
         pi.candidates = 0;
+        pi.hit = 0u;
         pi.cache_slot = 0xFFFFFFFFu;
         w.flag[p] = (fl & PF_CARRY) ? 0u : 1u;
     }
@@ -546,98 +556,138 @@ __device__ bool phase_pairs(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
     }
     tested = warp_sum(tested);
     if ((threadIdx.x & 31) == 0 && tested) atomicAdd(&w.ctr[C_PAIRS_TESTED], tested);
-    return g.sync();
+    if (!g.sync()) return false;
+    if (w.cfg.use_cache) {
+        // pairs consulting the cache, in pair order, for the replay warp
+        uint32_t nc = 0;
+        if (!group_scan(
+                g, P, [&](uint32_t i) { return (w.pinfo[i].flags & PF_CACHE) ? 1u : 0u; },
+                [&](uint32_t i, uint32_t pre) {
+                    if (w.pinfo[i].flags & PF_CACHE) w.clist[pre] = i;
+                },
+                w.scan, &nc))
+            return false;
+        if (g.rank() == 0) w.ctr[C_NCACHE] = nc;
+        return g.sync();
+    }
+    return true;
 }
 
 // ---------------------------------------------------------------------------
-// Phase: brick-pair cache replay (one warp, pairs in order)
+// Brick-pair cache replay (BrickPairCache.get / put, narrow_phase.zig:228-302)
 // ---------------------------------------------------------------------------
-template <class G>
-__device__ bool phase_cache(G& g, WorldDev& w) {
-    if (w.cfg.use_cache && g.rank() < 32u) {
-        const uint32_t lane = threadIdx.x & 31;
-        const unsigned long long frame = w.cframe[0];
-        const uint32_t cap = w.cache_cap;
-        const uint32_t maxp = cap < 16u ? cap : 16u;
-        uint32_t hits = 0, misses = 0, evictions = 0;
-        for (uint32_t base = 0; base < w.n_pairs; base += 32u) {
-            const uint32_t p0 = base + lane;
-            const bool is_c = p0 < w.n_pairs && (w.pinfo[p0].flags & PF_CACHE) && !(w.pinfo[p0].flags & PF_NOCOLL);
-            uint32_t m = __ballot_sync(0xffffffffu, is_c);
-            while (m) {
-                const uint32_t bit = __ffs(m) - 1;
-                m &= m - 1;
-                const uint32_t p = base + bit;
-                PairInfo& pi = w.pinfo[p];
-                const uint32_t ka = pi.key_a, kb = pi.key_b;
-                const unsigned long long th = pi.th;
-                const uint32_t start = (uint32_t)(cache_key_hash(ka, kb, th) % (unsigned long long)cap);
-                const uint32_t slot = (start + lane) % cap;
-                bool valid = false, match = false;
-                unsigned long long lu = ~0ull;
-                if (lane < maxp) {
-                    const volatile CacheKeyRec* e = &w.ckey[slot];
-                    valid = e->valid != 0u;
-                    match = valid && e->a == ka && e->b == kb && e->th == th;
-                    lu = e->last_used;
-                }
-                const uint32_t inv_m = __ballot_sync(0xffffffffu, lane < maxp && !valid);
-                const uint32_t mat_m = __ballot_sync(0xffffffffu, match);
-                const uint32_t fi = inv_m ? (uint32_t)(__ffs(inv_m) - 1) : 32u;
-                const uint32_t fm = mat_m ? (uint32_t)(__ffs(mat_m) - 1) : 32u;
-                uint32_t target;
-                bool hit = false;
-                if (fm < fi) {
-                    hit = true;
-                    target = (start + fm) % cap;
-                } else if (fi < 32u) {
-                    target = (start + fi) % cap;
-                } else {
-                    // evict the first least-recently-used entry of the window
-                    unsigned long long best = lane < maxp ? lu : ~0ull;
-                    uint32_t bl = lane < maxp ? lane : 32u;
-#pragma unroll
-                    for (int d = 16; d > 0; d >>= 1) {
-                        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, best, d);
-                        const uint32_t ol = __shfl_xor_sync(0xffffffffu, bl, d);
-                        if (ob < best || (ob == best && ol < bl)) {
-                            best = ob;
-                            bl = ol;
-                        }
-                    }
-                    target = (start + bl) % cap;
-                    ++evictions;
-                }
-                if (lane == 0) {
-                    if (hit) {
-                        w.ckey[target].last_used = frame;
-                        pi.flags |= PF_HIT;
-                        ++hits;
-                    } else {
-                        CacheKeyRec k;
-                        k.a = ka;
-                        k.b = kb;
-                        k.th = th;
-                        k.last_used = frame;
-                        k.valid = 1u;
-                        k._pad = 0u;
-                        w.ckey[target] = k;
-                        w.cwriter[target] = p;
-                        pi.flags |= PF_DETECT;
-                        ++misses;
-                    }
-                    pi.cache_slot = target;
-                }
-                __syncwarp();
-            }
+// The hit / miss decision of every cache lookup depends only on the keys and
+// on the order of the lookups, not on any contact value: a lookup is a get
+// (probe at most 16 slots from hash % capacity: stop at an empty slot = miss
+// or at the key = hit, which refreshes last_used) and, after a miss, a put
+// (the first empty slot of the window, else evict its least recently used
+// entry).  One warp replays the keys of this step in pair order on a
+// shared-memory copy of the table, 16 lanes probing a window at once, while
+// the other warps already detect every cache-consulting pair; a hit later
+// discards that detection and replays the cached contacts instead.  Values
+// are written after detection (phase_finalize), the last writer of a slot
+// winning, as the sequential puts would leave them.
+__device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t cap = w.cache_cap;
+    const uint32_t maxp = cap < 16u ? cap : 16u;
+    const uint32_t frame = (uint32_t)w.cframe[0];
+    const uint32_t n = w.ctr[C_NCACHE];
+    for (uint32_t i = lane; i < cap; i += 32u) {
+        const CacheKeyRec k = w.ckey[i];
+        t.ab[i] = make_uint2(k.a, k.b);
+        t.th[i] = k.th;
+        t.lu[i] = k.valid ? (uint32_t)k.last_used : 0u;
+    }
+    __syncwarp();
+    uint32_t hits = 0, misses = 0, evictions = 0;
+    for (uint32_t k0 = 0; k0 < n; k0 += 32u) {
+        uint32_t my_p = 0, my_a = 0, my_b = 0;
+        unsigned long long my_th = 0;
+        if (k0 + lane < n) {
+            my_p = w.clist[k0 + lane];
+            const PairInfo& pi = w.pinfo[my_p];
+            my_a = pi.key_a;
+            my_b = pi.key_b;
+            my_th = pi.th;
         }
-        if (lane == 0) {
-            w.ctr[C_CACHE_HITS] += hits;
-            w.ctr[C_CACHE_MISSES] += misses;
-            w.ctr[C_CACHE_EVICTIONS] += evictions;
+        const uint32_t cnt = min(32u, n - k0);
+        for (uint32_t j = 0; j < cnt; ++j) {
+            const uint32_t p = __shfl_sync(0xffffffffu, my_p, j);
+            const uint32_t ka = __shfl_sync(0xffffffffu, my_a, j), kb = __shfl_sync(0xffffffffu, my_b, j);
+            const unsigned long long th = __shfl_sync(0xffffffffu, my_th, j);
+            const uint32_t start = (uint32_t)(cache_key_hash(ka, kb, th) % (unsigned long long)cap);
+            uint32_t slot = start + lane;
+            if (slot >= cap) slot -= cap;
+            bool valid = false, match = false;
+            uint32_t lu = 0xFFFFFFFFu;
+            if (lane < maxp) {
+                lu = t.lu[slot];
+                valid = lu != 0u;
+                match = valid && t.ab[slot].x == ka && t.ab[slot].y == kb && t.th[slot] == th;
+            }
+            const uint32_t inv_m = __ballot_sync(0xffffffffu, lane < maxp && !valid);
+            const uint32_t mat_m = __ballot_sync(0xffffffffu, match);
+            const uint32_t fi = inv_m ? (uint32_t)(__ffs(inv_m) - 1) : 32u;
+            const uint32_t fm = mat_m ? (uint32_t)(__ffs(mat_m) - 1) : 32u;
+            uint32_t tl;
+            bool hit = false;
+            if (fm < fi) {
+                hit = true;
+                tl = fm;
+            } else if (fi < 32u) {
+                tl = fi;
+            } else {
+                // first least-recently-used entry of the window
+                uint32_t best = lane < maxp ? lu : 0xFFFFFFFFu;
+                uint32_t bl = lane < maxp ? lane : 32u;
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) {
+                    const uint32_t ob = __shfl_xor_sync(0xffffffffu, best, d);
+                    const uint32_t ol = __shfl_xor_sync(0xffffffffu, bl, d);
+                    if (ob < best || (ob == best && ol < bl)) {
+                        best = ob;
+                        bl = ol;
+                    }
+                }
+                tl = bl;
+                ++evictions;
+            }
+            uint32_t target = start + tl;
+            if (target >= cap) target -= cap;
+            if (lane == 0) {
+                PairInfo& pi = w.pinfo[p];
+                t.lu[target] = frame;
+                if (hit) {
+                    pi.hit = 1u;
+                    ++hits;
+                } else {
+                    t.ab[target] = make_uint2(ka, kb);
+                    t.th[target] = th;
+                    w.cwriter[target] = p;
+                    pi.hit = 2u;
+                    ++misses;
+                }
+                pi.cache_slot = target;
+            }
+            __syncwarp();
         }
     }
-    return g.sync();
+    for (uint32_t i = lane; i < cap; i += 32u) {
+        CacheKeyRec k;
+        k.a = t.ab[i].x;
+        k.b = t.ab[i].y;
+        k.th = t.th[i];
+        k.last_used = t.lu[i];
+        k.valid = t.lu[i] != 0u ? 1u : 0u;
+        k._pad = 0u;
+        w.ckey[i] = k;
+    }
+    if (lane == 0) {
+        w.ctr[C_CACHE_HITS] += hits;
+        w.ctr[C_CACHE_MISSES] += misses;
+        w.ctr[C_CACHE_EVICTIONS] += evictions;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -962,16 +1012,19 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
 }
 
 template <class G>
-__device__ bool phase_probe(G& g, WorldDev& w, const ColliderSet& cs, uint32_t cur, WarpManifold* warp_sm) {
+__device__ bool phase_probe(G& g, WorldDev& w, const ColliderSet& cs, uint32_t cur, WarpManifold* warp_sm,
+                            const CacheSmem& csm) {
     const uint32_t lane = threadIdx.x & 31;
     WarpManifold& sm = warp_sm[threadIdx.x >> 5];
+    // one warp replays the cache lookups, the others start detecting at once
+    if (w.cfg.use_cache && g.rank() < 32u) cache_replay(w, csm);
     for (;;) {
         uint32_t p = 0;
         if (lane == 0) p = atomicAdd(&w.ctr[C_WORK], 1u);
         p = __shfl_sync(0xffffffffu, p, 0);
         if (p >= w.n_pairs) break;
         const uint32_t fl = w.pinfo[p].flags;
-        if ((fl & PF_DETECT) && (fl & PF_REGION)) probe_pair(w, cs, cur, p, sm);
+        if ((fl & (PF_DETECT | PF_CACHE)) && (fl & PF_REGION)) probe_pair(w, cs, cur, p, sm);
     }
     return g.sync();
 }
@@ -1008,7 +1061,7 @@ __device__ bool phase_finalize(G& g, WorldDev& w, uint32_t cur, uint32_t prev) {
             else m.n = 0u;
         } else if (!(fl & PF_TESTED) || (fl & (PF_NOCOLL | PF_SEPARATED))) {
             m.n = 0u;
-        } else if (fl & PF_HIT) {
+        } else if ((fl & PF_CACHE) && pi.hit == 1u) {
             const CacheValRec& v = w.cval[pi.cache_slot];
             if (v.has_collision) {
                 const DBodyProp& a = w.prop[pi.ia];
@@ -1042,7 +1095,7 @@ __device__ bool phase_finalize(G& g, WorldDev& w, uint32_t cur, uint32_t prev) {
             } else {
                 m.n = 0u;
             }
-        } else if (fl & PF_DETECT) {
+        } else if ((fl & PF_DETECT) || (fl & PF_CACHE)) {
             if (!(fl & PF_REGION)) {
                 const DBodyProp& a = w.prop[pi.ia];
                 const DBodyProp& b = w.prop[pi.ib];
@@ -1086,7 +1139,7 @@ __device__ bool phase_finalize(G& g, WorldDev& w, uint32_t cur, uint32_t prev) {
     if (w.cfg.use_cache) {
         for (uint32_t p = g.rank(); p < w.n_pairs; p += g.size()) {
             const PairInfo& pi = w.pinfo[p];
-            if (!(pi.flags & PF_CACHE) || (pi.flags & PF_HIT) || !(pi.flags & PF_DETECT)) continue;
+            if (!(pi.flags & PF_CACHE) || pi.hit != 2u) continue;
             if (pi.flags & (PF_NOCOLL | PF_SEPARATED)) continue;
             const uint32_t s = pi.cache_slot;
             if (s == 0xFFFFFFFFu || w.cwriter[s] != p) continue;
@@ -1487,59 +1540,86 @@ __device__ void warm_manifold(WorldDev& w, uint32_t pos, float scale) {
     store_bv(w, cmv.y, b);
 }
 
+// The fields of one constraint point a velocity sweep reads.
+struct PtV {
+    F3 pt, n, ra, rb, t1, t2;
+    float nm, bias, tm0, tm1, ni, ti0, ti1;
+};
+__device__ __forceinline__ PtV load_ptv(const WorldDev& w, uint32_t i, uint32_t pos) {
+    PtV r;
+    r.pt = ld3(w, CP_PX, i, pos);
+    r.n = ld3(w, CP_NX, i, pos);
+    r.ra = ld3(w, CP_RAX, i, pos);
+    r.rb = ld3(w, CP_RBX, i, pos);
+    r.t1 = ld3(w, CP_T1X, i, pos);
+    r.t2 = ld3(w, CP_T2X, i, pos);
+    r.nm = w.cp[cpi(w, CP_NM, i, pos)];
+    r.bias = w.cp[cpi(w, CP_BIAS, i, pos)];
+    r.tm0 = w.cp[cpi(w, CP_TM0, i, pos)];
+    r.tm1 = w.cp[cpi(w, CP_TM1, i, pos)];
+    r.ni = w.cp[cpi(w, CP_NI, i, pos)];
+    r.ti0 = w.cp[cpi(w, CP_TI0, i, pos)];
+    r.ti1 = w.cp[cpi(w, CP_TI1, i, pos)];
+    return r;
+}
+
 // solveVelocityConstraints + solveFriction for one manifold (solver.zig:732-838).
+// Points run in slot order (Gauss-Seidel inside the manifold); the next
+// point's fields are loaded before this point's results are stored, so the
+// loads overlap the dependent arithmetic.
 __device__ void velocity_manifold(WorldDev& w, uint32_t pos, const Soft& soft, bool use_bias) {
     const uint4 cmv = w.cm[pos];
     const float fr = w.cfr[pos].x;
     BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
-    for (uint32_t i = 0; i < cmv.z; ++i) {
-        const F3 pt = ld3(w, CP_PX, i, pos);
-        const F3 n = ld3(w, CP_NX, i, pos);
-        const F3 ra = ld3(w, CP_RAX, i, pos), rb = ld3(w, CP_RBX, i, pos);
-        const float nm = w.cp[cpi(w, CP_NM, i, pos)];
-        float ni = w.cp[cpi(w, CP_NI, i, pos)];
-        const F3 rv = point_vel(b, pt) - point_vel(a, pt);
-        const float vn = dot3(rv, n);
+    const uint32_t n = cmv.z;
+    if (n == 0u) return;
+    PtV c = load_ptv(w, 0, pos);
+    for (uint32_t i = 0; i < n; ++i) {
+        PtV nx;
+        if (i + 1u < n) nx = load_ptv(w, i + 1u, pos);
+        const F3 rv = point_vel(b, c.pt) - point_vel(a, c.pt);
+        const float vn = dot3(rv, c.n);
         float imp;
         if (use_bias)
-            imp = -soft.mass_coeff * nm * (vn + w.cp[cpi(w, CP_BIAS, i, pos)]) - soft.impulse_coeff * ni;
+            imp = -soft.mass_coeff * c.nm * (vn + c.bias) - soft.impulse_coeff * c.ni;
         else
-            imp = -nm * vn;
-        const float nn = fmaxf(ni + imp, 0.0f);
-        imp = nn - ni;
-        ni = nn;
-        w.cp[cpi(w, CP_NI, i, pos)] = ni;
-        const F3 P = n * imp;
-        apply_impulse(a, -P, ra);
-        apply_impulse(b, P, rb);
+            imp = -c.nm * vn;
+        const float nn = fmaxf(c.ni + imp, 0.0f);
+        imp = nn - c.ni;
+        const float ni = nn;
+        const F3 P = c.n * imp;
+        apply_impulse(a, -P, c.ra);
+        apply_impulse(b, P, c.rb);
+        float ti0 = c.ti0, ti1 = c.ti1;
         if (w.cfg.friction_on && fr > 0.0f) {
-            const F3 t1 = ld3(w, CP_T1X, i, pos), t2 = ld3(w, CP_T2X, i, pos);
             const float mf = fr * ni;
             {
-                const F3 rv1 = point_vel(b, pt) - point_vel(a, pt);
-                const float vt1 = dot3(rv1, t1);
-                float f1 = -w.cp[cpi(w, CP_TM0, i, pos)] * vt1;
-                const float o1 = w.cp[cpi(w, CP_TI0, i, pos)];
-                const float t = clampf_ref(o1 + f1, -mf, mf);
-                w.cp[cpi(w, CP_TI0, i, pos)] = t;
-                f1 = t - o1;
-                const F3 I1 = t1 * f1;
-                apply_impulse(a, -I1, ra);
-                apply_impulse(b, I1, rb);
+                const F3 rv1 = point_vel(b, c.pt) - point_vel(a, c.pt);
+                const float vt1 = dot3(rv1, c.t1);
+                float f1 = -c.tm0 * vt1;
+                const float o1 = ti0;
+                ti0 = clampf_ref(o1 + f1, -mf, mf);
+                f1 = ti0 - o1;
+                const F3 I1 = c.t1 * f1;
+                apply_impulse(a, -I1, c.ra);
+                apply_impulse(b, I1, c.rb);
             }
             {
-                const F3 rv2 = point_vel(b, pt) - point_vel(a, pt);
-                const float vt2 = dot3(rv2, t2);
-                float f2 = -w.cp[cpi(w, CP_TM1, i, pos)] * vt2;
-                const float o2 = w.cp[cpi(w, CP_TI1, i, pos)];
-                const float t = clampf_ref(o2 + f2, -mf, mf);
-                w.cp[cpi(w, CP_TI1, i, pos)] = t;
-                f2 = t - o2;
-                const F3 I2 = t2 * f2;
-                apply_impulse(a, -I2, ra);
-                apply_impulse(b, I2, rb);
+                const F3 rv2 = point_vel(b, c.pt) - point_vel(a, c.pt);
+                const float vt2 = dot3(rv2, c.t2);
+                float f2 = -c.tm1 * vt2;
+                const float o2 = ti1;
+                ti1 = clampf_ref(o2 + f2, -mf, mf);
+                f2 = ti1 - o2;
+                const F3 I2 = c.t2 * f2;
+                apply_impulse(a, -I2, c.ra);
+                apply_impulse(b, I2, c.rb);
             }
         }
+        w.cp[cpi(w, CP_NI, i, pos)] = ni;
+        w.cp[cpi(w, CP_TI0, i, pos)] = ti0;
+        w.cp[cpi(w, CP_TI1, i, pos)] = ti1;
+        if (i + 1u < n) c = nx;
     }
     store_bv(w, cmv.x, a);
     store_bv(w, cmv.y, b);
@@ -1786,9 +1866,15 @@ __device__ bool phase_store(G& g, WorldDev& w, uint32_t cur, uint32_t M, bool so
 // One whole step (VoxelPhysicsSystem.step with the pairs given)
 // ---------------------------------------------------------------------------
 template <class G>
-__device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifold* warp_sm) {
+__device__ __forceinline__ void stamp(G& g, WorldDev& w, uint32_t slot) {
+    if (g.rank() == 0 && w.ts) w.ts[slot] = global_ns();
+}
+
+template <class G>
+__device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifold* warp_sm, const CacheSmem& csm) {
     const uint32_t ph = w.cfg.phases;
     const uint32_t f0 = *(volatile uint32_t*)&w.frame[0];
+    stamp(g, w, TS_START);
     w.n_pairs = *w.n_pairs_dev;
     if ((ph & PH_NARROW) && w.n_pairs > w.pair_cap) {
         // the pair list did not fit: leave every state untouched, the host
@@ -1798,6 +1884,7 @@ __device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifol
     }
     bool skipped = false;
     if (!phase_begin(g, w, (ph & PH_SKIP_TEST) != 0u, &skipped)) return;
+    stamp(g, w, TS_BEGIN);
     if (skipped) return;
     // ContactManager.beginFrame (narrow_phase.zig:1003-1008): the previous
     // "current" manifolds become "previous"
@@ -1808,18 +1895,30 @@ __device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifol
             w.frame[1] = w.n_pairs;
         }
         if (!phase_pairs(g, w, cs, cur)) return;
-        if (!phase_cache(g, w)) return;
-        if (!phase_probe(g, w, cs, cur, warp_sm)) return;
+        stamp(g, w, TS_PAIRS);
+        stamp(g, w, TS_CACHE);
+        if (!phase_probe(g, w, cs, cur, warp_sm, csm)) return;
+        stamp(g, w, TS_PROBE);
         if (!phase_finalize(g, w, cur, prev)) return;
         if (!g.sync()) return;
+        stamp(g, w, TS_FINALIZE);
     }
     if (ph & PH_SOLVE) {
+        // The solver's work per colour batch is a few hundred manifolds: run it
+        // on k blocks (one per 512 manifolds, at least 2) with a cheaper barrier.
+        const uint32_t nman = (ph & PH_NARROW) ? *(volatile uint32_t*)&w.ctr[C_MANIFOLDS] : w.n_pairs;
+        const uint32_t want = max(2u, (nman + w.cfg.solver_div - 1u) / w.cfg.solver_div);
+        G s = g.subgroup(min(want, g.nblocks()));
+        if (!s.member()) return;
         uint32_t M = 0, ncol = 0;
-        if (!phase_constraints(g, w, cur, &M, &ncol)) return;
+        if (!phase_constraints(s, w, cur, &M, &ncol)) return;
+        stamp(s, w, TS_CONSTRAINTS);
         const bool solved = w.cfg.dt > 0.0f && w.n_bodies > 0u;
-        if (solved && !phase_solve(g, w, M, ncol)) return;
-        if (!g.sync()) return;
-        if (!phase_store(g, w, cur, M, solved)) return;
+        if (solved && !phase_solve(s, w, M, ncol)) return;
+        if (!s.sync()) return;
+        stamp(s, w, TS_SOLVE);
+        if (!phase_store(s, w, cur, M, solved)) return;
+        stamp(s, w, TS_END);
     }
 }
 

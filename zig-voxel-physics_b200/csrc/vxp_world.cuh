@@ -12,7 +12,7 @@
 // Phase map (reference file:line → phase)
 //   system.narrowPhase filter        system.zig:586-655      phase_pairs
 //   NarrowPhase.processPair head     narrow_phase.zig:1414-1469 phase_pairs
-//   BrickPairCache.get/put           narrow_phase.zig:228-302 phase_cache
+//   BrickPairCache.get/put           narrow_phase.zig:228-302 cache_replay (in phase_probe)
 //   detectVoxelCollisions            narrow_phase.zig:722-857 phase_probe
 //   ContactManifold.addContact       narrow_phase.zig:451-481 phase_probe (replay)
 //   ContactManager.addManifold       narrow_phase.zig:1011-1059 phase_finalize
@@ -62,7 +62,7 @@ struct DBodyProp {
     uint32_t id, type, collider, sleeping;
 };
 
-// Flags of a pair after phase_pairs / phase_cache.
+// Flags of a pair after phase_pairs.
 enum : uint32_t {
     PF_INVALID = 1u << 0,   // a body id not found
     PF_CARRY = 1u << 1,     // both sleeping: previous manifold carried over
@@ -70,7 +70,6 @@ enum : uint32_t {
     PF_NOCOLL = 1u << 3,    // a body without collider
     PF_SEPARATED = 1u << 4, // SAT early-out
     PF_CACHE = 1u << 5,     // brick-pair cache consulted
-    PF_HIT = 1u << 6,       // cache hit
     PF_DETECT = 1u << 7,    // detectVoxelCollisions runs
     PF_REGION = 1u << 8,    // overlap region non-empty
     PF_TESTED = 1u << 9,    // processPair was called
@@ -79,6 +78,7 @@ enum : uint32_t {
 struct PairInfo {
     uint32_t ia, ib;
     uint32_t flags;
+    uint32_t hit;           // brick-pair cache: 0 not consulted, 1 hit, 2 miss
     uint32_t cache_slot;    // hit: entry read; miss: entry written
     int32_t rmin[3], rmax[3];
     uint32_t voxels_checked;
@@ -117,6 +117,16 @@ struct HashSlot {            // pairKey -> manifold index
     uint32_t idx, _pad;
 };
 
+// The brick-pair cache table while one warp replays this step's lookups:
+// shared-memory arrays of cache_cap entries (key ids, transform hash,
+// last-used frame with 0 = empty slot).
+constexpr uint32_t kMaxCacheSmem = 4096;
+struct CacheSmem {
+    uint2* ab;
+    unsigned long long* th;
+    uint32_t* lu;
+};
+
 // Step configuration (vxp_config distilled).
 struct StepCfg {
     float gravity[3];
@@ -133,6 +143,7 @@ struct StepCfg {
     uint32_t colouring;
     uint32_t dump_candidates;
     uint32_t phases;          // PH_* bits
+    uint32_t solver_div;      // grid launch: solver blocks = manifolds / solver_div
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 
@@ -160,8 +171,13 @@ enum : uint32_t {
     C_DUMP_N,        // candidates dumped
     C_AWAKE,         // dynamic awake bodies seen by the sleep check
     C_BRICKS,        // bricks of A in the overlap region + bricks of B in B's
+    C_NCACHE,        // pairs that consult the brick-pair cache this step
     C_ERROR = 31,    // sticky error bits (not cleared per step)
     C_NCTR = 32
+};
+// Phase boundaries recorded in WorldDev::ts by rank 0 (diagnostics).
+enum : uint32_t {
+    TS_START, TS_BEGIN, TS_PAIRS, TS_CACHE, TS_PROBE, TS_FINALIZE, TS_CONSTRAINTS, TS_SOLVE, TS_END, TS_N = 16
 };
 enum : uint32_t { ERR_TIMEOUT = 1u, ERR_CAP = 2u, ERR_COLOURS = 4u, ERR_OVERFLOW = 8u };
 
@@ -192,6 +208,7 @@ struct WorldDev {
     CacheKeyRec* ckey;
     CacheValRec* cval;
     uint32_t* cwriter;            // last pair writing each slot this frame
+    uint32_t* clist;              // pairs consulting the cache, in pair order
     unsigned long long* cframe;   // cache frame counter
     // constraints
     uint32_t* cons;               // constraint -> pair index (pair order)
@@ -212,6 +229,7 @@ struct WorldDev {
     uint32_t* scan;               // per-block partials for group scans
     uint32_t* flag;               // per-pair scratch flags (n_pairs)
     uint32_t* ctr;                // C_NCTR counters
+    unsigned long long* ts;       // phase timestamps (ns), TS_* slots
     // debug dump
     struct Cand {
         uint32_t pair_index;

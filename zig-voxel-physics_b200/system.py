@@ -169,7 +169,7 @@ class VoxelPhysicsSystem:
             self._check(rc)
         out = np.zeros(n.value, dtype=abi.CANDIDATE_DTYPE)
         self._check(self.lib.vxp_candidates_get(self.ctx, abi.ptr(out), len(out), ctypes.byref(n)))
-        return out
+        return out[: n.value]
 
     def last_step_ms(self) -> float:
         out = np.zeros(3, dtype=np.float32)
