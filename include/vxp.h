@@ -292,6 +292,39 @@ int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div);
  * solve, end]. */
 int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free pair source.  No counterpart in the reference (its broad
+ * phase is a host AABB tree); this is a variant of the device pair source
+ * behind vxp_pairs_from_bodies for callers that cannot let the library
+ * allocate device memory: an engine that runs its physics on a frame thread
+ * where cudaMalloc's implicit device synchronisation is not allowed, or one
+ * whose device memory is all handed out by its own allocator.  It creates no
+ * context and calls no cudaMalloc / cudaFree or other allocating routine.
+ *
+ * All pointers are device memory owned by the caller, for n bodies:
+ *   positions, rotations   n x 4 floats (x, y, z, unused) / (x, y, z, w)
+ *   local_aabbs            n x 8 floats: min x, y, z, unused, max x, y, z,
+ *                          unused; min > max marks a body without collider
+ *   ids                    n body ids, strictly ascending
+ *   body_types             n VXP_BODY_* values
+ *   out                    room for cap pairs; *count (device) receives the
+ *                          total, which may exceed cap (the list is cut)
+ * The result equals vxp_pairs_from_bodies for the same bodies and margin.
+ * Work is queued on `stream` (a cudaStream_t, or NULL) and is not waited for.
+ *
+ * Its scratch is one static device array sized for 16384 bodies (about
+ * 640 KiB), held by every GPU that loads the library until the process
+ * exits; n > 16384 returns VXP_ERR_CAP.  The first call on a device looks up
+ * the array's device address (once, with that device current); make that
+ * first call before capturing any stream.  Every call uses the same array:
+ * calls whose work overlaps on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller.  No scratch value carries over
+ * from one call to the next.
+ * ------------------------------------------------------------------------- */
+int vxp_pairs_noalloc(const float* positions, const float* rotations, const float* local_aabbs,
+                      const uint32_t* ids, const uint32_t* body_types, uint32_t n, float margin,
+                      vxp_pair* out, uint32_t cap, uint32_t* count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -216,6 +216,7 @@ SIGNATURES = {
     "vxp_set_launch_mode": (_I, [_VP, _I]),
     "vxp_phase_times": (_I, [_VP, _VP, _U32]),
     "vxp_set_solver_blocks_divisor": (_I, [_VP, _U32]),
+    "vxp_pairs_noalloc": (_I, [_VP, _VP, _VP, _VP, _VP, _U32, _F, _VP, _U32, _VP, _VP]),
 }
 
 _LIB = None

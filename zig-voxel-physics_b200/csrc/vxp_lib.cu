@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -632,6 +633,139 @@ int compute_device_pairs(vxp_ctx* ctx, float margin, bool wait_count, uint32_t* 
 }  // namespace
 
 // ===========================================================================
+// Allocation-free pair source (vxp_pairs_noalloc)
+// ===========================================================================
+// Some callers cannot let a library allocate device memory: an engine that
+// runs its physics step on a frame thread where cudaMalloc's implicit device
+// synchronisation would blow the frame budget, or one whose device memory is
+// all handed out by its own allocator.  vxp_pairs_noalloc lets them run the
+// broad-phase pair source on their own buffers: its only scratch (world
+// AABBs, per-row pair counts and offsets, the total) is this file-scope
+// array, sized for kNoAllocMaxBodies bodies, which every GPU that loads the
+// library holds until the process exits.
+constexpr uint32_t kNoAllocMaxBodies = 16384;
+constexpr size_t kNoAllocScratchBytes = (size_t)kNoAllocMaxBodies * (2 * sizeof(float4) + 2 * sizeof(uint32_t)) + 256;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocScratch {
+    float4* mn;
+    float4* mx;
+    uint32_t* counts;
+    uint32_t* offsets;
+    uint32_t* total;
+};
+__host__ __device__ inline NoAllocScratch noalloc_layout(unsigned char* base) {
+    NoAllocScratch s;
+    s.mn = reinterpret_cast<float4*>(base);
+    s.mx = s.mn + kNoAllocMaxBodies;
+    s.counts = reinterpret_cast<uint32_t*>(s.mx + kNoAllocMaxBodies);
+    s.offsets = s.counts + kNoAllocMaxBodies;
+    s.total = s.offsets + kNoAllocMaxBodies;
+    return s;
+}
+
+// World AABB of each body's local AABB (AABB.transform, math.zig:686-693)
+// inflated by margin; an empty local AABB (min > max) stands for a body
+// without collider, whose box is its position.
+__global__ void k_noalloc_aabbs(const float4* pos, const float4* rot, const float4* laabb, uint32_t n, float margin,
+                                unsigned char* base) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const NoAllocScratch s = noalloc_layout(base);
+    const F3 x = f3of(pos[i]);
+    const Qt q = qof(rot[i]);
+    const float4 lo4 = laabb[2 * i], hi4 = laabb[2 * i + 1];
+    F3 lo, hi;
+    if (lo4.x <= hi4.x && lo4.y <= hi4.y && lo4.z <= hi4.z) {
+        const float inf = __int_as_float(0x7f800000);
+        lo = F3{inf, inf, inf};
+        hi = F3{-inf, -inf, -inf};
+        for (int k = 0; k < 8; ++k) {
+            const F3 corner{(k & 1) ? hi4.x : lo4.x, (k & 2) ? hi4.y : lo4.y, (k & 4) ? hi4.z : lo4.z};
+            const F3 p = transform_point(x, q, corner);
+            lo = min3(lo, p);
+            hi = max3(hi, p);
+        }
+    } else {
+        lo = x;
+        hi = x;
+    }
+    lo = lo - F3{margin, margin, margin};
+    hi = hi + F3{margin, margin, margin};
+    s.mn[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    s.mx[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
+}
+
+// Same sweep as k_pairs over caller arrays (ids ascending, so row order is id
+// order).  Pass 0 counts per row, pass 1 writes at the scanned offsets.
+__global__ void k_noalloc_pairs(const uint32_t* ids, const uint32_t* types, uint32_t n, unsigned char* base,
+                                uint2* out, uint32_t cap, int pass) {
+    const uint32_t sidx = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    if (sidx >= n) return;
+    const NoAllocScratch s = noalloc_layout(base);
+    const float4 a0 = s.mn[sidx], a1 = s.mx[sidx];
+    const bool si = types[sidx] == 0u;
+    const uint32_t id_s = ids[sidx];
+    uint32_t o = pass ? s.offsets[sidx] : 0u;
+    uint32_t cnt = 0;
+    for (uint32_t t0 = sidx + 1; t0 < n; t0 += 32u) {
+        const uint32_t t = t0 + lane;
+        bool hit = false;
+        if (t < n && !(si && types[t] == 0u)) {
+            const float4 b0 = s.mn[t], b1 = s.mx[t];
+            hit = a0.x <= b1.x && a1.x >= b0.x && a0.y <= b1.y && a1.y >= b0.y && a0.z <= b1.z && a1.z >= b0.z;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (pass && hit) {
+            const uint32_t slot = o + __popc(m & ((1u << lane) - 1u));
+            if (slot < cap) out[slot] = make_uint2(id_s, ids[t]);
+        }
+        o += __popc(m);
+        cnt += __popc(m);
+    }
+    if (!pass && lane == 0) s.counts[sidx] = cnt;
+}
+
+__global__ void __launch_bounds__(1024) k_noalloc_scan(uint32_t n, unsigned char* base, uint32_t* count_out) {
+    const NoAllocScratch s = noalloc_layout(base);
+    uint32_t carry = 0;
+    for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
+        const uint32_t i = t0 + threadIdx.x;
+        const uint32_t v = i < n ? s.counts[i] : 0u;
+        uint32_t tile;
+        const uint32_t ex = block_excl_scan(v, &tile);
+        if (i < n) s.offsets[i] = carry + ex;
+        carry += tile;
+    }
+    if (threadIdx.x == 0) {
+        *s.total = carry;
+        *count_out = carry;
+    }
+}
+
+namespace {
+// Device address of g_noalloc_scratch, looked up once per device with that
+// device current (a host-side mention of the array names a host stand-in,
+// not device memory).
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[256] = {};
+
+int noalloc_scratch_for_current_device(unsigned char** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return VXP_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return VXP_ERR_CUDA;
+        g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return VXP_OK;
+}
+}  // namespace
+
+// ===========================================================================
 // C ABI
 // ===========================================================================
 extern "C" {
@@ -1078,6 +1212,29 @@ int vxp_last_step_ms(vxp_ctx* ctx, float out[3]) {
     out[1] = b;
     out[2] = c;
     return VXP_OK;
+}
+
+// See the allocation-free section above and include/vxp.h.
+int vxp_pairs_noalloc(const float* positions, const float* rotations, const float* local_aabbs, const uint32_t* ids,
+                      const uint32_t* body_types, uint32_t n, float margin, vxp_pair* out, uint32_t cap,
+                      uint32_t* count, void* stream) {
+    if (n > kNoAllocMaxBodies) return VXP_ERR_CAP;
+    if (!count || (n && (!positions || !rotations || !local_aabbs || !ids || !body_types)) || (cap && !out))
+        return VXP_ERR_ARG;
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_scratch_for_current_device(&base)) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        return cudaMemsetAsync(count, 0, sizeof(uint32_t), st) == cudaSuccess ? VXP_OK : VXP_ERR_CUDA;
+    }
+    const uint32_t tb = 256, nb = (n + tb - 1) / tb, wb = (n * 32u + tb - 1) / tb;
+    k_noalloc_aabbs<<<nb, tb, 0, st>>>(reinterpret_cast<const float4*>(positions),
+                                       reinterpret_cast<const float4*>(rotations),
+                                       reinterpret_cast<const float4*>(local_aabbs), n, margin, base);
+    k_noalloc_pairs<<<wb, tb, 0, st>>>(ids, body_types, n, base, nullptr, 0, 0);
+    k_noalloc_scan<<<1, 1024, 0, st>>>(n, base, count);
+    k_noalloc_pairs<<<wb, tb, 0, st>>>(ids, body_types, n, base, reinterpret_cast<uint2*>(out), cap, 1);
+    return cudaGetLastError() == cudaSuccess ? VXP_OK : VXP_ERR_CUDA;
 }
 
 // Phase boundaries of the last step, ns since its start (diagnostics).
