@@ -293,6 +293,46 @@ int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div);
 int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n);
 
 /* ---------------------------------------------------------------------------
+ * Batched worlds.  No counterpart in the reference (one VoxelPhysicsSystem
+ * steps one world); a batch steps many independent worlds at once, each one
+ * exactly as vxp_step_device_pairs would, in one kernel launch per step: one
+ * CTA per world runs that world's pair source, narrow phase and solver.  The
+ * launch is captured once in a CUDA graph and replayed every step.  Worlds
+ * share the batch's colliders and configuration; their bodies' collider_id
+ * values refer to vxp_batch_collider_upload ids.
+ * ------------------------------------------------------------------------- */
+typedef struct vxp_batch vxp_batch;
+
+int vxp_batch_create(const vxp_config* cfg, int device, uint32_t max_worlds, vxp_batch** out);
+void vxp_batch_destroy(vxp_batch* b);
+int vxp_batch_last_error(const vxp_batch* b, char* buf, size_t n);
+int vxp_batch_collider_upload(vxp_batch* b, uint32_t collider_id, float voxel_size, const vxp_brick* bricks,
+                              uint32_t n_bricks);
+/* (Re)starts world slot `world` with these bodies: empty contact manager and
+ * brick-pair cache.  pair_capacity 0 = 16 x n (grown on demand). */
+int vxp_batch_world_set(vxp_batch* b, uint32_t world, const vxp_body* bodies, uint32_t n, uint32_t pair_capacity);
+/* Empties the slot and frees its device memory. */
+int vxp_batch_world_clear(vxp_batch* b, uint32_t world);
+int vxp_batch_world_get(vxp_batch* b, uint32_t world, vxp_body* bodies, uint32_t n);
+int vxp_batch_world_stats(vxp_batch* b, uint32_t world, vxp_stats* out);
+/* Device bytes held by a world slot (admission accounting). */
+uint64_t vxp_batch_world_bytes(vxp_batch* b, uint32_t world);
+/* Every occupied slot advances n_steps steps of dt (queued, not waited for). */
+int vxp_batch_step(vxp_batch* b, float dt, uint32_t n_steps);
+/* Waits; reports device errors (VXP_ERR_CAP: a world's pair list overflowed
+ * and that world left its step undone; its buffers are grown) and grows the
+ * pair buffers of worlds close to capacity. */
+int vxp_batch_synchronize(vxp_batch* b);
+/* Device ms of the last vxp_batch_step call, and per slot the ms of its CTA
+ * in the last step (0 for empty slots). */
+int vxp_batch_times(vxp_batch* b, float* total_ms, float* world_ms, uint32_t n);
+/* Schedule: CTA size 256 or 512; order 0 = slot order, 1 = longest first. */
+int vxp_batch_set_schedule(vxp_batch* b, uint32_t threads, uint32_t order_mode);
+/* Autotuner: runs trial_steps real steps under each schedule, keeps the
+ * fastest; ms_out[4] = mean step ms of (256,0), (256,1), (512,0), (512,1). */
+int vxp_batch_autotune(vxp_batch* b, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice);
+
+/* ---------------------------------------------------------------------------
  * Allocation-free pair source.  No counterpart in the reference (its broad
  * phase is a host AABB tree); this is a variant of the device pair source
  * behind vxp_pairs_from_bodies for callers that cannot let the library

@@ -1,0 +1,113 @@
+"""Batched worlds: each world of a batch must give exactly the results of the
+same world stepped alone (single-world context, and the CPU oracle), under
+any schedule, with worlds joining and leaving between steps."""
+import numpy as np
+import pytest
+
+import oracle_api as O
+
+pytestmark = pytest.mark.gpu
+
+
+def small_mix(vxp, sizes, seed=7):
+    rng = np.random.default_rng(seed)
+    return [vxp.scenes.world_for_batch(rng, int(n), O.mass_fn, name=f"w{i}") for i, n in enumerate(sizes)]
+
+
+def run_alone(vxp, scene, steps, dt):
+    s = vxp.VoxelPhysicsSystem(substeps=4)
+    s.load_scene(scene)
+    for _ in range(steps):
+        s.step(dt)
+    out = s.get_bodies()
+    s.close()
+    return out
+
+
+def run_oracle(scene, steps, dt):
+    r = O.OracleWorld(substeps=4)
+    r.load_scene(scene)
+    for _ in range(steps):
+        r.step(dt)
+    out = r.get_bodies()
+    r.close()
+    return out
+
+
+def test_batch_equals_alone_and_oracle(vxp):
+    scenes = small_mix(vxp, [8, 30, 90, 17, 60])
+    dt = np.float32(1.0 / 60.0)
+    b = vxp.VoxelWorldBatch(len(scenes), substeps=4)
+    for i, sc in enumerate(scenes):
+        b.load_scene(i, sc, collider_offset=10000 * (i + 1))
+    steps = 80
+    b.step(dt, steps)
+    b.synchronize()
+    for i, sc in enumerate(scenes):
+        got = b.get_world(i)
+        alone = run_alone(vxp, sc, steps, dt)
+        got_cmp = got.copy()
+        got_cmp["collider_id"] -= 10000 * (i + 1)
+        assert got_cmp.tobytes() == alone.tobytes(), f"world {i} differs from the same world alone"
+        if i < 3:
+            ref = run_oracle(sc, steps, dt)
+            assert got_cmp.tobytes() == ref.tobytes(), f"world {i} differs from the oracle"
+    b.close()
+
+
+@pytest.mark.parametrize("threads,order", [(256, 0), (256, 1), (512, 0), (512, 1)])
+def test_schedule_does_not_change_results(vxp, threads, order):
+    scenes = small_mix(vxp, [40, 12, 70], seed=8)
+    dt = np.float32(1.0 / 60.0)
+    b = vxp.VoxelWorldBatch(3, substeps=4)
+    for i, sc in enumerate(scenes):
+        b.load_scene(i, sc, collider_offset=1000 * (i + 1))
+    b.set_schedule(threads, order)
+    b.step(dt, 40)
+    b.synchronize()
+    for i, sc in enumerate(scenes):
+        got = b.get_world(i)
+        got["collider_id"] -= 1000 * (i + 1)
+        assert got.tobytes() == run_alone(vxp, sc, 40, dt).tobytes()
+    b.close()
+
+
+def test_autotune_keeps_results(vxp):
+    scenes = small_mix(vxp, [50, 20, 8, 35], seed=9)
+    dt = np.float32(1.0 / 60.0)
+    b = vxp.VoxelWorldBatch(4, substeps=4)
+    for i, sc in enumerate(scenes):
+        b.load_scene(i, sc, collider_offset=1000 * (i + 1))
+    choice, ms = b.autotune(dt, trial_steps=2)  # 4 x (1 + 2) real steps
+    assert 0 <= choice < 4 and np.all(ms > 0)
+    b.step(dt, 8)
+    b.synchronize()
+    for i, sc in enumerate(scenes):
+        got = b.get_world(i)
+        got["collider_id"] -= 1000 * (i + 1)
+        assert got.tobytes() == run_alone(vxp, sc, 20, dt).tobytes()
+    b.close()
+
+
+def test_worlds_join_and_leave(vxp):
+    """Continuous batching: a slot is emptied and refilled between steps; the
+    new world's result equals the world alone, the others are undisturbed."""
+    scenes = small_mix(vxp, [25, 40, 15, 33], seed=10)
+    dt = np.float32(1.0 / 60.0)
+    b = vxp.VoxelWorldBatch(3, substeps=4)
+    for i in range(3):
+        b.load_scene(i, scenes[i], collider_offset=1000 * (i + 1))
+    b.step(dt, 20)
+    b.synchronize()
+    b.clear_world(1)
+    b.step(dt, 10)  # slot 1 empty
+    b.load_scene(1, scenes[3], collider_offset=5000)
+    b.step(dt, 30)
+    b.synchronize()
+    got0 = b.get_world(0)
+    got0["collider_id"] -= 1000
+    assert got0.tobytes() == run_alone(vxp, scenes[0], 60, dt).tobytes()
+    got1 = b.get_world(1)
+    got1["collider_id"] -= 5000
+    assert got1.tobytes() == run_alone(vxp, scenes[3], 30, dt).tobytes()
+    b.close()

@@ -10,6 +10,6 @@ The directory name is not a Python identifier: import it with
 importlib.import_module("zig-voxel-physics_b200").
 """
 from . import abi, scenes  # noqa: F401
-from .system import VoxelPhysicsSystem, VxpError  # noqa: F401
+from .system import VoxelPhysicsSystem, VoxelWorldBatch, VxpError  # noqa: F401
 
-__all__ = ["abi", "scenes", "VoxelPhysicsSystem", "VxpError"]
+__all__ = ["abi", "scenes", "VoxelPhysicsSystem", "VoxelWorldBatch", "VxpError"]

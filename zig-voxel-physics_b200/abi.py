@@ -217,6 +217,20 @@ SIGNATURES = {
     "vxp_phase_times": (_I, [_VP, _VP, _U32]),
     "vxp_set_solver_blocks_divisor": (_I, [_VP, _U32]),
     "vxp_pairs_noalloc": (_I, [_VP, _VP, _VP, _VP, _VP, _U32, _F, _VP, _U32, _VP, _VP]),
+    "vxp_batch_create": (_I, [_VP, _I, _U32, ctypes.POINTER(_VP)]),
+    "vxp_batch_destroy": (None, [_VP]),
+    "vxp_batch_last_error": (_I, [_VP, ctypes.c_char_p, ctypes.c_size_t]),
+    "vxp_batch_collider_upload": (_I, [_VP, _U32, _F, _VP, _U32]),
+    "vxp_batch_world_set": (_I, [_VP, _U32, _VP, _U32, _U32]),
+    "vxp_batch_world_clear": (_I, [_VP, _U32]),
+    "vxp_batch_world_get": (_I, [_VP, _U32, _VP, _U32]),
+    "vxp_batch_world_stats": (_I, [_VP, _U32, _VP]),
+    "vxp_batch_world_bytes": (ctypes.c_uint64, [_VP, _U32]),
+    "vxp_batch_step": (_I, [_VP, _F, _U32]),
+    "vxp_batch_synchronize": (_I, [_VP]),
+    "vxp_batch_times": (_I, [_VP, _VP, _VP, _U32]),
+    "vxp_batch_set_schedule": (_I, [_VP, _U32, _U32]),
+    "vxp_batch_autotune": (_I, [_VP, _F, _U32, _VP, _VP]),
 }
 
 _LIB = None

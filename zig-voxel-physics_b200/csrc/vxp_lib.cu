@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -38,8 +39,9 @@ __device__ __forceinline__ CacheSmem cache_smem(unsigned char* raw, uint32_t nwa
     return c;
 }
 
-// One world per CTA.
-__global__ void __launch_bounds__(512) k_step_block(WorldDev* worlds, ColliderSet cs) {
+// One world per CTA: block b steps worlds[b].
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 512 / kThreads) k_step_block(WorldDev* worlds, ColliderSet cs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WarpManifold* wsm = reinterpret_cast<WarpManifold*>(smem_raw);
     WorldDev w = worlds[blockIdx.x];
@@ -47,6 +49,8 @@ __global__ void __launch_bounds__(512) k_step_block(WorldDev* worlds, ColliderSe
     BlockGroup g;
     world_step(g, w, cs, wsm, csm);
 }
+template __global__ void k_step_block<256>(WorldDev*, ColliderSet);
+template __global__ void k_step_block<512>(WorldDev*, ColliderSet);
 
 // One world over a cooperative grid.
 __global__ void __launch_bounds__(512) k_step_grid(const WorldDev* world, ColliderSet cs, GridBar* bar,
@@ -156,8 +160,8 @@ namespace {
 struct HostCollider {
     uint32_t id;
     float vs;
-    std::vector<int32_t> pos;     // 3 per brick
-    std::vector<uint8_t> vox;     // 512 per brick
+    std::vector<int32_t> pos;  // 3 per brick
+    std::vector<uint8_t> vox;  // 512 per brick
     int32_t min_bound[3], max_bound[3];
     float aabb_min[3], aabb_max[3];
     uint32_t solid;
@@ -166,8 +170,14 @@ struct HostCollider {
 template <class T> struct DBuf {
     T* p = nullptr;
     size_t n = 0;
-    ~DBuf() {
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
         if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
     }
     cudaError_t reserve(size_t k, bool keep = false) {
         if (k <= n && p) return cudaSuccess;
@@ -182,6 +192,7 @@ template <class T> struct DBuf {
         n = std::max<size_t>(k, 1);
         return cudaSuccess;
     }
+    size_t bytes() const { return n * sizeof(T); }
 };
 
 uint32_t next_pow2(uint32_t x) {
@@ -190,88 +201,19 @@ uint32_t next_pow2(uint32_t x) {
     return p;
 }
 
-}  // namespace
-
-struct vxp_ctx {
-    vxp_config cfg;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    int sm_count = 148;
-    // colliders
-    std::vector<HostCollider> colliders;
-    std::unordered_map<uint32_t, uint32_t> collider_index;
-    bool colliders_dirty = true;
-    DBuf<DCollider> d_col;
-    DBuf<int32_t> d_grid;
-    DBuf<uint8_t> d_vox;
-    uint32_t n_col_dev = 0;
-    // bodies
-    uint32_t n_bodies = 0;
-    std::vector<uint32_t> body_collider_public;  // public collider id per body
-    DBuf<DBody> body;
-    DBuf<DBodyProp> prop;
-    DBuf<float4> p0, qn, aabb_mn, aabb_mx;
-    DBuf<uint2> ids;
-    DBuf<uint32_t> pair_counts, pair_offsets;
-    // pairs and everything sized by pair_cap
-    uint32_t pair_cap = 0, ht_cap = 0;
-    DBuf<uint2> pairs;
-    DBuf<uint32_t> n_pairs_dev;
-    DBuf<PairInfo> pinfo;
-    DBuf<ManifoldRec> man0, man1;
-    DBuf<HashSlot> ht0, ht1;
-    DBuf<uint32_t> frame;
-    DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag, clist;
-    DBuf<float> cp;
-    DBuf<uint4> cm;
-    DBuf<float2> cfr;
-    // body-sized
-    DBuf<uint32_t> adj_off, adj_cur, bmask;
-    // fixed
-    DBuf<uint32_t> colour_cnt, colour_cur, scan, ctr, cwriter;
-    DBuf<unsigned long long> ts;
-    DBuf<CacheKeyRec> ckey;
-    DBuf<CacheValRec> cval;
-    DBuf<unsigned long long> cframe;
-    DBuf<WorldDev> d_world;
-    DBuf<GridBar> bar;
-    DBuf<WorldDev::Cand> dump;
-    uint32_t dump_cap = 0;
-    uint32_t body_cap = 0;
-    uint32_t grid_blocks = 0;
-    uint32_t last_pairs = 0;
-    cudaEvent_t ev_start = nullptr, ev0 = nullptr, ev1 = nullptr, ev_count = nullptr;
-    uint32_t* h_count = nullptr;  // pinned mirror of the device pair count
-    bool count_pending = false;
-    float last_ms[3] = {0, 0, 0};
-    int use_grid = -1;  // -1 auto, 0 block, 1 grid
-    uint32_t solver_div = 128;
-};
-
-namespace {
-
-int fail(vxp_ctx* c, int code, const char* fmt, ...) {
-    if (c) {
-        char buf[512];
-        va_list ap;
-        va_start(ap, fmt);
-        vsnprintf(buf, sizeof(buf), fmt, ap);
-        va_end(ap);
-        c->err = buf;
-    }
-    return code;
+std::string fmt(const char* f, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, f);
+    vsnprintf(buf, sizeof(buf), f, ap);
+    va_end(ap);
+    return buf;
 }
-#define CK(call)                                                                                 \
-    do {                                                                                         \
-        cudaError_t e_ = (call);                                                                 \
-        if (e_ != cudaSuccess) return fail(ctx, VXP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-    } while (0)
 
 constexpr uint32_t kBlockThreads = 512;
-constexpr size_t kWarpSmem = sizeof(WarpManifold) * (kBlockThreads / 32);
-size_t step_smem(uint32_t cache_cap) {
-    return kWarpSmem + (size_t)cache_cap * (sizeof(uint2) + sizeof(unsigned long long) + sizeof(uint32_t));
+size_t step_smem(uint32_t threads, uint32_t cache_cap) {
+    return sizeof(WarpManifold) * (threads / 32) +
+           (size_t)cache_cap * (sizeof(uint2) + sizeof(unsigned long long) + sizeof(uint32_t));
 }
 
 uint64_t hash_brick_pos(int32_t x, int32_t y, int32_t z) {  // collider.zig:187-192
@@ -322,151 +264,135 @@ void collider_metadata(HostCollider& h) {
     }
 }
 
-int sync_colliders(vxp_ctx* ctx) {
-    if (!ctx->colliders_dirty) return VXP_OK;
-    std::vector<DCollider> dc(ctx->colliders.size());
-    std::vector<int32_t> grid;
-    std::vector<uint8_t> vox;
-    uint32_t brick_total = 0;
-    for (size_t ci = 0; ci < ctx->colliders.size(); ++ci) {
-        const HostCollider& h = ctx->colliders[ci];
-        DCollider& d = dc[ci];
-        std::memset(&d, 0, sizeof(d));
-        d.vs = h.vs;
-        for (int k = 0; k < 3; ++k) {
-            d.min_bound[k] = h.min_bound[k];
-            d.max_bound[k] = h.max_bound[k];
-            d.aabb_min[k] = h.aabb_min[k];
-            d.aabb_max[k] = h.aabb_max[k];
-        }
-        d.solid_count = h.solid;
-        const size_t nb = h.pos.size() / 3;
-        // The reference finds a brick through hashBrickPos (collider.zig:187-192,
-        // 241-248), and distinct positions can share a hash.  Every voxel the
-        // step looks up lies in [min_bound, max_bound] (the overlap region is
-        // clamped to the bounds, inclusive; B probes pass isValidCoord), so
-        // the grid covers those bricks and resolves each cell by its hash.
-        std::unordered_map<uint64_t, int32_t> by_hash;
-        for (size_t b = 0; b < nb; ++b)
-            by_hash.emplace(hash_brick_pos(h.pos[b * 3], h.pos[b * 3 + 1], h.pos[b * 3 + 2]), (int32_t)b);
-        int32_t lo[3], hi[3];
-        for (int k = 0; k < 3; ++k) {
-            lo[k] = h.min_bound[k] >> 3;
-            hi[k] = h.max_bound[k] >> 3;
-            d.bmin[k] = lo[k];
-            d.bdim[k] = hi[k] - lo[k] + 1;
-        }
-        d.grid_off = (uint32_t)grid.size();
-        d.brick_off = brick_total;
-        d.n_bricks = (uint32_t)nb;
-        const size_t cells = (size_t)d.bdim[0] * d.bdim[1] * d.bdim[2];
-        if (cells > (size_t)1 << 28) return fail(ctx, VXP_ERR_CAP, "collider %u brick grid too large", h.id);
-        grid.resize(grid.size() + cells, -1);
-        for (int32_t bz = lo[2]; bz <= hi[2]; ++bz)
-            for (int32_t by = lo[1]; by <= hi[1]; ++by)
-                for (int32_t bx = lo[0]; bx <= hi[0]; ++bx) {
-                    auto it = by_hash.find(hash_brick_pos(bx, by, bz));
-                    if (it == by_hash.end()) continue;
-                    grid[d.grid_off + (size_t)(bx - lo[0]) +
-                         (size_t)d.bdim[0] * ((size_t)(by - lo[1]) + (size_t)d.bdim[1] * (size_t)(bz - lo[2]))] =
-                        it->second;
-                }
-        vox.insert(vox.end(), h.vox.begin(), h.vox.end());
-        brick_total += (uint32_t)nb;
-    }
-    if (ctx->d_col.reserve(dc.size()) != cudaSuccess || ctx->d_grid.reserve(grid.size()) != cudaSuccess ||
-        ctx->d_vox.reserve(vox.size()) != cudaSuccess)
-        return fail(ctx, VXP_ERR_OOM, "collider upload: device allocation failed");
-    if (!dc.empty()) CK(cudaMemcpy(ctx->d_col.p, dc.data(), dc.size() * sizeof(DCollider), cudaMemcpyHostToDevice));
-    if (!grid.empty()) CK(cudaMemcpy(ctx->d_grid.p, grid.data(), grid.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    if (!vox.empty()) CK(cudaMemcpy(ctx->d_vox.p, vox.data(), vox.size(), cudaMemcpyHostToDevice));
-    ctx->n_col_dev = (uint32_t)dc.size();
-    ctx->colliders_dirty = false;
-    return VXP_OK;
-}
+// The colliders of a context or batch, mirrored on the device as a dense
+// brick grid per collider over one voxel pool.
+struct ColliderStore {
+    std::vector<HostCollider> colliders;
+    std::unordered_map<uint32_t, uint32_t> index;
+    bool dirty = true;
+    DBuf<DCollider> d_col;
+    DBuf<int32_t> d_grid;
+    DBuf<uint8_t> d_vox;
+    uint32_t n_dev = 0;
 
-ColliderSet collider_set(vxp_ctx* ctx) {
-    return ColliderSet{ctx->d_col.p, ctx->d_grid.p, ctx->d_vox.p, ctx->n_col_dev};
-}
-
-// Grows every pair-sized buffer to hold cap pairs; keeps the previous frame's
-// manifolds and rebuilds their hash table.
-int ensure_pair_cap(vxp_ctx* ctx, uint32_t need) {
-    if (need <= ctx->pair_cap && ctx->pair_cap) return VXP_OK;
-    uint32_t cap = std::max<uint32_t>(1024, ctx->pair_cap);
-    while (cap < need) cap *= 2;
-    const uint32_t old_cap = ctx->pair_cap;
-    const uint32_t ht_cap = next_pow2(cap * 2);
-    bool ok = true;
-    ok &= ctx->pairs.reserve(cap) == cudaSuccess;
-    ok &= ctx->pinfo.reserve(cap) == cudaSuccess;
-    ok &= ctx->man0.reserve(cap, true) == cudaSuccess;
-    ok &= ctx->man1.reserve(cap, true) == cudaSuccess;
-    ok &= ctx->cons.reserve(cap) == cudaSuccess;
-    ok &= ctx->colour.reserve(cap) == cudaSuccess;
-    ok &= ctx->pos_of.reserve(cap) == cudaSuccess;
-    ok &= ctx->packed_pair.reserve(cap) == cudaSuccess;
-    ok &= ctx->adj.reserve((size_t)2 * cap) == cudaSuccess;
-    ok &= ctx->flag.reserve(cap) == cudaSuccess;
-    ok &= ctx->clist.reserve(cap) == cudaSuccess;
-    ok &= ctx->cp.reserve((size_t)CP_NFIELDS * 4 * cap) == cudaSuccess;
-    ok &= ctx->cm.reserve(cap) == cudaSuccess;
-    ok &= ctx->cfr.reserve(cap) == cudaSuccess;
-    if (!ok) return fail(ctx, VXP_ERR_OOM, "pair buffers: device allocation of %u pairs failed", cap);
-    if (ht_cap != ctx->ht_cap) {
-        // frame parity decides which table is "previous": rebuild both
-        DBuf<HashSlot> n0, n1;
-        if (n0.reserve(ht_cap) != cudaSuccess || n1.reserve(ht_cap) != cudaSuccess)
-            return fail(ctx, VXP_ERR_OOM, "hash tables: allocation failed");
-        std::swap(ctx->ht0.p, n0.p);
-        std::swap(ctx->ht0.n, n0.n);
-        std::swap(ctx->ht1.p, n1.p);
-        std::swap(ctx->ht1.n, n1.n);
-        ctx->ht_cap = ht_cap;
-        if (old_cap) {
-            uint32_t fr[2] = {0, 0};
-            CK(cudaMemcpy(fr, ctx->frame.p, sizeof(fr), cudaMemcpyDeviceToHost));
-            const uint32_t prev_n = fr[1];
-            const uint32_t prev_slot = fr[0] & 1u;  // the latest manifolds: next step's "previous"
-            if (prev_n) {
-                ManifoldRec* m = prev_slot ? ctx->man1.p : ctx->man0.p;
-                HashSlot* h = prev_slot ? ctx->ht1.p : ctx->ht0.p;
-                k_rehash<<<(prev_n + 255) / 256, 256>>>(m, prev_n, h, ht_cap);
-                CK(cudaGetLastError());
-                CK(cudaDeviceSynchronize());
+    int upload(uint32_t id, float vs, const vxp_brick* bricks, uint32_t n, std::string& err) {
+        if (!bricks && n) {
+            err = "null bricks";
+            return VXP_ERR_ARG;
+        }
+        if (!(vs > 0.0f)) {
+            err = "voxel_size must be positive";
+            return VXP_ERR_ARG;
+        }
+        HostCollider h;
+        h.id = id;
+        h.vs = vs;
+        h.pos.resize((size_t)n * 3);
+        h.vox.resize((size_t)n * 512);
+        std::unordered_map<uint64_t, uint32_t> seen;
+        for (uint32_t i = 0; i < n; ++i) {
+            for (int k = 0; k < 3; ++k) h.pos[(size_t)i * 3 + k] = bricks[i].pos[k];
+            std::memcpy(&h.vox[(size_t)i * 512], bricks[i].voxels, 512);
+            const uint64_t hb = hash_brick_pos(bricks[i].pos[0], bricks[i].pos[1], bricks[i].pos[2]);
+            auto ins = seen.emplace(hb, i);
+            if (!ins.second) {
+                err = fmt("collider %u: bricks %u and %u share a hashBrickPos value", id, ins.first->second, i);
+                return VXP_ERR_ARG;
             }
         }
+        collider_metadata(h);
+        auto it = index.find(id);
+        if (it != index.end()) colliders[it->second] = std::move(h);
+        else {
+            index[id] = (uint32_t)colliders.size();
+            colliders.push_back(std::move(h));
+        }
+        dirty = true;
+        return VXP_OK;
     }
-    ctx->pair_cap = cap;
-    return VXP_OK;
-}
-
-int ensure_body_cap(vxp_ctx* ctx, uint32_t n) {
-    if (n <= ctx->body_cap && ctx->body_cap) return VXP_OK;
-    uint32_t cap = std::max<uint32_t>(256, ctx->body_cap);
-    while (cap < n) cap *= 2;
-    bool ok = true;
-    ok &= ctx->body.reserve(cap) == cudaSuccess;
-    ok &= ctx->prop.reserve(cap) == cudaSuccess;
-    ok &= ctx->p0.reserve(cap) == cudaSuccess;
-    ok &= ctx->qn.reserve(cap) == cudaSuccess;
-    ok &= ctx->aabb_mn.reserve(cap) == cudaSuccess;
-    ok &= ctx->aabb_mx.reserve(cap) == cudaSuccess;
-    ok &= ctx->ids.reserve(cap) == cudaSuccess;
-    ok &= ctx->pair_counts.reserve(cap) == cudaSuccess;
-    ok &= ctx->pair_offsets.reserve(cap) == cudaSuccess;
-    ok &= ctx->adj_off.reserve((size_t)cap + 1) == cudaSuccess;
-    ok &= ctx->adj_cur.reserve(cap) == cudaSuccess;
-    ok &= ctx->bmask.reserve((size_t)cap * 8) == cudaSuccess;
-    if (!ok) return fail(ctx, VXP_ERR_OOM, "body buffers: device allocation of %u bodies failed", cap);
-    ctx->body_cap = cap;
-    return VXP_OK;
-}
+    uint32_t index_of(uint32_t id) const {
+        auto it = index.find(id);
+        return it == index.end() ? 0xFFFFFFFFu : it->second;
+    }
+    int sync(std::string& err) {
+        if (!dirty) return VXP_OK;
+        std::vector<DCollider> dc(colliders.size());
+        std::vector<int32_t> grid;
+        std::vector<uint8_t> vox;
+        uint32_t brick_total = 0;
+        for (size_t ci = 0; ci < colliders.size(); ++ci) {
+            const HostCollider& h = colliders[ci];
+            DCollider& d = dc[ci];
+            std::memset(&d, 0, sizeof(d));
+            d.vs = h.vs;
+            for (int k = 0; k < 3; ++k) {
+                d.min_bound[k] = h.min_bound[k];
+                d.max_bound[k] = h.max_bound[k];
+                d.aabb_min[k] = h.aabb_min[k];
+                d.aabb_max[k] = h.aabb_max[k];
+            }
+            d.solid_count = h.solid;
+            const size_t nb = h.pos.size() / 3;
+            // The reference finds a brick through hashBrickPos (collider.zig:
+            // 187-192, 241-248), and distinct positions can share a hash.  Every
+            // voxel the step looks up lies in [min_bound, max_bound] (the overlap
+            // region is clamped to the bounds, inclusive; B probes pass
+            // isValidCoord), so the grid covers those bricks and resolves each
+            // cell by its hash.
+            std::unordered_map<uint64_t, int32_t> by_hash;
+            for (size_t b = 0; b < nb; ++b)
+                by_hash.emplace(hash_brick_pos(h.pos[b * 3], h.pos[b * 3 + 1], h.pos[b * 3 + 2]), (int32_t)b);
+            int32_t lo[3], hi[3];
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = h.min_bound[k] >> 3;
+                hi[k] = h.max_bound[k] >> 3;
+                d.bmin[k] = lo[k];
+                d.bdim[k] = hi[k] - lo[k] + 1;
+            }
+            d.grid_off = (uint32_t)grid.size();
+            d.brick_off = brick_total;
+            d.n_bricks = (uint32_t)nb;
+            const size_t cells = (size_t)d.bdim[0] * d.bdim[1] * d.bdim[2];
+            if (cells > (size_t)1 << 28) {
+                err = fmt("collider %u brick grid too large", h.id);
+                return VXP_ERR_CAP;
+            }
+            grid.resize(grid.size() + cells, -1);
+            for (int32_t bz = lo[2]; bz <= hi[2]; ++bz)
+                for (int32_t by = lo[1]; by <= hi[1]; ++by)
+                    for (int32_t bx = lo[0]; bx <= hi[0]; ++bx) {
+                        auto it = by_hash.find(hash_brick_pos(bx, by, bz));
+                        if (it == by_hash.end()) continue;
+                        grid[d.grid_off + (size_t)(bx - lo[0]) +
+                             (size_t)d.bdim[0] * ((size_t)(by - lo[1]) + (size_t)d.bdim[1] * (size_t)(bz - lo[2]))] =
+                            it->second;
+                    }
+            vox.insert(vox.end(), h.vox.begin(), h.vox.end());
+            brick_total += (uint32_t)nb;
+        }
+        if (d_col.reserve(dc.size()) != cudaSuccess || d_grid.reserve(grid.size()) != cudaSuccess ||
+            d_vox.reserve(vox.size()) != cudaSuccess) {
+            err = "collider upload: device allocation failed";
+            return VXP_ERR_OOM;
+        }
+        if ((!dc.empty() && cudaMemcpy(d_col.p, dc.data(), dc.size() * sizeof(DCollider), cudaMemcpyHostToDevice) !=
+                                cudaSuccess) ||
+            (!grid.empty() &&
+             cudaMemcpy(d_grid.p, grid.data(), grid.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) ||
+            (!vox.empty() && cudaMemcpy(d_vox.p, vox.data(), vox.size(), cudaMemcpyHostToDevice) != cudaSuccess)) {
+            err = "collider upload: copy failed";
+            return VXP_ERR_CUDA;
+        }
+        n_dev = (uint32_t)dc.size();
+        dirty = false;
+        return VXP_OK;
+    }
+    ColliderSet set() const { return ColliderSet{d_col.p, d_grid.p, d_vox.p, n_dev}; }
+};
 
 StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) {
     StepCfg s;
-    s.phases = phases;
-    s.solver_div = 128;
+    std::memset(&s, 0, sizeof(s));
     for (int i = 0; i < 3; ++i) s.gravity[i] = c.gravity[i];
     s.dt = dt;
     s.substeps = c.substeps;
@@ -489,68 +415,409 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
     s.reference_caps = c.reference_caps;
     s.colouring = c.colouring;
     s.dump_candidates = dump;
+    s.phases = phases;
+    s.solver_div = 128;
+    s.device_pairs = 0;
+    s.margin = 0.1f;
     return s;
 }
 
-WorldDev make_world(vxp_ctx* ctx, float dt, uint32_t phases) {
-    WorldDev w;
-    std::memset(&w, 0, sizeof(w));
-    w.cfg = step_cfg(ctx->cfg, dt, ctx->dump_cap ? 1u : 0u, phases);
-    w.cfg.solver_div = ctx->solver_div;
-    w.n_bodies = ctx->n_bodies;
-    w.n_pairs = 0;
-    w.n_pairs_dev = ctx->n_pairs_dev.p;
-    w.pair_cap = ctx->pair_cap;
-    w.ht_cap = ctx->ht_cap;
-    w.cache_cap = ctx->cfg.brick_pair_cache_size ? ctx->cfg.brick_pair_cache_size : 1024u;
-    w.dump_cap = ctx->dump_cap;
-    w.body = ctx->body.p;
-    w.prop = ctx->prop.p;
-    w.p0 = ctx->p0.p;
-    w.qn = ctx->qn.p;
-    w.ids = ctx->ids.p;
-    w.pairs = ctx->pairs.p;
-    w.pinfo = ctx->pinfo.p;
-    w.man[0] = ctx->man0.p;
-    w.man[1] = ctx->man1.p;
-    w.ht[0] = ctx->ht0.p;
-    w.ht[1] = ctx->ht1.p;
-    w.frame = ctx->frame.p;
-    w.ckey = ctx->ckey.p;
-    w.cval = ctx->cval.p;
-    w.cwriter = ctx->cwriter.p;
-    w.clist = ctx->clist.p;
-    w.cframe = ctx->cframe.p;
-    w.cons = ctx->cons.p;
-    w.colour = ctx->colour.p;
-    w.pos_of = ctx->pos_of.p;
-    w.packed_pair = ctx->packed_pair.p;
-    w.adj_off = ctx->adj_off.p;
-    w.adj = ctx->adj.p;
-    w.adj_cur = ctx->adj_cur.p;
-    w.colour_cnt = ctx->colour_cnt.p;
-    w.colour_cur = ctx->colour_cur.p;
-    w.bmask = ctx->bmask.p;
-    w.cp = ctx->cp.p;
-    w.cm = ctx->cm.p;
-    w.cfr = ctx->cfr.p;
-    w.scan = ctx->scan.p;
-    w.flag = ctx->flag.p;
-    w.ctr = ctx->ctr.p;
-    w.ts = ctx->ts.p;
-    w.dump = ctx->dump.p;
-    return w;
-}
+// Device memory of one world: body state, pair list, contact manager, cache,
+// constraint arrays and scratch.
+struct WorldBuffers {
+    uint32_t n_bodies = 0, body_cap = 0, pair_cap = 0, ht_cap = 0, cache_cap = 1024, dump_cap = 0, scan_blocks = 1;
+    std::vector<uint32_t> collider_public;
+    DBuf<DBody> body;
+    DBuf<DBodyProp> prop;
+    DBuf<float4> p0, qn, aabb_mn, aabb_mx;
+    DBuf<uint2> ids;
+    DBuf<uint32_t> pcount, poff, adj_off, adj_cur, bmask;
+    DBuf<uint2> pairs;
+    DBuf<uint32_t> n_pairs_dev;
+    DBuf<PairInfo> pinfo;
+    DBuf<ManifoldRec> man0, man1;
+    DBuf<HashSlot> ht0, ht1;
+    DBuf<uint32_t> frame;
+    DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag, clist;
+    DBuf<float> cp;
+    DBuf<uint4> cm;
+    DBuf<float2> cfr;
+    DBuf<uint32_t> colour_cnt, colour_cur, scan, ctr, cwriter;
+    DBuf<unsigned long long> ts, cframe;
+    DBuf<CacheKeyRec> ckey;
+    DBuf<CacheValRec> cval;
+    DBuf<WorldDev::Cand> dump;
 
-// Runs the step kernel for the pairs already in ctx->pairs / n_pairs_dev.
-int launch_step(vxp_ctx* ctx, float dt, uint32_t n_pairs_hint, uint32_t phases) {
-    if (int rc = sync_colliders(ctx)) return rc;
-    WorldDev w = make_world(ctx, dt, phases);
+    int init(uint32_t cache, uint32_t blocks, std::string& err) {
+        cache_cap = cache;
+        scan_blocks = blocks;
+        bool ok = true;
+        ok &= n_pairs_dev.reserve(1) == cudaSuccess;
+        ok &= frame.reserve(2) == cudaSuccess;
+        ok &= colour_cnt.reserve(257) == cudaSuccess;
+        ok &= colour_cur.reserve(256) == cudaSuccess;
+        ok &= scan.reserve(blocks + 64) == cudaSuccess;
+        ok &= ctr.reserve(C_NCTR) == cudaSuccess;
+        ok &= ts.reserve(TS_N) == cudaSuccess;
+        ok &= ckey.reserve(cache) == cudaSuccess;
+        ok &= cval.reserve(cache) == cudaSuccess;
+        ok &= cwriter.reserve(cache) == cudaSuccess;
+        ok &= cframe.reserve(1) == cudaSuccess;
+        if (!ok) {
+            err = "world buffers: device allocation failed";
+            return VXP_ERR_OOM;
+        }
+        return VXP_OK;
+    }
+
+    // Grows every pair-sized buffer to hold `need` pairs; keeps the latest
+    // frame's manifolds and rebuilds their hash table.
+    int ensure_pairs(uint32_t need, std::string& err) {
+        if (need <= pair_cap && pair_cap) return VXP_OK;
+        uint32_t cap = std::max<uint32_t>(1024, pair_cap);
+        while (cap < need) cap *= 2;
+        const uint32_t old_cap = pair_cap;
+        const uint32_t new_ht = next_pow2(cap * 2);
+        bool ok = true;
+        ok &= pairs.reserve(cap) == cudaSuccess;
+        ok &= pinfo.reserve(cap) == cudaSuccess;
+        ok &= man0.reserve(cap, true) == cudaSuccess;
+        ok &= man1.reserve(cap, true) == cudaSuccess;
+        ok &= cons.reserve(cap) == cudaSuccess;
+        ok &= colour.reserve(cap) == cudaSuccess;
+        ok &= pos_of.reserve(cap) == cudaSuccess;
+        ok &= packed_pair.reserve(cap) == cudaSuccess;
+        ok &= adj.reserve((size_t)2 * cap) == cudaSuccess;
+        ok &= flag.reserve(cap) == cudaSuccess;
+        ok &= clist.reserve(cap) == cudaSuccess;
+        ok &= cp.reserve((size_t)CP_NFIELDS * 4 * cap) == cudaSuccess;
+        ok &= cm.reserve(cap) == cudaSuccess;
+        ok &= cfr.reserve(cap) == cudaSuccess;
+        if (!ok) {
+            err = fmt("pair buffers: device allocation of %u pairs failed", cap);
+            return VXP_ERR_OOM;
+        }
+        if (new_ht != ht_cap) {
+            ht0.release();
+            ht1.release();
+            if (ht0.reserve(new_ht) != cudaSuccess || ht1.reserve(new_ht) != cudaSuccess) {
+                err = "hash tables: allocation failed";
+                return VXP_ERR_OOM;
+            }
+            ht_cap = new_ht;
+            if (old_cap) {
+                uint32_t fr[2] = {0, 0};
+                if (cudaMemcpy(fr, frame.p, sizeof(fr), cudaMemcpyDeviceToHost) != cudaSuccess) {
+                    err = "frame read failed";
+                    return VXP_ERR_CUDA;
+                }
+                const uint32_t latest_n = fr[1];
+                const uint32_t latest = fr[0] & 1u;  // the next step reads it as previous
+                if (latest_n) {
+                    ManifoldRec* m = latest ? man1.p : man0.p;
+                    HashSlot* h = latest ? ht1.p : ht0.p;
+                    k_rehash<<<(latest_n + 255) / 256, 256>>>(m, latest_n, h, new_ht);
+                    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+                        err = "rehash failed";
+                        return VXP_ERR_CUDA;
+                    }
+                }
+            }
+        }
+        pair_cap = cap;
+        return VXP_OK;
+    }
+
+    int ensure_bodies(uint32_t n, std::string& err) {
+        if (n <= body_cap && body_cap) return VXP_OK;
+        uint32_t cap = std::max<uint32_t>(64, body_cap);
+        while (cap < n) cap *= 2;
+        bool ok = true;
+        ok &= body.reserve(cap) == cudaSuccess;
+        ok &= prop.reserve(cap) == cudaSuccess;
+        ok &= p0.reserve(cap) == cudaSuccess;
+        ok &= qn.reserve(cap) == cudaSuccess;
+        ok &= aabb_mn.reserve(cap) == cudaSuccess;
+        ok &= aabb_mx.reserve(cap) == cudaSuccess;
+        ok &= ids.reserve(cap) == cudaSuccess;
+        ok &= pcount.reserve(cap) == cudaSuccess;
+        ok &= poff.reserve(cap) == cudaSuccess;
+        ok &= adj_off.reserve((size_t)cap + 1) == cudaSuccess;
+        ok &= adj_cur.reserve(cap) == cudaSuccess;
+        ok &= bmask.reserve((size_t)cap * 8) == cudaSuccess;
+        if (!ok) {
+            err = fmt("body buffers: device allocation of %u bodies failed", cap);
+            return VXP_ERR_OOM;
+        }
+        body_cap = cap;
+        return VXP_OK;
+    }
+
+    int set_bodies(const vxp_body* b, uint32_t n, const ColliderStore& cols, std::string& err) {
+        if (!b && n) {
+            err = "null bodies";
+            return VXP_ERR_ARG;
+        }
+        if (int rc = ensure_bodies(n, err)) return rc;
+        std::vector<DBody> db(n);
+        std::vector<DBodyProp> dp(n);
+        std::vector<uint2> id(n);
+        collider_public.resize(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const vxp_body& s = b[i];
+            if (s.body_type > 2u) {
+                err = fmt("body %u: bad body_type %u", i, s.body_type);
+                return VXP_ERR_ARG;
+            }
+            DBody& d = db[i];
+            d.p = make_float4(s.position[0], s.position[1], s.position[2], s.inv_mass);
+            d.q = make_float4(s.rotation[0], s.rotation[1], s.rotation[2], s.rotation[3]);
+            d.v = make_float4(s.linear_velocity[0], s.linear_velocity[1], s.linear_velocity[2], 0.f);
+            d.w = make_float4(s.angular_velocity[0], s.angular_velocity[1], s.angular_velocity[2], 0.f);
+            d.i0 = d.i1 = d.i2 = make_float4(0.f, 0.f, 0.f, 0.f);
+            DBodyProp& p = dp[i];
+            for (int k = 0; k < 9; ++k) p.il[k] = s.inv_inertia_local[k];
+            p.friction = s.friction;
+            p.restitution = s.restitution;
+            p.lin_damp = s.linear_damping;
+            p.ang_damp = s.angular_damping;
+            p.sleep_timer = s.sleep_timer;
+            p.id = s.id;
+            p.type = s.body_type;
+            p.collider = cols.index_of(s.collider_id);
+            p.sleeping = s.is_sleeping ? 1u : 0u;
+            collider_public[i] = s.collider_id;
+            id[i] = make_uint2(s.id, i);
+        }
+        std::sort(id.begin(), id.end(), [](const uint2& x, const uint2& y) { return x.x < y.x; });
+        for (uint32_t i = 1; i < n; ++i)
+            if (id[i].x == id[i - 1].x) {
+                err = fmt("duplicate body id %u", id[i].x);
+                return VXP_ERR_ARG;
+            }
+        if (n && (cudaMemcpy(body.p, db.data(), n * sizeof(DBody), cudaMemcpyHostToDevice) != cudaSuccess ||
+                  cudaMemcpy(prop.p, dp.data(), n * sizeof(DBodyProp), cudaMemcpyHostToDevice) != cudaSuccess ||
+                  cudaMemcpy(ids.p, id.data(), n * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess)) {
+            err = "body upload failed";
+            return VXP_ERR_CUDA;
+        }
+        n_bodies = n;
+        return VXP_OK;
+    }
+
+    int get_bodies(vxp_body* b, uint32_t n, cudaStream_t stream, std::string& err) {
+        if (n != n_bodies) {
+            err = fmt("expected %u bodies, got %u", n_bodies, n);
+            return VXP_ERR_ARG;
+        }
+        std::vector<DBody> db(n);
+        std::vector<DBodyProp> dp(n);
+        if (n && (cudaMemcpyAsync(db.data(), body.p, n * sizeof(DBody), cudaMemcpyDeviceToHost, stream) !=
+                      cudaSuccess ||
+                  cudaMemcpyAsync(dp.data(), prop.p, n * sizeof(DBodyProp), cudaMemcpyDeviceToHost, stream) !=
+                      cudaSuccess ||
+                  cudaStreamSynchronize(stream) != cudaSuccess)) {
+            err = "body download failed";
+            return VXP_ERR_CUDA;
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            vxp_body& s = b[i];
+            const DBody& d = db[i];
+            const DBodyProp& p = dp[i];
+            s.id = p.id;
+            s.body_type = p.type;
+            s.collider_id = collider_public[i];
+            s.is_sleeping = p.sleeping;
+            s.position[0] = d.p.x; s.position[1] = d.p.y; s.position[2] = d.p.z;
+            s.rotation[0] = d.q.x; s.rotation[1] = d.q.y; s.rotation[2] = d.q.z; s.rotation[3] = d.q.w;
+            s.linear_velocity[0] = d.v.x; s.linear_velocity[1] = d.v.y; s.linear_velocity[2] = d.v.z;
+            s.angular_velocity[0] = d.w.x; s.angular_velocity[1] = d.w.y; s.angular_velocity[2] = d.w.z;
+            s.inv_mass = d.p.w;
+            for (int k = 0; k < 9; ++k) s.inv_inertia_local[k] = p.il[k];
+            s.friction = p.friction;
+            s.restitution = p.restitution;
+            s.linear_damping = p.lin_damp;
+            s.angular_damping = p.ang_damp;
+            s.sleep_timer = p.sleep_timer;
+        }
+        return VXP_OK;
+    }
+
+    WorldDev make(const vxp_config& cfg, float dt, uint32_t phases, uint32_t solver_div, bool device_pairs,
+                  float margin) const {
+        WorldDev w;
+        std::memset(&w, 0, sizeof(w));
+        w.cfg = step_cfg(cfg, dt, dump_cap ? 1u : 0u, phases);
+        w.cfg.solver_div = solver_div;
+        w.cfg.device_pairs = device_pairs ? 1u : 0u;
+        w.cfg.margin = margin;
+        w.n_bodies = n_bodies;
+        w.n_pairs_dev = n_pairs_dev.p;
+        w.pair_cap = pair_cap;
+        w.ht_cap = ht_cap;
+        w.cache_cap = cache_cap;
+        w.dump_cap = dump_cap;
+        w.body = body.p;
+        w.prop = prop.p;
+        w.p0 = p0.p;
+        w.qn = qn.p;
+        w.ids = ids.p;
+        w.aabb_mn = aabb_mn.p;
+        w.aabb_mx = aabb_mx.p;
+        w.pcount = pcount.p;
+        w.poff = poff.p;
+        w.pairs = pairs.p;
+        w.pinfo = pinfo.p;
+        w.man[0] = man0.p;
+        w.man[1] = man1.p;
+        w.ht[0] = ht0.p;
+        w.ht[1] = ht1.p;
+        w.frame = frame.p;
+        w.ckey = ckey.p;
+        w.cval = cval.p;
+        w.cwriter = cwriter.p;
+        w.clist = clist.p;
+        w.cframe = cframe.p;
+        w.cons = cons.p;
+        w.colour = colour.p;
+        w.pos_of = pos_of.p;
+        w.packed_pair = packed_pair.p;
+        w.adj_off = adj_off.p;
+        w.adj = adj.p;
+        w.adj_cur = adj_cur.p;
+        w.colour_cnt = colour_cnt.p;
+        w.colour_cur = colour_cur.p;
+        w.bmask = bmask.p;
+        w.cp = cp.p;
+        w.cm = cm.p;
+        w.cfr = cfr.p;
+        w.scan = scan.p;
+        w.flag = flag.p;
+        w.ctr = ctr.p;
+        w.ts = ts.p;
+        w.dump = dump.p;
+        return w;
+    }
+
+    size_t device_bytes() const {
+        return body.bytes() + prop.bytes() + p0.bytes() + qn.bytes() + aabb_mn.bytes() + aabb_mx.bytes() +
+               ids.bytes() + pcount.bytes() + poff.bytes() + adj_off.bytes() + adj_cur.bytes() + bmask.bytes() +
+               pairs.bytes() + pinfo.bytes() + man0.bytes() + man1.bytes() + ht0.bytes() + ht1.bytes() +
+               cons.bytes() + colour.bytes() + pos_of.bytes() + packed_pair.bytes() + adj.bytes() + flag.bytes() +
+               clist.bytes() + cp.bytes() + cm.bytes() + cfr.bytes() + ckey.bytes() + cval.bytes() +
+               cwriter.bytes() + scan.bytes() + ctr.bytes() + ts.bytes() + dump.bytes();
+    }
+
+    // Counters -> vxp_stats.
+    int stats(vxp_stats* s, uint32_t pairs_in, cudaStream_t stream, std::string& err) const {
+        uint32_t c[C_NCTR];
+        if (cudaMemcpyAsync(c, ctr.p, sizeof(c), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            err = "counter read failed";
+            return VXP_ERR_CUDA;
+        }
+        std::memset(s, 0, sizeof(*s));
+        s->pairs_in = pairs_in;
+        s->pairs_tested = c[C_PAIRS_TESTED];
+        s->pairs_colliding = c[C_PAIRS_COLLIDING];
+        s->voxels_checked = c[C_VOXELS_CHECKED];
+        s->contacts_generated = c[C_CONTACTS];
+        s->pairs_skipped_sleeping = c[C_SKIPPED_SLEEPING];
+        s->manifolds_preserved = c[C_PRESERVED];
+        s->cache_hits = c[C_CACHE_HITS];
+        s->cache_misses = c[C_CACHE_MISSES];
+        s->cache_evictions = c[C_CACHE_EVICTIONS];
+        s->manifolds = c[C_MANIFOLDS];
+        s->constraints = c[C_CONSTRAINTS];
+        s->contact_points = c[C_POINTS];
+        s->colours = c[C_COLOURS];
+        s->position_iterations_run = c[C_POS_ITERS];
+        s->step_skipped = c[C_STEP_SKIPPED];
+        const int32_t k = (int32_t)c[C_MAX_PEN_KEY];
+        int32_t bits = k >= 0 ? k : (k ^ 0x7FFFFFFF);
+        std::memcpy(&s->max_penetration, &bits, 4);
+        s->candidates = c[C_CANDIDATES];
+        s->bricks_touched = c[C_BRICKS];
+        return VXP_OK;
+    }
+
+    // Reads and clears the sticky error word.
+    int take_error(cudaStream_t stream, std::string& err) const {
+        uint32_t e = 0;
+        if (cudaMemcpyAsync(&e, ctr.p + C_ERROR, sizeof(e), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            err = "error word read failed";
+            return VXP_ERR_CUDA;
+        }
+        if (!e) return VXP_OK;
+        const uint32_t z = 0;
+        cudaMemcpy(ctr.p + C_ERROR, &z, sizeof(z), cudaMemcpyHostToDevice);
+        if (e & ERR_TIMEOUT) {
+            err = fmt("a grid barrier wait ran out (error bits 0x%x)", e);
+            return VXP_ERR_TIMEOUT;
+        }
+        if (e & ERR_CAP) {
+            err = fmt("pair list exceeded the device capacity; the step left the state untouched (bits 0x%x)", e);
+            return VXP_ERR_CAP;
+        }
+        if (e & ERR_COLOURS) {
+            err = fmt("more than 255 colours needed (error bits 0x%x)", e);
+            return VXP_ERR_CAP;
+        }
+        err = fmt("device error bits 0x%x", e);
+        return VXP_ERR_STATE;
+    }
+};
+
+}  // namespace
+
+struct vxp_ctx {
+    vxp_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int sm_count = 148;
+    ColliderStore cols;
+    WorldBuffers w;
+    DBuf<WorldDev> d_world;
+    DBuf<GridBar> bar;
+    DBuf<uint32_t> pair_counts, pair_offsets;
+    uint32_t grid_blocks = 0;
+    uint32_t last_pairs = 0;
+    cudaEvent_t ev_start = nullptr, ev0 = nullptr, ev1 = nullptr, ev_count = nullptr;
+    uint32_t* h_count = nullptr;  // pinned mirror of the device pair count
+    bool count_pending = false;
+    int use_grid = -1;  // -1 auto, 0 block, 1 grid
+    uint32_t solver_div = 128;
+};
+
+namespace {
+
+int fail(vxp_ctx* c, int code, const char* f, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, f);
+        vsnprintf(buf, sizeof(buf), f, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+#define CK(call)                                                                                         \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) return fail(ctx, VXP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// Runs the step kernel.  device_pairs: the kernel builds the pair list itself.
+int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, float margin) {
+    if (int rc = ctx->cols.sync(ctx->err)) return rc;
+    WorldDev w = ctx->w.make(ctx->cfg, dt, phases, ctx->solver_div, device_pairs, margin);
     CK(cudaMemcpyAsync(ctx->d_world.p, &w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemsetAsync(ctx->ctr.p, 0, sizeof(uint32_t) * C_ERROR, ctx->stream));
-    const ColliderSet cs = collider_set(ctx);
-    (void)n_pairs_hint;
-    bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->n_bodies >= 512);
+    const ColliderSet cs = ctx->cols.set();
+    const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
+    const size_t smem = step_smem(kBlockThreads, w.cache_cap);
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (grid) {
         CK(cudaMemsetAsync(ctx->bar.p, 0, 2 * sizeof(GridBar), ctx->stream));
@@ -559,74 +826,53 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t n_pairs_hint, uint32_t phases) 
         unsigned long long timeout = 10ull * 1000ull * 1000ull * 1000ull;  // 10 s per barrier wait
         void* args[] = {(void*)&wp, (void*)&cs, (void*)&bp, (void*)&timeout};
         CK(cudaLaunchCooperativeKernel((const void*)k_step_grid, dim3(ctx->grid_blocks), dim3(kBlockThreads), args,
-                                       step_smem(w.cache_cap), ctx->stream));
+                                       smem, ctx->stream));
     } else {
-        k_step_block<<<1, kBlockThreads, step_smem(w.cache_cap), ctx->stream>>>(ctx->d_world.p, cs);
+        k_step_block<kBlockThreads><<<1, kBlockThreads, smem, ctx->stream>>>(ctx->d_world.p, cs);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    if (device_pairs && !ctx->count_pending) {
+        CK(cudaMemcpyAsync(ctx->h_count, ctx->w.n_pairs_dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaEventRecord(ctx->ev_count, ctx->stream));
+        ctx->count_pending = true;
+    }
     return VXP_OK;
 }
 
 int check_device_error(vxp_ctx* ctx) {
     CK(cudaStreamSynchronize(ctx->stream));
-    uint32_t e = 0;
-    CK(cudaMemcpy(&e, ctx->ctr.p + C_ERROR, sizeof(e), cudaMemcpyDeviceToHost));
-    if (e) {
-        const uint32_t z = 0;
-        cudaMemcpy(ctx->ctr.p + C_ERROR, &z, sizeof(z), cudaMemcpyHostToDevice);
-        if (e & ERR_TIMEOUT) return fail(ctx, VXP_ERR_TIMEOUT, "a grid barrier wait ran out (error bits 0x%x)", e);
-        if (e & ERR_CAP) return fail(ctx, VXP_ERR_CAP, "pair list exceeded the device capacity (error bits 0x%x)", e);
-        if (e & ERR_COLOURS) return fail(ctx, VXP_ERR_CAP, "more than 255 colours needed (error bits 0x%x)", e);
-        return fail(ctx, VXP_ERR_STATE, "device error bits 0x%x", e);
-    }
-    return VXP_OK;
+    return ctx->w.take_error(ctx->stream, ctx->err);
 }
 
-// The pair source on the device.  With wait_count the pair count is read back
-// (growing the buffers and rewriting when it did not fit); without, nothing
-// waits: the step kernel refuses a list that overflowed (VXP_ERR_CAP at the
-// next wait, state untouched) and the buffers grow ahead of need from the
-// count of an earlier step, copied back asynchronously.
-int compute_device_pairs(vxp_ctx* ctx, float margin, bool wait_count, uint32_t* n_out) {
-    if (int rc = sync_colliders(ctx)) return rc;
-    const uint32_t n = ctx->n_bodies;
-    const ColliderSet cs = collider_set(ctx);
-    if (!wait_count && ctx->count_pending && cudaEventQuery(ctx->ev_count) == cudaSuccess) {
-        ctx->count_pending = false;
-        const uint32_t seen = *ctx->h_count;
-        if (seen > ctx->pair_cap - ctx->pair_cap / 4u) {
-            CK(cudaStreamSynchronize(ctx->stream));
-            if (int rc = ensure_pair_cap(ctx, seen + seen / 2u + 1024u)) return rc;
-        }
-    }
+// The pair list of the current body state into ctx->w.pairs (host waits).
+int compute_device_pairs(vxp_ctx* ctx, float margin, uint32_t* n_out) {
+    if (int rc = ctx->cols.sync(ctx->err)) return rc;
+    WorldBuffers& w = ctx->w;
+    const uint32_t n = w.n_bodies;
+    const ColliderSet cs = ctx->cols.set();
     if (n == 0) {
         *n_out = 0;
-        CK(cudaMemsetAsync(ctx->n_pairs_dev.p, 0, sizeof(uint32_t), ctx->stream));
         return VXP_OK;
     }
+    if (ctx->pair_counts.reserve(w.body_cap) != cudaSuccess || ctx->pair_offsets.reserve(w.body_cap) != cudaSuccess)
+        return fail(ctx, VXP_ERR_OOM, "pair scratch");
     const uint32_t tb = 256, nb = (n + tb - 1) / tb;
     const uint32_t wb = (n * 32u + tb - 1) / tb;
-    k_body_aabbs<<<nb, tb, 0, ctx->stream>>>(ctx->body.p, ctx->prop.p, n, cs, margin, ctx->aabb_mn.p, ctx->aabb_mx.p);
-    k_pairs<<<wb, tb, 0, ctx->stream>>>(ctx->ids.p, ctx->prop.p, n, ctx->aabb_mn.p, ctx->aabb_mx.p,
-                                        ctx->pair_counts.p, nullptr, nullptr, 0, 0);
-    k_scan1<<<1, 1024, 0, ctx->stream>>>(ctx->pair_counts.p, ctx->pair_offsets.p, n, ctx->n_pairs_dev.p);
+    k_body_aabbs<<<nb, tb, 0, ctx->stream>>>(w.body.p, w.prop.p, n, cs, margin, w.aabb_mn.p, w.aabb_mx.p);
+    k_pairs<<<wb, tb, 0, ctx->stream>>>(w.ids.p, w.prop.p, n, w.aabb_mn.p, w.aabb_mx.p, ctx->pair_counts.p, nullptr,
+                                        nullptr, 0, 0);
+    k_scan1<<<1, 1024, 0, ctx->stream>>>(ctx->pair_counts.p, ctx->pair_offsets.p, n, w.n_pairs_dev.p);
     CK(cudaGetLastError());
     uint32_t total = 0;
-    if (wait_count) {
-        CK(cudaMemcpyAsync(&total, ctx->n_pairs_dev.p, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        if (int rc = ensure_pair_cap(ctx, total)) return rc;
-    }
-    k_pairs<<<wb, tb, 0, ctx->stream>>>(ctx->ids.p, ctx->prop.p, n, ctx->aabb_mn.p, ctx->aabb_mx.p, nullptr,
-                                        ctx->pair_offsets.p, ctx->pairs.p, ctx->pair_cap, 1);
+    CK(cudaMemcpyAsync(&total, w.n_pairs_dev.p, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (int rc = w.ensure_pairs(total, ctx->err)) return rc;
+    k_pairs<<<wb, tb, 0, ctx->stream>>>(w.ids.p, w.prop.p, n, w.aabb_mn.p, w.aabb_mx.p, nullptr, ctx->pair_offsets.p,
+                                        w.pairs.p, w.pair_cap, 1);
     CK(cudaGetLastError());
-    if (!wait_count && !ctx->count_pending) {
-        CK(cudaMemcpyAsync(ctx->h_count, ctx->n_pairs_dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaEventRecord(ctx->ev_count, ctx->stream));
-        ctx->count_pending = true;
-    }
-    *n_out = wait_count ? total : ctx->pair_cap;
+    *n_out = total;
     return VXP_OK;
 }
 
@@ -766,7 +1012,7 @@ int noalloc_scratch_for_current_device(unsigned char** out) {
 }  // namespace
 
 // ===========================================================================
-// C ABI
+// C ABI: single world
 // ===========================================================================
 extern "C" {
 
@@ -802,6 +1048,17 @@ void vxp_config_default(vxp_config* c) {
     c->max_pairs = 0;
 }
 
+static int set_kernel_smem(uint32_t cache_cap) {
+    if (cudaFuncSetAttribute(k_step_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)step_smem(256, cache_cap)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_step_block<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)step_smem(512, cache_cap)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_step_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)step_smem(512, cache_cap)) != cudaSuccess)
+        return VXP_ERR_CUDA;
+    return VXP_OK;
+}
+
 int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     if (!cfg || !out) return VXP_ERR_ARG;
     *out = nullptr;
@@ -827,34 +1084,17 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     if (cudaMallocHost(&ctx->h_count, sizeof(uint32_t)) != cudaSuccess) return bail(VXP_ERR_OOM);
     *ctx->h_count = 0;
     const uint32_t cache_cap = cfg->brick_pair_cache_size ? cfg->brick_pair_cache_size : 1024u;
-    if (cudaFuncSetAttribute(k_step_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)step_smem(cache_cap)) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_step_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)step_smem(cache_cap)) !=
-            cudaSuccess)
-        return bail(VXP_ERR_CUDA);
+    if (set_kernel_smem(cache_cap)) return bail(VXP_ERR_CUDA);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads, step_smem(cache_cap)) !=
-            cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads,
+                                                      step_smem(kBlockThreads, cache_cap)) != cudaSuccess ||
         per_sm < 1)
         return bail(VXP_ERR_CUDA);
     ctx->grid_blocks = (uint32_t)(smc * std::min(per_sm, 2));
-    bool ok = true;
-    ok &= ctx->n_pairs_dev.reserve(1) == cudaSuccess;
-    ok &= ctx->frame.reserve(2) == cudaSuccess;
-    ok &= ctx->colour_cnt.reserve(257) == cudaSuccess;
-    ok &= ctx->colour_cur.reserve(256) == cudaSuccess;
-    ok &= ctx->scan.reserve(ctx->grid_blocks + 64) == cudaSuccess;
-    ok &= ctx->ctr.reserve(C_NCTR) == cudaSuccess;
-    ok &= ctx->ts.reserve(TS_N) == cudaSuccess;
-    ok &= ctx->ckey.reserve(cache_cap) == cudaSuccess;
-    ok &= ctx->cval.reserve(cache_cap) == cudaSuccess;
-    ok &= ctx->cwriter.reserve(cache_cap) == cudaSuccess;
-    ok &= ctx->cframe.reserve(1) == cudaSuccess;
-    ok &= ctx->d_world.reserve(1) == cudaSuccess;
-    ok &= ctx->bar.reserve(2) == cudaSuccess;
-    if (!ok) return bail(VXP_ERR_OOM);
-    if (ensure_pair_cap(ctx, std::max<uint32_t>(cfg->max_pairs, 1024)) != VXP_OK) return bail(VXP_ERR_OOM);
-    if (ensure_body_cap(ctx, std::max<uint32_t>(cfg->max_bodies, 256)) != VXP_OK) return bail(VXP_ERR_OOM);
+    if (ctx->w.init(cache_cap, ctx->grid_blocks, ctx->err)) return bail(VXP_ERR_OOM);
+    if (ctx->d_world.reserve(1) != cudaSuccess || ctx->bar.reserve(2) != cudaSuccess) return bail(VXP_ERR_OOM);
+    if (ctx->w.ensure_pairs(std::max<uint32_t>(cfg->max_pairs, 1024), ctx->err)) return bail(VXP_ERR_OOM);
+    if (ctx->w.ensure_bodies(std::max<uint32_t>(cfg->max_bodies, 256), ctx->err)) return bail(VXP_ERR_OOM);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(VXP_ERR_CUDA);
     *out = ctx;
     return VXP_OK;
@@ -880,107 +1120,20 @@ int vxp_last_error(const vxp_ctx* ctx, char* buf, size_t n) {
 
 int vxp_collider_upload(vxp_ctx* ctx, uint32_t collider_id, float voxel_size, const vxp_brick* bricks,
                         uint32_t n_bricks) {
-    if (!ctx || (!bricks && n_bricks)) return fail(ctx, VXP_ERR_ARG, "null argument");
-    if (!(voxel_size > 0.0f)) return fail(ctx, VXP_ERR_ARG, "voxel_size must be positive");
-    HostCollider h;
-    h.id = collider_id;
-    h.vs = voxel_size;
-    h.pos.resize((size_t)n_bricks * 3);
-    h.vox.resize((size_t)n_bricks * 512);
-    std::unordered_map<uint64_t, uint32_t> seen;
-    for (uint32_t i = 0; i < n_bricks; ++i) {
-        for (int k = 0; k < 3; ++k) h.pos[(size_t)i * 3 + k] = bricks[i].pos[k];
-        std::memcpy(&h.vox[(size_t)i * 512], bricks[i].voxels, 512);
-        if (!seen.emplace(hash_brick_pos(bricks[i].pos[0], bricks[i].pos[1], bricks[i].pos[2]), i).second)
-            return fail(ctx, VXP_ERR_ARG, "collider %u: bricks %u and %u share a hashBrickPos value", collider_id,
-                        seen[hash_brick_pos(bricks[i].pos[0], bricks[i].pos[1], bricks[i].pos[2])], i);
-    }
-    collider_metadata(h);
-    auto it = ctx->collider_index.find(collider_id);
-    if (it != ctx->collider_index.end()) ctx->colliders[it->second] = std::move(h);
-    else {
-        ctx->collider_index[collider_id] = (uint32_t)ctx->colliders.size();
-        ctx->colliders.push_back(std::move(h));
-    }
-    ctx->colliders_dirty = true;
-    return VXP_OK;
+    if (!ctx) return VXP_ERR_ARG;
+    return ctx->cols.upload(collider_id, voxel_size, bricks, n_bricks, ctx->err);
 }
 
 int vxp_bodies_set(vxp_ctx* ctx, const vxp_body* b, uint32_t n) {
-    if (!ctx || (!b && n)) return fail(ctx, VXP_ERR_ARG, "null argument");
-    if (int rc = ensure_body_cap(ctx, n)) return rc;
-    std::vector<DBody> db(n);
-    std::vector<DBodyProp> dp(n);
-    std::vector<uint2> ids(n);
-    ctx->body_collider_public.resize(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        const vxp_body& s = b[i];
-        if (s.body_type > 2u) return fail(ctx, VXP_ERR_ARG, "body %u: bad body_type %u", i, s.body_type);
-        DBody& d = db[i];
-        d.p = make_float4(s.position[0], s.position[1], s.position[2], s.inv_mass);
-        d.q = make_float4(s.rotation[0], s.rotation[1], s.rotation[2], s.rotation[3]);
-        d.v = make_float4(s.linear_velocity[0], s.linear_velocity[1], s.linear_velocity[2], 0.f);
-        d.w = make_float4(s.angular_velocity[0], s.angular_velocity[1], s.angular_velocity[2], 0.f);
-        d.i0 = d.i1 = d.i2 = make_float4(0.f, 0.f, 0.f, 0.f);
-        DBodyProp& p = dp[i];
-        for (int k = 0; k < 9; ++k) p.il[k] = s.inv_inertia_local[k];
-        p.friction = s.friction;
-        p.restitution = s.restitution;
-        p.lin_damp = s.linear_damping;
-        p.ang_damp = s.angular_damping;
-        p.sleep_timer = s.sleep_timer;
-        p.id = s.id;
-        p.type = s.body_type;
-        auto it = ctx->collider_index.find(s.collider_id);
-        p.collider = it == ctx->collider_index.end() ? 0xFFFFFFFFu : it->second;
-        p.sleeping = s.is_sleeping ? 1u : 0u;
-        ctx->body_collider_public[i] = s.collider_id;
-        ids[i] = make_uint2(s.id, i);
-    }
-    std::sort(ids.begin(), ids.end(), [](const uint2& x, const uint2& y) { return x.x < y.x; });
-    for (uint32_t i = 1; i < n; ++i)
-        if (ids[i].x == ids[i - 1].x) return fail(ctx, VXP_ERR_ARG, "duplicate body id %u", ids[i].x);
+    if (!ctx) return VXP_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream));
-    if (n) {
-        CK(cudaMemcpy(ctx->body.p, db.data(), n * sizeof(DBody), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->prop.p, dp.data(), n * sizeof(DBodyProp), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->ids.p, ids.data(), n * sizeof(uint2), cudaMemcpyHostToDevice));
-    }
-    ctx->n_bodies = n;
-    return VXP_OK;
+    return ctx->w.set_bodies(b, n, ctx->cols, ctx->err);
 }
 
 int vxp_bodies_get(vxp_ctx* ctx, vxp_body* b, uint32_t n) {
     if (!ctx || (!b && n)) return fail(ctx, VXP_ERR_ARG, "null argument");
-    if (n != ctx->n_bodies) return fail(ctx, VXP_ERR_ARG, "expected %u bodies, got %u", ctx->n_bodies, n);
     if (int rc = check_device_error(ctx)) return rc;
-    std::vector<DBody> db(n);
-    std::vector<DBodyProp> dp(n);
-    if (n) {
-        CK(cudaMemcpy(db.data(), ctx->body.p, n * sizeof(DBody), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(dp.data(), ctx->prop.p, n * sizeof(DBodyProp), cudaMemcpyDeviceToHost));
-    }
-    for (uint32_t i = 0; i < n; ++i) {
-        vxp_body& s = b[i];
-        const DBody& d = db[i];
-        const DBodyProp& p = dp[i];
-        s.id = p.id;
-        s.body_type = p.type;
-        s.collider_id = ctx->body_collider_public[i];
-        s.is_sleeping = p.sleeping;
-        s.position[0] = d.p.x; s.position[1] = d.p.y; s.position[2] = d.p.z;
-        s.rotation[0] = d.q.x; s.rotation[1] = d.q.y; s.rotation[2] = d.q.z; s.rotation[3] = d.q.w;
-        s.linear_velocity[0] = d.v.x; s.linear_velocity[1] = d.v.y; s.linear_velocity[2] = d.v.z;
-        s.angular_velocity[0] = d.w.x; s.angular_velocity[1] = d.w.y; s.angular_velocity[2] = d.w.z;
-        s.inv_mass = d.p.w;
-        for (int k = 0; k < 9; ++k) s.inv_inertia_local[k] = p.il[k];
-        s.friction = p.friction;
-        s.restitution = p.restitution;
-        s.linear_damping = p.lin_damp;
-        s.angular_damping = p.ang_damp;
-        s.sleep_timer = p.sleep_timer;
-    }
-    return VXP_OK;
+    return ctx->w.get_bodies(b, n, ctx->stream, ctx->err);
 }
 
 int vxp_mass_properties(float vs, const vxp_brick* bricks, uint32_t n, float density, float* inv_mass,
@@ -1047,55 +1200,64 @@ int vxp_mass_properties(float vs, const vxp_brick* bricks, uint32_t n, float den
     return VXP_OK;
 }
 
-int vxp_narrow_phase(vxp_ctx* ctx, const vxp_pair* pairs, uint32_t n_pairs);
-
 int vxp_step(vxp_ctx* ctx, float dt, const vxp_pair* pairs, uint32_t n_pairs) {
     if (!ctx || (!pairs && n_pairs)) return fail(ctx, VXP_ERR_ARG, "null argument");
-    if (int rc = ensure_pair_cap(ctx, n_pairs)) return rc;
+    if (int rc = ctx->w.ensure_pairs(n_pairs, ctx->err)) return rc;
     CK(cudaEventRecord(ctx->ev_start, ctx->stream));
-    if (n_pairs) CK(cudaMemcpyAsync(ctx->pairs.p, pairs, n_pairs * sizeof(vxp_pair), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->n_pairs_dev.p, &n_pairs, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    if (n_pairs)
+        CK(cudaMemcpyAsync(ctx->w.pairs.p, pairs, n_pairs * sizeof(vxp_pair), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->w.n_pairs_dev.p, &n_pairs, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     ctx->last_pairs = n_pairs;
-    return launch_step(ctx, dt, n_pairs, PH_STEP);
+    return launch_step(ctx, dt, PH_STEP, false, 0.0f);
 }
 
 int vxp_step_device_pairs(vxp_ctx* ctx, float dt, float margin) {
     if (!ctx) return VXP_ERR_ARG;
-    uint32_t n = 0;
+    // grow ahead of need from the pair count of an earlier step (copied back
+    // without waiting); a list that still overflows leaves the step undone
+    // and is reported as VXP_ERR_CAP at the next wait
+    if (ctx->count_pending && cudaEventQuery(ctx->ev_count) == cudaSuccess) {
+        ctx->count_pending = false;
+        const uint32_t seen = *ctx->h_count;
+        ctx->last_pairs = seen;
+        if (seen > ctx->w.pair_cap - ctx->w.pair_cap / 4u) {
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (int rc = ctx->w.ensure_pairs(seen + seen / 2u + 1024u, ctx->err)) return rc;
+        }
+    }
     CK(cudaEventRecord(ctx->ev_start, ctx->stream));
-    if (int rc = compute_device_pairs(ctx, margin, false, &n)) return rc;
-    ctx->last_pairs = n;
-    return launch_step(ctx, dt, n, PH_STEP);
+    return launch_step(ctx, dt, PH_STEP, true, margin);
 }
 
 // system.narrowPhase() alone: no all-sleeping early return (that test is
 // VoxelPhysicsSystem.step's).
 int vxp_narrow_phase(vxp_ctx* ctx, const vxp_pair* pairs, uint32_t n_pairs) {
     if (!ctx || (!pairs && n_pairs)) return fail(ctx, VXP_ERR_ARG, "null argument");
-    if (int rc = ensure_pair_cap(ctx, n_pairs)) return rc;
+    if (int rc = ctx->w.ensure_pairs(n_pairs, ctx->err)) return rc;
     CK(cudaEventRecord(ctx->ev_start, ctx->stream));
-    if (n_pairs) CK(cudaMemcpyAsync(ctx->pairs.p, pairs, n_pairs * sizeof(vxp_pair), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->n_pairs_dev.p, &n_pairs, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    if (n_pairs)
+        CK(cudaMemcpyAsync(ctx->w.pairs.p, pairs, n_pairs * sizeof(vxp_pair), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->w.n_pairs_dev.p, &n_pairs, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     ctx->last_pairs = n_pairs;
-    return launch_step(ctx, 0.0f, n_pairs, PH_NARROW);
+    return launch_step(ctx, 0.0f, PH_NARROW, false, 0.0f);
 }
 
 // system.solve() + updateSleepStates on the manifolds of the last narrow phase.
 int vxp_solve(vxp_ctx* ctx, float dt) {
     if (!ctx) return VXP_ERR_ARG;
     CK(cudaEventRecord(ctx->ev_start, ctx->stream));
-    return launch_step(ctx, dt, ctx->last_pairs, PH_SOLVE);
+    return launch_step(ctx, dt, PH_SOLVE, false, 0.0f);
 }
 
 int vxp_manifolds_get(vxp_ctx* ctx, vxp_manifold* out, uint32_t cap, uint32_t* n_out) {
     if (!ctx || !n_out) return VXP_ERR_ARG;
     if (int rc = check_device_error(ctx)) return rc;
     uint32_t fr[2];
-    CK(cudaMemcpy(fr, ctx->frame.p, sizeof(fr), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(fr, ctx->w.frame.p, sizeof(fr), cudaMemcpyDeviceToHost));
     // the latest narrow phase wrote man[frame & 1] with fr[1] slots
     const uint32_t slot = fr[0] & 1u;
-    const ManifoldRec* m = slot ? ctx->man1.p : ctx->man0.p;
-    const uint32_t P = fr[1];
+    const ManifoldRec* m = slot ? ctx->w.man1.p : ctx->w.man0.p;
+    const uint32_t P = std::min<uint32_t>(fr[1], ctx->w.pair_cap);
     std::vector<ManifoldRec> hm(P);
     if (P) CK(cudaMemcpy(hm.data(), m, P * sizeof(ManifoldRec), cudaMemcpyDeviceToHost));
     uint32_t k = 0;
@@ -1103,11 +1265,11 @@ int vxp_manifolds_get(vxp_ctx* ctx, vxp_manifold* out, uint32_t cap, uint32_t* n
         if (hm[p].n == 0u) continue;
         if (k < cap && out) {
             // slots past contact_count hold stale data on the device
-            ManifoldRec m = hm[p];
-            m._pad = 0u;
-            for (uint32_t i = m.n; i < 4u; ++i) std::memset(&m.c[i], 0, sizeof(ContactRec));
-            for (uint32_t i = 0; i < m.n; ++i) m.c[i]._pad = 0u;
-            std::memcpy(&out[k], &m, sizeof(vxp_manifold));
+            ManifoldRec r = hm[p];
+            r._pad = 0u;
+            for (uint32_t i = r.n; i < 4u; ++i) std::memset(&r.c[i], 0, sizeof(ContactRec));
+            for (uint32_t i = 0; i < r.n; ++i) r.c[i]._pad = 0u;
+            std::memcpy(&out[k], &r, sizeof(vxp_manifold));
         }
         ++k;
     }
@@ -1117,8 +1279,8 @@ int vxp_manifolds_get(vxp_ctx* ctx, vxp_manifold* out, uint32_t cap, uint32_t* n
 
 int vxp_set_candidate_dump(vxp_ctx* ctx, uint32_t capacity) {
     if (!ctx) return VXP_ERR_ARG;
-    if (capacity && ctx->dump.reserve(capacity) != cudaSuccess) return fail(ctx, VXP_ERR_OOM, "dump buffer");
-    ctx->dump_cap = capacity;
+    if (capacity && ctx->w.dump.reserve(capacity) != cudaSuccess) return fail(ctx, VXP_ERR_OOM, "dump buffer");
+    ctx->w.dump_cap = capacity;
     return VXP_OK;
 }
 
@@ -1126,18 +1288,19 @@ int vxp_candidates_get(vxp_ctx* ctx, vxp_candidate* out, uint32_t cap, uint32_t*
     if (!ctx || !n_out) return VXP_ERR_ARG;
     if (int rc = check_device_error(ctx)) return rc;
     uint32_t n = 0;
-    CK(cudaMemcpy(&n, ctx->ctr.p + C_DUMP_N, sizeof(n), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&n, ctx->w.ctr.p + C_DUMP_N, sizeof(n), cudaMemcpyDeviceToHost));
     *n_out = n;
-    if (n > ctx->dump_cap) return fail(ctx, VXP_ERR_CAP, "candidate dump overflow: %u > %u", n, ctx->dump_cap);
+    if (n > ctx->w.dump_cap) return fail(ctx, VXP_ERR_CAP, "candidate dump overflow: %u > %u", n, ctx->w.dump_cap);
     // cache-consulting pairs are detected speculatively while the cache is
     // replayed; the records of the pairs that hit are not part of the step
     static_assert(sizeof(WorldDev::Cand) == sizeof(vxp_candidate), "candidate layout");
     std::vector<vxp_candidate> all(n);
-    if (n) CK(cudaMemcpy(all.data(), ctx->dump.p, n * sizeof(vxp_candidate), cudaMemcpyDeviceToHost));
+    if (n) CK(cudaMemcpy(all.data(), ctx->w.dump.p, n * sizeof(vxp_candidate), cudaMemcpyDeviceToHost));
     uint32_t P = 0;
-    CK(cudaMemcpy(&P, ctx->frame.p + 1, sizeof(P), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&P, ctx->w.frame.p + 1, sizeof(P), cudaMemcpyDeviceToHost));
+    P = std::min<uint32_t>(P, ctx->w.pair_cap);
     std::vector<PairInfo> pi(P);
-    if (P) CK(cudaMemcpy(pi.data(), ctx->pinfo.p, P * sizeof(PairInfo), cudaMemcpyDeviceToHost));
+    if (P) CK(cudaMemcpy(pi.data(), ctx->w.pinfo.p, P * sizeof(PairInfo), cudaMemcpyDeviceToHost));
     uint32_t k = 0;
     for (uint32_t i = 0; i < n; ++i) {
         const uint32_t p = all[i].pair_index;
@@ -1152,52 +1315,28 @@ int vxp_candidates_get(vxp_ctx* ctx, vxp_candidate* out, uint32_t cap, uint32_t*
 int vxp_stats_get(vxp_ctx* ctx, vxp_stats* s) {
     if (!ctx || !s) return VXP_ERR_ARG;
     if (int rc = check_device_error(ctx)) return rc;
-    uint32_t c[C_NCTR];
-    CK(cudaMemcpy(c, ctx->ctr.p, sizeof(c), cudaMemcpyDeviceToHost));
-    std::memset(s, 0, sizeof(*s));
-    s->pairs_in = ctx->last_pairs;
-    s->pairs_tested = c[C_PAIRS_TESTED];
-    s->pairs_colliding = c[C_PAIRS_COLLIDING];
-    s->voxels_checked = c[C_VOXELS_CHECKED];
-    s->contacts_generated = c[C_CONTACTS];
-    s->pairs_skipped_sleeping = c[C_SKIPPED_SLEEPING];
-    s->manifolds_preserved = c[C_PRESERVED];
-    s->cache_hits = c[C_CACHE_HITS];
-    s->cache_misses = c[C_CACHE_MISSES];
-    s->cache_evictions = c[C_CACHE_EVICTIONS];
-    s->manifolds = c[C_MANIFOLDS];
-    s->constraints = c[C_CONSTRAINTS];
-    s->contact_points = c[C_POINTS];
-    s->colours = c[C_COLOURS];
-    s->position_iterations_run = c[C_POS_ITERS];
-    s->step_skipped = c[C_STEP_SKIPPED];
-    const int32_t k = (int32_t)c[C_MAX_PEN_KEY];
-    int32_t bits = k >= 0 ? k : (k ^ 0x7FFFFFFF);
-    std::memcpy(&s->max_penetration, &bits, 4);
-    s->candidates = c[C_CANDIDATES];
-    s->bricks_touched = c[C_BRICKS];
-    return VXP_OK;
+    return ctx->w.stats(s, ctx->last_pairs, ctx->stream, ctx->err);
 }
 
 int vxp_colours_get(vxp_ctx* ctx, uint32_t* colours, uint32_t cap, uint32_t* n_out) {
     if (!ctx || !n_out) return VXP_ERR_ARG;
     if (int rc = check_device_error(ctx)) return rc;
     uint32_t M = 0;
-    CK(cudaMemcpy(&M, ctx->ctr.p + C_CONSTRAINTS, sizeof(M), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&M, ctx->w.ctr.p + C_CONSTRAINTS, sizeof(M), cudaMemcpyDeviceToHost));
     *n_out = M;
     const uint32_t k = std::min(M, cap);
-    if (k && colours) CK(cudaMemcpy(colours, ctx->colour.p, k * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (k && colours) CK(cudaMemcpy(colours, ctx->w.colour.p, k * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     return VXP_OK;
 }
 
 int vxp_pairs_from_bodies(vxp_ctx* ctx, float margin, vxp_pair* out, uint32_t cap, uint32_t* n_out) {
     if (!ctx || !n_out) return VXP_ERR_ARG;
     uint32_t n = 0;
-    if (int rc = compute_device_pairs(ctx, margin, true, &n)) return rc;
+    if (int rc = compute_device_pairs(ctx, margin, &n)) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     *n_out = n;
     const uint32_t k = std::min(n, cap);
-    if (k && out) CK(cudaMemcpy(out, ctx->pairs.p, k * sizeof(vxp_pair), cudaMemcpyDeviceToHost));
+    if (k && out) CK(cudaMemcpy(out, ctx->w.pairs.p, k * sizeof(vxp_pair), cudaMemcpyDeviceToHost));
     return n > cap ? fail(ctx, VXP_ERR_CAP, "pair output holds %u, need %u", cap, n) : VXP_OK;
 }
 
@@ -1242,12 +1381,11 @@ int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n) {
     if (!ctx || !out) return VXP_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream));
     unsigned long long t[TS_N];
-    CK(cudaMemcpy(t, ctx->ts.p, sizeof(t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(t, ctx->w.ts.p, sizeof(t), cudaMemcpyDeviceToHost));
     for (uint32_t i = 0; i < n && i < TS_N; ++i) out[i] = t[i] >= t[0] ? (uint64_t)(t[i] - t[0]) : 0u;
     return VXP_OK;
 }
 
-// Extensions beyond the reference seams (declared in vxp.h).
 int vxp_synchronize(vxp_ctx* ctx) {
     if (!ctx) return VXP_ERR_ARG;
     return check_device_error(ctx);
@@ -1259,11 +1397,326 @@ int vxp_set_launch_mode(vxp_ctx* ctx, int mode) {
     return VXP_OK;
 }
 
-// Tuning: manifolds per solver block in the grid launch.
 int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div) {
     if (!ctx || div == 0) return VXP_ERR_ARG;
     ctx->solver_div = div;
     return VXP_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched worlds
+// ===========================================================================
+// Many independent worlds advance together: one launch of k_step_block, block
+// b stepping the b-th world of the launch order with the whole step (pair
+// source, narrow phase, solver) inside the CTA.  The launch is captured once
+// in a CUDA graph and replayed every step.  Each world's arithmetic does not
+// depend on the launch shape, so every schedule gives the same bits.
+struct vxp_batch {
+    vxp_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    ColliderStore cols;
+    std::vector<std::unique_ptr<WorldBuffers>> slots;
+    std::vector<uint8_t> active;
+    std::vector<float> est_ms;        // last measured step time per slot
+    std::vector<uint32_t> order;      // launch position -> slot
+    DBuf<WorldDev> d_worlds;
+    DBuf<unsigned long long> d_ts;    // per launch position: [start, end]
+    uint32_t threads = 256;           // CTA size
+    uint32_t order_mode = 1;          // 0: slot order, 1: longest measured / largest first
+    float margin = 0.1f;
+    float built_dt = -1.0f;
+    bool rebuild = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void* graph_key[3] = {nullptr, nullptr, nullptr};
+    uint32_t graph_n = 0, graph_threads = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t cache_cap = 1024;
+};
+
+namespace {
+
+int bfail(vxp_batch* b, int code, const char* f, ...) {
+    if (b) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, f);
+        vsnprintf(buf, sizeof(buf), f, ap);
+        va_end(ap);
+        b->err = buf;
+    }
+    return code;
+}
+#define BK(call)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) return bfail(bt, VXP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+__global__ void k_batch_times(const WorldDev* worlds, uint32_t n, unsigned long long* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long* ts = worlds[i].ts;
+    out[2 * i] = ts[TS_START];
+    out[2 * i + 1] = ts[TS_END] > ts[TS_START] ? ts[TS_END] : ts[TS_START];
+}
+
+// Launch order, device WorldDev array and the graph of one step.
+int batch_prepare(vxp_batch* bt, float dt) {
+    if (int rc = bt->cols.sync(bt->err)) return rc;
+    if (bt->rebuild || dt != bt->built_dt) {
+        std::vector<uint32_t> ord;
+        for (uint32_t s = 0; s < bt->slots.size(); ++s)
+            if (bt->active[s] && bt->slots[s]) ord.push_back(s);
+        if (bt->order_mode == 1) {
+            std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t c) {
+                const float ea = bt->est_ms[a] > 0 ? bt->est_ms[a] : 1e-6f * (float)bt->slots[a]->n_bodies;
+                const float ec = bt->est_ms[c] > 0 ? bt->est_ms[c] : 1e-6f * (float)bt->slots[c]->n_bodies;
+                return ea > ec;
+            });
+        }
+        bt->order = ord;
+        std::vector<WorldDev> wd(ord.size());
+        for (size_t i = 0; i < ord.size(); ++i)
+            wd[i] = bt->slots[ord[i]]->make(bt->cfg, dt, PH_STEP, 128, true, bt->margin);
+        if (bt->d_worlds.reserve(std::max<size_t>(wd.size(), 1)) != cudaSuccess ||
+            bt->d_ts.reserve(2 * std::max<size_t>(wd.size(), 1)) != cudaSuccess)
+            return bfail(bt, VXP_ERR_OOM, "batch world table");
+        if (!wd.empty())
+            BK(cudaMemcpyAsync(bt->d_worlds.p, wd.data(), wd.size() * sizeof(WorldDev), cudaMemcpyHostToDevice,
+                               bt->stream));
+        BK(cudaStreamSynchronize(bt->stream));
+        bt->built_dt = dt;
+        bt->rebuild = false;
+    }
+    const ColliderSet cs = bt->cols.set();
+    const void* key[3] = {bt->d_worlds.p, cs.c, cs.vox};
+    const uint32_t n = (uint32_t)bt->order.size();
+    if (bt->exec && key[0] == bt->graph_key[0] && key[1] == bt->graph_key[1] && key[2] == bt->graph_key[2] &&
+        n == bt->graph_n && bt->threads == bt->graph_threads)
+        return VXP_OK;
+    if (bt->exec) {
+        cudaGraphExecDestroy(bt->exec);
+        bt->exec = nullptr;
+    }
+    if (bt->graph) {
+        cudaGraphDestroy(bt->graph);
+        bt->graph = nullptr;
+    }
+    if (n == 0) return VXP_OK;
+    const size_t smem = step_smem(bt->threads, bt->cache_cap);
+    BK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
+    if (bt->threads == 512) k_step_block<512><<<n, 512, smem, bt->stream>>>(bt->d_worlds.p, cs);
+    else k_step_block<256><<<n, 256, smem, bt->stream>>>(bt->d_worlds.p, cs);
+    const cudaError_t le = cudaGetLastError();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(bt->stream, &g);
+    if (le != cudaSuccess || ce != cudaSuccess)
+        return bfail(bt, VXP_ERR_CUDA, "graph capture: %s / %s", cudaGetErrorString(le), cudaGetErrorString(ce));
+    bt->graph = g;
+    BK(cudaGraphInstantiate(&bt->exec, bt->graph, 0));
+    for (int i = 0; i < 3; ++i) bt->graph_key[i] = key[i];
+    bt->graph_n = n;
+    bt->graph_threads = bt->threads;
+    return VXP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vxp_batch_create(const vxp_config* cfg, int device, uint32_t max_worlds, vxp_batch** out) {
+    if (!cfg || !out || max_worlds == 0) return VXP_ERR_ARG;
+    *out = nullptr;
+    if (cfg->substeps == 0 || cfg->position_iterations > 16 || cfg->brick_pair_cache_size > kMaxCacheSmem)
+        return VXP_ERR_ARG;
+    vxp_batch* bt = new vxp_batch;
+    bt->cfg = *cfg;
+    bt->device = device;
+    bt->cache_cap = cfg->brick_pair_cache_size ? cfg->brick_pair_cache_size : 1024u;
+    bt->slots.resize(max_worlds);
+    bt->active.assign(max_worlds, 0);
+    bt->est_ms.assign(max_worlds, 0.0f);
+    auto bail = [&](int rc) {
+        vxp_batch_destroy(bt);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(VXP_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(VXP_ERR_CUDA);
+    if (cudaEventCreate(&bt->ev0) != cudaSuccess || cudaEventCreate(&bt->ev1) != cudaSuccess)
+        return bail(VXP_ERR_CUDA);
+    if (set_kernel_smem(bt->cache_cap)) return bail(VXP_ERR_CUDA);
+    *out = bt;
+    return VXP_OK;
+}
+
+void vxp_batch_destroy(vxp_batch* bt) {
+    if (!bt) return;
+    if (bt->stream) cudaStreamSynchronize(bt->stream);
+    if (bt->exec) cudaGraphExecDestroy(bt->exec);
+    if (bt->graph) cudaGraphDestroy(bt->graph);
+    if (bt->ev0) cudaEventDestroy(bt->ev0);
+    if (bt->ev1) cudaEventDestroy(bt->ev1);
+    if (bt->stream) cudaStreamDestroy(bt->stream);
+    delete bt;
+}
+
+int vxp_batch_last_error(const vxp_batch* bt, char* buf, size_t n) {
+    if (!bt || !buf || n == 0) return VXP_ERR_ARG;
+    std::snprintf(buf, n, "%s", bt->err.c_str());
+    return VXP_OK;
+}
+
+int vxp_batch_collider_upload(vxp_batch* bt, uint32_t collider_id, float voxel_size, const vxp_brick* bricks,
+                              uint32_t n_bricks) {
+    if (!bt) return VXP_ERR_ARG;
+    BK(cudaStreamSynchronize(bt->stream));
+    return bt->cols.upload(collider_id, voxel_size, bricks, n_bricks, bt->err);
+}
+
+int vxp_batch_world_set(vxp_batch* bt, uint32_t world, const vxp_body* bodies, uint32_t n, uint32_t pair_capacity) {
+    if (!bt || world >= bt->slots.size()) return bfail(bt, VXP_ERR_ARG, "world index out of range");
+    BK(cudaStreamSynchronize(bt->stream));
+    auto& slot = bt->slots[world];
+    // a fresh world starts with an empty contact manager and cache
+    slot.reset(new WorldBuffers);
+    if (int rc = slot->init(bt->cache_cap, 1, bt->err)) return rc;
+    if (int rc = slot->set_bodies(bodies, n, bt->cols, bt->err)) return rc;
+    const uint32_t want = pair_capacity ? pair_capacity : std::max<uint32_t>(1024, 16u * n);
+    if (int rc = slot->ensure_pairs(want, bt->err)) return rc;
+    bt->active[world] = n ? 1 : 0;
+    bt->est_ms[world] = 0.0f;
+    bt->rebuild = true;
+    return VXP_OK;
+}
+
+int vxp_batch_world_clear(vxp_batch* bt, uint32_t world) {
+    if (!bt || world >= bt->slots.size()) return bfail(bt, VXP_ERR_ARG, "world index out of range");
+    BK(cudaStreamSynchronize(bt->stream));
+    bt->slots[world].reset();
+    bt->active[world] = 0;
+    bt->rebuild = true;
+    return VXP_OK;
+}
+
+int vxp_batch_world_get(vxp_batch* bt, uint32_t world, vxp_body* bodies, uint32_t n) {
+    if (!bt || world >= bt->slots.size() || !bt->slots[world]) return bfail(bt, VXP_ERR_ARG, "no such world");
+    BK(cudaStreamSynchronize(bt->stream));
+    return bt->slots[world]->get_bodies(bodies, n, bt->stream, bt->err);
+}
+
+int vxp_batch_world_stats(vxp_batch* bt, uint32_t world, vxp_stats* s) {
+    if (!bt || !s || world >= bt->slots.size() || !bt->slots[world]) return bfail(bt, VXP_ERR_ARG, "no such world");
+    BK(cudaStreamSynchronize(bt->stream));
+    uint32_t np = 0;
+    BK(cudaMemcpy(&np, bt->slots[world]->n_pairs_dev.p, sizeof(np), cudaMemcpyDeviceToHost));
+    return bt->slots[world]->stats(s, np, bt->stream, bt->err);
+}
+
+uint64_t vxp_batch_world_bytes(vxp_batch* bt, uint32_t world) {
+    if (!bt || world >= bt->slots.size() || !bt->slots[world]) return 0;
+    return bt->slots[world]->device_bytes();
+}
+
+int vxp_batch_step(vxp_batch* bt, float dt, uint32_t n_steps) {
+    if (!bt) return VXP_ERR_ARG;
+    if (int rc = batch_prepare(bt, dt)) return rc;
+    if (!bt->exec) return VXP_OK;
+    BK(cudaEventRecord(bt->ev0, bt->stream));
+    for (uint32_t s = 0; s < n_steps; ++s) BK(cudaGraphLaunch(bt->exec, bt->stream));
+    BK(cudaEventRecord(bt->ev1, bt->stream));
+    return VXP_OK;
+}
+
+// Waits; per-world errors; grows worlds whose pair list came close to (or
+// over) capacity.  VXP_ERR_CAP: some world left its last step undone.
+int vxp_batch_synchronize(vxp_batch* bt) {
+    if (!bt) return VXP_ERR_ARG;
+    BK(cudaStreamSynchronize(bt->stream));
+    int rc = VXP_OK;
+    for (uint32_t s = 0; s < bt->slots.size(); ++s) {
+        if (!bt->active[s] || !bt->slots[s]) continue;
+        WorldBuffers& w = *bt->slots[s];
+        std::string e;
+        const int r = w.take_error(bt->stream, e);
+        uint32_t np = 0;
+        BK(cudaMemcpy(&np, w.n_pairs_dev.p, sizeof(np), cudaMemcpyDeviceToHost));
+        if (np > w.pair_cap - w.pair_cap / 4u) {
+            if (int g = w.ensure_pairs(np + np / 2u + 1024u, bt->err)) return g;
+            bt->rebuild = true;
+        }
+        if (r != VXP_OK && rc == VXP_OK) {
+            rc = r;
+            bt->err = fmt("world %u: %s", s, e.c_str());
+        }
+    }
+    return rc;
+}
+
+// Device time of the last step call (ms) and, per world, of its own CTA in
+// the last step (ms, indexed by world slot; 0 for empty slots).
+int vxp_batch_times(vxp_batch* bt, float* total_ms, float* world_ms, uint32_t n) {
+    if (!bt) return VXP_ERR_ARG;
+    BK(cudaStreamSynchronize(bt->stream));
+    if (total_ms) BK(cudaEventElapsedTime(total_ms, bt->ev0, bt->ev1));
+    const uint32_t k = (uint32_t)bt->order.size();
+    if (k) {
+        k_batch_times<<<(k + 127) / 128, 128, 0, bt->stream>>>(bt->d_worlds.p, k, bt->d_ts.p);
+        std::vector<unsigned long long> t(2 * k);
+        BK(cudaMemcpyAsync(t.data(), bt->d_ts.p, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           bt->stream));
+        BK(cudaStreamSynchronize(bt->stream));
+        for (uint32_t i = 0; i < k; ++i) {
+            const float ms = (float)(t[2 * i + 1] - t[2 * i]) * 1e-6f;
+            bt->est_ms[bt->order[i]] = ms;
+        }
+    }
+    if (world_ms)
+        for (uint32_t s = 0; s < n && s < bt->slots.size(); ++s) world_ms[s] = bt->active[s] ? bt->est_ms[s] : 0.0f;
+    return VXP_OK;
+}
+
+// Launch schedule: CTA size (256 or 512) and world order (0 slot order,
+// 1 longest-first by the last measured world time, else by body count).
+int vxp_batch_set_schedule(vxp_batch* bt, uint32_t threads, uint32_t order_mode) {
+    if (!bt || (threads != 256 && threads != 512) || order_mode > 1) return VXP_ERR_ARG;
+    bt->threads = threads;
+    bt->order_mode = order_mode;
+    bt->rebuild = true;
+    return VXP_OK;
+}
+
+// Tries each schedule for trial_steps real steps (each world's results do
+// not depend on the schedule) and keeps the fastest.  ms_out[4] receives the
+// mean step time of (256, slot order), (256, longest first), (512, slot
+// order), (512, longest first); *choice the index kept.
+int vxp_batch_autotune(vxp_batch* bt, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice) {
+    if (!bt || trial_steps == 0) return VXP_ERR_ARG;
+    float best = 1e30f;
+    uint32_t best_i = 0;
+    for (uint32_t i = 0; i < 4; ++i) {
+        if (int rc = vxp_batch_set_schedule(bt, i < 2 ? 256u : 512u, i & 1u)) return rc;
+        if (int rc = vxp_batch_step(bt, dt, 1)) return rc;  // measures world times, builds the graph
+        if (int rc = vxp_batch_synchronize(bt)) return rc;
+        if (int rc = vxp_batch_times(bt, nullptr, nullptr, 0)) return rc;
+        bt->rebuild = true;  // re-sort with the measured times
+        if (int rc = vxp_batch_step(bt, dt, trial_steps)) return rc;
+        if (int rc = vxp_batch_synchronize(bt)) return rc;
+        float ms = 0.f;
+        if (int rc = vxp_batch_times(bt, &ms, nullptr, 0)) return rc;
+        ms /= (float)trial_steps;
+        if (ms_out) ms_out[i] = ms;
+        if (ms < best) {
+            best = ms;
+            best_i = i;
+        }
+    }
+    if (choice) *choice = best_i;
+    return vxp_batch_set_schedule(bt, best_i < 2 ? 256u : 512u, best_i & 1u);
 }
 
 }  // extern "C"

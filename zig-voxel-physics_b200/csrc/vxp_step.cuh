@@ -466,6 +466,91 @@ __device__ bool phase_begin(G& g, WorldDev& w, bool skip_test, bool* skipped) {
 }
 
 // ---------------------------------------------------------------------------
+// Phase: broad phase (the pair list of the step, built on the device)
+// ---------------------------------------------------------------------------
+// The reference hands narrowPhase() the pairs of its AABB trees
+// (broad_phase.zig:606-619).  This pair source keeps every (min id, max id)
+// pair, not both static, whose world AABBs (AABB.transform of the collider's
+// local AABB, math.zig:686-693) inflated by `margin` overlap, sorted by
+// (body_a, body_b): one warp per id-sorted row, lanes sweeping the later
+// rows, a ballot keeping them in order.  *overflow: the list does not fit
+// pair_cap (nothing is written; the host grows the buffers).
+template <class G>
+__device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool* overflow) {
+    const uint32_t N = w.n_bodies;
+    const float m = w.cfg.margin;
+    for (uint32_t i = g.rank(); i < N; i += g.size()) {
+        const DBody b = w.body[i];
+        const F3 x = f3of(b.p);
+        const Qt q = qof(b.q);
+        F3 lo, hi;
+        const uint32_t ci = w.prop[i].collider;
+        if (ci < cs.n) {
+            const DCollider& c = cs.c[ci];
+            const float inf = __int_as_float(0x7f800000);
+            lo = F3{inf, inf, inf};
+            hi = F3{-inf, -inf, -inf};
+            for (int k = 0; k < 8; ++k) {
+                const F3 corner{(k & 1) ? c.aabb_max[0] : c.aabb_min[0], (k & 2) ? c.aabb_max[1] : c.aabb_min[1],
+                                (k & 4) ? c.aabb_max[2] : c.aabb_min[2]};
+                const F3 p = transform_point(x, q, corner);
+                lo = min3(lo, p);
+                hi = max3(hi, p);
+            }
+        } else {
+            lo = x;
+            hi = x;
+        }
+        lo = lo - F3{m, m, m};
+        hi = hi + F3{m, m, m};
+        w.aabb_mn[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
+        w.aabb_mx[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
+    }
+    if (!g.sync()) return false;
+    const uint32_t lane = threadIdx.x & 31, wid = g.rank() >> 5, nw = g.size() >> 5;
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            uint32_t total = 0;
+            if (!group_scan(
+                    g, N, [&](uint32_t i) { return w.pcount[i]; }, [&](uint32_t i, uint32_t pre) { w.poff[i] = pre; },
+                    w.scan, &total))
+                return false;
+            *overflow = total > w.pair_cap;
+            w.n_pairs = total;
+            if (g.rank() == 0) *w.n_pairs_dev = total;
+            if (*overflow) return true;
+        }
+        for (uint32_t s = wid; s < N; s += nw) {
+            const uint2 is = w.ids[s];
+            const float4 a0 = w.aabb_mn[is.y], a1 = w.aabb_mx[is.y];
+            const bool si = w.prop[is.y].type == 0u;
+            uint32_t o = pass ? w.poff[s] : 0u;
+            uint32_t cnt = 0;
+            for (uint32_t t0 = s + 1; t0 < N; t0 += 32u) {
+                const uint32_t t = t0 + lane;
+                bool hit = false;
+                uint2 it = make_uint2(0u, 0u);
+                if (t < N) {
+                    it = w.ids[t];
+                    if (!(si && w.prop[it.y].type == 0u)) {
+                        const float4 b0 = w.aabb_mn[it.y], b1 = w.aabb_mx[it.y];
+                        hit = a0.x <= b1.x && a1.x >= b0.x && a0.y <= b1.y && a1.y >= b0.y && a0.z <= b1.z &&
+                              a1.z >= b0.z;
+                    }
+                }
+                const uint32_t mk = __ballot_sync(0xffffffffu, hit);
+                if (pass && hit) w.pairs[o + __popc(mk & ((1u << lane) - 1u))] = make_uint2(is.x, it.x);
+                o += __popc(mk);
+                cnt += __popc(mk);
+            }
+            if (!pass && lane == 0) w.pcount[s] = cnt;
+        }
+        if (!g.sync()) return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Phase: pairs (system.narrowPhase filter + processPair head)
 // ---------------------------------------------------------------------------
 template <class G>
@@ -1875,17 +1960,30 @@ __device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifol
     const uint32_t ph = w.cfg.phases;
     const uint32_t f0 = *(volatile uint32_t*)&w.frame[0];
     stamp(g, w, TS_START);
-    w.n_pairs = *w.n_pairs_dev;
-    if ((ph & PH_NARROW) && w.n_pairs > w.pair_cap) {
-        // the pair list did not fit: leave every state untouched, the host
-        // grows the buffers and runs the step again
-        if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_CAP);
-        return;
-    }
+    if (w.n_bodies == 0u) return;  // an empty batch slot
+    // per-step counters (the sticky error word excepted)
+    if (g.rank() < C_ERROR) w.ctr[g.rank()] = 0u;
+    if (!g.sync()) return;
     bool skipped = false;
     if (!phase_begin(g, w, (ph & PH_SKIP_TEST) != 0u, &skipped)) return;
     stamp(g, w, TS_BEGIN);
     if (skipped) return;
+    if ((ph & PH_NARROW) && w.cfg.device_pairs) {
+        bool overflow = false;
+        if (!phase_broadphase(g, w, cs, &overflow)) return;
+        if (overflow) {
+            if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_CAP);
+            return;
+        }
+    } else {
+        w.n_pairs = *w.n_pairs_dev;
+        if ((ph & PH_NARROW) && w.n_pairs > w.pair_cap) {
+            // the pair list did not fit: leave every state untouched, the
+            // host grows the buffers and runs the step again
+            if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_CAP);
+            return;
+        }
+    }
     // ContactManager.beginFrame (narrow_phase.zig:1003-1008): the previous
     // "current" manifolds become "previous"
     const uint32_t cur = (ph & PH_NARROW) ? ((f0 + 1u) & 1u) : (f0 & 1u), prev = cur ^ 1u;

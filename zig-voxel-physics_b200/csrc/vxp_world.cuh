@@ -144,6 +144,8 @@ struct StepCfg {
     uint32_t dump_candidates;
     uint32_t phases;          // PH_* bits
     uint32_t solver_div;      // grid launch: solver blocks = manifolds / solver_div
+    uint32_t device_pairs;    // 1: the step builds its own pair list (phase_broadphase)
+    float margin;             // AABB inflation of that pair list
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 
@@ -185,7 +187,7 @@ struct WorldDev {
     StepCfg cfg;
     uint32_t n_bodies;
     uint32_t n_pairs;             // set from *n_pairs_dev at kernel start
-    const uint32_t* n_pairs_dev;  // pair count of this step (device)
+    uint32_t* n_pairs_dev;        // pair count of this step (device)
     uint32_t pair_cap;
     uint32_t ht_cap;              // power of two >= 2 * pair_cap
     uint32_t cache_cap;
@@ -196,6 +198,11 @@ struct WorldDev {
     float4* p0;                   // position at step start (writeBack NaN reset)
     float4* qn;                   // normalised rotation per body (transformPoint)
     uint2* ids;                   // (id, index) sorted by id
+    // pair source
+    float4* aabb_mn;              // inflated world AABB per body
+    float4* aabb_mx;
+    uint32_t* pcount;             // pairs per id-sorted row
+    uint32_t* poff;               // their exclusive prefix
     // pairs
     uint2* pairs;                 // (body_a id, body_b id)
     PairInfo* pinfo;

@@ -175,3 +175,94 @@ class VoxelPhysicsSystem:
         out = np.zeros(3, dtype=np.float32)
         self._check(self.lib.vxp_last_step_ms(self.ctx, abi.ptr(out)))
         return float(out[2])
+
+
+class VoxelWorldBatch:
+    """Many independent worlds stepped together (one CTA per world, one
+    launch per step replayed from a CUDA graph).  Each world's results equal
+    VoxelPhysicsSystem.step(dt) on that world alone."""
+
+    def __init__(self, max_worlds: int, config: abi.Config | None = None, device: int = 0, **overrides):
+        self.lib = abi.load()
+        self.config = config if config is not None else abi.default_config(**overrides)
+        h = ctypes.c_void_p()
+        rc = self.lib.vxp_batch_create(ctypes.byref(self.config), device, int(max_worlds), ctypes.byref(h))
+        if rc != 0 or not h.value:
+            raise VxpError(rc, "vxp_batch_create failed")
+        self.b = h
+        self.max_worlds = int(max_worlds)
+        self.sizes = {}
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.vxp_batch_last_error(self.b, buf, len(buf))
+            raise VxpError(rc, buf.value.decode(errors="replace"))
+
+    def close(self) -> None:
+        if getattr(self, "b", None) is not None and self.b.value:
+            self.lib.vxp_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_collider(self, collider_id: int, voxel_size: float, bricks: np.ndarray) -> None:
+        bricks = np.ascontiguousarray(bricks, dtype=abi.BRICK_DTYPE)
+        self._check(self.lib.vxp_batch_collider_upload(self.b, int(collider_id), np.float32(voxel_size),
+                                                       abi.ptr(bricks), len(bricks)))
+
+    def set_world(self, world: int, bodies: np.ndarray, pair_capacity: int = 0) -> None:
+        bodies = np.ascontiguousarray(bodies, dtype=abi.BODY_DTYPE)
+        self._check(self.lib.vxp_batch_world_set(self.b, int(world), abi.ptr(bodies), len(bodies), int(pair_capacity)))
+        self.sizes[int(world)] = len(bodies)
+
+    def load_scene(self, world: int, scene, collider_offset: int) -> None:
+        """Uploads the scene's colliders under ids offset + id and fills the slot."""
+        for c in scene.colliders:
+            self.add_collider(collider_offset + c.id, c.voxel_size, c.bricks)
+        bodies = scene.bodies.copy()
+        bodies["collider_id"] = bodies["collider_id"] + collider_offset
+        self.set_world(world, bodies)
+
+    def clear_world(self, world: int) -> None:
+        self._check(self.lib.vxp_batch_world_clear(self.b, int(world)))
+        self.sizes.pop(int(world), None)
+
+    def get_world(self, world: int) -> np.ndarray:
+        out = np.zeros(self.sizes[int(world)], dtype=abi.BODY_DTYPE)
+        self._check(self.lib.vxp_batch_world_get(self.b, int(world), abi.ptr(out), len(out)))
+        return out
+
+    def world_stats(self, world: int) -> dict:
+        s = abi.Stats()
+        self._check(self.lib.vxp_batch_world_stats(self.b, int(world), ctypes.byref(s)))
+        return s.as_dict()
+
+    def world_bytes(self, world: int) -> int:
+        return int(self.lib.vxp_batch_world_bytes(self.b, int(world)))
+
+    def step(self, dt: float, n_steps: int = 1) -> None:
+        self._check(self.lib.vxp_batch_step(self.b, np.float32(dt), int(n_steps)))
+
+    def synchronize(self) -> None:
+        self._check(self.lib.vxp_batch_synchronize(self.b))
+
+    def times(self) -> tuple:
+        total = ctypes.c_float(0)
+        per = np.zeros(self.max_worlds, dtype=np.float32)
+        self._check(self.lib.vxp_batch_times(self.b, ctypes.byref(total), abi.ptr(per), self.max_worlds))
+        return float(total.value), per
+
+    def set_schedule(self, threads: int, order_mode: int) -> None:
+        self._check(self.lib.vxp_batch_set_schedule(self.b, int(threads), int(order_mode)))
+
+    def autotune(self, dt: float, trial_steps: int = 3) -> tuple:
+        ms = np.zeros(4, dtype=np.float32)
+        choice = ctypes.c_uint32(0)
+        self._check(self.lib.vxp_batch_autotune(self.b, np.float32(dt), int(trial_steps), abi.ptr(ms),
+                                                ctypes.byref(choice)))
+        return int(choice.value), ms
