@@ -9,7 +9,7 @@ host-side mirror of the reference interface (system.py), the ctypes layer
 The directory name is not a Python identifier: import it with
 importlib.import_module("zig-voxel-physics_b200").
 """
-from . import abi, scenes  # noqa: F401
+from . import abi, scenes, server  # noqa: F401
 from .system import VoxelPhysicsSystem, VoxelWorldBatch, VxpError  # noqa: F401
 
-__all__ = ["abi", "scenes", "VoxelPhysicsSystem", "VoxelWorldBatch", "VxpError"]
+__all__ = ["abi", "scenes", "server", "VoxelPhysicsSystem", "VoxelWorldBatch", "VxpError"]

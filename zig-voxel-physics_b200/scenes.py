@@ -362,19 +362,70 @@ def config1(mass_fn: MassFn | None = None, n_side: int = 4, seed: int = 1, steps
                  notes=f"{n} cubes 8^3 vs0.2 on 64x1x64 slab, seed {seed}")
 
 
+_BOX_CACHE: dict = {}
+
+
+def _box(key, vs, mass_fn):
+    """Bricks and mass properties of one solid box shape (cached by extents)."""
+    k = (key, float(vs), id(mass_fn))
+    if k not in _BOX_CACHE:
+        br = solid_box(*key)
+        _BOX_CACHE[k] = (br, mass_fn(vs, br, np.float32(1.0 / (vs ** 3))))
+    return _BOX_CACHE[k]
+
+
 def _random_box_colliders(rng, n, first_cid, vs, mass_fn, lo=2, hi=16):
     ext = rng.integers(lo, hi + 1, size=(n, 3))
     cols, mass = [], {}
-    cache = {}
-    density = np.float32(1.0 / (vs ** 3))
     for i in range(n):
         key = tuple(int(v) for v in ext[i])
-        if key not in cache:
-            cache[key] = solid_box(*key)
+        br, m = _box(key, vs, mass_fn)
         cid = first_cid + i
-        cols.append(Collider(cid, vs, cache[key]))
-        mass[cid] = mass_fn(vs, cache[key], density)
+        cols.append(Collider(cid, vs, br))
+        mass[cid] = m
     return cols, mass, ext
+
+
+def box_shape_id(ex: int, ey: int, ez: int, lo: int = 2, hi: int = 16) -> int:
+    """Id of a box shape in the shared shape library (1 + index of the extents)."""
+    span = hi - lo + 1
+    return 1 + ((ex - lo) * span + (ey - lo)) * span + (ez - lo)
+
+
+def shape_library(mass_fn=None, vs: float = 0.1, lo: int = 2, hi: int = 16) -> list:
+    """Every config-2 box shape once, ids box_shape_id(...), plus the 64x1x64
+    ground slab as id 0: a server uploads these once and jobs refer to them."""
+    mass_fn = mass_fn or default_mass_fn()
+    out = [Collider(0, vs, slab(64, 64))]
+    for ex in range(lo, hi + 1):
+        for ey in range(lo, hi + 1):
+            for ez in range(lo, hi + 1):
+                br, _ = _box((ex, ey, ez), vs, mass_fn)
+                out.append(Collider(box_shape_id(ex, ey, ez, lo, hi), vs, br))
+    return out
+
+
+def job_bodies(job: dict, mass_fn=None, vs: float = 0.1) -> np.ndarray:
+    """Body table of a served job, its colliders given as shape-library ids."""
+    mass_fn = mass_fn or default_mass_fn()
+    rng = np.random.default_rng(job["seed"])
+    n = job["bodies"]
+    ext = rng.integers(2, 17, size=(n, 3))
+    mass = {}
+    cids = np.zeros(n, dtype=np.int64)
+    for i in range(n):
+        key = tuple(int(v) for v in ext[i])
+        cids[i] = box_shape_id(*key)
+        mass[int(cids[i])] = _box(key, vs, mass_fn)[1]
+    k = np.arange(n)
+    layer, cell = np.divmod(k, 9)
+    cx, cz = np.divmod(cell, 3)
+    half = ext * vs * 0.5
+    pos = np.stack([(cx - 1) * 2.2, 1.5 + layer * 2.8, (cz - 1) * 2.2], axis=1).astype(np.float64) - half
+    pos += rng.uniform(-0.1, 0.1, size=pos.shape)
+    rot = shoemake_quat(rng, n)
+    return np.concatenate([_static_body(1, 0, (-3.2, -vs, -3.2)),
+                           _dynamic_bodies(np.arange(2, n + 2), cids, pos, rot, mass)])
 
 
 def config2(mass_fn: MassFn | None = None, n_side: int = 16, seed: int = 2, steps: int = 600) -> Scene:
