@@ -46,6 +46,13 @@ L2_FLUSH_BYTES = 256 << 20
 SOLVER_V, SOLVER_Q = 1, 2
 
 
+# DRAM bytes (read + write) per launch of the step kernel, from one ncu
+# capture of the same workload (settled pile); re-captured when the kernel
+# changes.
+PROFILED_TRAFFIC = {
+    "config2_pile_4096": (32_957_184, "profiles/k_step_grid_config2_pile.md"),
+}
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -61,6 +68,9 @@ def parse():
                     help="pile: the 4096-body pile (the headline); batched: 256 independent worlds; "
                          "serving: Poisson-arriving jobs through the continuous-batching server")
     ap.add_argument("--jobs", type=int, default=300)
+    ap.add_argument("--state-out", default=None, help="save the body table after settling (npy)")
+    ap.add_argument("--state-in", default=None, help="start from a saved body table instead of settling")
+    ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--slots", type=int, default=512)
     ap.add_argument("--worlds", type=int, default=256)
     return ap.parse_args()
@@ -243,11 +253,16 @@ def ours(args):
     sysm.load_scene(scene)
     sysm.set_launch_mode(args.launch_mode)
     dt = np.float32(scene.dt)
-    for i in range(args.settle):
-        sysm.step(dt)
-        if i % 32 == 31:
-            sysm.synchronize()
+    if args.state_in:
+        sysm.set_bodies(np.load(args.state_in))
+    else:
+        for i in range(args.settle):
+            sysm.step(dt)
+            if i % 32 == 31:
+                sysm.synchronize()
     sysm.synchronize()
+    if args.state_out:
+        np.save(args.state_out, sysm.get_bodies())
     for _ in range(args.warmup):
         sysm.step(dt)
         sysm.synchronize()
@@ -293,7 +308,7 @@ def ours(args):
         pg.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(0 if args.no_e2e else args.steps):
         n = ctypes.c_uint32(0)
         sysm._check(sysm.lib.vxp_pairs_from_bodies(sysm.ctx, np.float32(sysm.pair_margin), abi.ptr(pin_pairs), cap,
                                                     ctypes.byref(n)))
@@ -301,12 +316,12 @@ def ours(args):
         sysm._check(sysm.lib.vxp_bodies_get(sysm.ctx, abi.ptr(pin_bodies), len(pin_bodies)))
         h2d += 8 * n.value
         d2h += 8 * n.value + 128 * len(pin_bodies)
-    e2e_s = time.perf_counter() - t0
+    e2e_s = max(time.perf_counter() - t0, 1e-9)
     if pg:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = ws * n_dyn * 8 * args.steps / e2e_s
+    e2e_value = None if args.no_e2e else ws * n_dyn * 8 * args.steps / e2e_s
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -334,14 +349,16 @@ def ours(args):
             "step_latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                                 "kernel_mean": statistics.mean(kern_ms), "pairs_mean": statistics.mean(pair_ms)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": PROFILED_TRAFFIC.get(f"config2_pile_{n_dyn}", (None,))[0],
+                         "traffic_source": PROFILED_TRAFFIC.get(f"config2_pile_{n_dyn}", (None, None))[1],
+                         "peak_kind": peak_kind,
                          "kernel": "k_step_grid" if n_dyn >= 512 else "k_step_block",
                          "alg_bytes_per_launch": statistics.mean(nb)},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "body-substeps/s", "h2d_bytes_per_step": h2d // args.steps,
-                    "d2h_bytes_per_step": d2h // args.steps},
+            "e2e": {"value": e2e_value, "unit": "body-substeps/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
+                    "d2h_bytes_per_step": d2h // max(1, args.steps)},
             "clocks": clk,
-            "gpu_launches": 5 * args.steps,
+            "gpu_launches": args.steps,
         }
         print(json.dumps(line), flush=True)
     if pg:
