@@ -216,6 +216,7 @@ SIGNATURES = {
     "vxp_set_launch_mode": (_I, [_VP, _I]),
     "vxp_phase_times": (_I, [_VP, _VP, _U32]),
     "vxp_set_solver_blocks_divisor": (_I, [_VP, _U32]),
+    "vxp_set_solver_mode": (_I, [_VP, _U32]),
     "vxp_pairs_noalloc": (_I, [_VP, _VP, _VP, _VP, _VP, _U32, _F, _VP, _U32, _VP, _VP]),
     "vxp_batch_create": (_I, [_VP, _I, _U32, ctypes.POINTER(_VP)]),
     "vxp_batch_destroy": (None, [_VP]),
@@ -230,6 +231,7 @@ SIGNATURES = {
     "vxp_batch_synchronize": (_I, [_VP]),
     "vxp_batch_times": (_I, [_VP, _VP, _VP, _U32]),
     "vxp_batch_set_schedule": (_I, [_VP, _U32, _U32]),
+    "vxp_batch_set_solver_mode": (_I, [_VP, _U32]),
     "vxp_batch_autotune": (_I, [_VP, _F, _U32, _VP, _VP]),
 }
 

@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) k_step_block(WorldDe
     WorldDev w = worlds[blockIdx.x];
     const CacheSmem csm = cache_smem(smem_raw, blockDim.x / 32u, w.cache_cap);
     BlockGroup g;
-    world_step(g, w, cs, wsm, csm);
+    world_step(g, w, cs, wsm, csm, reinterpret_cast<float*>(smem_raw));
 }
 template __global__ void k_step_block<256>(WorldDev*, ColliderSet);
 template __global__ void k_step_block<512>(WorldDev*, ColliderSet);
@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(512) k_step_grid(const WorldDev* world, Collid
     WorldDev w = *world;
     const CacheSmem csm = cache_smem(smem_raw, blockDim.x / 32u, w.cache_cap);
     GridGroup g{bar, &w.ctr[C_ERROR], timeout_ns, gridDim.x};
-    world_step(g, w, cs, wsm, csm);
+    world_step(g, w, cs, wsm, csm, reinterpret_cast<float*>(smem_raw));
 }
 
 // Pair source: world AABB of each body's collider (AABB.transform,
@@ -215,6 +215,13 @@ size_t step_smem(uint32_t threads, uint32_t cache_cap) {
     return sizeof(WarpManifold) * (threads / 32) +
            (size_t)cache_cap * (sizeof(uint2) + sizeof(unsigned long long) + sizeof(uint32_t));
 }
+// The grid kernel (one CTA per SM) also keeps up to kGridFlowChunks chunks of
+// constraint rows per block in shared memory during the solve.
+constexpr uint32_t kGridFlowChunks = 4;
+size_t grid_smem(uint32_t cache_cap) {
+    return std::max(step_smem(512, cache_cap), (size_t)kGridFlowChunks * kChunkFloats * sizeof(float));
+}
+uint32_t flow_chunks(size_t smem) { return (uint32_t)(smem / (kChunkFloats * sizeof(float))); }
 
 uint64_t hash_brick_pos(int32_t x, int32_t y, int32_t z) {  // collider.zig:187-192
     const uint64_t ux = (uint64_t)(int64_t)x, uy = (uint64_t)(int64_t)y, uz = (uint64_t)(int64_t)z;
@@ -419,6 +426,7 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
     s.solver_div = 128;
     s.device_pairs = 0;
     s.margin = 0.1f;
+    s.solver_flow = 1;
     return s;
 }
 
@@ -440,8 +448,11 @@ struct WorldBuffers {
     DBuf<uint32_t> frame;
     DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag, clist;
     DBuf<float> cp;
-    DBuf<uint4> cm;
+    DBuf<uint4> cm, rk;
     DBuf<float2> cfr;
+    DBuf<uint32_t> ev;
+    DBuf<DBody> snap;
+    DBuf<uint2> chunk;
     DBuf<uint32_t> colour_cnt, colour_cur, scan, ctr, cwriter;
     DBuf<unsigned long long> ts, cframe;
     DBuf<CacheKeyRec> ckey;
@@ -492,6 +503,8 @@ struct WorldBuffers {
         ok &= clist.reserve(cap) == cudaSuccess;
         ok &= cp.reserve((size_t)CP_NFIELDS * 4 * cap) == cudaSuccess;
         ok &= cm.reserve(cap) == cudaSuccess;
+        ok &= rk.reserve(cap) == cudaSuccess;
+        ok &= chunk.reserve((size_t)cap / 32 + 257) == cudaSuccess;
         ok &= cfr.reserve(cap) == cudaSuccess;
         if (!ok) {
             err = fmt("pair buffers: device allocation of %u pairs failed", cap);
@@ -545,6 +558,8 @@ struct WorldBuffers {
         ok &= adj_off.reserve((size_t)cap + 1) == cudaSuccess;
         ok &= adj_cur.reserve(cap) == cudaSuccess;
         ok &= bmask.reserve((size_t)cap * 8) == cudaSuccess;
+        ok &= ev.reserve(cap) == cudaSuccess;
+        ok &= snap.reserve((size_t)cap * 2) == cudaSuccess;
         if (!ok) {
             err = fmt("body buffers: device allocation of %u bodies failed", cap);
             return VXP_ERR_OOM;
@@ -644,11 +659,12 @@ struct WorldBuffers {
     }
 
     WorldDev make(const vxp_config& cfg, float dt, uint32_t phases, uint32_t solver_div, bool device_pairs,
-                  float margin) const {
+                  float margin, uint32_t solver_flow) const {
         WorldDev w;
         std::memset(&w, 0, sizeof(w));
         w.cfg = step_cfg(cfg, dt, dump_cap ? 1u : 0u, phases);
         w.cfg.solver_div = solver_div;
+        w.cfg.solver_flow = solver_flow;
         w.cfg.device_pairs = device_pairs ? 1u : 0u;
         w.cfg.margin = margin;
         w.n_bodies = n_bodies;
@@ -690,6 +706,10 @@ struct WorldBuffers {
         w.bmask = bmask.p;
         w.cp = cp.p;
         w.cm = cm.p;
+        w.rk = rk.p;
+        w.ev = ev.p;
+        w.snap = snap.p;
+        w.chunk = chunk.p;
         w.cfr = cfr.p;
         w.scan = scan.p;
         w.flag = flag.p;
@@ -704,7 +724,8 @@ struct WorldBuffers {
                ids.bytes() + pcount.bytes() + poff.bytes() + adj_off.bytes() + adj_cur.bytes() + bmask.bytes() +
                pairs.bytes() + pinfo.bytes() + man0.bytes() + man1.bytes() + ht0.bytes() + ht1.bytes() +
                cons.bytes() + colour.bytes() + pos_of.bytes() + packed_pair.bytes() + adj.bytes() + flag.bytes() +
-               clist.bytes() + cp.bytes() + cm.bytes() + cfr.bytes() + ckey.bytes() + cval.bytes() +
+               clist.bytes() + cp.bytes() + cm.bytes() + rk.bytes() + ev.bytes() + snap.bytes() + chunk.bytes() + cfr.bytes() +
+               ckey.bytes() + cval.bytes() +
                cwriter.bytes() + scan.bytes() + ctr.bytes() + ts.bytes() + dump.bytes();
     }
 
@@ -753,8 +774,12 @@ struct WorldBuffers {
         const uint32_t z = 0;
         cudaMemcpy(ctr.p + C_ERROR, &z, sizeof(z), cudaMemcpyHostToDevice);
         if (e & ERR_TIMEOUT) {
-            err = fmt("a grid barrier wait ran out (error bits 0x%x)", e);
+            err = fmt("a grid barrier or solver wait ran out (error bits 0x%x)", e);
             return VXP_ERR_TIMEOUT;
+        }
+        if (e & ERR_BOUNDS) {
+            err = fmt("an index of the solver's constraint table was out of range (error bits 0x%x)", e);
+            return VXP_ERR_STATE;
         }
         if (e & ERR_CAP) {
             err = fmt("pair list exceeded the device capacity; the step left the state untouched (bits 0x%x)", e);
@@ -789,6 +814,7 @@ struct vxp_ctx {
     bool count_pending = false;
     int use_grid = -1;  // -1 auto, 0 block, 1 grid
     uint32_t solver_div = 128;
+    uint32_t solver_flow = 1;
 };
 
 namespace {
@@ -813,11 +839,12 @@ int fail(vxp_ctx* c, int code, const char* f, ...) {
 // Runs the step kernel.  device_pairs: the kernel builds the pair list itself.
 int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, float margin) {
     if (int rc = ctx->cols.sync(ctx->err)) return rc;
-    WorldDev w = ctx->w.make(ctx->cfg, dt, phases, ctx->solver_div, device_pairs, margin);
+    WorldDev w = ctx->w.make(ctx->cfg, dt, phases, ctx->solver_div, device_pairs, margin, ctx->solver_flow);
+    const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
+    const size_t smem = grid ? grid_smem(w.cache_cap) : step_smem(kBlockThreads, w.cache_cap);
+    w.cfg.flow_smem_chunks = flow_chunks(smem);
     CK(cudaMemcpyAsync(ctx->d_world.p, &w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
     const ColliderSet cs = ctx->cols.set();
-    const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
-    const size_t smem = step_smem(kBlockThreads, w.cache_cap);
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (grid) {
         CK(cudaMemsetAsync(ctx->bar.p, 0, 2 * sizeof(GridBar), ctx->stream));
@@ -1054,7 +1081,7 @@ static int set_kernel_smem(uint32_t cache_cap) {
         cudaFuncSetAttribute(k_step_block<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)step_smem(512, cache_cap)) != cudaSuccess ||
         cudaFuncSetAttribute(k_step_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)step_smem(512, cache_cap)) != cudaSuccess)
+                             (int)grid_smem(cache_cap)) != cudaSuccess)
         return VXP_ERR_CUDA;
     return VXP_OK;
 }
@@ -1086,8 +1113,8 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     const uint32_t cache_cap = cfg->brick_pair_cache_size ? cfg->brick_pair_cache_size : 1024u;
     if (set_kernel_smem(cache_cap)) return bail(VXP_ERR_CUDA);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads,
-                                                      step_smem(kBlockThreads, cache_cap)) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads, grid_smem(cache_cap)) !=
+            cudaSuccess ||
         per_sm < 1)
         return bail(VXP_ERR_CUDA);
     ctx->grid_blocks = (uint32_t)(smc * std::min(per_sm, 2));
@@ -1403,6 +1430,12 @@ int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div) {
     return VXP_OK;
 }
 
+int vxp_set_solver_mode(vxp_ctx* ctx, uint32_t mode) {
+    if (!ctx || mode > 1u) return VXP_ERR_ARG;
+    ctx->solver_flow = mode;
+    return VXP_OK;
+}
+
 }  // extern "C"
 
 // ===========================================================================
@@ -1436,6 +1469,7 @@ struct vxp_batch {
     uint32_t graph_n = 0, graph_threads = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t cache_cap = 1024;
+    uint32_t solver_flow = 1;
 };
 
 namespace {
@@ -1482,7 +1516,8 @@ int batch_prepare(vxp_batch* bt, float dt) {
         bt->order = ord;
         std::vector<WorldDev> wd(ord.size());
         for (size_t i = 0; i < ord.size(); ++i)
-            wd[i] = bt->slots[ord[i]]->make(bt->cfg, dt, PH_STEP, 128, true, bt->margin);
+            wd[i] = bt->slots[ord[i]]->make(bt->cfg, dt, PH_STEP, 128, true, bt->margin, bt->solver_flow);
+        for (auto& x : wd) x.cfg.flow_smem_chunks = flow_chunks(step_smem(bt->threads, x.cache_cap));
         if (bt->d_worlds.reserve(std::max<size_t>(wd.size(), 1)) != cudaSuccess ||
             bt->d_ts.reserve(2 * std::max<size_t>(wd.size(), 1)) != cudaSuccess)
             return bfail(bt, VXP_ERR_OOM, "batch world table");
@@ -1682,6 +1717,13 @@ int vxp_batch_times(vxp_batch* bt, float* total_ms, float* world_ms, uint32_t n)
 
 // Launch schedule: CTA size (256 or 512) and world order (0 slot order,
 // 1 longest-first by the last measured world time, else by body count).
+int vxp_batch_set_solver_mode(vxp_batch* bt, uint32_t mode) {
+    if (!bt || mode > 1u) return VXP_ERR_ARG;
+    bt->solver_flow = mode;
+    bt->rebuild = true;
+    return VXP_OK;
+}
+
 int vxp_batch_set_schedule(vxp_batch* bt, uint32_t threads, uint32_t order_mode) {
     if (!bt || (threads != 256 && threads != 512) || order_mode > 1) return VXP_ERR_ARG;
     bt->threads = threads;

@@ -1314,7 +1314,42 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
     if ((threadIdx.x & 31) == 0 && pts) atomicAdd(&w.ctr[C_POINTS], pts);
     if (g.rank() == 0) w.ctr[C_CONSTRAINTS] = M;
 
-    // 2. colouring
+    // 2. adjacency of the bodies the solver writes (dynamic, awake): the
+    // constraints of each, for the colouring and for event-ordered sweeps
+    uint32_t kin = 0;
+    for (uint32_t k = g.rank(); k < M; k += g.size()) {
+        const PairInfo& pi = w.pinfo[w.cons[k]];
+        const DBodyProp& pa = w.prop[pi.ia];
+        const DBodyProp& pb = w.prop[pi.ib];
+        if (writable(pa)) atomicAdd(&w.adj_off[pi.ia], 1u);
+        if (writable(pb)) atomicAdd(&w.adj_off[pi.ib], 1u);
+        kin += ((pa.type == 1u && !pa.sleeping) || (pb.type == 1u && !pb.sleeping)) ? 1u : 0u;
+    }
+    kin = warp_sum(kin);
+    if ((threadIdx.x & 31) == 0 && kin) atomicAdd(&w.ctr[C_KIN_CONTACT], kin);
+    if (!g.sync()) return false;
+    {
+        uint32_t tot;
+        // in-place exclusive scan: read counts into adj_cur, write offsets
+        for (uint32_t i = g.rank(); i < N; i += g.size()) w.adj_cur[i] = w.adj_off[i];
+        if (!g.sync()) return false;
+        if (!group_scan(
+                g, N, [&](uint32_t i) { return w.adj_cur[i]; }, [&](uint32_t i, uint32_t pre) { w.adj_off[i] = pre; },
+                w.scan, &tot))
+            return false;
+        if (g.rank() == 0) w.adj_off[N] = tot;
+        for (uint32_t i = g.rank(); i < N; i += g.size()) w.adj_cur[i] = 0u;
+        if (!g.sync()) return false;
+        for (uint32_t k = g.rank(); k < M; k += g.size()) {
+            const PairInfo& pi = w.pinfo[w.cons[k]];
+            if (writable(w.prop[pi.ia])) w.adj[w.adj_off[pi.ia] + atomicAdd(&w.adj_cur[pi.ia], 1u)] = k;
+            if (writable(w.prop[pi.ib])) w.adj[w.adj_off[pi.ib] + atomicAdd(&w.adj_cur[pi.ib], 1u)] = k;
+            w.colour[k] = 0xFFFFFFFFu;
+        }
+        if (!g.sync()) return false;
+    }
+
+    // 3. colouring
     if (w.cfg.colouring == 1u) {
         // GraphColoring.build (islands.zig:668-736) over every manifold in
         // pair order, all bodies as nodes; one thread.
@@ -1340,30 +1375,6 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
         if (!g.sync()) return false;
     } else {
         // Jones-Plassmann over writable bodies == greedy in priority order.
-        for (uint32_t k = g.rank(); k < M; k += g.size()) {
-            const PairInfo& pi = w.pinfo[w.cons[k]];
-            if (writable(w.prop[pi.ia])) atomicAdd(&w.adj_off[pi.ia], 1u);
-            if (writable(w.prop[pi.ib])) atomicAdd(&w.adj_off[pi.ib], 1u);
-            w.colour[k] = 0xFFFFFFFFu;
-        }
-        if (!g.sync()) return false;
-        uint32_t tot;
-        // in-place exclusive scan: read counts into adj_cur, write offsets
-        for (uint32_t i = g.rank(); i < N; i += g.size()) w.adj_cur[i] = w.adj_off[i];
-        if (!g.sync()) return false;
-        if (!group_scan(
-                g, N, [&](uint32_t i) { return w.adj_cur[i]; }, [&](uint32_t i, uint32_t pre) { w.adj_off[i] = pre; },
-                w.scan, &tot))
-            return false;
-        if (g.rank() == 0) w.adj_off[N] = tot;
-        for (uint32_t i = g.rank(); i < N; i += g.size()) w.adj_cur[i] = 0u;
-        if (!g.sync()) return false;
-        for (uint32_t k = g.rank(); k < M; k += g.size()) {
-            const PairInfo& pi = w.pinfo[w.cons[k]];
-            if (writable(w.prop[pi.ia])) w.adj[w.adj_off[pi.ia] + atomicAdd(&w.adj_cur[pi.ia], 1u)] = k;
-            if (writable(w.prop[pi.ib])) w.adj[w.adj_off[pi.ib] + atomicAdd(&w.adj_cur[pi.ib], 1u)] = k;
-        }
-        if (!g.sync()) return false;
         // rounds; three rotating counters at scan[nblocks .. nblocks+3)
         uint32_t* rem = w.scan + g.nblocks();
         for (uint32_t round = 0;; ++round) {
@@ -1420,7 +1431,7 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
             if (r == 0u) break;
         }
     }
-    // 3. colour-major packing + ContactSolver.addManifold (solver.zig:449-491)
+    // 4. colour-major packing + ContactSolver.addManifold (solver.zig:449-491)
     for (uint32_t k = g.rank(); k < M; k += g.size()) {
         if (w.colour[k] > 255u) w.colour[k] = 255u;  // only after ERR_COLOURS
         atomicAdd(&w.colour_cnt[w.colour[k]], 1u);
@@ -1519,6 +1530,43 @@ __device__ __forceinline__ Qt integrate_rotation_small(Qt r, F3 d) {  // solver.
     return qnormalize(Qt{r.x + dq.x, r.y + dq.y, r.z + dq.z, r.w + dq.w});
 }
 
+// applyGravity for one dynamic awake body (solver.zig:564-605): gravity,
+// extra damping below 0.5 m/s, damping, zeroing of tiny velocities.
+__device__ __forceinline__ void body_gravity(float4& v4, float4& w4, const DBodyProp& pr, F3 grav, float h) {
+    F3 v = f3of(v4), av = f3of(w4);
+    v = v + grav * h;
+    float ld = pr.lin_damp, adp = pr.ang_damp;
+    const float ls = len3(v), as = len3(av);
+    if (ls < 0.5f) ld += 5.0f * (1.0f - (ls / 0.5f));
+    if (as < 0.5f) adp += 5.0f * (1.0f - (as / 0.5f));
+    const float ldec = fmaxf(0.0f, 1.0f - ld * h), adec = fmaxf(0.0f, 1.0f - adp * h);
+    v = v * ldec;
+    av = av * adec;
+    if (lensq3(v) < 0.001f * 0.001f) v = F3{0.f, 0.f, 0.f};
+    if (lensq3(av) < 0.001f * 0.001f) av = F3{0.f, 0.f, 0.f};
+    v4 = make_float4(v.x, v.y, v.z, 0.f);
+    w4 = make_float4(av.x, av.y, av.z, 0.f);
+}
+// BodyState.integratePosition for one awake non-static body
+// (solver.zig:341-356): position, rotation and, for dynamic bodies, the world
+// inverse inertia.
+__device__ __forceinline__ void body_integrate(DBody& b, const DBodyProp& pr, float h, bool disable_rotation) {
+    const F3 x = f3of(b.p) + f3of(b.v) * h;
+    Qt q = qof(b.q);
+    if (!disable_rotation) q = integrate_rotation(q, f3of(b.w), h);
+    b.p = make_float4(x.x, x.y, x.z, b.p.w);
+    b.q = f4of(q);
+    if (pr.type == 2u) {
+        M33 il;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) il.m[k] = pr.il[k];
+        const M33 m = world_inv_inertia(q, il);
+        b.i0 = make_float4(m.m[0], m.m[1], m.m[2], 0.f);
+        b.i1 = make_float4(m.m[3], m.m[4], m.m[5], 0.f);
+        b.i2 = make_float4(m.m[6], m.m[7], m.m[8], 0.f);
+    }
+}
+
 // Local copy of one body's velocity state for a manifold sweep.
 struct BV {
     F3 p, v, w;
@@ -1551,27 +1599,37 @@ __device__ __forceinline__ void store_bv(WorldDev& w, uint32_t i, const BV& b) {
     w.body[i].v = make_float4(b.v.x, b.v.y, b.v.z, 0.f);
     w.body[i].w = make_float4(b.w.x, b.w.y, b.w.z, 0.f);
 }
-__device__ __forceinline__ F3 ld3(const WorldDev& w, uint32_t f, uint32_t s, uint32_t pos) {
-    return F3{w.cp[cpi(w, f, s, pos)], w.cp[cpi(w, f + 1, s, pos)], w.cp[cpi(w, f + 2, s, pos)]};
+// The constraint-point fields of one manifold: field f of point slot s is
+// b[(f * 4 + s) * st].  In global memory b = cp + position, st = pair
+// capacity; a chunk held in shared memory has b = chunk + lane, st = 32.
+struct CPV {
+    float* b;
+    uint32_t st;
+};
+__device__ __forceinline__ CPV cpv_global(const WorldDev& w, uint32_t pos) { return CPV{w.cp + pos, w.pair_cap}; }
+__device__ __forceinline__ float& cpr(const CPV& v, uint32_t f, uint32_t s) {
+    return v.b[(size_t)(f * 4u + s) * v.st];
 }
-__device__ __forceinline__ void st3(WorldDev& w, uint32_t f, uint32_t s, uint32_t pos, F3 v) {
-    w.cp[cpi(w, f, s, pos)] = v.x;
-    w.cp[cpi(w, f + 1, s, pos)] = v.y;
-    w.cp[cpi(w, f + 2, s, pos)] = v.z;
+__device__ __forceinline__ F3 ld3(const CPV& v, uint32_t f, uint32_t s) {
+    return F3{cpr(v, f, s), cpr(v, f + 1, s), cpr(v, f + 2, s)};
+}
+__device__ __forceinline__ void st3(const CPV& v, uint32_t f, uint32_t s, F3 x) {
+    cpr(v, f, s) = x.x;
+    cpr(v, f + 1, s) = x.y;
+    cpr(v, f + 2, s) = x.z;
 }
 
-// prepareConstraints for one point (solver.zig:608-699).
-__device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft& soft, float hinv) {
-    const uint4 cmv = w.cm[pos];
-    const BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
-    const Qt qa = qof(w.body[cmv.x].q), qb = qof(w.body[cmv.y].q);
-    const F3 n = ld3(w, CP_NX, i, pos);
-    const F3 wa = qrotate(qa, ld3(w, CP_LAX, i, pos)) + a.p;
-    const F3 wb = qrotate(qb, ld3(w, CP_LBX, i, pos)) + b.p;
+// prepareConstraints for one point (solver.zig:608-699), from the two
+// bodies' state after applyGravity.
+__device__ void prepare_point_s(const WorldDev& w, const CPV& v, float restitution, uint32_t i, const Soft& soft,
+                                float hinv, const BV& a, Qt qa, const BV& b, Qt qb) {
+    const F3 n = ld3(v, CP_NX, i);
+    const F3 wa = qrotate(qa, ld3(v, CP_LAX, i)) + a.p;
+    const F3 wb = qrotate(qb, ld3(v, CP_LBX, i)) + b.p;
     const F3 ra = wa - a.p, rb = wb - b.p;
     const F3 pt = (wa + wb) * 0.5f;
     const F3 ad = wb - wa;
-    const float sep = w.cp[cpi(w, CP_BASE, i, pos)] + dot3(ad, n);
+    const float sep = cpr(v, CP_BASE, i) + dot3(ad, n);
     const F3 rna = cross3(ra, n), rnb = cross3(rb, n);
     float k = a.im + b.im;
     k += dot3(rna, mat3_mul_vec(a.I, rna));
@@ -1582,12 +1640,12 @@ __device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft&
     float bias;
     if (sep > 0.0f) bias = sep * hinv;
     else bias = fmaxf(soft.bias_rate * sep, -0.2f);
-    if (w.cfg.restitution_on && vn < -1.0f) bias = fmaxf(bias, -w.cfr[pos].y * vn);
-    st3(w, CP_RAX, i, pos, ra);
-    st3(w, CP_RBX, i, pos, rb);
-    st3(w, CP_PX, i, pos, pt);
-    w.cp[cpi(w, CP_NM, i, pos)] = nm;
-    w.cp[cpi(w, CP_BIAS, i, pos)] = bias;
+    if (w.cfg.restitution_on && vn < -1.0f) bias = fmaxf(bias, -restitution * vn);
+    st3(v, CP_RAX, i, ra);
+    st3(v, CP_RBX, i, rb);
+    st3(v, CP_PX, i, pt);
+    cpr(v, CP_NM, i) = nm;
+    cpr(v, CP_BIAS, i) = bias;
     if (w.cfg.friction_on) {
         const F3 t1 = compute_orthogonal(n);
         const F3 t2 = cross3(n, t1);
@@ -1599,28 +1657,37 @@ __device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft&
         float k2 = a.im + b.im;
         k2 += dot3(r2a, mat3_mul_vec(a.I, r2a));
         k2 += dot3(r2b, mat3_mul_vec(b.I, r2b));
-        st3(w, CP_T1X, i, pos, t1);
-        st3(w, CP_T2X, i, pos, t2);
-        w.cp[cpi(w, CP_TM0, i, pos)] = k1 > kEpsilon ? 1.0f / k1 : 0.0f;
-        w.cp[cpi(w, CP_TM1, i, pos)] = k2 > kEpsilon ? 1.0f / k2 : 0.0f;
+        st3(v, CP_T1X, i, t1);
+        st3(v, CP_T2X, i, t2);
+        cpr(v, CP_TM0, i) = k1 > kEpsilon ? 1.0f / k1 : 0.0f;
+        cpr(v, CP_TM1, i) = k2 > kEpsilon ? 1.0f / k2 : 0.0f;
     }
+}
+__device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft& soft, float hinv) {
+    const uint4 cmv = w.cm[pos];
+    const BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
+    const Qt qa = qof(w.body[cmv.x].q), qb = qof(w.body[cmv.y].q);
+    prepare_point_s(w, cpv_global(w, pos), w.cfr[pos].y, i, soft, hinv, a, qa, b, qb);
 }
 
 // warmStart for one manifold (solver.zig:702-729).
+__device__ void warm_points(const CPV& v, uint32_t n, float scale, BV& a, BV& b) {
+    for (uint32_t i = 0; i < n; ++i) {
+        const float sn = cpr(v, CP_NI, i) * scale;
+        const float s1 = cpr(v, CP_TI0, i) * scale;
+        const float s2 = cpr(v, CP_TI1, i) * scale;
+        const F3 imp = (ld3(v, CP_NX, i) * sn + ld3(v, CP_T1X, i) * s1) + ld3(v, CP_T2X, i) * s2;
+        apply_impulse(a, -imp, ld3(v, CP_RAX, i));
+        apply_impulse(b, imp, ld3(v, CP_RBX, i));
+        cpr(v, CP_NI, i) = sn;
+        cpr(v, CP_TI0, i) = s1;
+        cpr(v, CP_TI1, i) = s2;
+    }
+}
 __device__ void warm_manifold(WorldDev& w, uint32_t pos, float scale) {
     const uint4 cmv = w.cm[pos];
     BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
-    for (uint32_t i = 0; i < cmv.z; ++i) {
-        const float sn = w.cp[cpi(w, CP_NI, i, pos)] * scale;
-        const float s1 = w.cp[cpi(w, CP_TI0, i, pos)] * scale;
-        const float s2 = w.cp[cpi(w, CP_TI1, i, pos)] * scale;
-        const F3 imp = (ld3(w, CP_NX, i, pos) * sn + ld3(w, CP_T1X, i, pos) * s1) + ld3(w, CP_T2X, i, pos) * s2;
-        apply_impulse(a, -imp, ld3(w, CP_RAX, i, pos));
-        apply_impulse(b, imp, ld3(w, CP_RBX, i, pos));
-        w.cp[cpi(w, CP_NI, i, pos)] = sn;
-        w.cp[cpi(w, CP_TI0, i, pos)] = s1;
-        w.cp[cpi(w, CP_TI1, i, pos)] = s2;
-    }
+    warm_points(cpv_global(w, pos), cmv.z, scale, a, b);
     store_bv(w, cmv.x, a);
     store_bv(w, cmv.y, b);
 }
@@ -1630,21 +1697,21 @@ struct PtV {
     F3 pt, n, ra, rb, t1, t2;
     float nm, bias, tm0, tm1, ni, ti0, ti1;
 };
-__device__ __forceinline__ PtV load_ptv(const WorldDev& w, uint32_t i, uint32_t pos) {
+__device__ __forceinline__ PtV load_ptv(const CPV& v, uint32_t i) {
     PtV r;
-    r.pt = ld3(w, CP_PX, i, pos);
-    r.n = ld3(w, CP_NX, i, pos);
-    r.ra = ld3(w, CP_RAX, i, pos);
-    r.rb = ld3(w, CP_RBX, i, pos);
-    r.t1 = ld3(w, CP_T1X, i, pos);
-    r.t2 = ld3(w, CP_T2X, i, pos);
-    r.nm = w.cp[cpi(w, CP_NM, i, pos)];
-    r.bias = w.cp[cpi(w, CP_BIAS, i, pos)];
-    r.tm0 = w.cp[cpi(w, CP_TM0, i, pos)];
-    r.tm1 = w.cp[cpi(w, CP_TM1, i, pos)];
-    r.ni = w.cp[cpi(w, CP_NI, i, pos)];
-    r.ti0 = w.cp[cpi(w, CP_TI0, i, pos)];
-    r.ti1 = w.cp[cpi(w, CP_TI1, i, pos)];
+    r.pt = ld3(v, CP_PX, i);
+    r.n = ld3(v, CP_NX, i);
+    r.ra = ld3(v, CP_RAX, i);
+    r.rb = ld3(v, CP_RBX, i);
+    r.t1 = ld3(v, CP_T1X, i);
+    r.t2 = ld3(v, CP_T2X, i);
+    r.nm = cpr(v, CP_NM, i);
+    r.bias = cpr(v, CP_BIAS, i);
+    r.tm0 = cpr(v, CP_TM0, i);
+    r.tm1 = cpr(v, CP_TM1, i);
+    r.ni = cpr(v, CP_NI, i);
+    r.ti0 = cpr(v, CP_TI0, i);
+    r.ti1 = cpr(v, CP_TI1, i);
     return r;
 }
 
@@ -1652,16 +1719,13 @@ __device__ __forceinline__ PtV load_ptv(const WorldDev& w, uint32_t i, uint32_t 
 // Points run in slot order (Gauss-Seidel inside the manifold); the next
 // point's fields are loaded before this point's results are stored, so the
 // loads overlap the dependent arithmetic.
-__device__ void velocity_manifold(WorldDev& w, uint32_t pos, const Soft& soft, bool use_bias) {
-    const uint4 cmv = w.cm[pos];
-    const float fr = w.cfr[pos].x;
-    BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
-    const uint32_t n = cmv.z;
+__device__ void velocity_points(const WorldDev& w, const CPV& v, uint32_t n, float fr, const Soft& soft,
+                                bool use_bias, BV& a, BV& b) {
     if (n == 0u) return;
-    PtV c = load_ptv(w, 0, pos);
+    PtV c = load_ptv(v, 0);
     for (uint32_t i = 0; i < n; ++i) {
         PtV nx;
-        if (i + 1u < n) nx = load_ptv(w, i + 1u, pos);
+        if (i + 1u < n) nx = load_ptv(v, i + 1u);
         const F3 rv = point_vel(b, c.pt) - point_vel(a, c.pt);
         const float vn = dot3(rv, c.n);
         float imp;
@@ -1701,39 +1765,62 @@ __device__ void velocity_manifold(WorldDev& w, uint32_t pos, const Soft& soft, b
                 apply_impulse(b, I2, c.rb);
             }
         }
-        w.cp[cpi(w, CP_NI, i, pos)] = ni;
-        w.cp[cpi(w, CP_TI0, i, pos)] = ti0;
-        w.cp[cpi(w, CP_TI1, i, pos)] = ti1;
+        cpr(v, CP_NI, i) = ni;
+        cpr(v, CP_TI0, i) = ti0;
+        cpr(v, CP_TI1, i) = ti1;
         if (i + 1u < n) c = nx;
     }
+}
+__device__ void velocity_manifold(WorldDev& w, uint32_t pos, const Soft& soft, bool use_bias) {
+    const uint4 cmv = w.cm[pos];
+    if (cmv.z == 0u) return;
+    const float fr = w.cfr[pos].x;
+    BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
+    velocity_points(w, cpv_global(w, pos), cmv.z, fr, soft, use_bias, a, b);
     store_bv(w, cmv.x, a);
     store_bv(w, cmv.y, b);
 }
 
+// One body's pose state for a position sweep.
+struct PB {
+    F3 x;
+    Qt q;
+    float im;
+    M33 I;
+    bool wr;
+};
+__device__ __forceinline__ PB pb_of(float4 p, float4 q, float4 i0, float4 i1, float4 i2, bool wr) {
+    PB r;
+    r.x = f3of(p);
+    r.q = qof(q);
+    r.im = p.w;
+    r.I.m[0] = i0.x; r.I.m[1] = i0.y; r.I.m[2] = i0.z;
+    r.I.m[3] = i1.x; r.I.m[4] = i1.y; r.I.m[5] = i1.z;
+    r.I.m[6] = i2.x; r.I.m[7] = i2.y; r.I.m[8] = i2.z;
+    r.wr = wr;
+    return r;
+}
+__device__ __forceinline__ void store_pb(WorldDev& w, uint32_t i, const PB& b) {
+    if (!b.wr) return;
+    w.body[i].p = make_float4(b.x.x, b.x.y, b.x.z, b.im);
+    w.body[i].q = f4of(b.q);
+}
+
 // solvePositionConstraints for one manifold (solver.zig:860-923).
-__device__ void position_manifold(WorldDev& w, uint32_t pos, float* min_sep, float* max_pen) {
-    const uint4 cmv = w.cm[pos];
-    const DBodyProp& pa = w.prop[cmv.x];
-    const DBodyProp& pb = w.prop[cmv.y];
-    if (pa.type == 0u && pb.type == 0u) return;
-    DBody& A = w.body[cmv.x];
-    DBody& B = w.body[cmv.y];
-    F3 xa = f3of(A.p), xb = f3of(B.p);
-    Qt qa = qof(A.q), qb = qof(B.q);
-    const float ima = A.p.w, imb = B.p.w;
-    M33 Ia, Ib;
-    Ia.m[0] = A.i0.x; Ia.m[1] = A.i0.y; Ia.m[2] = A.i0.z; Ia.m[3] = A.i1.x; Ia.m[4] = A.i1.y;
-    Ia.m[5] = A.i1.z; Ia.m[6] = A.i2.x; Ia.m[7] = A.i2.y; Ia.m[8] = A.i2.z;
-    Ib.m[0] = B.i0.x; Ib.m[1] = B.i0.y; Ib.m[2] = B.i0.z; Ib.m[3] = B.i1.x; Ib.m[4] = B.i1.y;
-    Ib.m[5] = B.i1.z; Ib.m[6] = B.i2.x; Ib.m[7] = B.i2.y; Ib.m[8] = B.i2.z;
-    const bool wa_ = writable(pa), wb_ = writable(pb);
+__device__ void position_points(const WorldDev& w, const CPV& v, uint32_t n, PB& A, PB& B, float* min_sep,
+                                float* max_pen) {
+    F3 xa = A.x, xb = B.x;
+    Qt qa = A.q, qb = B.q;
+    const float ima = A.im, imb = B.im;
+    const M33 Ia = A.I, Ib = B.I;
+    const bool wa_ = A.wr, wb_ = B.wr;
     const float slop = w.cfg.slop;
-    for (uint32_t i = 0; i < cmv.z; ++i) {
-        const F3 n = ld3(w, CP_NX, i, pos);
-        const F3 wa = qrotate(qa, ld3(w, CP_LAX, i, pos)) + xa;
-        const F3 wb = qrotate(qb, ld3(w, CP_LBX, i, pos)) + xb;
+    for (uint32_t i = 0; i < n; ++i) {
+        const F3 n = ld3(v, CP_NX, i);
+        const F3 wa = qrotate(qa, ld3(v, CP_LAX, i)) + xa;
+        const F3 wb = qrotate(qb, ld3(v, CP_LBX, i)) + xb;
         const F3 ad = wb - wa;
-        const float sep = w.cp[cpi(w, CP_BASE, i, pos)] + dot3(ad, n);
+        const float sep = cpr(v, CP_BASE, i) + dot3(ad, n);
         *min_sep = fminf(*min_sep, sep);
         *max_pen = fmaxf(*max_pen, -sep);
         if (sep >= -slop) continue;
@@ -1754,14 +1841,45 @@ __device__ void position_manifold(WorldDev& w, uint32_t pos, float* min_sep, flo
             qb = integrate_rotation_small(qb, mat3_mul_vec(Ib, cross3(rb, pimp)));
         }
     }
-    if (wa_) {
-        A.p = make_float4(xa.x, xa.y, xa.z, ima);
-        A.q = f4of(qa);
+    A.x = xa;
+    A.q = qa;
+    B.x = xb;
+    B.q = qb;
+}
+__device__ void position_manifold(WorldDev& w, uint32_t pos, float* min_sep, float* max_pen) {
+    const uint4 cmv = w.cm[pos];
+    const DBodyProp& pa = w.prop[cmv.x];
+    const DBodyProp& pb = w.prop[cmv.y];
+    if (pa.type == 0u && pb.type == 0u) return;
+    const DBody& A = w.body[cmv.x];
+    const DBody& B = w.body[cmv.y];
+    PB a = pb_of(A.p, A.q, A.i0, A.i1, A.i2, writable(pa));
+    PB b = pb_of(B.p, B.q, B.i0, B.i1, B.i2, writable(pb));
+    position_points(w, cpv_global(w, pos), cmv.z, a, b, min_sep, max_pen);
+    store_pb(w, cmv.x, a);
+    store_pb(w, cmv.y, b);
+}
+
+// End of one position sweep: reduce its min separation and max penetration
+// over the group and decide the early break (solver.zig:917-921).
+template <class G>
+__device__ bool pos_sweep_end(G& g, WorldDev& w, uint32_t it, float mn, float mx, bool* brk) {
+    int32_t kmn = fkey(mn), kmx = fkey(mx);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        kmn = min(kmn, __shfl_xor_sync(0xffffffffu, kmn, d));
+        kmx = max(kmx, __shfl_xor_sync(0xffffffffu, kmx, d));
     }
-    if (wb_) {
-        B.p = make_float4(xb.x, xb.y, xb.z, imb);
-        B.q = f4of(qb);
+    int32_t* minsep = reinterpret_cast<int32_t*>(w.scan + g.nblocks() + 4u);  // 16 slots
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&minsep[it & 15u], kmn);
+        atomicMax(reinterpret_cast<int32_t*>(&w.ctr[C_MAX_PEN_KEY]), kmx);
     }
+    if (g.rank() == 0) w.ctr[C_POS_ITERS] += 1u;
+    if (!g.sync()) return false;
+    const float ms = fkey_inv(*(volatile int32_t*)&minsep[it & 15u]);
+    *brk = ms >= -3.0f * w.cfg.slop;
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -1784,19 +1902,10 @@ __device__ bool phase_solve(G& g, WorldDev& w, uint32_t M, uint32_t ncol) {
             const DBodyProp& pr = w.prop[i];
             if (!(pr.type == 2u && pr.sleeping == 0u)) continue;
             DBody& b = w.body[i];
-            F3 v = f3of(b.v), av = f3of(b.w);
-            v = v + grav * h;
-            float ld = pr.lin_damp, adp = pr.ang_damp;
-            const float ls = len3(v), as = len3(av);
-            if (ls < 0.5f) ld += 5.0f * (1.0f - (ls / 0.5f));
-            if (as < 0.5f) adp += 5.0f * (1.0f - (as / 0.5f));
-            const float ldec = fmaxf(0.0f, 1.0f - ld * h), adec = fmaxf(0.0f, 1.0f - adp * h);
-            v = v * ldec;
-            av = av * adec;
-            if (lensq3(v) < 0.001f * 0.001f) v = F3{0.f, 0.f, 0.f};
-            if (lensq3(av) < 0.001f * 0.001f) av = F3{0.f, 0.f, 0.f};
-            b.v = make_float4(v.x, v.y, v.z, 0.f);
-            b.w = make_float4(av.x, av.y, av.z, 0.f);
+            float4 v = b.v, av = b.w;
+            body_gravity(v, av, pr, grav, h);
+            b.v = v;
+            b.w = av;
         }
         if (!g.sync()) return false;
         if (has) {
@@ -1824,21 +1933,9 @@ __device__ bool phase_solve(G& g, WorldDev& w, uint32_t M, uint32_t ncol) {
         for (uint32_t i = g.rank(); i < N; i += g.size()) {
             const DBodyProp& pr = w.prop[i];
             if (pr.type == 0u || pr.sleeping) continue;
-            DBody& b = w.body[i];
-            const F3 x = f3of(b.p) + f3of(b.v) * h;
-            Qt q = qof(b.q);
-            if (!cf.disable_rotation) q = integrate_rotation(q, f3of(b.w), h);
-            b.p = make_float4(x.x, x.y, x.z, b.p.w);
-            b.q = f4of(q);
-            if (pr.type == 2u) {
-                M33 il;
-#pragma unroll
-                for (int k = 0; k < 9; ++k) il.m[k] = pr.il[k];
-                const M33 m = world_inv_inertia(q, il);
-                b.i0 = make_float4(m.m[0], m.m[1], m.m[2], 0.f);
-                b.i1 = make_float4(m.m[3], m.m[4], m.m[5], 0.f);
-                b.i2 = make_float4(m.m[6], m.m[7], m.m[8], 0.f);
-            }
+            DBody b = w.body[i];
+            body_integrate(b, pr, h, cf.disable_rotation != 0u);
+            w.body[i] = b;
         }
         if (!g.sync()) return false;
         if (has) {
@@ -1857,22 +1954,359 @@ __device__ bool phase_solve(G& g, WorldDev& w, uint32_t M, uint32_t ncol) {
                 for (uint32_t pos = lo + g.rank(); pos < hi; pos += g.size()) position_manifold(w, pos, &mn, &mx);
                 if (!g.sync()) return false;
             }
-            // reduce min separation / max penetration of this sweep
-            int32_t kmn = fkey(mn), kmx = fkey(mx);
-#pragma unroll
-            for (int d = 16; d > 0; d >>= 1) {
-                kmn = min(kmn, __shfl_xor_sync(0xffffffffu, kmn, d));
-                kmx = max(kmx, __shfl_xor_sync(0xffffffffu, kmx, d));
+            bool brk = false;
+            if (!pos_sweep_end(g, w, it, mn, mx, &brk)) return false;
+            if (brk) break;
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Phase: solve with event-ordered sweeps
+// ---------------------------------------------------------------------------
+// Every sweep of ContactSolver.solve visits the manifolds in colour-major
+// order, and a manifold reads and writes only its two bodies.  The result of
+// the sweeps is therefore fixed by the order in which each body sees its own
+// manifolds: in sweep k, body b (d_b manifolds) sees them in position order as
+// events k*d_b .. k*d_b + d_b - 1.  Here each manifold waits until every body
+// it writes has seen exactly the events before its own (one counter per
+// body), applies itself and advances those counters.  Nothing waits for a
+// whole colour batch or a whole sweep: a manifold of the next sweep starts as
+// soon as its own bodies are through.  The body steps between sweeps are done
+// by the manifold that applies a body's last event of the sweep before them
+// (integrate after the last velocity sweep of a substep, gravity after the
+// relax sweep), and prepare reads a copy of each body taken right after its
+// gravity step.  Each body sees the same operations in the same order as with
+// a barrier after every colour batch, so the results are bit-identical.
+//
+// Progress: a warp takes its chunks in increasing (sweep, chunk) order, the
+// chunks are colour-major and a chunk only waits for chunks earlier in that
+// order (a chunk's manifolds share no written body), so the earliest
+// unfinished chunk of the whole group is always ready; all blocks of a group
+// are resident.  Every wait is bounded (kFlowTimeoutNs) and ends the step with
+// ERR_TIMEOUT, which also stops every other waiting warp.  A step whose
+// colouring overflowed (ERR_COLOURS: one colour may then hold manifolds of
+// the same body) uses colour barriers instead.
+constexpr unsigned long long kFlowTimeoutNs = 2000000000ull;
+
+enum : uint32_t { FK_WARM = 0, FK_VEL = 1, FK_RELAX = 2, FK_POS = 3 };
+struct FlowSweep {
+    uint32_t kind, s, r;  // kind, substep, velocity iteration (FK_VEL) or position iteration (FK_POS)
+};
+// Floats of one chunk's constraint-point fields in shared memory.
+constexpr uint32_t kChunkFloats = CP_NFIELDS * 4u * 32u;
+struct FlowCtx {
+    uint32_t W, S, V;  // warm-start sweep (0/1), substeps, velocity iterations
+    uint32_t smem_chunks;  // chunks of each block held in shared memory
+    Soft soft, hard;
+    float h, hinv, warm_scale;
+    F3 grav;
+    bool dis_rot;
+};
+__device__ __forceinline__ FlowSweep flow_sweep(uint32_t k, const FlowCtx& fc) {
+    if (fc.W) {
+        if (k == 0u) return FlowSweep{FK_WARM, 0u, 0u};
+        k -= 1u;
+    }
+    const uint32_t per = fc.V + 1u;
+    if (k < fc.S * per) {
+        const uint32_t s = k / per, r = k - s * per;
+        return FlowSweep{r < fc.V ? FK_VEL : FK_RELAX, s, r};
+    }
+    return FlowSweep{FK_POS, fc.S, k - fc.S * per};
+}
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// A body record read through L2: another SM may have written it this step.
+__device__ __forceinline__ DBody ld_body_cg(const DBody* b) {
+    const float4* f = reinterpret_cast<const float4*>(b);
+    DBody r;
+    r.p = __ldcg(f + 0);
+    r.q = __ldcg(f + 1);
+    r.v = __ldcg(f + 2);
+    r.w = __ldcg(f + 3);
+    r.i0 = __ldcg(f + 4);
+    r.i1 = __ldcg(f + 5);
+    r.i2 = __ldcg(f + 6);
+    return r;
+}
+__device__ __forceinline__ BV bv_of(const DBody& d, bool wr) {
+    BV r;
+    r.p = f3of(d.p);
+    r.im = d.p.w;
+    r.v = f3of(d.v);
+    r.w = f3of(d.w);
+    r.I.m[0] = d.i0.x; r.I.m[1] = d.i0.y; r.I.m[2] = d.i0.z;
+    r.I.m[3] = d.i1.x; r.I.m[4] = d.i1.y; r.I.m[5] = d.i1.z;
+    r.I.m[6] = d.i2.x; r.I.m[7] = d.i2.y; r.I.m[8] = d.i2.z;
+    r.wr = wr;
+    return r;
+}
+
+// Writes one body back after a velocity-type sweep event, with the body step
+// that follows its last event of the sweep.
+// The body step after a body's last event of sweep sw: 1 integrate, 2 gravity.
+__device__ __forceinline__ uint32_t flow_body_op(const FlowCtx& fc, const FlowSweep& sw, uint32_t rank, uint32_t deg) {
+    if (rank == 0xFFFFFFFFu || rank + 1u != deg) return 0u;
+    if (sw.kind == FK_VEL && sw.r + 1u == fc.V) return 1u;
+    if (sw.kind == FK_RELAX && sw.s + 1u < fc.S) return 2u;
+    return 0u;
+}
+__device__ __forceinline__ void flow_body_out(WorldDev& w, const FlowCtx& fc, uint32_t op, uint32_t i, const BV& x,
+                                              DBody d, const DBodyProp& pr, uint32_t snap_par) {
+    d.v = make_float4(x.v.x, x.v.y, x.v.z, 0.f);
+    d.w = make_float4(x.w.x, x.w.y, x.w.z, 0.f);
+    if (op == 1u) {
+        body_integrate(d, pr, fc.h, fc.dis_rot);  // integratePositions of substep s
+        w.body[i] = d;
+    } else if (op == 2u) {
+        body_gravity(d.v, d.w, pr, fc.grav, fc.h);  // applyGravity of substep s + 1
+        w.body[i].v = d.v;
+        w.body[i].w = d.w;
+        w.snap[(size_t)snap_par * w.n_bodies + i] = d;
+    } else {
+        w.body[i].v = d.v;
+        w.body[i].w = d.w;
+    }
+}
+
+// prepareConstraints of substep s for one manifold, from its bodies' state
+// right after applyGravity of that substep (the copy in w.snap for bodies the
+// solver writes; the others do not change during the solve).
+__device__ __noinline__ void flow_prepare(WorldDev& w, const FlowCtx& fc, uint32_t s, uint32_t pos, const CPV& v,
+                                          const uint4& cmv, const uint4& rkv) {
+    if (cmv.z == 0u) return;
+    const bool wa = rkv.x != 0xFFFFFFFFu, wb = rkv.z != 0xFFFFFFFFu;
+    const size_t so = (size_t)(s & 1u) * w.n_bodies;
+    const DBody SA = ld_body_cg((wa ? w.snap + so : w.body) + cmv.x);
+    const DBody SB = ld_body_cg((wb ? w.snap + so : w.body) + cmv.y);
+    const BV sa = bv_of(SA, wa), sb = bv_of(SB, wb);
+    const float rest = w.cfr[pos].y;
+    for (uint32_t i = 0; i < cmv.z; ++i) prepare_point_s(w, v, rest, i, fc.soft, fc.hinv, sa, qof(SA.q), sb, qof(SB.q));
+}
+
+// One manifold in one sweep, once its bodies are ready.
+__device__ __noinline__ void flow_item(WorldDev& w, const FlowCtx& fc, uint32_t k, uint32_t pos, const CPV& v,
+                                       const uint4& cmv, const uint4& rkv, float* mn, float* mx) {
+    const FlowSweep sw = flow_sweep(k, fc);
+    const bool wa = rkv.x != 0xFFFFFFFFu, wb = rkv.z != 0xFFFFFFFFu;
+    const uint32_t opa = flow_body_op(fc, sw, rkv.x, rkv.y), opb = flow_body_op(fc, sw, rkv.z, rkv.w);
+    DBodyProp pa, pb;
+    if (opa) pa = w.prop[cmv.x];
+    if (opb) pb = w.prop[cmv.y];
+    const DBody A = ld_body_cg(w.body + cmv.x), B = ld_body_cg(w.body + cmv.y);
+    if (sw.kind == FK_POS) {
+        if (!wa && !wb && w.prop[cmv.x].type == 0u && w.prop[cmv.y].type == 0u) return;
+        PB a = pb_of(A.p, A.q, A.i0, A.i1, A.i2, wa), b = pb_of(B.p, B.q, B.i0, B.i1, B.i2, wb);
+        position_points(w, v, cmv.z, a, b, mn, mx);
+        store_pb(w, cmv.x, a);
+        store_pb(w, cmv.y, b);
+        return;
+    }
+    BV a = bv_of(A, wa), b = bv_of(B, wb);
+    if (sw.kind == FK_WARM)
+        warm_points(v, cmv.z, fc.warm_scale, a, b);
+    else
+        velocity_points(w, v, cmv.z, w.cfr[pos].x, sw.kind == FK_VEL ? fc.soft : fc.hard, sw.kind == FK_VEL, a, b);
+    const uint32_t par = (sw.s + 1u) & 1u;
+    if (wa) flow_body_out(w, fc, opa, cmv.x, a, A, pa, par);
+    if (wb) flow_body_out(w, fc, opb, cmv.y, b, B, pb, par);
+}
+
+// Waits until every lane of the warp sees its bodies' event counters at the
+// values given (at_least: at or past them).  Bounded: gives up after
+// kFlowTimeoutNs or when another warp gave up, returning false.
+__device__ __forceinline__ bool flow_wait(WorldDev& w, bool need_a, uint32_t a, uint32_t ea, bool need_b, uint32_t b,
+                                          uint32_t eb, bool at_least) {
+    bool ready = !need_a && !need_b;
+    uint32_t spins = 0;
+    unsigned long long t0 = 0;
+    while (true) {
+        if (!ready) {
+            const uint32_t va = need_a ? ld_relaxed_u32(w.ev + a) : ea;
+            const uint32_t vb = need_b ? ld_relaxed_u32(w.ev + b) : eb;
+            ready = at_least ? (va >= ea && vb >= eb) : (va == ea && vb == eb);
+        }
+        if (__all_sync(0xffffffffu, ready)) return true;
+        if (spins == 0u) t0 = global_ns();
+        ++spins;
+        bool stop = false;
+        if ((spins & 63u) == 0u) {
+            if (global_ns() - t0 > kFlowTimeoutNs) atomicOr(&w.ctr[C_ERROR], ERR_TIMEOUT);
+            stop = (ld_relaxed_u32(&w.ctr[C_ERROR]) & ERR_TIMEOUT) != 0u;
+        }
+        if (__any_sync(0xffffffffu, stop)) return false;
+        __nanosleep(20);
+    }
+}
+
+// Runs sweeps [k0, k1).  The packed manifolds are cut into chunks of at most
+// 32 positions that never cross a colour boundary (w.chunk: first and end
+// position), so the manifolds of one chunk share no body the solver writes.
+// Warp gw of the group takes chunks gw, gw + nwarps, ... in every sweep; it
+// waits until all 32 lanes' bodies are ready, then the whole warp applies its
+// chunk at once.  Warps are numbered across blocks first, spreading the
+// chunks of a sweep over as many SMs as the group has.  Block b's L-th chunk
+// is chunk L * nblocks + b; the first fc.smem_chunks of them keep their
+// constraint-point fields in shared memory (fsm) for the whole solve.
+template <class G>
+__device__ bool flow_run(G& g, WorldDev& w, const FlowCtx& fc, float* fsm, uint32_t T, uint32_t k0, uint32_t k1,
+                         float* mn, float* mx) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwb = blockDim.x >> 5;
+    const uint32_t gw = (threadIdx.x >> 5) * g.nblocks() + g.block(), nw = nwb * g.nblocks();
+    const uint32_t nj = gw < T ? (T - gw + nw - 1u) / nw : 0u;
+    if (nj == 0u) return true;  // uniform over the warp
+    for (uint32_t k = k0; k < k1; ++k) {
+        const FlowSweep sw = flow_sweep(k, fc);
+        const bool first = sw.kind == FK_WARM || (sw.kind == FK_VEL && sw.r == 0u && !(fc.W && sw.s == 0u));
+        for (uint32_t j = 0; j < nj; ++j) {
+            const uint2 ch = w.chunk[gw + j * nw];
+            const uint32_t pos = ch.x + lane;
+            bool valid = pos < ch.y && ch.y <= w.pair_cap;
+            const uint32_t L = (threadIdx.x >> 5) + j * nwb;
+            const CPV v = L < fc.smem_chunks ? CPV{fsm + (size_t)L * kChunkFloats + lane, 32u} : cpv_global(w, pos);
+            uint4 cmv = make_uint4(0u, 0u, 0u, 0u), rkv = make_uint4(0xFFFFFFFFu, 0u, 0xFFFFFFFFu, 0u);
+            if (valid) {
+                cmv = w.cm[pos];
+                rkv = w.rk[pos];
+                // guard: an index out of range is reported, never followed
+                if (cmv.x >= w.n_bodies || cmv.y >= w.n_bodies || cmv.z > 4u ||
+                    (rkv.x != 0xFFFFFFFFu && rkv.x >= rkv.y) || (rkv.z != 0xFFFFFFFFu && rkv.z >= rkv.w)) {
+                    atomicOr(&w.ctr[C_ERROR], ERR_BOUNDS);
+                    valid = false;
+                    cmv = make_uint4(0u, 0u, 0u, 0u);
+                    rkv = make_uint4(0xFFFFFFFFu, 0u, 0xFFFFFFFFu, 0u);
+                }
             }
-            int32_t* minsep = reinterpret_cast<int32_t*>(w.scan + g.nblocks() + 4u);  // 16 slots
-            if ((threadIdx.x & 31) == 0) {
-                atomicMin(&minsep[it & 15u], kmn);
-                atomicMax(reinterpret_cast<int32_t*>(&w.ctr[C_MAX_PEN_KEY]), kmx);
+            const bool need_a = rkv.x != 0xFFFFFFFFu, need_b = rkv.z != 0xFFFFFFFFu;
+            if (first) {
+                // first sweep of a substep: prepare as soon as both bodies are
+                // through the previous sweep (their gravity copy is written),
+                // ahead of this manifold's own turn in the sweep
+                if (!flow_wait(w, need_a, cmv.x, k * rkv.y, need_b, cmv.y, k * rkv.w, true)) return false;
+                fence_acq_rel_gpu();
+                if (valid) flow_prepare(w, fc, sw.s, pos, v, cmv, rkv);
             }
-            if (g.rank() == 0) w.ctr[C_POS_ITERS] += 1u;
-            if (!g.sync()) return false;
-            const float ms = fkey_inv(*(volatile int32_t*)&minsep[it & 15u]);
-            if (ms >= -3.0f * cf.slop) break;
+            const uint32_t ea = k * rkv.y + rkv.x, eb = k * rkv.w + rkv.z;
+            if (!flow_wait(w, need_a, cmv.x, ea, need_b, cmv.y, eb, false)) return false;
+            fence_acq_rel_gpu();
+            if (valid) flow_item(w, fc, k, pos, v, cmv, rkv, mn, mx);
+            fence_acq_rel_gpu();
+            if (need_a) st_relaxed_u32(w.ev + cmv.x, ea + 1u);
+            if (need_b) st_relaxed_u32(w.ev + cmv.y, eb + 1u);
+        }
+    }
+    return true;
+}
+
+template <class G>
+__device__ bool phase_solve_flow(G& g, WorldDev& w, float* fsm, uint32_t M, uint32_t ncol) {
+    const StepCfg& cf = w.cfg;
+    FlowCtx fc;
+    fc.S = cf.substeps;
+    fc.V = cf.vel_iters;
+    fc.W = (cf.warm_starting && M > 0u) ? 1u : 0u;
+    fc.h = cf.dt / (float)cf.substeps;
+    fc.soft = soft_params(cf.hertz, cf.damping_ratio, fc.h);
+    fc.hard = Soft{0.f, 1.f, 1.f};
+    fc.hinv = fc.h > kEpsilon ? 1.0f / fc.h : 0.0f;
+    fc.warm_scale = cf.warm_scale;
+    fc.grav = F3{cf.gravity[0], cf.gravity[1], cf.gravity[2]};
+    fc.dis_rot = cf.disable_rotation != 0u;
+    fc.smem_chunks = cf.flow_smem_chunks;
+    const uint32_t N = w.n_bodies;
+    // Bodies: counters to zero; gravity of substep 0 and its copy for
+    // prepare; a moving body without constraints takes all its substeps now.
+    for (uint32_t i = g.rank(); i < N; i += g.size()) {
+        w.ev[i] = 0u;
+        const DBodyProp& pr = w.prop[i];
+        const bool dyn = pr.type == 2u && !pr.sleeping, kin = pr.type == 1u && !pr.sleeping;
+        if (!dyn && !kin) continue;
+        DBody b = w.body[i];
+        const uint32_t deg = dyn ? w.adj_off[i + 1u] - w.adj_off[i] : 0u;
+        if (deg == 0u) {
+            for (uint32_t s = 0; s < fc.S; ++s) {
+                if (dyn) body_gravity(b.v, b.w, pr, fc.grav, fc.h);
+                body_integrate(b, pr, fc.h, fc.dis_rot);
+            }
+        } else {
+            body_gravity(b.v, b.w, pr, fc.grav, fc.h);
+            w.snap[i] = b;
+        }
+        w.body[i] = b;
+    }
+    // Manifolds: rank among the constraints of each writable body, in
+    // position order, and that body's constraint count.
+    for (uint32_t k = g.rank(); k < M; k += g.size()) {
+        const uint32_t pos = w.pos_of[k];
+        const uint4 cmv = w.cm[pos];
+        uint32_t r[2] = {0xFFFFFFFFu, 0xFFFFFFFFu}, d[2] = {0u, 0u};
+        const uint32_t bodies[2] = {cmv.x, cmv.y};
+        for (int t = 0; t < 2; ++t) {
+            const uint32_t bi = bodies[t];
+            if (!writable(w.prop[bi])) continue;
+            const uint32_t lo = w.adj_off[bi], hi = w.adj_off[bi + 1u];
+            uint32_t c = 0;
+            for (uint32_t e = lo; e < hi; ++e) c += w.pos_of[w.adj[e]] < pos ? 1u : 0u;
+            r[t] = c;
+            d[t] = hi - lo;
+        }
+        w.rk[pos] = make_uint4(r[0], d[0], r[1], d[1]);
+    }
+    // Chunks: colour c's positions [colour_cnt[c], colour_cnt[c + 1]) in
+    // pieces of 32, colour-major.
+    uint32_t T = 0;
+    for (uint32_t c = 0; c < ncol; ++c) {
+        const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
+        const uint32_t nch = (hi - lo + 31u) >> 5;
+        for (uint32_t i = g.rank(); i < nch; i += g.size())
+            w.chunk[T + i] = make_uint2(lo + 32u * i, min(lo + 32u * i + 32u, hi));
+        T += nch;
+    }
+    if (!g.sync()) return false;
+    if (M == 0u) return true;
+    // this block's shared-memory chunks: fields from the packed arrays
+    const uint32_t nb = g.nblocks(), blk = g.block();
+    for (uint32_t L = 0; L < fc.smem_chunks && L * nb + blk < T; ++L) {
+        const uint2 ch = w.chunk[L * nb + blk];
+        for (uint32_t e = threadIdx.x; e < CP_NFIELDS * 4u * 32u; e += blockDim.x) {
+            const uint32_t fs = e >> 5, ln = e & 31u;
+            fsm[(size_t)L * kChunkFloats + e] = ch.x + ln < ch.y ? w.cp[(size_t)fs * w.pair_cap + ch.x + ln] : 0.0f;
+        }
+    }
+    __syncthreads();
+    const uint32_t K0 = fc.W + fc.S * (fc.V + 1u);
+    float mn = 0.0f, mx = -__int_as_float(0x7f800000);
+    if (!flow_run(g, w, fc, fsm, T, 0u, K0 + (cf.pos_iters ? 1u : 0u), &mn, &mx)) return false;
+    for (uint32_t it = 0; it < cf.pos_iters; ++it) {
+        if (it > 0u) {
+            mn = 0.0f;
+            mx = -__int_as_float(0x7f800000);
+            if (!flow_run(g, w, fc, fsm, T, K0 + it, K0 + it + 1u, &mn, &mx)) return false;
+        }
+        bool brk = false;
+        if (!pos_sweep_end(g, w, it, mn, mx, &brk)) return false;
+        if (brk) break;
+    }
+    // impulses and masses back to the packed arrays (storeImpulses reads them)
+    __syncthreads();
+    const uint32_t back[6] = {CP_NM, CP_TM0, CP_TM1, CP_NI, CP_TI0, CP_TI1};
+    for (uint32_t L = 0; L < fc.smem_chunks && L * nb + blk < T; ++L) {
+        const uint2 ch = w.chunk[L * nb + blk];
+        for (uint32_t e = threadIdx.x; e < 6u * 4u * 32u; e += blockDim.x) {
+            const uint32_t fs = back[e >> 7] * 4u + ((e >> 5) & 3u), ln = e & 31u;
+            if (ch.x + ln < ch.y) w.cp[(size_t)fs * w.pair_cap + ch.x + ln] = fsm[(size_t)L * kChunkFloats + fs * 32u + ln];
         }
     }
     return true;
@@ -1956,7 +2390,8 @@ __device__ __forceinline__ void stamp(G& g, WorldDev& w, uint32_t slot) {
 }
 
 template <class G>
-__device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifold* warp_sm, const CacheSmem& csm) {
+__device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifold* warp_sm, const CacheSmem& csm,
+                           float* fsm) {
     const uint32_t ph = w.cfg.phases;
     const uint32_t f0 = *(volatile uint32_t*)&w.frame[0];
     stamp(g, w, TS_START);
@@ -2005,14 +2440,23 @@ __device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifol
         // The solver's work per colour batch is a few hundred manifolds: run it
         // on k blocks (one per 512 manifolds, at least 2) with a cheaper barrier.
         const uint32_t nman = (ph & PH_NARROW) ? *(volatile uint32_t*)&w.ctr[C_MANIFOLDS] : w.n_pairs;
-        const uint32_t want = max(2u, (nman + w.cfg.solver_div - 1u) / w.cfg.solver_div);
+        uint32_t want = max(2u, (nman + w.cfg.solver_div - 1u) / w.cfg.solver_div);
+        // event-ordered sweeps: enough blocks to hold every chunk (at most
+        // nman / 32 + one partial chunk per colour) in shared memory
+        if (w.cfg.solver_flow && w.cfg.flow_smem_chunks)
+            want = max(want, (nman / 32u + 64u + w.cfg.flow_smem_chunks - 1u) / w.cfg.flow_smem_chunks);
         G s = g.subgroup(min(want, g.nblocks()));
         if (!s.member()) return;
         uint32_t M = 0, ncol = 0;
         if (!phase_constraints(s, w, cur, &M, &ncol)) return;
         stamp(s, w, TS_CONSTRAINTS);
         const bool solved = w.cfg.dt > 0.0f && w.n_bodies > 0u;
-        if (solved && !phase_solve(s, w, M, ncol)) return;
+        // event-ordered sweeps unless a kinematic body (moved every substep,
+        // written by nobody) sits in a constraint
+        const bool flow = w.cfg.solver_flow && w.cfg.vel_iters > 0u && w.cfg.substeps > 0u &&
+                          *(volatile uint32_t*)&w.ctr[C_KIN_CONTACT] == 0u &&
+                          (*(volatile uint32_t*)&w.ctr[C_ERROR] & ERR_COLOURS) == 0u;
+        if (solved && !(flow ? phase_solve_flow(s, w, fsm, M, ncol) : phase_solve(s, w, M, ncol))) return;
         if (!s.sync()) return;
         stamp(s, w, TS_SOLVE);
         if (!phase_store(s, w, cur, M, solved)) return;

@@ -146,6 +146,8 @@ struct StepCfg {
     uint32_t solver_div;      // grid launch: solver blocks = manifolds / solver_div
     uint32_t device_pairs;    // 1: the step builds its own pair list (phase_broadphase)
     float margin;             // AABB inflation of that pair list
+    uint32_t solver_flow;     // 1: sweeps ordered by per-body event counters, 0: colour barriers
+    uint32_t flow_smem_chunks;  // constraint chunks per block the launch's shared memory holds
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 
@@ -174,6 +176,7 @@ enum : uint32_t {
     C_AWAKE,         // dynamic awake bodies seen by the sleep check
     C_BRICKS,        // bricks of A in the overlap region + bricks of B in B's
     C_NCACHE,        // pairs that consult the brick-pair cache this step
+    C_KIN_CONTACT,   // constraints touching an awake kinematic body
     C_ERROR = 31,    // sticky error bits (not cleared per step)
     C_NCTR = 32
 };
@@ -181,7 +184,7 @@ enum : uint32_t {
 enum : uint32_t {
     TS_START, TS_BEGIN, TS_PAIRS, TS_CACHE, TS_PROBE, TS_FINALIZE, TS_CONSTRAINTS, TS_SOLVE, TS_END, TS_N = 16
 };
-enum : uint32_t { ERR_TIMEOUT = 1u, ERR_CAP = 2u, ERR_COLOURS = 4u, ERR_OVERFLOW = 8u };
+enum : uint32_t { ERR_TIMEOUT = 1u, ERR_CAP = 2u, ERR_COLOURS = 4u, ERR_OVERFLOW = 8u, ERR_BOUNDS = 16u };
 
 struct WorldDev {
     StepCfg cfg;
@@ -228,6 +231,14 @@ struct WorldDev {
     uint32_t* colour_cnt;         // 257: counts, then offsets
     uint32_t* colour_cur;         // 256 cursors
     uint32_t* bmask;              // reference colouring: 8 words per body
+    // event-ordered sweeps: per packed manifold (rank on body a, degree of a,
+    // rank on body b, degree of b), ~0u for a body the solver never writes;
+    // per body the number of sweep events applied so far; per body the state
+    // that prepare reads (after gravity), two substeps deep
+    uint4* rk;
+    uint32_t* ev;
+    DBody* snap;
+    uint2* chunk;                 // [first, end) positions of <= 32 manifolds of one colour
     // packed constraint data, slot-major [slot][M]; see CP_* field ids
     float* cp;                    // CP_NFIELDS * 4 * pair_cap floats
     uint4* cm;                    // per packed manifold: ia, ib, n, pair
