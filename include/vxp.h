@@ -287,11 +287,13 @@ int vxp_set_launch_mode(vxp_ctx* ctx, int mode);
  * ceil(manifolds / div) blocks (at least 2); default div 128. */
 int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div);
 
-/* Order of the solver's sweeps (ContactSolver.solve, src/solver.zig:494-561).
+/* Order of the solver's sweeps (ContactSolver.solve, src/solver.zig:494-561)
+ * when a world is stepped by the cooperative grid (vxp_set_launch_mode).
  * 1 (default): each manifold waits only for the earlier manifolds of its own
  * two bodies (per-body event counters), so colour batches and sweeps overlap;
  * 0: a barrier after every colour batch.  Both give bit-identical results; a
- * step with a kinematic body in a constraint always uses 0. */
+ * step with a kinematic body in a constraint always uses 0, and so does every
+ * world stepped by a single CTA (small worlds, batches). */
 #define VXP_SOLVER_BARRIERS 0u
 #define VXP_SOLVER_EVENTS 1u
 int vxp_set_solver_mode(vxp_ctx* ctx, uint32_t mode);
@@ -337,8 +339,6 @@ int vxp_batch_synchronize(vxp_batch* b);
 int vxp_batch_times(vxp_batch* b, float* total_ms, float* world_ms, uint32_t n);
 /* Schedule: CTA size 256 or 512; order 0 = slot order, 1 = longest first. */
 int vxp_batch_set_schedule(vxp_batch* b, uint32_t threads, uint32_t order_mode);
-/* VXP_SOLVER_* for every world of the batch (default VXP_SOLVER_EVENTS). */
-int vxp_batch_set_solver_mode(vxp_batch* b, uint32_t mode);
 /* Autotuner: runs trial_steps real steps under each schedule, keeps the
  * fastest; ms_out[4] = mean step ms of (256,0), (256,1), (512,0), (512,1). */
 int vxp_batch_autotune(vxp_batch* b, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice);

@@ -231,7 +231,6 @@ SIGNATURES = {
     "vxp_batch_synchronize": (_I, [_VP]),
     "vxp_batch_times": (_I, [_VP, _VP, _VP, _U32]),
     "vxp_batch_set_schedule": (_I, [_VP, _U32, _U32]),
-    "vxp_batch_set_solver_mode": (_I, [_VP, _U32]),
     "vxp_batch_autotune": (_I, [_VP, _F, _U32, _VP, _VP]),
 }
 

@@ -842,7 +842,7 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
     WorldDev w = ctx->w.make(ctx->cfg, dt, phases, ctx->solver_div, device_pairs, margin, ctx->solver_flow);
     const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
     const size_t smem = grid ? grid_smem(w.cache_cap) : step_smem(kBlockThreads, w.cache_cap);
-    w.cfg.flow_smem_chunks = flow_chunks(smem);
+    w.cfg.flow_smem_chunks = grid ? flow_chunks(smem) : 0u;
     CK(cudaMemcpyAsync(ctx->d_world.p, &w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
     const ColliderSet cs = ctx->cols.set();
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -1469,7 +1469,6 @@ struct vxp_batch {
     uint32_t graph_n = 0, graph_threads = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t cache_cap = 1024;
-    uint32_t solver_flow = 1;
 };
 
 namespace {
@@ -1516,8 +1515,7 @@ int batch_prepare(vxp_batch* bt, float dt) {
         bt->order = ord;
         std::vector<WorldDev> wd(ord.size());
         for (size_t i = 0; i < ord.size(); ++i)
-            wd[i] = bt->slots[ord[i]]->make(bt->cfg, dt, PH_STEP, 128, true, bt->margin, bt->solver_flow);
-        for (auto& x : wd) x.cfg.flow_smem_chunks = flow_chunks(step_smem(bt->threads, x.cache_cap));
+            wd[i] = bt->slots[ord[i]]->make(bt->cfg, dt, PH_STEP, 128, true, bt->margin, 0u);
         if (bt->d_worlds.reserve(std::max<size_t>(wd.size(), 1)) != cudaSuccess ||
             bt->d_ts.reserve(2 * std::max<size_t>(wd.size(), 1)) != cudaSuccess)
             return bfail(bt, VXP_ERR_OOM, "batch world table");
@@ -1717,13 +1715,6 @@ int vxp_batch_times(vxp_batch* bt, float* total_ms, float* world_ms, uint32_t n)
 
 // Launch schedule: CTA size (256 or 512) and world order (0 slot order,
 // 1 longest-first by the last measured world time, else by body count).
-int vxp_batch_set_solver_mode(vxp_batch* bt, uint32_t mode) {
-    if (!bt || mode > 1u) return VXP_ERR_ARG;
-    bt->solver_flow = mode;
-    bt->rebuild = true;
-    return VXP_OK;
-}
-
 int vxp_batch_set_schedule(vxp_batch* bt, uint32_t threads, uint32_t order_mode) {
     if (!bt || (threads != 256 && threads != 512) || order_mode > 1) return VXP_ERR_ARG;
     bt->threads = threads;

@@ -36,6 +36,9 @@ __device__ __forceinline__ float fkey_inv(int32_t k) {
 // Groups
 // ---------------------------------------------------------------------------
 struct BlockGroup {
+    // One CTA's barriers are cheap: the solver sweeps colour batch by colour
+    // batch (the event-ordered sweeps are not compiled for this group).
+    static constexpr bool kEventSweeps = false;
     __device__ uint32_t rank() const { return threadIdx.x; }
     __device__ uint32_t size() const { return blockDim.x; }
     __device__ uint32_t block() const { return 0; }
@@ -55,6 +58,7 @@ struct GridBar {
 };
 
 struct GridGroup {
+    static constexpr bool kEventSweeps = true;
     GridBar* bar;
     uint32_t* err;
     unsigned long long timeout_ns;
@@ -1532,10 +1536,11 @@ __device__ __forceinline__ Qt integrate_rotation_small(Qt r, F3 d) {  // solver.
 
 // applyGravity for one dynamic awake body (solver.zig:564-605): gravity,
 // extra damping below 0.5 m/s, damping, zeroing of tiny velocities.
-__device__ __forceinline__ void body_gravity(float4& v4, float4& w4, const DBodyProp& pr, F3 grav, float h) {
+__device__ __forceinline__ void body_gravity_d(float4& v4, float4& w4, float lin_damp, float ang_damp, F3 grav,
+                                               float h) {
     F3 v = f3of(v4), av = f3of(w4);
     v = v + grav * h;
-    float ld = pr.lin_damp, adp = pr.ang_damp;
+    float ld = lin_damp, adp = ang_damp;
     const float ls = len3(v), as = len3(av);
     if (ls < 0.5f) ld += 5.0f * (1.0f - (ls / 0.5f));
     if (as < 0.5f) adp += 5.0f * (1.0f - (as / 0.5f));
@@ -1547,24 +1552,31 @@ __device__ __forceinline__ void body_gravity(float4& v4, float4& w4, const DBody
     v4 = make_float4(v.x, v.y, v.z, 0.f);
     w4 = make_float4(av.x, av.y, av.z, 0.f);
 }
+__device__ __forceinline__ void body_gravity(float4& v4, float4& w4, const DBodyProp& pr, F3 grav, float h) {
+    body_gravity_d(v4, w4, pr.lin_damp, pr.ang_damp, grav, h);
+}
 // BodyState.integratePosition for one awake non-static body
 // (solver.zig:341-356): position, rotation and, for dynamic bodies, the world
 // inverse inertia.
-__device__ __forceinline__ void body_integrate(DBody& b, const DBodyProp& pr, float h, bool disable_rotation) {
+__device__ __forceinline__ void body_integrate_il(DBody& b, const float* il_local, bool dynamic, float h,
+                                                  bool disable_rotation) {
     const F3 x = f3of(b.p) + f3of(b.v) * h;
     Qt q = qof(b.q);
     if (!disable_rotation) q = integrate_rotation(q, f3of(b.w), h);
     b.p = make_float4(x.x, x.y, x.z, b.p.w);
     b.q = f4of(q);
-    if (pr.type == 2u) {
+    if (dynamic) {
         M33 il;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) il.m[k] = pr.il[k];
+        for (int k = 0; k < 9; ++k) il.m[k] = il_local[k];
         const M33 m = world_inv_inertia(q, il);
         b.i0 = make_float4(m.m[0], m.m[1], m.m[2], 0.f);
         b.i1 = make_float4(m.m[3], m.m[4], m.m[5], 0.f);
         b.i2 = make_float4(m.m[6], m.m[7], m.m[8], 0.f);
     }
+}
+__device__ __forceinline__ void body_integrate(DBody& b, const DBodyProp& pr, float h, bool disable_rotation) {
+    body_integrate_il(b, pr.il, pr.type == 2u, h, disable_rotation);
 }
 
 // Local copy of one body's velocity state for a manifold sweep.
@@ -1769,6 +1781,57 @@ __device__ void velocity_points(const WorldDev& w, const CPV& v, uint32_t n, flo
         cpr(v, CP_TI0, i) = ti0;
         cpr(v, CP_TI1, i) = ti1;
         if (i + 1u < n) c = nx;
+    }
+}
+// The same sweep without look-ahead: each point's fields are read when the
+// point starts, which keeps fewer registers live (the event-ordered sweeps
+// mostly read their rows from shared memory, where look-ahead gains little).
+__device__ void velocity_points_near(const WorldDev& w, const CPV& v, uint32_t n, float fr, const Soft& soft,
+                                     bool use_bias, BV& a, BV& b) {
+    for (uint32_t i = 0; i < n; ++i) {
+        const PtV c = load_ptv(v, i);
+        const F3 rv = point_vel(b, c.pt) - point_vel(a, c.pt);
+        const float vn = dot3(rv, c.n);
+        float imp;
+        if (use_bias)
+            imp = -soft.mass_coeff * c.nm * (vn + c.bias) - soft.impulse_coeff * c.ni;
+        else
+            imp = -c.nm * vn;
+        const float nn = fmaxf(c.ni + imp, 0.0f);
+        imp = nn - c.ni;
+        const float ni = nn;
+        const F3 P = c.n * imp;
+        apply_impulse(a, -P, c.ra);
+        apply_impulse(b, P, c.rb);
+        float ti0 = c.ti0, ti1 = c.ti1;
+        if (w.cfg.friction_on && fr > 0.0f) {
+            const float mf = fr * ni;
+            {
+                const F3 rv1 = point_vel(b, c.pt) - point_vel(a, c.pt);
+                const float vt1 = dot3(rv1, c.t1);
+                float f1 = -c.tm0 * vt1;
+                const float o1 = ti0;
+                ti0 = clampf_ref(o1 + f1, -mf, mf);
+                f1 = ti0 - o1;
+                const F3 I1 = c.t1 * f1;
+                apply_impulse(a, -I1, c.ra);
+                apply_impulse(b, I1, c.rb);
+            }
+            {
+                const F3 rv2 = point_vel(b, c.pt) - point_vel(a, c.pt);
+                const float vt2 = dot3(rv2, c.t2);
+                float f2 = -c.tm1 * vt2;
+                const float o2 = ti1;
+                ti1 = clampf_ref(o2 + f2, -mf, mf);
+                f2 = ti1 - o2;
+                const F3 I2 = c.t2 * f2;
+                apply_impulse(a, -I2, c.ra);
+                apply_impulse(b, I2, c.rb);
+            }
+        }
+        cpr(v, CP_NI, i) = ni;
+        cpr(v, CP_TI0, i) = ti0;
+        cpr(v, CP_TI1, i) = ti1;
     }
 }
 __device__ void velocity_manifold(WorldDev& w, uint32_t pos, const Soft& soft, bool use_bias) {
@@ -2062,21 +2125,43 @@ __device__ __forceinline__ uint32_t flow_body_op(const FlowCtx& fc, const FlowSw
     if (sw.kind == FK_RELAX && sw.s + 1u < fc.S) return 2u;
     return 0u;
 }
-__device__ __forceinline__ void flow_body_out(WorldDev& w, const FlowCtx& fc, uint32_t op, uint32_t i, const BV& x,
-                                              DBody d, const DBodyProp& pr, uint32_t snap_par) {
-    d.v = make_float4(x.v.x, x.v.y, x.v.z, 0.f);
-    d.w = make_float4(x.w.x, x.w.y, x.w.z, 0.f);
+// Prefetch for that body step: op 1 the local inverse inertia, op 2 the two
+// damping coefficients.
+__device__ __forceinline__ void flow_ld_prop(const WorldDev& w, uint32_t op, uint32_t i, float pr[9]) {
     if (op == 1u) {
-        body_integrate(d, pr, fc.h, fc.dis_rot);  // integratePositions of substep s
-        w.body[i] = d;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) pr[k] = w.prop[i].il[k];
     } else if (op == 2u) {
-        body_gravity(d.v, d.w, pr, fc.grav, fc.h);  // applyGravity of substep s + 1
+        pr[0] = w.prop[i].lin_damp;
+        pr[1] = w.prop[i].ang_damp;
+    }
+}
+// Writes one body back after a velocity-type sweep event, with the body step
+// that follows its last event of the sweep.
+__device__ __forceinline__ void flow_body_out(WorldDev& w, const FlowCtx& fc, uint32_t op, uint32_t i, const BV& x,
+                                              Qt q, const float pr[9], uint32_t snap_par) {
+    const float4 v4 = make_float4(x.v.x, x.v.y, x.v.z, 0.f), w4 = make_float4(x.w.x, x.w.y, x.w.z, 0.f);
+    if (op == 0u) {
+        w.body[i].v = v4;
+        w.body[i].w = w4;
+        return;
+    }
+    DBody d;
+    d.p = make_float4(x.p.x, x.p.y, x.p.z, x.im);
+    d.q = f4of(q);
+    d.v = v4;
+    d.w = w4;
+    d.i0 = make_float4(x.I.m[0], x.I.m[1], x.I.m[2], 0.f);
+    d.i1 = make_float4(x.I.m[3], x.I.m[4], x.I.m[5], 0.f);
+    d.i2 = make_float4(x.I.m[6], x.I.m[7], x.I.m[8], 0.f);
+    if (op == 1u) {
+        body_integrate_il(d, pr, true, fc.h, fc.dis_rot);  // integratePositions of substep s
+        w.body[i] = d;
+    } else {
+        body_gravity_d(d.v, d.w, pr[0], pr[1], fc.grav, fc.h);  // applyGravity of substep s + 1
         w.body[i].v = d.v;
         w.body[i].w = d.w;
         w.snap[(size_t)snap_par * w.n_bodies + i] = d;
-    } else {
-        w.body[i].v = d.v;
-        w.body[i].w = d.w;
     }
 }
 
@@ -2100,27 +2185,36 @@ __device__ __noinline__ void flow_item(WorldDev& w, const FlowCtx& fc, uint32_t 
                                        const uint4& cmv, const uint4& rkv, float* mn, float* mx) {
     const FlowSweep sw = flow_sweep(k, fc);
     const bool wa = rkv.x != 0xFFFFFFFFu, wb = rkv.z != 0xFFFFFFFFu;
-    const uint32_t opa = flow_body_op(fc, sw, rkv.x, rkv.y), opb = flow_body_op(fc, sw, rkv.z, rkv.w);
-    DBodyProp pa, pb;
-    if (opa) pa = w.prop[cmv.x];
-    if (opb) pb = w.prop[cmv.y];
-    const DBody A = ld_body_cg(w.body + cmv.x), B = ld_body_cg(w.body + cmv.y);
     if (sw.kind == FK_POS) {
         if (!wa && !wb && w.prop[cmv.x].type == 0u && w.prop[cmv.y].type == 0u) return;
+        const DBody A = ld_body_cg(w.body + cmv.x), B = ld_body_cg(w.body + cmv.y);
         PB a = pb_of(A.p, A.q, A.i0, A.i1, A.i2, wa), b = pb_of(B.p, B.q, B.i0, B.i1, B.i2, wb);
         position_points(w, v, cmv.z, a, b, mn, mx);
         store_pb(w, cmv.x, a);
         store_pb(w, cmv.y, b);
         return;
     }
-    BV a = bv_of(A, wa), b = bv_of(B, wb);
+    const uint32_t opa = flow_body_op(fc, sw, rkv.x, rkv.y), opb = flow_body_op(fc, sw, rkv.z, rkv.w);
+    float pra[9], prb[9];
+    flow_ld_prop(w, opa, cmv.x, pra);
+    flow_ld_prop(w, opb, cmv.y, prb);
+    Qt qa, qb;
+    BV a, b;
+    {
+        const DBody A = ld_body_cg(w.body + cmv.x), B = ld_body_cg(w.body + cmv.y);
+        a = bv_of(A, wa);
+        b = bv_of(B, wb);
+        qa = qof(A.q);
+        qb = qof(B.q);
+    }
+    const float fr = w.cfr[pos].x;
     if (sw.kind == FK_WARM)
         warm_points(v, cmv.z, fc.warm_scale, a, b);
     else
-        velocity_points(w, v, cmv.z, w.cfr[pos].x, sw.kind == FK_VEL ? fc.soft : fc.hard, sw.kind == FK_VEL, a, b);
+        velocity_points_near(w, v, cmv.z, fr, sw.kind == FK_VEL ? fc.soft : fc.hard, sw.kind == FK_VEL, a, b);
     const uint32_t par = (sw.s + 1u) & 1u;
-    if (wa) flow_body_out(w, fc, opa, cmv.x, a, A, pa, par);
-    if (wb) flow_body_out(w, fc, opb, cmv.y, b, B, pb, par);
+    if (wa) flow_body_out(w, fc, opa, cmv.x, a, qa, pra, par);
+    if (wb) flow_body_out(w, fc, opb, cmv.y, b, qb, prb, par);
 }
 
 // Waits until every lane of the warp sees its bodies' event counters at the
@@ -2443,7 +2537,7 @@ __device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifol
         uint32_t want = max(2u, (nman + w.cfg.solver_div - 1u) / w.cfg.solver_div);
         // event-ordered sweeps: enough blocks to hold every chunk (at most
         // nman / 32 + one partial chunk per colour) in shared memory
-        if (w.cfg.solver_flow && w.cfg.flow_smem_chunks)
+        if (G::kEventSweeps && w.cfg.solver_flow && w.cfg.flow_smem_chunks)
             want = max(want, (nman / 32u + 64u + w.cfg.flow_smem_chunks - 1u) / w.cfg.flow_smem_chunks);
         G s = g.subgroup(min(want, g.nblocks()));
         if (!s.member()) return;
@@ -2453,10 +2547,18 @@ __device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifol
         const bool solved = w.cfg.dt > 0.0f && w.n_bodies > 0u;
         // event-ordered sweeps unless a kinematic body (moved every substep,
         // written by nobody) sits in a constraint
-        const bool flow = w.cfg.solver_flow && w.cfg.vel_iters > 0u && w.cfg.substeps > 0u &&
-                          *(volatile uint32_t*)&w.ctr[C_KIN_CONTACT] == 0u &&
-                          (*(volatile uint32_t*)&w.ctr[C_ERROR] & ERR_COLOURS) == 0u;
-        if (solved && !(flow ? phase_solve_flow(s, w, fsm, M, ncol) : phase_solve(s, w, M, ncol))) return;
+        if (solved) {
+            bool ok;
+            if constexpr (G::kEventSweeps) {
+                const bool flow = w.cfg.solver_flow && w.cfg.vel_iters > 0u && w.cfg.substeps > 0u &&
+                                  *(volatile uint32_t*)&w.ctr[C_KIN_CONTACT] == 0u &&
+                                  (*(volatile uint32_t*)&w.ctr[C_ERROR] & ERR_COLOURS) == 0u;
+                ok = flow ? phase_solve_flow(s, w, fsm, M, ncol) : phase_solve(s, w, M, ncol);
+            } else {
+                ok = phase_solve(s, w, M, ncol);
+            }
+            if (!ok) return;
+        }
         if (!s.sync()) return;
         stamp(s, w, TS_SOLVE);
         if (!phase_store(s, w, cur, M, solved)) return;

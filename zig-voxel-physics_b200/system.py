@@ -131,7 +131,8 @@ class VoxelPhysicsSystem:
 
     # -------------------------------------------------------------- outputs
     def set_solver_mode(self, mode: int) -> None:
-        """1: event-ordered sweeps (default); 0: a barrier after every colour batch."""
+        """Grid-stepped worlds: 1 event-ordered sweeps (default), 0 a barrier
+        after every colour batch.  Worlds stepped by one CTA always use 0."""
         self._check(self.lib.vxp_set_solver_mode(self.ctx, int(mode)))
 
     def pairs(self, margin: float | None = None) -> np.ndarray:
@@ -260,9 +261,6 @@ class VoxelWorldBatch:
         per = np.zeros(self.max_worlds, dtype=np.float32)
         self._check(self.lib.vxp_batch_times(self.b, ctypes.byref(total), abi.ptr(per), self.max_worlds))
         return float(total.value), per
-
-    def set_solver_mode(self, mode: int) -> None:
-        self._check(self.lib.vxp_batch_set_solver_mode(self.b, int(mode)))
 
     def set_schedule(self, threads: int, order_mode: int) -> None:
         self._check(self.lib.vxp_batch_set_schedule(self.b, int(threads), int(order_mode)))
