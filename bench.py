@@ -46,12 +46,11 @@ L2_FLUSH_BYTES = 256 << 20
 SOLVER_V, SOLVER_Q = 1, 2
 
 
-# DRAM bytes (read + write) per launch of the step kernel, from one ncu
-# capture of the same workload (settled pile); re-captured when the kernel
-# changes.
-PROFILED_TRAFFIC = {
-    "config2_pile_4096": (32_957_184, "profiles/k_step_grid_config2_pile.md"),
-}
+# DRAM bytes (read + write) per launch of each step kernel on the settled
+# pile, keyed by (workload, kernel), from one ncu capture of the same
+# workload; re-captured when a kernel changes.
+PROFILED_TRAFFIC = {}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -272,7 +271,7 @@ def ours(args):
         pg.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    step_ms, kern_ms, pair_ms, stats = [], [], [], []
+    step_ms, kern_ms, pair_ms, stats, part_ms = [], [], [], [], []
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -282,6 +281,9 @@ def ours(args):
         pair_ms.append(float(out[0]))
         kern_ms.append(float(out[1]))
         step_ms.append(float(out[2]))
+        parts = np.zeros(2, dtype=np.float32)
+        sysm._check(sysm.lib.vxp_last_kernel_ms(sysm.ctx, abi.ptr(parts)))
+        part_ms.append((float(parts[0]), float(parts[1])))
         stats.append(sysm.stats())
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -298,6 +300,22 @@ def ours(args):
     nb = [sum(alg_bytes(s, 8, n_dyn_awake, n_nonstatic)) for s in stats]
     peak, peak_kind = peaks()
     achieved = sum(nb) / (sum(kern_ms) / 1e3) / 1e9
+    # per kernel of the step: narrow part (k_step_grid) and solve part
+    # (k_solve_grid), each its algorithmic bytes over its own event time
+    nb_parts = [alg_bytes(s, 8, n_dyn_awake, n_nonstatic) for s in stats]
+    grid = n_dyn >= 512
+    kernels = {}
+    if grid:
+        for j, name in ((0, "k_step_grid"), (1, "k_solve_grid")):
+            t = sum(x[j] for x in part_ms) / 1e3
+            b = sum(x[j] for x in nb_parts)
+            kernels[name] = {"ms_mean": 1e3 * t / len(part_ms), "alg_bytes_per_launch": b / len(nb_parts),
+                             "achieved": b / t / 1e9, "frac": b / t / 1e9 / peak}
+        dominant = max(kernels, key=lambda k: kernels[k]["ms_mean"])
+    else:
+        dominant = "k_step_block"
+        kernels[dominant] = {"ms_mean": statistics.mean(kern_ms), "alg_bytes_per_launch": statistics.mean(nb),
+                             "achieved": achieved, "frac": achieved / peak}
 
     # ---- e2e through the public API with pinned host buffers
     cap = max(65536, 16 * n_dyn)
@@ -348,17 +366,20 @@ def ours(args):
             "contacts_per_s": contacts_per_s,
             "step_latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                                 "kernel_mean": statistics.mean(kern_ms), "pairs_mean": statistics.mean(pair_ms)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": PROFILED_TRAFFIC.get(f"config2_pile_{n_dyn}", (None,))[0],
-                         "traffic_source": PROFILED_TRAFFIC.get(f"config2_pile_{n_dyn}", (None, None))[1],
-                         "peak_kind": peak_kind,
-                         "kernel": "k_step_grid" if n_dyn >= 512 else "k_step_block",
-                         "alg_bytes_per_launch": statistics.mean(nb)},
+            "roofline": {"bound": "hbm", "achieved": kernels[dominant]["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": kernels[dominant]["frac"],
+                         "traffic": PROFILED_TRAFFIC.get((f"config2_pile_{n_dyn}", dominant), (None,))[0],
+                         "traffic_source": PROFILED_TRAFFIC.get((f"config2_pile_{n_dyn}", dominant), (None, None))[1],
+                         "peak_kind": peak_kind, "kernel": dominant,
+                         "alg_bytes_per_launch": kernels[dominant]["alg_bytes_per_launch"],
+                         "step": {"achieved": achieved, "frac": achieved / peak,
+                                  "alg_bytes_per_step": statistics.mean(nb)},
+                         "kernels": kernels},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "body-substeps/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
                     "d2h_bytes_per_step": d2h // max(1, args.steps)},
             "clocks": clk,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * (2 if grid else 1),
         }
         print(json.dumps(line), flush=True)
     if pg:
@@ -437,7 +458,7 @@ def batched(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"config3_batched_{len(scenes)}", "worlds": len(scenes), "bodies": n_dyn,
                    "substeps": 4, "dt": "1/60", "l2": "flushed (256 MiB write) between timed steps",
-                   "schedule": {"choice": ["256/slot", "256/longest-first", "512/slot", "512/longest-first"][choice],
+                   "schedule": {"choice": ["slot order", "longest first"][choice],
                                 "autotune_ms": [float(x) for x in tune_ms]}},
         "plain_single_world": {"value": plain_value, "ms_per_batch_step": plain_ms,
                                "method": "each world alone, its own launches, 3 timed steps after 2, summed"},
@@ -466,7 +487,7 @@ def serving(args):
     batch = vxp.VoxelWorldBatch(args.slots, substeps=4)
     for c in lib:
         batch.add_collider(c.id, c.voxel_size, c.bricks)
-    batch.set_schedule(512, 1)
+    batch.set_schedule(256, 1)
     server = vxp.server.SimulationServer(batch, 1.0 / 60.0, max_slots=args.slots, budget_bytes=120 * 10**9)
     clocks = Clocks(0)
     clocks.start()

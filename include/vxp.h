@@ -271,6 +271,12 @@ int vxp_pairs_from_bodies(vxp_ctx* ctx, float margin, vxp_pair* out, uint32_t ca
  * stream): [pair source and copies, step kernel, whole call]. */
 int vxp_last_step_ms(vxp_ctx* ctx, float out[3]);
 
+/* Device time (ms) of the last step's kernels: [narrow part, solve part].  A
+ * world stepped by the cooperative grid runs them as two kernels
+ * (k_step_grid, k_solve_grid); a world stepped by one CTA runs both parts in
+ * one kernel, reported in out[0] with out[1] = 0. */
+int vxp_last_kernel_ms(vxp_ctx* ctx, float out[2]);
+
 /* Step calls queue work on the context's stream and return; a call that
  * returns data (bodies, manifolds, stats, colours, candidates) waits for it.
  * vxp_synchronize waits without copying and reports any device-side error
@@ -337,10 +343,11 @@ int vxp_batch_synchronize(vxp_batch* b);
 /* Device ms of the last vxp_batch_step call, and per slot the ms of its CTA
  * in the last step (0 for empty slots). */
 int vxp_batch_times(vxp_batch* b, float* total_ms, float* world_ms, uint32_t n);
-/* Schedule: CTA size 256 or 512; order 0 = slot order, 1 = longest first. */
+/* Schedule: CTA size (256 threads; anything else is VXP_ERR_ARG); launch
+ * order 0 = slot order, 1 = longest measured world first. */
 int vxp_batch_set_schedule(vxp_batch* b, uint32_t threads, uint32_t order_mode);
-/* Autotuner: runs trial_steps real steps under each schedule, keeps the
- * fastest; ms_out[4] = mean step ms of (256,0), (256,1), (512,0), (512,1). */
+/* Autotuner: runs trial_steps real steps under each launch order, keeps the
+ * fastest; ms_out[2] = mean step ms of order 0 and order 1. */
 int vxp_batch_autotune(vxp_batch* b, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice);
 
 /* ---------------------------------------------------------------------------

@@ -50,17 +50,24 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) k_step_block(WorldDe
     world_step(g, w, cs, wsm, csm, reinterpret_cast<float*>(smem_raw));
 }
 template __global__ void k_step_block<256>(WorldDev*, ColliderSet);
-template __global__ void k_step_block<512>(WorldDev*, ColliderSet);
 
-// One world over a cooperative grid.
-__global__ void __launch_bounds__(512) k_step_grid(const WorldDev* world, ColliderSet cs, GridBar* bar,
-                                                   unsigned long long timeout_ns) {
+// One world over a cooperative grid, in two kernels: the narrow part of the
+// step, then its solve part (barrier words bar[0] and bar[1]).
+__global__ void __launch_bounds__(512, 1) k_step_grid(const WorldDev* world, ColliderSet cs, GridBar* bar,
+                                                      unsigned long long timeout_ns) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WarpManifold* wsm = reinterpret_cast<WarpManifold*>(smem_raw);
     WorldDev w = *world;
     const CacheSmem csm = cache_smem(smem_raw, blockDim.x / 32u, w.cache_cap);
     GridGroup g{bar, &w.ctr[C_ERROR], timeout_ns, gridDim.x};
-    world_step(g, w, cs, wsm, csm, reinterpret_cast<float*>(smem_raw));
+    world_step_narrow(g, w, cs, wsm, csm);
+}
+__global__ void __launch_bounds__(256, 1) k_solve_grid(const WorldDev* world, GridBar* bar,
+                                                       unsigned long long timeout_ns) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WorldDev w = *world;
+    GridGroup g{bar, &w.ctr[C_ERROR], timeout_ns, gridDim.x};
+    world_step_solve(g, w, reinterpret_cast<float*>(smem_raw), true);
 }
 
 // Pair source: world AABB of each body's collider (AABB.transform,
@@ -210,17 +217,21 @@ std::string fmt(const char* f, ...) {
     return buf;
 }
 
-constexpr uint32_t kBlockThreads = 512;
+constexpr uint32_t kBlockThreads = 256;
+// CTA sizes of the two cooperative grid kernels of a large world's step (one
+// CTA per SM each): the narrow part wants many warps to hide its memory
+// latency, the solve part wants registers for its long dependent chains.
+constexpr uint32_t kGridThreads = 512;
+constexpr uint32_t kSolveThreads = 256;
 size_t step_smem(uint32_t threads, uint32_t cache_cap) {
     return sizeof(WarpManifold) * (threads / 32) +
            (size_t)cache_cap * (sizeof(uint2) + sizeof(unsigned long long) + sizeof(uint32_t));
 }
-// The grid kernel (one CTA per SM) also keeps up to kGridFlowChunks chunks of
-// constraint rows per block in shared memory during the solve.
+// The grid solve kernel (one CTA per SM) keeps up to kGridFlowChunks chunks
+// of constraint rows per block in shared memory.
 constexpr uint32_t kGridFlowChunks = 4;
-size_t grid_smem(uint32_t cache_cap) {
-    return std::max(step_smem(512, cache_cap), (size_t)kGridFlowChunks * kChunkFloats * sizeof(float));
-}
+size_t grid_smem(uint32_t cache_cap) { return step_smem(kGridThreads, cache_cap); }
+size_t solve_smem() { return (size_t)kGridFlowChunks * kChunkFloats * sizeof(float); }
 uint32_t flow_chunks(size_t smem) { return (uint32_t)(smem / (kChunkFloats * sizeof(float))); }
 
 uint64_t hash_brick_pos(int32_t x, int32_t y, int32_t z) {  // collider.zig:187-192
@@ -809,7 +820,8 @@ struct vxp_ctx {
     DBuf<uint32_t> pair_counts, pair_offsets;
     uint32_t grid_blocks = 0;
     uint32_t last_pairs = 0;
-    cudaEvent_t ev_start = nullptr, ev0 = nullptr, ev1 = nullptr, ev_count = nullptr;
+    cudaEvent_t ev_start = nullptr, ev0 = nullptr, ev1 = nullptr, ev_count = nullptr, ev_mid = nullptr;
+    bool last_grid = false;
     uint32_t* h_count = nullptr;  // pinned mirror of the device pair count
     bool count_pending = false;
     int use_grid = -1;  // -1 auto, 0 block, 1 grid
@@ -842,7 +854,7 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
     WorldDev w = ctx->w.make(ctx->cfg, dt, phases, ctx->solver_div, device_pairs, margin, ctx->solver_flow);
     const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
     const size_t smem = grid ? grid_smem(w.cache_cap) : step_smem(kBlockThreads, w.cache_cap);
-    w.cfg.flow_smem_chunks = grid ? flow_chunks(smem) : 0u;
+    w.cfg.flow_smem_chunks = grid ? flow_chunks(solve_smem()) : 0u;
     CK(cudaMemcpyAsync(ctx->d_world.p, &w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
     const ColliderSet cs = ctx->cols.set();
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -852,13 +864,18 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
         GridBar* bp = ctx->bar.p;
         unsigned long long timeout = 10ull * 1000ull * 1000ull * 1000ull;  // 10 s per barrier wait
         void* args[] = {(void*)&wp, (void*)&cs, (void*)&bp, (void*)&timeout};
-        CK(cudaLaunchCooperativeKernel((const void*)k_step_grid, dim3(ctx->grid_blocks), dim3(kBlockThreads), args,
+        CK(cudaLaunchCooperativeKernel((const void*)k_step_grid, dim3(ctx->grid_blocks), dim3(kGridThreads), args,
                                        smem, ctx->stream));
+        CK(cudaEventRecord(ctx->ev_mid, ctx->stream));
+        void* sargs[] = {(void*)&wp, (void*)&bp, (void*)&timeout};
+        CK(cudaLaunchCooperativeKernel((const void*)k_solve_grid, dim3(ctx->grid_blocks), dim3(kSolveThreads), sargs,
+                                       solve_smem(), ctx->stream));
     } else {
         k_step_block<kBlockThreads><<<1, kBlockThreads, smem, ctx->stream>>>(ctx->d_world.p, cs);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->last_grid = grid;
     if (device_pairs && !ctx->count_pending) {
         CK(cudaMemcpyAsync(ctx->h_count, ctx->w.n_pairs_dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                            ctx->stream));
@@ -1078,10 +1095,10 @@ void vxp_config_default(vxp_config* c) {
 static int set_kernel_smem(uint32_t cache_cap) {
     if (cudaFuncSetAttribute(k_step_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)step_smem(256, cache_cap)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_step_block<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)step_smem(512, cache_cap)) != cudaSuccess ||
         cudaFuncSetAttribute(k_step_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)grid_smem(cache_cap)) != cudaSuccess)
+                             (int)grid_smem(cache_cap)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_solve_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem()) !=
+            cudaSuccess)
         return VXP_ERR_CUDA;
     return VXP_OK;
 }
@@ -1105,7 +1122,7 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     ctx->sm_count = smc;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(VXP_ERR_CUDA);
     if (cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev0) != cudaSuccess ||
-        cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev1) != cudaSuccess || cudaEventCreate(&ctx->ev_mid) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_count, cudaEventDisableTiming) != cudaSuccess)
         return bail(VXP_ERR_CUDA);
     if (cudaMallocHost(&ctx->h_count, sizeof(uint32_t)) != cudaSuccess) return bail(VXP_ERR_OOM);
@@ -1113,11 +1130,15 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     const uint32_t cache_cap = cfg->brick_pair_cache_size ? cfg->brick_pair_cache_size : 1024u;
     if (set_kernel_smem(cache_cap)) return bail(VXP_ERR_CUDA);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kBlockThreads, grid_smem(cache_cap)) !=
+    int per_sm_solve = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, kGridThreads, grid_smem(cache_cap)) !=
             cudaSuccess ||
-        per_sm < 1)
+        per_sm < 1 ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_solve, k_solve_grid, kSolveThreads, solve_smem()) !=
+            cudaSuccess ||
+        per_sm_solve < 1)
         return bail(VXP_ERR_CUDA);
-    ctx->grid_blocks = (uint32_t)(smc * std::min(per_sm, 2));
+    ctx->grid_blocks = (uint32_t)smc;  // one CTA per SM for both grid kernels
     if (ctx->w.init(cache_cap, ctx->grid_blocks, ctx->err)) return bail(VXP_ERR_OOM);
     if (ctx->d_world.reserve(1) != cudaSuccess || ctx->bar.reserve(2) != cudaSuccess) return bail(VXP_ERR_OOM);
     if (ctx->w.ensure_pairs(std::max<uint32_t>(cfg->max_pairs, 1024), ctx->err)) return bail(VXP_ERR_OOM);
@@ -1133,6 +1154,7 @@ void vxp_destroy(vxp_ctx* ctx) {
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->ev_mid) cudaEventDestroy(ctx->ev_mid);
     if (ctx->ev_count) cudaEventDestroy(ctx->ev_count);
     if (ctx->h_count) cudaFreeHost(ctx->h_count);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1413,6 +1435,19 @@ int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n) {
     return VXP_OK;
 }
 
+int vxp_last_kernel_ms(vxp_ctx* ctx, float out[2]) {
+    if (!ctx || !out) return VXP_ERR_ARG;
+    CK(cudaEventSynchronize(ctx->ev1));
+    if (ctx->last_grid) {
+        CK(cudaEventElapsedTime(&out[0], ctx->ev0, ctx->ev_mid));
+        CK(cudaEventElapsedTime(&out[1], ctx->ev_mid, ctx->ev1));
+    } else {
+        CK(cudaEventElapsedTime(&out[0], ctx->ev0, ctx->ev1));
+        out[1] = 0.0f;
+    }
+    return VXP_OK;
+}
+
 int vxp_synchronize(vxp_ctx* ctx) {
     if (!ctx) return VXP_ERR_ARG;
     return check_device_error(ctx);
@@ -1543,8 +1578,7 @@ int batch_prepare(vxp_batch* bt, float dt) {
     if (n == 0) return VXP_OK;
     const size_t smem = step_smem(bt->threads, bt->cache_cap);
     BK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
-    if (bt->threads == 512) k_step_block<512><<<n, 512, smem, bt->stream>>>(bt->d_worlds.p, cs);
-    else k_step_block<256><<<n, 256, smem, bt->stream>>>(bt->d_worlds.p, cs);
+    k_step_block<256><<<n, 256, smem, bt->stream>>>(bt->d_worlds.p, cs);
     const cudaError_t le = cudaGetLastError();
     cudaGraph_t g = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(bt->stream, &g);
@@ -1716,23 +1750,23 @@ int vxp_batch_times(vxp_batch* bt, float* total_ms, float* world_ms, uint32_t n)
 // Launch schedule: CTA size (256 or 512) and world order (0 slot order,
 // 1 longest-first by the last measured world time, else by body count).
 int vxp_batch_set_schedule(vxp_batch* bt, uint32_t threads, uint32_t order_mode) {
-    if (!bt || (threads != 256 && threads != 512) || order_mode > 1) return VXP_ERR_ARG;
+    if (!bt || order_mode > 1) return VXP_ERR_ARG;
+    if (threads != 256) return bfail(bt, VXP_ERR_ARG, "a batch CTA has 256 threads");
     bt->threads = threads;
     bt->order_mode = order_mode;
     bt->rebuild = true;
     return VXP_OK;
 }
 
-// Tries each schedule for trial_steps real steps (each world's results do
-// not depend on the schedule) and keeps the fastest.  ms_out[4] receives the
-// mean step time of (256, slot order), (256, longest first), (512, slot
-// order), (512, longest first); *choice the index kept.
+// Tries each launch order for trial_steps real steps (each world's results
+// do not depend on it) and keeps the fastest.  ms_out[2] receives the mean
+// step time of slot order and longest first; *choice the index kept.
 int vxp_batch_autotune(vxp_batch* bt, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice) {
     if (!bt || trial_steps == 0) return VXP_ERR_ARG;
     float best = 1e30f;
     uint32_t best_i = 0;
-    for (uint32_t i = 0; i < 4; ++i) {
-        if (int rc = vxp_batch_set_schedule(bt, i < 2 ? 256u : 512u, i & 1u)) return rc;
+    for (uint32_t i = 0; i < 2; ++i) {
+        if (int rc = vxp_batch_set_schedule(bt, 256u, i)) return rc;
         if (int rc = vxp_batch_step(bt, dt, 1)) return rc;  // measures world times, builds the graph
         if (int rc = vxp_batch_synchronize(bt)) return rc;
         if (int rc = vxp_batch_times(bt, nullptr, nullptr, 0)) return rc;
@@ -1749,7 +1783,7 @@ int vxp_batch_autotune(vxp_batch* bt, float dt, uint32_t trial_steps, float* ms_
         }
     }
     if (choice) *choice = best_i;
-    return vxp_batch_set_schedule(bt, best_i < 2 ? 256u : 512u, best_i & 1u);
+    return vxp_batch_set_schedule(bt, 256u, best_i);
 }
 
 }  // extern "C"

@@ -1611,6 +1611,15 @@ __device__ __forceinline__ void store_bv(WorldDev& w, uint32_t i, const BV& b) {
     w.body[i].v = make_float4(b.v.x, b.v.y, b.v.z, 0.f);
     w.body[i].w = make_float4(b.w.x, b.w.y, b.w.z, 0.f);
 }
+// The solver settings the per-point arithmetic reads, as values.
+struct SolveFlags {
+    bool friction, restitution;
+    float slop, pos_rate, max_corr;
+};
+__device__ __forceinline__ SolveFlags solve_flags(const StepCfg& c) {
+    return SolveFlags{c.friction_on != 0u, c.restitution_on != 0u, c.slop, c.pos_rate, c.max_pos_corr};
+}
+
 // The constraint-point fields of one manifold: field f of point slot s is
 // b[(f * 4 + s) * st].  In global memory b = cp + position, st = pair
 // capacity; a chunk held in shared memory has b = chunk + lane, st = 32.
@@ -1633,7 +1642,7 @@ __device__ __forceinline__ void st3(const CPV& v, uint32_t f, uint32_t s, F3 x) 
 
 // prepareConstraints for one point (solver.zig:608-699), from the two
 // bodies' state after applyGravity.
-__device__ void prepare_point_s(const WorldDev& w, const CPV& v, float restitution, uint32_t i, const Soft& soft,
+__device__ void prepare_point_s(const SolveFlags sf, const CPV v, float restitution, uint32_t i, const Soft& soft,
                                 float hinv, const BV& a, Qt qa, const BV& b, Qt qb) {
     const F3 n = ld3(v, CP_NX, i);
     const F3 wa = qrotate(qa, ld3(v, CP_LAX, i)) + a.p;
@@ -1652,13 +1661,13 @@ __device__ void prepare_point_s(const WorldDev& w, const CPV& v, float restituti
     float bias;
     if (sep > 0.0f) bias = sep * hinv;
     else bias = fmaxf(soft.bias_rate * sep, -0.2f);
-    if (w.cfg.restitution_on && vn < -1.0f) bias = fmaxf(bias, -restitution * vn);
+    if (sf.restitution && vn < -1.0f) bias = fmaxf(bias, -restitution * vn);
     st3(v, CP_RAX, i, ra);
     st3(v, CP_RBX, i, rb);
     st3(v, CP_PX, i, pt);
     cpr(v, CP_NM, i) = nm;
     cpr(v, CP_BIAS, i) = bias;
-    if (w.cfg.friction_on) {
+    if (sf.friction) {
         const F3 t1 = compute_orthogonal(n);
         const F3 t2 = cross3(n, t1);
         const F3 r1a = cross3(ra, t1), r1b = cross3(rb, t1);
@@ -1679,7 +1688,7 @@ __device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft&
     const uint4 cmv = w.cm[pos];
     const BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
     const Qt qa = qof(w.body[cmv.x].q), qb = qof(w.body[cmv.y].q);
-    prepare_point_s(w, cpv_global(w, pos), w.cfr[pos].y, i, soft, hinv, a, qa, b, qb);
+    prepare_point_s(solve_flags(w.cfg), cpv_global(w, pos), w.cfr[pos].y, i, soft, hinv, a, qa, b, qb);
 }
 
 // warmStart for one manifold (solver.zig:702-729).
@@ -1786,7 +1795,7 @@ __device__ void velocity_points(const WorldDev& w, const CPV& v, uint32_t n, flo
 // The same sweep without look-ahead: each point's fields are read when the
 // point starts, which keeps fewer registers live (the event-ordered sweeps
 // mostly read their rows from shared memory, where look-ahead gains little).
-__device__ void velocity_points_near(const WorldDev& w, const CPV& v, uint32_t n, float fr, const Soft& soft,
+__device__ void velocity_points_near(bool friction, const CPV v, uint32_t n, float fr, const Soft& soft,
                                      bool use_bias, BV& a, BV& b) {
     for (uint32_t i = 0; i < n; ++i) {
         const PtV c = load_ptv(v, i);
@@ -1804,7 +1813,7 @@ __device__ void velocity_points_near(const WorldDev& w, const CPV& v, uint32_t n
         apply_impulse(a, -P, c.ra);
         apply_impulse(b, P, c.rb);
         float ti0 = c.ti0, ti1 = c.ti1;
-        if (w.cfg.friction_on && fr > 0.0f) {
+        if (friction && fr > 0.0f) {
             const float mf = fr * ni;
             {
                 const F3 rv1 = point_vel(b, c.pt) - point_vel(a, c.pt);
@@ -1863,21 +1872,21 @@ __device__ __forceinline__ PB pb_of(float4 p, float4 q, float4 i0, float4 i1, fl
     r.wr = wr;
     return r;
 }
-__device__ __forceinline__ void store_pb(WorldDev& w, uint32_t i, const PB& b) {
+__device__ __forceinline__ void store_pb(DBody* body, uint32_t i, const PB& b) {
     if (!b.wr) return;
-    w.body[i].p = make_float4(b.x.x, b.x.y, b.x.z, b.im);
-    w.body[i].q = f4of(b.q);
+    body[i].p = make_float4(b.x.x, b.x.y, b.x.z, b.im);
+    body[i].q = f4of(b.q);
 }
 
 // solvePositionConstraints for one manifold (solver.zig:860-923).
-__device__ void position_points(const WorldDev& w, const CPV& v, uint32_t n, PB& A, PB& B, float* min_sep,
+__device__ void position_points(const SolveFlags sf, const CPV v, uint32_t n, PB& A, PB& B, float* min_sep,
                                 float* max_pen) {
     F3 xa = A.x, xb = B.x;
     Qt qa = A.q, qb = B.q;
     const float ima = A.im, imb = B.im;
     const M33 Ia = A.I, Ib = B.I;
     const bool wa_ = A.wr, wb_ = B.wr;
-    const float slop = w.cfg.slop;
+    const float slop = sf.slop;
     for (uint32_t i = 0; i < n; ++i) {
         const F3 n = ld3(v, CP_NX, i);
         const F3 wa = qrotate(qa, ld3(v, CP_LAX, i)) + xa;
@@ -1887,7 +1896,7 @@ __device__ void position_points(const WorldDev& w, const CPV& v, uint32_t n, PB&
         *min_sep = fminf(*min_sep, sep);
         *max_pen = fmaxf(*max_pen, -sep);
         if (sep >= -slop) continue;
-        const float corr = fmaxf(w.cfg.pos_rate * (sep + slop), -w.cfg.max_pos_corr);
+        const float corr = fmaxf(sf.pos_rate * (sep + slop), -sf.max_corr);
         const F3 ra = wa - xa, rb = wb - xb;
         const F3 rna = cross3(ra, n), rnb = cross3(rb, n);
         float k = ima + imb;
@@ -1918,9 +1927,9 @@ __device__ void position_manifold(WorldDev& w, uint32_t pos, float* min_sep, flo
     const DBody& B = w.body[cmv.y];
     PB a = pb_of(A.p, A.q, A.i0, A.i1, A.i2, writable(pa));
     PB b = pb_of(B.p, B.q, B.i0, B.i1, B.i2, writable(pb));
-    position_points(w, cpv_global(w, pos), cmv.z, a, b, min_sep, max_pen);
-    store_pb(w, cmv.x, a);
-    store_pb(w, cmv.y, b);
+    position_points(solve_flags(w.cfg), cpv_global(w, pos), cmv.z, a, b, min_sep, max_pen);
+    store_pb(w.body, cmv.x, a);
+    store_pb(w.body, cmv.y, b);
 }
 
 // End of one position sweep: reduce its min separation and max penetration
@@ -2059,6 +2068,8 @@ struct FlowSweep {
 };
 // Floats of one chunk's constraint-point fields in shared memory.
 constexpr uint32_t kChunkFloats = CP_NFIELDS * 4u * 32u;
+// Everything the per-manifold steps read besides their own rows, passed by
+// value so that none of it is re-read from memory between points.
 struct FlowCtx {
     uint32_t W, S, V;  // warm-start sweep (0/1), substeps, velocity iterations
     uint32_t smem_chunks;  // chunks of each block held in shared memory
@@ -2066,6 +2077,12 @@ struct FlowCtx {
     float h, hinv, warm_scale;
     F3 grav;
     bool dis_rot;
+    SolveFlags sf;
+    DBody* body;
+    DBody* snap;
+    const DBodyProp* prop;
+    const float2* cfr;
+    uint32_t n_bodies;
 };
 __device__ __forceinline__ FlowSweep flow_sweep(uint32_t k, const FlowCtx& fc) {
     if (fc.W) {
@@ -2125,25 +2142,32 @@ __device__ __forceinline__ uint32_t flow_body_op(const FlowCtx& fc, const FlowSw
     if (sw.kind == FK_RELAX && sw.s + 1u < fc.S) return 2u;
     return 0u;
 }
-// Prefetch for that body step: op 1 the local inverse inertia, op 2 the two
-// damping coefficients.
-__device__ __forceinline__ void flow_ld_prop(const WorldDev& w, uint32_t op, uint32_t i, float pr[9]) {
+// The body properties that body step reads (op 1: local inverse inertia,
+// op 2: the two damping coefficients), asked into L1 ahead of use ...
+__device__ __forceinline__ void flow_prefetch_prop(const FlowCtx& fc, uint32_t op, uint32_t i) {
+    if (op == 0u) return;
+    const char* p = reinterpret_cast<const char*>(fc.prop + i);
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p + sizeof(DBodyProp) - 1));
+}
+// ... and read when the step runs.
+__device__ __forceinline__ void flow_ld_prop(const FlowCtx& fc, uint32_t op, uint32_t i, float pr[9]) {
     if (op == 1u) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) pr[k] = w.prop[i].il[k];
+        for (int k = 0; k < 9; ++k) pr[k] = fc.prop[i].il[k];
     } else if (op == 2u) {
-        pr[0] = w.prop[i].lin_damp;
-        pr[1] = w.prop[i].ang_damp;
+        pr[0] = fc.prop[i].lin_damp;
+        pr[1] = fc.prop[i].ang_damp;
     }
 }
 // Writes one body back after a velocity-type sweep event, with the body step
 // that follows its last event of the sweep.
-__device__ __forceinline__ void flow_body_out(WorldDev& w, const FlowCtx& fc, uint32_t op, uint32_t i, const BV& x,
-                                              Qt q, const float pr[9], uint32_t snap_par) {
+__device__ __forceinline__ void flow_body_out(const FlowCtx& fc, uint32_t op, uint32_t i, const BV& x, Qt q,
+                                              const float pr[9], uint32_t snap_par) {
     const float4 v4 = make_float4(x.v.x, x.v.y, x.v.z, 0.f), w4 = make_float4(x.w.x, x.w.y, x.w.z, 0.f);
     if (op == 0u) {
-        w.body[i].v = v4;
-        w.body[i].w = w4;
+        fc.body[i].v = v4;
+        fc.body[i].w = w4;
         return;
     }
     DBody d;
@@ -2156,65 +2180,72 @@ __device__ __forceinline__ void flow_body_out(WorldDev& w, const FlowCtx& fc, ui
     d.i2 = make_float4(x.I.m[6], x.I.m[7], x.I.m[8], 0.f);
     if (op == 1u) {
         body_integrate_il(d, pr, true, fc.h, fc.dis_rot);  // integratePositions of substep s
-        w.body[i] = d;
+        fc.body[i] = d;
     } else {
         body_gravity_d(d.v, d.w, pr[0], pr[1], fc.grav, fc.h);  // applyGravity of substep s + 1
-        w.body[i].v = d.v;
-        w.body[i].w = d.w;
-        w.snap[(size_t)snap_par * w.n_bodies + i] = d;
+        fc.body[i].v = d.v;
+        fc.body[i].w = d.w;
+        fc.snap[(size_t)snap_par * fc.n_bodies + i] = d;
     }
 }
 
 // prepareConstraints of substep s for one manifold, from its bodies' state
 // right after applyGravity of that substep (the copy in w.snap for bodies the
 // solver writes; the others do not change during the solve).
-__device__ __noinline__ void flow_prepare(WorldDev& w, const FlowCtx& fc, uint32_t s, uint32_t pos, const CPV& v,
-                                          const uint4& cmv, const uint4& rkv) {
+__device__ __noinline__ void flow_prepare(const FlowCtx fc, uint32_t s, uint32_t pos, const CPV v, const uint4 cmv,
+                                          const uint4 rkv) {
     if (cmv.z == 0u) return;
     const bool wa = rkv.x != 0xFFFFFFFFu, wb = rkv.z != 0xFFFFFFFFu;
-    const size_t so = (size_t)(s & 1u) * w.n_bodies;
-    const DBody SA = ld_body_cg((wa ? w.snap + so : w.body) + cmv.x);
-    const DBody SB = ld_body_cg((wb ? w.snap + so : w.body) + cmv.y);
+    const size_t so = (size_t)(s & 1u) * fc.n_bodies;
+    const DBody SA = ld_body_cg((wa ? fc.snap + so : fc.body) + cmv.x);
+    const DBody SB = ld_body_cg((wb ? fc.snap + so : fc.body) + cmv.y);
     const BV sa = bv_of(SA, wa), sb = bv_of(SB, wb);
-    const float rest = w.cfr[pos].y;
-    for (uint32_t i = 0; i < cmv.z; ++i) prepare_point_s(w, v, rest, i, fc.soft, fc.hinv, sa, qof(SA.q), sb, qof(SB.q));
+    const float rest = fc.cfr[pos].y;
+    for (uint32_t i = 0; i < cmv.z; ++i)
+        prepare_point_s(fc.sf, v, rest, i, fc.soft, fc.hinv, sa, qof(SA.q), sb, qof(SB.q));
 }
 
 // One manifold in one sweep, once its bodies are ready.
-__device__ __noinline__ void flow_item(WorldDev& w, const FlowCtx& fc, uint32_t k, uint32_t pos, const CPV& v,
-                                       const uint4& cmv, const uint4& rkv, float* mn, float* mx) {
+__device__ __noinline__ void flow_item(const FlowCtx fc, uint32_t k, uint32_t pos, const CPV v, const uint4 cmv,
+                                       const uint4 rkv, float* mn, float* mx) {
     const FlowSweep sw = flow_sweep(k, fc);
     const bool wa = rkv.x != 0xFFFFFFFFu, wb = rkv.z != 0xFFFFFFFFu;
     if (sw.kind == FK_POS) {
-        if (!wa && !wb && w.prop[cmv.x].type == 0u && w.prop[cmv.y].type == 0u) return;
-        const DBody A = ld_body_cg(w.body + cmv.x), B = ld_body_cg(w.body + cmv.y);
+        if (!wa && !wb && fc.prop[cmv.x].type == 0u && fc.prop[cmv.y].type == 0u) return;
+        const DBody A = ld_body_cg(fc.body + cmv.x), B = ld_body_cg(fc.body + cmv.y);
         PB a = pb_of(A.p, A.q, A.i0, A.i1, A.i2, wa), b = pb_of(B.p, B.q, B.i0, B.i1, B.i2, wb);
-        position_points(w, v, cmv.z, a, b, mn, mx);
-        store_pb(w, cmv.x, a);
-        store_pb(w, cmv.y, b);
+        position_points(fc.sf, v, cmv.z, a, b, mn, mx);
+        store_pb(fc.body, cmv.x, a);
+        store_pb(fc.body, cmv.y, b);
         return;
     }
     const uint32_t opa = flow_body_op(fc, sw, rkv.x, rkv.y), opb = flow_body_op(fc, sw, rkv.z, rkv.w);
-    float pra[9], prb[9];
-    flow_ld_prop(w, opa, cmv.x, pra);
-    flow_ld_prop(w, opb, cmv.y, prb);
+    flow_prefetch_prop(fc, opa, cmv.x);
+    flow_prefetch_prop(fc, opb, cmv.y);
     Qt qa, qb;
     BV a, b;
     {
-        const DBody A = ld_body_cg(w.body + cmv.x), B = ld_body_cg(w.body + cmv.y);
+        const DBody A = ld_body_cg(fc.body + cmv.x), B = ld_body_cg(fc.body + cmv.y);
         a = bv_of(A, wa);
         b = bv_of(B, wb);
         qa = qof(A.q);
         qb = qof(B.q);
     }
-    const float fr = w.cfr[pos].x;
+    const float fr = fc.cfr[pos].x;
     if (sw.kind == FK_WARM)
         warm_points(v, cmv.z, fc.warm_scale, a, b);
     else
-        velocity_points_near(w, v, cmv.z, fr, sw.kind == FK_VEL ? fc.soft : fc.hard, sw.kind == FK_VEL, a, b);
+        velocity_points_near(fc.sf.friction, v, cmv.z, fr, sw.kind == FK_VEL ? fc.soft : fc.hard, sw.kind == FK_VEL, a, b);
     const uint32_t par = (sw.s + 1u) & 1u;
-    if (wa) flow_body_out(w, fc, opa, cmv.x, a, qa, pra, par);
-    if (wb) flow_body_out(w, fc, opb, cmv.y, b, qb, prb, par);
+    float pr[9];
+    if (wa) {
+        flow_ld_prop(fc, opa, cmv.x, pr);
+        flow_body_out(fc, opa, cmv.x, a, qa, pr, par);
+    }
+    if (wb) {
+        flow_ld_prop(fc, opb, cmv.y, pr);
+        flow_body_out(fc, opb, cmv.y, b, qb, pr, par);
+    }
 }
 
 // Waits until every lane of the warp sees its bodies' event counters at the
@@ -2290,12 +2321,12 @@ __device__ bool flow_run(G& g, WorldDev& w, const FlowCtx& fc, float* fsm, uint3
                 // ahead of this manifold's own turn in the sweep
                 if (!flow_wait(w, need_a, cmv.x, k * rkv.y, need_b, cmv.y, k * rkv.w, true)) return false;
                 fence_acq_rel_gpu();
-                if (valid) flow_prepare(w, fc, sw.s, pos, v, cmv, rkv);
+                if (valid) flow_prepare(fc, sw.s, pos, v, cmv, rkv);
             }
             const uint32_t ea = k * rkv.y + rkv.x, eb = k * rkv.w + rkv.z;
             if (!flow_wait(w, need_a, cmv.x, ea, need_b, cmv.y, eb, false)) return false;
             fence_acq_rel_gpu();
-            if (valid) flow_item(w, fc, k, pos, v, cmv, rkv, mn, mx);
+            if (valid) flow_item(fc, k, pos, v, cmv, rkv, mn, mx);
             fence_acq_rel_gpu();
             if (need_a) st_relaxed_u32(w.ev + cmv.x, ea + 1u);
             if (need_b) st_relaxed_u32(w.ev + cmv.y, eb + 1u);
@@ -2319,6 +2350,12 @@ __device__ bool phase_solve_flow(G& g, WorldDev& w, float* fsm, uint32_t M, uint
     fc.grav = F3{cf.gravity[0], cf.gravity[1], cf.gravity[2]};
     fc.dis_rot = cf.disable_rotation != 0u;
     fc.smem_chunks = cf.flow_smem_chunks;
+    fc.sf = solve_flags(cf);
+    fc.body = w.body;
+    fc.snap = w.snap;
+    fc.prop = w.prop;
+    fc.cfr = w.cfr;
+    fc.n_bodies = w.n_bodies;
     const uint32_t N = w.n_bodies;
     // Bodies: counters to zero; gravity of substep 0 and its copy for
     // prepare; a moving body without constraints takes all its substeps now.
@@ -2483,26 +2520,29 @@ __device__ __forceinline__ void stamp(G& g, WorldDev& w, uint32_t slot) {
     if (g.rank() == 0 && w.ts) w.ts[slot] = global_ns();
 }
 
+// The narrow part of one step: counters, begin (all-sleeping skip, world
+// inverse inertia), the pair list, the narrow phase.  Returns true, and
+// leaves C_SOLVE_GO set, when the solve part of the step is to run.
 template <class G>
-__device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifold* warp_sm, const CacheSmem& csm,
-                           float* fsm) {
+__device__ bool world_step_narrow(G& g, WorldDev& w, const ColliderSet& cs, WarpManifold* warp_sm,
+                                  const CacheSmem& csm) {
     const uint32_t ph = w.cfg.phases;
     const uint32_t f0 = *(volatile uint32_t*)&w.frame[0];
     stamp(g, w, TS_START);
-    if (w.n_bodies == 0u) return;  // an empty batch slot
+    if (w.n_bodies == 0u) return false;  // an empty batch slot
     // per-step counters (the sticky error word excepted)
     if (g.rank() < C_ERROR) w.ctr[g.rank()] = 0u;
-    if (!g.sync()) return;
+    if (!g.sync()) return false;
     bool skipped = false;
-    if (!phase_begin(g, w, (ph & PH_SKIP_TEST) != 0u, &skipped)) return;
+    if (!phase_begin(g, w, (ph & PH_SKIP_TEST) != 0u, &skipped)) return false;
     stamp(g, w, TS_BEGIN);
-    if (skipped) return;
+    if (skipped) return false;
     if ((ph & PH_NARROW) && w.cfg.device_pairs) {
         bool overflow = false;
-        if (!phase_broadphase(g, w, cs, &overflow)) return;
+        if (!phase_broadphase(g, w, cs, &overflow)) return false;
         if (overflow) {
             if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_CAP);
-            return;
+            return false;
         }
     } else {
         w.n_pairs = *w.n_pairs_dev;
@@ -2510,60 +2550,80 @@ __device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifol
             // the pair list did not fit: leave every state untouched, the
             // host grows the buffers and runs the step again
             if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_CAP);
-            return;
+            return false;
         }
     }
     // ContactManager.beginFrame (narrow_phase.zig:1003-1008): the previous
     // "current" manifolds become "previous"
-    const uint32_t cur = (ph & PH_NARROW) ? ((f0 + 1u) & 1u) : (f0 & 1u), prev = cur ^ 1u;
     if (ph & PH_NARROW) {
+        const uint32_t cur = (f0 + 1u) & 1u, prev = cur ^ 1u;
         if (g.rank() == 0) {
             w.frame[0] = f0 + 1u;
             w.frame[1] = w.n_pairs;
         }
-        if (!phase_pairs(g, w, cs, cur)) return;
+        if (!phase_pairs(g, w, cs, cur)) return false;
         stamp(g, w, TS_PAIRS);
         stamp(g, w, TS_CACHE);
-        if (!phase_probe(g, w, cs, cur, warp_sm, csm)) return;
+        if (!phase_probe(g, w, cs, cur, warp_sm, csm)) return false;
         stamp(g, w, TS_PROBE);
-        if (!phase_finalize(g, w, cur, prev)) return;
-        if (!g.sync()) return;
+        if (!phase_finalize(g, w, cur, prev)) return false;
         stamp(g, w, TS_FINALIZE);
     }
-    if (ph & PH_SOLVE) {
-        // The solver's work per colour batch is a few hundred manifolds: run it
-        // on k blocks (one per 512 manifolds, at least 2) with a cheaper barrier.
-        const uint32_t nman = (ph & PH_NARROW) ? *(volatile uint32_t*)&w.ctr[C_MANIFOLDS] : w.n_pairs;
-        uint32_t want = max(2u, (nman + w.cfg.solver_div - 1u) / w.cfg.solver_div);
-        // event-ordered sweeps: enough blocks to hold every chunk (at most
-        // nman / 32 + one partial chunk per colour) in shared memory
-        if (G::kEventSweeps && w.cfg.solver_flow && w.cfg.flow_smem_chunks)
-            want = max(want, (nman / 32u + 64u + w.cfg.flow_smem_chunks - 1u) / w.cfg.flow_smem_chunks);
-        G s = g.subgroup(min(want, g.nblocks()));
-        if (!s.member()) return;
-        uint32_t M = 0, ncol = 0;
-        if (!phase_constraints(s, w, cur, &M, &ncol)) return;
-        stamp(s, w, TS_CONSTRAINTS);
-        const bool solved = w.cfg.dt > 0.0f && w.n_bodies > 0u;
-        // event-ordered sweeps unless a kinematic body (moved every substep,
-        // written by nobody) sits in a constraint
-        if (solved) {
-            bool ok;
-            if constexpr (G::kEventSweeps) {
-                const bool flow = w.cfg.solver_flow && w.cfg.vel_iters > 0u && w.cfg.substeps > 0u &&
-                                  *(volatile uint32_t*)&w.ctr[C_KIN_CONTACT] == 0u &&
-                                  (*(volatile uint32_t*)&w.ctr[C_ERROR] & ERR_COLOURS) == 0u;
-                ok = flow ? phase_solve_flow(s, w, fsm, M, ncol) : phase_solve(s, w, M, ncol);
-            } else {
-                ok = phase_solve(s, w, M, ncol);
-            }
-            if (!ok) return;
+    if (g.rank() == 0) w.ctr[C_SOLVE_GO] = 1u;
+    return g.sync();
+}
+
+// The solve part of one step: constraints, colouring, ContactSolver.solve,
+// store and sleep.  check_go: read the narrow part's verdict from C_SOLVE_GO
+// (the parts run as two kernels).
+template <class G>
+__device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go) {
+    const uint32_t ph = w.cfg.phases;
+    if (!(ph & PH_SOLVE) || w.n_bodies == 0u) return;
+    if (check_go && *(volatile uint32_t*)&w.ctr[C_SOLVE_GO] == 0u) return;
+    w.n_pairs = *(volatile uint32_t*)w.n_pairs_dev;
+    const uint32_t cur = *(volatile uint32_t*)&w.frame[0] & 1u;  // the latest manifolds
+    // The solver's work per colour batch is a few hundred manifolds: run it
+    // on k blocks (one per solver_div manifolds, at least 2) with a cheaper
+    // barrier.
+    const uint32_t nman = (ph & PH_NARROW) ? *(volatile uint32_t*)&w.ctr[C_MANIFOLDS] : w.n_pairs;
+    uint32_t want = max(2u, (nman + w.cfg.solver_div - 1u) / w.cfg.solver_div);
+    // event-ordered sweeps: enough blocks to hold every chunk (at most
+    // nman / 32 + one partial chunk per colour) in shared memory
+    if (G::kEventSweeps && w.cfg.solver_flow && w.cfg.flow_smem_chunks)
+        want = max(want, (nman / 32u + 64u + w.cfg.flow_smem_chunks - 1u) / w.cfg.flow_smem_chunks);
+    G s = g.subgroup(min(want, g.nblocks()));
+    if (!s.member()) return;
+    uint32_t M = 0, ncol = 0;
+    if (!phase_constraints(s, w, cur, &M, &ncol)) return;
+    stamp(s, w, TS_CONSTRAINTS);
+    const bool solved = w.cfg.dt > 0.0f && w.n_bodies > 0u;
+    // event-ordered sweeps unless a kinematic body (moved every substep,
+    // written by nobody) sits in a constraint
+    if (solved) {
+        bool ok;
+        if constexpr (G::kEventSweeps) {
+            const bool flow = w.cfg.solver_flow && w.cfg.vel_iters > 0u && w.cfg.substeps > 0u &&
+                              *(volatile uint32_t*)&w.ctr[C_KIN_CONTACT] == 0u &&
+                              (*(volatile uint32_t*)&w.ctr[C_ERROR] & ERR_COLOURS) == 0u;
+            ok = flow ? phase_solve_flow(s, w, fsm, M, ncol) : phase_solve(s, w, M, ncol);
+        } else {
+            ok = phase_solve(s, w, M, ncol);
         }
-        if (!s.sync()) return;
-        stamp(s, w, TS_SOLVE);
-        if (!phase_store(s, w, cur, M, solved)) return;
-        stamp(s, w, TS_END);
+        if (!ok) return;
     }
+    if (!s.sync()) return;
+    stamp(s, w, TS_SOLVE);
+    if (!phase_store(s, w, cur, M, solved)) return;
+    stamp(s, w, TS_END);
+}
+
+// One whole step (VoxelPhysicsSystem.step with the pairs given) in one
+// kernel: the narrow part, then the solve part.
+template <class G>
+__device__ void world_step(G& g, WorldDev& w, const ColliderSet& cs, WarpManifold* warp_sm, const CacheSmem& csm,
+                           float* fsm) {
+    if (world_step_narrow(g, w, cs, warp_sm, csm)) world_step_solve(g, w, fsm, false);
 }
 
 }  // namespace vxp

@@ -177,6 +177,7 @@ enum : uint32_t {
     C_BRICKS,        // bricks of A in the overlap region + bricks of B in B's
     C_NCACHE,        // pairs that consult the brick-pair cache this step
     C_KIN_CONTACT,   // constraints touching an awake kinematic body
+    C_SOLVE_GO,      // set by the narrow part of a step when its solve part may run
     C_ERROR = 31,    // sticky error bits (not cleared per step)
     C_NCTR = 32
 };
