@@ -49,7 +49,10 @@ SOLVER_V, SOLVER_Q = 1, 2
 # DRAM bytes (read + write) per launch of each step kernel on the settled
 # pile, keyed by (workload, kernel), from one ncu capture of the same
 # workload; re-captured when a kernel changes.
-PROFILED_TRAFFIC = {}
+PROFILED_TRAFFIC = {
+    ("config2_pile_4096", "k_step_grid"): (24_773_888, "profiles/k_step_grid_k_solve_grid_config2_pile.md"),
+    ("config2_pile_4096", "k_solve_grid"): (8_487_936, "profiles/k_step_grid_k_solve_grid_config2_pile.md"),
+}
 
 
 def parse():
@@ -374,7 +377,8 @@ def ours(args):
                          "alg_bytes_per_launch": kernels[dominant]["alg_bytes_per_launch"],
                          "step": {"achieved": achieved, "frac": achieved / peak,
                                   "alg_bytes_per_step": statistics.mean(nb)},
-                         "kernels": kernels},
+                         "kernels": {k: dict(v, traffic=PROFILED_TRAFFIC.get((f"config2_pile_{n_dyn}", k), (None,))[0])
+                                     for k, v in kernels.items()}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "body-substeps/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
                     "d2h_bytes_per_step": d2h // max(1, args.steps)},
