@@ -98,6 +98,18 @@ def dist_setup(args):
     return ws, rank, local, pg
 
 
+def max_over_ranks(pg, x: float, device: str) -> float:
+    """The largest x over all ranks (the job's time is its slowest rank's);
+    x itself without a process group."""
+    if not pg:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 class Clocks:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -291,10 +303,7 @@ def ours(args):
     torch.cuda.synchronize()
     clk = clocks.stop()
     total_s = sum(step_ms) / 1e3
-    if pg:
-        t = torch.tensor([total_s], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_s = float(t.item())
+    total_s = max_over_ranks(pg, total_s, f"cuda:{local}")
     value = ws * n_dyn * 8 * args.steps / total_s
     pts = [s["contact_points"] for s in stats]
     contacts_per_s = ws * sum(pts) * 8 / total_s
@@ -338,10 +347,7 @@ def ours(args):
         h2d += 8 * n.value
         d2h += 8 * n.value + 128 * len(pin_bodies)
     e2e_s = max(time.perf_counter() - t0, 1e-9)
-    if pg:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(pg, e2e_s, f"cuda:{local}")
     e2e_value = None if args.no_e2e else ws * n_dyn * 8 * args.steps / e2e_s
 
     cpu = None
