@@ -271,6 +271,17 @@ int vxp_pairs_from_bodies(vxp_ctx* ctx, float margin, vxp_pair* out, uint32_t ca
  * stream): [pair source and copies, step kernel, whole call]. */
 int vxp_last_step_ms(vxp_ctx* ctx, float out[3]);
 
+/* Per-substep parity hook.  With recording on, each step writes every body's
+ * state after each substep's relax sweep (BodyState after relaxConstraints,
+ * src/solver.zig:848-856; before the position sweeps and writeBack) as 13
+ * floats: position[3], rotation[4], linear_velocity[3], angular_velocity[3],
+ * substep-major, bodies in vxp_bodies_set order.  Recording steps sweep colour
+ * batch by colour batch (bit-identical to the event-ordered sweeps).
+ * vxp_substeps_get waits for the last step; *n_substeps = substeps recorded
+ * (0 when the step was skipped); cap_floats must hold n_substeps x bodies x 13. */
+int vxp_snapshot_substeps(vxp_ctx* ctx, int enable);
+int vxp_substeps_get(vxp_ctx* ctx, float* out, uint32_t cap_floats, uint32_t* n_substeps);
+
 /* Device time (ms) of the last step's kernels: [narrow part, solve part].  A
  * world stepped by the cooperative grid runs them as two kernels
  * (k_step_grid, k_solve_grid); a world stepped by one CTA runs both parts in

@@ -290,6 +290,22 @@ int vxo_colours_get(void* p, uint32_t* out, uint32_t cap, uint32_t* n_out) {
     return overflow;
 }
 
+// Per-substep body states of the last solve (test hook): 13 floats per body
+// per substep (position, rotation, linear and angular velocity).
+int vxo_set_substep_record(void* p, int on) {
+    DISPATCH(p, { h->w.solver.record_substeps = on != 0; });
+    return 0;
+}
+int vxo_substeps_get(void* p, float* out, uint32_t cap_floats, uint32_t* n_substeps) {
+    DISPATCH(p, {
+        const auto& g = h->w.solver.substep_log;
+        const size_t n = std::min<size_t>(cap_floats, g.size());
+        for (size_t i = 0; i < n; ++i) out[i] = g[i];
+        *n_substeps = h->w.solver.substeps_logged;
+    });
+    return 0;
+}
+
 int vxo_set_candidate_dump(void* p, int on) {
     DISPATCH(p, { h->w.dump = on != 0; });
     return 0;

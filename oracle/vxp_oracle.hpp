@@ -1145,6 +1145,12 @@ template <class R> struct ContactSolver {
     uint32_t position_iterations_run = 0;
     R max_penetration = 0;
     uint32_t colours = 0;
+    // Per-substep record (test hook): after each substep's relax sweep, every
+    // body's position, rotation, linear and angular velocity as float, in
+    // body order (13 floats per body).
+    bool record_substeps = false;
+    std::vector<float> substep_log;
+    uint32_t substeps_logged = 0;
 
     void clear() {
         bodies.clear();
@@ -1235,6 +1241,8 @@ template <class R> struct ContactSolver {
         const bool has = !cons.empty();
         const R h = dt / (R)cfg.substeps;
         const SoftParams<R> soft = computeSoftParams(cfg.hertz, cfg.damping_ratio, h);
+        substep_log.clear();
+        substeps_logged = 0;
         for (uint32_t s = 0; s < cfg.substeps; ++s) {
             applyGravity(h);
             if (has) {
@@ -1244,6 +1252,15 @@ template <class R> struct ContactSolver {
             }
             for (auto& b : bodies) b.integratePosition(h, cfg.disable_rotation);
             if (has) solveVelocity(SoftParams<R>{0, 1, 1}, false);
+            if (record_substeps) {
+                for (const auto& b : bodies) {
+                    const float r[13] = {(float)b.p.x, (float)b.p.y, (float)b.p.z, (float)b.q.x, (float)b.q.y,
+                                         (float)b.q.z, (float)b.q.w, (float)b.v.x, (float)b.v.y, (float)b.v.z,
+                                         (float)b.w.x, (float)b.w.y, (float)b.w.z};
+                    substep_log.insert(substep_log.end(), r, r + 13);
+                }
+                ++substeps_logged;
+            }
         }
         if (has) {
             for (uint32_t it = 0; it < cfg.position_iterations; ++it) {
@@ -1515,6 +1532,8 @@ template <class R> struct World {
     void step(R dt, const std::vector<std::pair<uint32_t, uint32_t>>& pairs) {  // system.zig:537-555
         stats = Stats{};
         stats.pairs_in = (uint32_t)pairs.size();
+        solver.substep_log.clear();
+        solver.substeps_logged = 0;
         if (wcfg.enable_sleeping && allDynamicSleeping()) {
             stats.step_skipped = 1;
             return;

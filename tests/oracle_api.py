@@ -41,6 +41,8 @@ for name, res, args in [
     ("vxo_stats_get", _I, [_VP, _VP]),
     ("vxo_colours_get", _I, [_VP, _VP, _U32, _PU32]),
     ("vxo_set_candidate_dump", _I, [_VP, _I]),
+    ("vxo_set_substep_record", _I, [_VP, _I]),
+    ("vxo_substeps_get", _I, [_VP, _VP, _U32, _PU32]),
     ("vxo_candidates_get", _I, [_VP, _VP, _U32, _PU32]),
     ("vxo_pairs_find", _I, [_VP, _F, _VP, _U32, _PU32]),
     ("vxo_narrow_phase_threaded", _I, [_VP, _VP, _U32, _I]),
@@ -184,6 +186,19 @@ class OracleWorld:
         out = np.zeros(n.value, dtype=np.uint32)
         overflow = L.vxo_colours_get(self.h, abi.ptr(out), len(out), ctypes.byref(n))
         return out, bool(overflow)
+
+    def set_substep_record(self, on=True):
+        L.vxo_set_substep_record(self.h, 1 if on else 0)
+
+    def substeps(self):
+        """Body states after each substep of the last step: (substeps, bodies, 13) float32
+        (position, rotation, linear velocity, angular velocity)."""
+        n = len(self.get_bodies())
+        cap = 64 * n * 13
+        out = np.zeros(cap, dtype=np.float32)
+        ns = ctypes.c_uint32(0)
+        L.vxo_substeps_get(self.h, out.ctypes.data, cap, ctypes.byref(ns))
+        return out[: ns.value * n * 13].reshape(ns.value, n, 13)
 
     def set_candidate_dump(self, on=True):
         L.vxo_set_candidate_dump(self.h, 1 if on else 0)

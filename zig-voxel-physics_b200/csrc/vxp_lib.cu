@@ -827,6 +827,8 @@ struct vxp_ctx {
     int use_grid = -1;  // -1 auto, 0 block, 1 grid
     uint32_t solver_div = 128;
     uint32_t solver_flow = 1;
+    bool record_substeps = false;
+    DBuf<float> subrec;
 };
 
 namespace {
@@ -855,6 +857,12 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
     const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
     const size_t smem = grid ? grid_smem(w.cache_cap) : step_smem(kBlockThreads, w.cache_cap);
     w.cfg.flow_smem_chunks = grid ? flow_chunks(solve_smem()) : 0u;
+    if (ctx->record_substeps) {
+        const size_t need = (size_t)std::max(1u, ctx->cfg.substeps) * std::max(1u, ctx->w.n_bodies) * 13u;
+        if (ctx->subrec.reserve(need) != cudaSuccess) return fail(ctx, VXP_ERR_OOM, "substep record buffer");
+        w.cfg.record_substeps = 1u;
+        w.subrec = ctx->subrec.p;
+    }
     CK(cudaMemcpyAsync(ctx->d_world.p, &w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
     const ColliderSet cs = ctx->cols.set();
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -1432,6 +1440,25 @@ int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n) {
     unsigned long long t[TS_N];
     CK(cudaMemcpy(t, ctx->w.ts.p, sizeof(t), cudaMemcpyDeviceToHost));
     for (uint32_t i = 0; i < n && i < TS_N; ++i) out[i] = t[i] >= t[0] ? (uint64_t)(t[i] - t[0]) : 0u;
+    return VXP_OK;
+}
+
+int vxp_snapshot_substeps(vxp_ctx* ctx, int enable) {
+    if (!ctx) return VXP_ERR_ARG;
+    ctx->record_substeps = enable != 0;
+    return VXP_OK;
+}
+
+int vxp_substeps_get(vxp_ctx* ctx, float* out, uint32_t cap_floats, uint32_t* n_substeps) {
+    if (!ctx || !n_substeps || (!out && cap_floats)) return VXP_ERR_ARG;
+    if (int rc = check_device_error(ctx)) return rc;
+    uint32_t ns = 0;
+    CK(cudaMemcpy(&ns, ctx->w.ctr.p + C_SUBREC, sizeof(ns), cudaMemcpyDeviceToHost));
+    if (!ctx->record_substeps || !ctx->subrec.p) ns = 0;
+    const size_t need = (size_t)ns * ctx->w.n_bodies * 13u;
+    if (need > cap_floats) return fail(ctx, VXP_ERR_ARG, "substep record needs %zu floats", need);
+    if (need) CK(cudaMemcpy(out, ctx->subrec.p, need * sizeof(float), cudaMemcpyDeviceToHost));
+    *n_substeps = ns;
     return VXP_OK;
 }
 

@@ -2017,6 +2017,19 @@ __device__ bool phase_solve(G& g, WorldDev& w, uint32_t M, uint32_t ncol) {
                 if (!g.sync()) return false;
             }
         }
+        // test hook: every body's state after this substep (the thread that
+        // records body i also applies its next gravity step)
+        if (cf.record_substeps && w.subrec) {
+            for (uint32_t i = g.rank(); i < N; i += g.size()) {
+                const DBody b = w.body[i];
+                float* r = w.subrec + ((size_t)s * N + i) * 13u;
+                r[0] = b.p.x; r[1] = b.p.y; r[2] = b.p.z;
+                r[3] = b.q.x; r[4] = b.q.y; r[5] = b.q.z; r[6] = b.q.w;
+                r[7] = b.v.x; r[8] = b.v.y; r[9] = b.v.z;
+                r[10] = b.w.x; r[11] = b.w.y; r[12] = b.w.z;
+            }
+            if (g.rank() == 0) w.ctr[C_SUBREC] = s + 1u;
+        }
     }
     if (has) {
         for (uint32_t it = 0; it < cf.pos_iters; ++it) {
@@ -2603,7 +2616,8 @@ __device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go) {
     if (solved) {
         bool ok;
         if constexpr (G::kEventSweeps) {
-            const bool flow = w.cfg.solver_flow && w.cfg.vel_iters > 0u && w.cfg.substeps > 0u &&
+            const bool flow = w.cfg.solver_flow && !w.cfg.record_substeps && w.cfg.vel_iters > 0u &&
+                              w.cfg.substeps > 0u &&
                               *(volatile uint32_t*)&w.ctr[C_KIN_CONTACT] == 0u &&
                               (*(volatile uint32_t*)&w.ctr[C_ERROR] & ERR_COLOURS) == 0u;
             ok = flow ? phase_solve_flow(s, w, fsm, M, ncol) : phase_solve(s, w, M, ncol);

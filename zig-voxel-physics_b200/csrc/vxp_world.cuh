@@ -148,6 +148,7 @@ struct StepCfg {
     float margin;             // AABB inflation of that pair list
     uint32_t solver_flow;     // 1: sweeps ordered by per-body event counters, 0: colour barriers
     uint32_t flow_smem_chunks;  // constraint chunks per block the launch's shared memory holds
+    uint32_t record_substeps;   // 1: write every body's state after each substep to subrec
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 
@@ -178,6 +179,7 @@ enum : uint32_t {
     C_NCACHE,        // pairs that consult the brick-pair cache this step
     C_KIN_CONTACT,   // constraints touching an awake kinematic body
     C_SOLVE_GO,      // set by the narrow part of a step when its solve part may run
+    C_SUBREC,        // substeps recorded in subrec by the last solve
     C_ERROR = 31,    // sticky error bits (not cleared per step)
     C_NCTR = 32
 };
@@ -240,6 +242,7 @@ struct WorldDev {
     uint32_t* ev;
     DBody* snap;
     uint2* chunk;                 // [first, end) positions of <= 32 manifolds of one colour
+    float* subrec;                // per substep and body: position, rotation, v, w (13 floats)
     // packed constraint data, slot-major [slot][M]; see CP_* field ids
     float* cp;                    // CP_NFIELDS * 4 * pair_cap floats
     uint4* cm;                    // per packed manifold: ia, ib, n, pair

@@ -135,6 +135,19 @@ class VoxelPhysicsSystem:
         after every colour batch.  Worlds stepped by one CTA always use 0."""
         self._check(self.lib.vxp_set_solver_mode(self.ctx, int(mode)))
 
+    def set_substep_record(self, on: bool = True) -> None:
+        self._check(self.lib.vxp_snapshot_substeps(self.ctx, 1 if on else 0))
+
+    def substeps(self) -> np.ndarray:
+        """Body states after each substep of the last step: (substeps, bodies, 13)
+        float32 (position, rotation, linear velocity, angular velocity)."""
+        n = len(self.get_bodies())
+        cap = max(1, int(self.config.substeps)) * n * 13
+        out = np.zeros(cap, dtype=np.float32)
+        ns = ctypes.c_uint32(0)
+        self._check(self.lib.vxp_substeps_get(self.ctx, abi.ptr(out), cap, ctypes.byref(ns)))
+        return out[: ns.value * n * 13].reshape(ns.value, n, 13)
+
     def pairs(self, margin: float | None = None) -> np.ndarray:
         m = self.pair_margin if margin is None else margin
         n = ctypes.c_uint32(0)
