@@ -468,7 +468,7 @@ def batched(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"config3_batched_{len(scenes)}", "worlds": len(scenes), "bodies": n_dyn,
                    "substeps": 4, "dt": "1/60", "l2": "flushed (256 MiB write) between timed steps",
-                   "schedule": {"choice": ["slot order", "longest first"][choice],
+                   "schedule": {"choice": ["256/slot", "256/longest-first", "512/slot", "512/longest-first"][choice],
                                 "autotune_ms": [float(x) for x in tune_ms]}},
         "plain_single_world": {"value": plain_value, "ms_per_batch_step": plain_ms,
                                "method": "each world alone, its own launches, 3 timed steps after 2, summed"},
@@ -497,7 +497,7 @@ def serving(args):
     batch = vxp.VoxelWorldBatch(args.slots, substeps=4)
     for c in lib:
         batch.add_collider(c.id, c.voxel_size, c.bricks)
-    batch.set_schedule(256, 1)
+    batch.set_schedule(512, 1)
     server = vxp.server.SimulationServer(batch, 1.0 / 60.0, max_slots=args.slots, budget_bytes=120 * 10**9)
     clocks = Clocks(0)
     clocks.start()

@@ -354,11 +354,11 @@ int vxp_batch_synchronize(vxp_batch* b);
 /* Device ms of the last vxp_batch_step call, and per slot the ms of its CTA
  * in the last step (0 for empty slots). */
 int vxp_batch_times(vxp_batch* b, float* total_ms, float* world_ms, uint32_t n);
-/* Schedule: CTA size (256 threads; anything else is VXP_ERR_ARG); launch
- * order 0 = slot order, 1 = longest measured world first. */
+/* Schedule: CTA size 256 or 512; launch order 0 = slot order, 1 = longest
+ * measured world first. */
 int vxp_batch_set_schedule(vxp_batch* b, uint32_t threads, uint32_t order_mode);
-/* Autotuner: runs trial_steps real steps under each launch order, keeps the
- * fastest; ms_out[2] = mean step ms of order 0 and order 1. */
+/* Autotuner: runs trial_steps real steps under each schedule, keeps the
+ * fastest; ms_out[4] = mean step ms of (256,0), (256,1), (512,0), (512,1). */
 int vxp_batch_autotune(vxp_batch* b, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice);
 
 /* ---------------------------------------------------------------------------

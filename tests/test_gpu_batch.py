@@ -55,14 +55,14 @@ def test_batch_equals_alone_and_oracle(vxp):
     b.close()
 
 
-@pytest.mark.parametrize("order", [0, 1])
-def test_schedule_does_not_change_results(vxp, order):
+@pytest.mark.parametrize("threads,order", [(256, 0), (256, 1), (512, 0), (512, 1)])
+def test_schedule_does_not_change_results(vxp, threads, order):
     scenes = small_mix(vxp, [40, 12, 70], seed=8)
     dt = np.float32(1.0 / 60.0)
     b = vxp.VoxelWorldBatch(3, substeps=4)
     for i, sc in enumerate(scenes):
         b.load_scene(i, sc, collider_offset=1000 * (i + 1))
-    b.set_schedule(256, order)
+    b.set_schedule(threads, order)
     b.step(dt, 40)
     b.synchronize()
     for i, sc in enumerate(scenes):
@@ -78,9 +78,9 @@ def test_autotune_keeps_results(vxp):
     b = vxp.VoxelWorldBatch(4, substeps=4)
     for i, sc in enumerate(scenes):
         b.load_scene(i, sc, collider_offset=1000 * (i + 1))
-    choice, ms = b.autotune(dt, trial_steps=2)  # 2 x (1 + 2) real steps
-    assert 0 <= choice < 2 and np.all(ms > 0)
-    b.step(dt, 14)
+    choice, ms = b.autotune(dt, trial_steps=2)  # 4 x (1 + 2) real steps
+    assert 0 <= choice < 4 and np.all(ms > 0)
+    b.step(dt, 8)
     b.synchronize()
     for i, sc in enumerate(scenes):
         got = b.get_world(i)

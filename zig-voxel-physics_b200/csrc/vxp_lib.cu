@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) k_step_block(WorldDe
     world_step(g, w, cs, wsm, csm, reinterpret_cast<float*>(smem_raw));
 }
 template __global__ void k_step_block<256>(WorldDev*, ColliderSet);
+template __global__ void k_step_block<512>(WorldDev*, ColliderSet);
 
 // One world over a cooperative grid, in two kernels: the narrow part of the
 // step, then its solve part (barrier words bar[0] and bar[1]).
@@ -217,7 +218,7 @@ std::string fmt(const char* f, ...) {
     return buf;
 }
 
-constexpr uint32_t kBlockThreads = 256;
+constexpr uint32_t kBlockThreads = 512;
 // CTA sizes of the two cooperative grid kernels of a large world's step (one
 // CTA per SM each): the narrow part wants many warps to hide its memory
 // latency, the solve part wants registers for its long dependent chains.
@@ -1103,6 +1104,8 @@ void vxp_config_default(vxp_config* c) {
 static int set_kernel_smem(uint32_t cache_cap) {
     if (cudaFuncSetAttribute(k_step_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)step_smem(256, cache_cap)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_step_block<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)step_smem(512, cache_cap)) != cudaSuccess ||
         cudaFuncSetAttribute(k_step_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)grid_smem(cache_cap)) != cudaSuccess ||
         cudaFuncSetAttribute(k_solve_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem()) !=
@@ -1128,7 +1131,11 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     int smc = 0;
     if (cudaDeviceGetAttribute(&smc, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return bail(VXP_ERR_CUDA);
     ctx->sm_count = smc;
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(VXP_ERR_CUDA);
+    // A blocking stream: buffers are zero-filled (cudaMemset) and uploaded
+    // (cudaMemcpy from pageable memory) on the legacy default stream, and
+    // both can return before the device is done; a blocking stream orders
+    // every kernel after that work.
+    if (cudaStreamCreate(&ctx->stream) != cudaSuccess) return bail(VXP_ERR_CUDA);
     if (cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev0) != cudaSuccess ||
         cudaEventCreate(&ctx->ev1) != cudaSuccess || cudaEventCreate(&ctx->ev_mid) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_count, cudaEventDisableTiming) != cudaSuccess)
@@ -1520,6 +1527,7 @@ struct vxp_batch {
     std::vector<uint32_t> order;      // launch position -> slot
     DBuf<WorldDev> d_worlds;
     DBuf<unsigned long long> d_ts;    // per launch position: [start, end]
+    DBuf<uint32_t> d_status;          // per launch position: [error word, pair count]
     uint32_t threads = 256;           // CTA size
     uint32_t order_mode = 1;          // 0: slot order, 1: longest measured / largest first
     float margin = 0.1f;
@@ -1560,6 +1568,15 @@ __global__ void k_batch_times(const WorldDev* worlds, uint32_t n, unsigned long 
     out[2 * i + 1] = ts[TS_END] > ts[TS_START] ? ts[TS_END] : ts[TS_START];
 }
 
+// Per launch position: the world's sticky error word and its pair count of
+// the last step, gathered so the host reads every world with one copy.
+__global__ void k_batch_status(const WorldDev* worlds, uint32_t n, uint32_t* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[2 * i] = worlds[i].ctr[C_ERROR];
+    out[2 * i + 1] = *worlds[i].n_pairs_dev;
+}
+
 // Launch order, device WorldDev array and the graph of one step.
 int batch_prepare(vxp_batch* bt, float dt) {
     if (int rc = bt->cols.sync(bt->err)) return rc;
@@ -1579,7 +1596,8 @@ int batch_prepare(vxp_batch* bt, float dt) {
         for (size_t i = 0; i < ord.size(); ++i)
             wd[i] = bt->slots[ord[i]]->make(bt->cfg, dt, PH_STEP, 128, true, bt->margin, 0u);
         if (bt->d_worlds.reserve(std::max<size_t>(wd.size(), 1)) != cudaSuccess ||
-            bt->d_ts.reserve(2 * std::max<size_t>(wd.size(), 1)) != cudaSuccess)
+            bt->d_ts.reserve(2 * std::max<size_t>(wd.size(), 1)) != cudaSuccess ||
+            bt->d_status.reserve(2 * std::max<size_t>(wd.size(), 1)) != cudaSuccess)
             return bfail(bt, VXP_ERR_OOM, "batch world table");
         if (!wd.empty())
             BK(cudaMemcpyAsync(bt->d_worlds.p, wd.data(), wd.size() * sizeof(WorldDev), cudaMemcpyHostToDevice,
@@ -1605,7 +1623,8 @@ int batch_prepare(vxp_batch* bt, float dt) {
     if (n == 0) return VXP_OK;
     const size_t smem = step_smem(bt->threads, bt->cache_cap);
     BK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
-    k_step_block<256><<<n, 256, smem, bt->stream>>>(bt->d_worlds.p, cs);
+    if (bt->threads == 512) k_step_block<512><<<n, 512, smem, bt->stream>>>(bt->d_worlds.p, cs);
+    else k_step_block<256><<<n, 256, smem, bt->stream>>>(bt->d_worlds.p, cs);
     const cudaError_t le = cudaGetLastError();
     cudaGraph_t g = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(bt->stream, &g);
@@ -1640,7 +1659,8 @@ int vxp_batch_create(const vxp_config* cfg, int device, uint32_t max_worlds, vxp
         return rc;
     };
     if (cudaSetDevice(device) != cudaSuccess) return bail(VXP_ERR_CUDA);
-    if (cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(VXP_ERR_CUDA);
+    // blocking, for the same reason as a context's stream (vxp_create)
+    if (cudaStreamCreate(&bt->stream) != cudaSuccess) return bail(VXP_ERR_CUDA);
     if (cudaEventCreate(&bt->ev0) != cudaSuccess || cudaEventCreate(&bt->ev1) != cudaSuccess)
         return bail(VXP_ERR_CUDA);
     if (set_kernel_smem(bt->cache_cap)) return bail(VXP_ERR_CUDA);
@@ -1731,21 +1751,48 @@ int vxp_batch_step(vxp_batch* bt, float dt, uint32_t n_steps) {
 int vxp_batch_synchronize(vxp_batch* bt) {
     if (!bt) return VXP_ERR_ARG;
     BK(cudaStreamSynchronize(bt->stream));
+    // every stepped world's error word and pair count in one read
+    const uint32_t k = (uint32_t)bt->order.size();
+    std::vector<uint32_t> st(2 * (size_t)k);
+    if (k && bt->d_status.p && !bt->rebuild) {
+        k_batch_status<<<(k + 127) / 128, 128, 0, bt->stream>>>(bt->d_worlds.p, k, bt->d_status.p);
+        BK(cudaGetLastError());
+        BK(cudaMemcpyAsync(st.data(), bt->d_status.p, st.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           bt->stream));
+        BK(cudaStreamSynchronize(bt->stream));
+    }
     int rc = VXP_OK;
-    for (uint32_t s = 0; s < bt->slots.size(); ++s) {
+    if (bt->rebuild) {
+        // worlds changed since the last step: the launch table may name
+        // buffers that are gone, so read each current world directly
+        for (uint32_t s = 0; s < bt->slots.size(); ++s) {
+            if (!bt->active[s] || !bt->slots[s]) continue;
+            WorldBuffers& w = *bt->slots[s];
+            std::string e;
+            const int r = w.take_error(bt->stream, e);
+            if (r != VXP_OK && rc == VXP_OK) {
+                rc = r;
+                bt->err = fmt("world %u: %s", s, e.c_str());
+            }
+        }
+        return rc;
+    }
+    for (uint32_t i = 0; i < k; ++i) {
+        const uint32_t s = bt->order[i];
         if (!bt->active[s] || !bt->slots[s]) continue;
         WorldBuffers& w = *bt->slots[s];
-        std::string e;
-        const int r = w.take_error(bt->stream, e);
-        uint32_t np = 0;
-        BK(cudaMemcpy(&np, w.n_pairs_dev.p, sizeof(np), cudaMemcpyDeviceToHost));
+        const uint32_t np = st[2 * i + 1];
         if (np > w.pair_cap - w.pair_cap / 4u) {
             if (int g = w.ensure_pairs(np + np / 2u + 1024u, bt->err)) return g;
             bt->rebuild = true;
         }
-        if (r != VXP_OK && rc == VXP_OK) {
-            rc = r;
-            bt->err = fmt("world %u: %s", s, e.c_str());
+        if (st[2 * i] != 0u) {
+            std::string e;
+            const int r = w.take_error(bt->stream, e);
+            if (r != VXP_OK && rc == VXP_OK) {
+                rc = r;
+                bt->err = fmt("world %u: %s", s, e.c_str());
+            }
         }
     }
     return rc;
@@ -1777,23 +1824,23 @@ int vxp_batch_times(vxp_batch* bt, float* total_ms, float* world_ms, uint32_t n)
 // Launch schedule: CTA size (256 or 512) and world order (0 slot order,
 // 1 longest-first by the last measured world time, else by body count).
 int vxp_batch_set_schedule(vxp_batch* bt, uint32_t threads, uint32_t order_mode) {
-    if (!bt || order_mode > 1) return VXP_ERR_ARG;
-    if (threads != 256) return bfail(bt, VXP_ERR_ARG, "a batch CTA has 256 threads");
+    if (!bt || (threads != 256 && threads != 512) || order_mode > 1) return VXP_ERR_ARG;
     bt->threads = threads;
     bt->order_mode = order_mode;
     bt->rebuild = true;
     return VXP_OK;
 }
 
-// Tries each launch order for trial_steps real steps (each world's results
-// do not depend on it) and keeps the fastest.  ms_out[2] receives the mean
-// step time of slot order and longest first; *choice the index kept.
+// Tries each schedule for trial_steps real steps (each world's results do
+// not depend on the schedule) and keeps the fastest.  ms_out[4] receives the
+// mean step time of (256, slot order), (256, longest first), (512, slot
+// order), (512, longest first); *choice the index kept.
 int vxp_batch_autotune(vxp_batch* bt, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice) {
     if (!bt || trial_steps == 0) return VXP_ERR_ARG;
     float best = 1e30f;
     uint32_t best_i = 0;
-    for (uint32_t i = 0; i < 2; ++i) {
-        if (int rc = vxp_batch_set_schedule(bt, 256u, i)) return rc;
+    for (uint32_t i = 0; i < 4; ++i) {
+        if (int rc = vxp_batch_set_schedule(bt, i < 2 ? 256u : 512u, i & 1u)) return rc;
         if (int rc = vxp_batch_step(bt, dt, 1)) return rc;  // measures world times, builds the graph
         if (int rc = vxp_batch_synchronize(bt)) return rc;
         if (int rc = vxp_batch_times(bt, nullptr, nullptr, 0)) return rc;
@@ -1810,7 +1857,7 @@ int vxp_batch_autotune(vxp_batch* bt, float dt, uint32_t trial_steps, float* ms_
         }
     }
     if (choice) *choice = best_i;
-    return vxp_batch_set_schedule(bt, 256u, best_i);
+    return vxp_batch_set_schedule(bt, best_i < 2 ? 256u : 512u, best_i & 1u);
 }
 
 }  // extern "C"

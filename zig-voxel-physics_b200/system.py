@@ -279,7 +279,7 @@ class VoxelWorldBatch:
         self._check(self.lib.vxp_batch_set_schedule(self.b, int(threads), int(order_mode)))
 
     def autotune(self, dt: float, trial_steps: int = 3) -> tuple:
-        ms = np.zeros(2, dtype=np.float32)
+        ms = np.zeros(4, dtype=np.float32)
         choice = ctypes.c_uint32(0)
         self._check(self.lib.vxp_batch_autotune(self.b, np.float32(dt), int(trial_steps), abi.ptr(ms),
                                                 ctypes.byref(choice)))
