@@ -304,6 +304,12 @@ int vxp_set_launch_mode(vxp_ctx* ctx, int mode);
  * ceil(manifolds / div) blocks (at least 2); default div 128. */
 int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div);
 
+/* Narrow-phase work split: a pair whose overlap region holds at least n
+ * voxels is probed by a whole CTA before the other pairs, which are probed one
+ * warp each (default 1024; 0: every pair by one warp).  Results do not depend
+ * on it. */
+int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n);
+
 /* Order of the solver's sweeps (ContactSolver.solve, src/solver.zig:494-561)
  * when a world is stepped by the cooperative grid (vxp_set_launch_mode).
  * 1 (default): each manifold waits only for the earlier manifolds of its own

@@ -231,3 +231,38 @@ def test_tolerance_bound_recorded(vxp):
         a, b = gb[f].astype(np.float64), rb[f].astype(np.float64)
         assert np.all(np.abs(a - b) <= 1e-5 * np.maximum(np.abs(b), 1e-3))
     g.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("heavy", [0, 1, 200])
+def test_heavy_pair_split_keeps_results(vxp, mode, heavy):
+    """Pairs probed by a whole CTA (every pair at heavy=1, those with >= 200
+    region voxels at heavy=200, none at 0) give the oracle's manifolds,
+    counters and bodies bit for bit, and so does the candidate set."""
+    sc = vxp.scenes.config1(mass_fn=O.mass_fn)
+    g = vxp.VoxelPhysicsSystem(substeps=4)
+    g.load_scene(sc)
+    g.set_launch_mode(mode)
+    g.set_heavy_pair_voxels(heavy)
+    g.set_candidate_dump(1 << 20)
+    r = O.OracleWorld(substeps=4)
+    r.load_scene(sc)
+    r.set_candidate_dump(True)
+    dt = np.float32(sc.dt)
+    key = lambda c: np.lexsort([c["b"][:, 2], c["b"][:, 1], c["b"][:, 0], c["a"][:, 2], c["a"][:, 1],
+                                c["a"][:, 0], c["pair_index"]])
+    for s in range(60):
+        pairs = r.pairs()
+        g.step(dt, pairs)
+        r.step(dt, pairs)
+        gm, rm = g.manifolds(), r.manifolds()
+        assert gm.tobytes() == rm.tobytes(), f"step {s}: manifolds differ"
+        gs, rs = g.stats(), r.stats()
+        for k in STAT_KEYS:
+            assert gs[k] == rs[k], f"step {s}: stats[{k}] gpu {gs[k]} oracle {rs[k]}"
+        gc, rc = g.candidates(), r.candidates()
+        gc, rc = gc[key(gc)], rc[key(rc)]
+        assert gc.tobytes() == rc.tobytes(), f"step {s}: candidate sets differ"
+        assert g.get_bodies().tobytes() == r.get_bodies().tobytes(), f"step {s}: bodies differ"
+    g.close()
+    r.close()

@@ -439,6 +439,7 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
     s.device_pairs = 0;
     s.margin = 0.1f;
     s.solver_flow = 1;
+    s.heavy_voxels = 1024;
     return s;
 }
 
@@ -828,6 +829,7 @@ struct vxp_ctx {
     int use_grid = -1;  // -1 auto, 0 block, 1 grid
     uint32_t solver_div = 128;
     uint32_t solver_flow = 1;
+    uint32_t heavy_voxels = 1024;
     bool record_substeps = false;
     DBuf<float> subrec;
 };
@@ -858,6 +860,7 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
     const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
     const size_t smem = grid ? grid_smem(w.cache_cap) : step_smem(kBlockThreads, w.cache_cap);
     w.cfg.flow_smem_chunks = grid ? flow_chunks(solve_smem()) : 0u;
+    w.cfg.heavy_voxels = ctx->heavy_voxels;
     if (ctx->record_substeps) {
         const size_t need = (size_t)std::max(1u, ctx->cfg.substeps) * std::max(1u, ctx->w.n_bodies) * 13u;
         if (ctx->subrec.reserve(need) != cudaSuccess) return fail(ctx, VXP_ERR_OOM, "substep record buffer");
@@ -1496,6 +1499,12 @@ int vxp_set_launch_mode(vxp_ctx* ctx, int mode) {
 int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div) {
     if (!ctx || div == 0) return VXP_ERR_ARG;
     ctx->solver_div = div;
+    return VXP_OK;
+}
+
+int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n) {
+    if (!ctx) return VXP_ERR_ARG;
+    ctx->heavy_voxels = n;
     return VXP_OK;
 }
 

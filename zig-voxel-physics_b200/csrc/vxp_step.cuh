@@ -637,7 +637,18 @@ __device__ bool phase_pairs(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
         }
         I3 rmin, rmax;
         if (overlap_region(ca, xa, qa, cb, xb, qb, &rmin, &rmax)) {
-            if (rmin.x <= rmax.x && rmin.y <= rmax.y && rmin.z <= rmax.z) fl |= PF_REGION;
+            if (rmin.x <= rmax.x && rmin.y <= rmax.y && rmin.z <= rmax.z) {
+                fl |= PF_REGION;
+                // a large region is probed by a whole CTA (listed in w.cons,
+                // which is free until phase_constraints)
+                const unsigned long long V = (unsigned long long)(rmax.x - rmin.x + 1) *
+                                             (unsigned long long)(rmax.y - rmin.y + 1) *
+                                             (unsigned long long)(rmax.z - rmin.z + 1);
+                if (w.cfg.heavy_voxels && V >= w.cfg.heavy_voxels) {
+                    fl |= PF_HEAVY;
+                    w.cons[atomicAdd(&w.ctr[C_NHEAVY], 1u)] = p;
+                }
+            }
             pi.rmin[0] = rmin.x; pi.rmin[1] = rmin.y; pi.rmin[2] = rmin.z;
             pi.rmax[0] = rmax.x; pi.rmax[1] = rmax.y; pi.rmax[2] = rmax.z;
         }
@@ -1100,6 +1111,211 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
     __syncwarp();
 }
 
+// The same narrow phase for one pair with a large overlap region, run by the
+// whole CTA: each pass covers blockDim.x consecutive voxels of the inclusive
+// z, y, x loop (one per thread).  The manifold's order-dependent reduction is
+// reproduced as in probe_pair, with a CTA-wide exclusive scan of the
+// threads' top-4 multisets in voxel order; the candidates that enter are
+// listed in that order and replayed by one thread, which rebuilds each
+// contact from its A voxel and probe alone.
+constexpr uint32_t kReplayList = 256;
+__device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cur, uint32_t p, WarpManifold& sm) {
+    __shared__ Top4 s_top[32];
+    __shared__ uint32_t s_list[kReplayList];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
+    PairInfo& pi = w.pinfo[p];
+    const uint32_t ia = pi.ia, ib = pi.ib;
+    const DBody& A = w.body[ia];
+    const DBody& B = w.body[ib];
+    const DBodyProp& prA = w.prop[ia];
+    const DBodyProp& prB = w.prop[ib];
+    ProbeCtx c;
+    c.ca = &cs.c[prA.collider];
+    c.cb = &cs.c[prB.collider];
+    c.pa = f3of(A.p);
+    c.pb = f3of(B.p);
+    c.qa = qof(A.q);
+    c.qb = qof(B.q);
+    c.qna = qof(w.qn[ia]);
+    c.qnb = qof(w.qn[ib]);
+    c.vs_a = c.ca->vs;
+    c.vs_b = c.cb->vs;
+    {
+        const float cds = c.vs_a * c.vs_a * 1.0f * 1.0f;
+        c.spec = cds + 0.02f * 0.02f + 2.0f * sqrtf(cds) * 0.02f;
+    }
+    const DCollider& ca = *c.ca;
+    const DCollider& cb = *c.cb;
+    const int32_t nx = pi.rmax[0] - pi.rmin[0] + 1, ny = pi.rmax[1] - pi.rmin[1] + 1,
+                  nz = pi.rmax[2] - pi.rmin[2] + 1;
+    const unsigned long long V = (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
+    if (tid == 0) sm.n = 0u;
+    if (wid == 0) {
+        // traffic accounting: A bricks in the region, B bricks in B's region
+        uint32_t nb = warp_count_bricks(cs, ca, I3{pi.rmin[0], pi.rmin[1], pi.rmin[2]},
+                                        I3{pi.rmax[0], pi.rmax[1], pi.rmax[2]});
+        I3 blo, bhi;
+        if (overlap_region(cb, c.pb, c.qb, ca, c.pa, c.qa, &blo, &bhi)) nb += warp_count_bricks(cs, cb, blo, bhi);
+        if (lane == 0) atomicAdd(&w.ctr[C_BRICKS], nb);
+    }
+    __syncthreads();
+    Top4 state = top4_empty();
+    uint32_t checked = 0, ncand = 0;
+    for (unsigned long long base = 0; base < V; base += blockDim.x) {
+        const unsigned long long l = base + tid;
+        uint32_t va = 0u;
+        int32_t x = 0, y = 0, z = 0;
+        if (l < V) {
+            const uint32_t li = (uint32_t)l;
+            x = pi.rmin[0] + (int32_t)(li % (uint32_t)nx);
+            y = pi.rmin[1] + (int32_t)((li / (uint32_t)nx) % (uint32_t)ny);
+            z = pi.rmin[2] + (int32_t)(li / ((uint32_t)nx * (uint32_t)ny));
+            va = voxel_at(cs, ca, x, y, z);
+        }
+        uint32_t mask = 0u;
+        Top4 t = top4_empty();
+        F3 wa{0.f, 0.f, 0.f};
+        I3 cbv{0, 0, 0};
+        const uint32_t ta = vtype(va);
+        if (ta != kEmpty) {
+            wa = transform_point_n(c.pa, c.qna, voxel_to_local(c.vs_a, x, y, z));
+            cbv = local_to_voxel(c.vs_b, inverse_transform_point(c.pb, c.qb, wa));
+            for (uint32_t k = 0; k < 27u; ++k) {
+                const I3 o = probe_offset(k);
+                const int32_t bx = cbv.x + o.x, by = cbv.y + o.y, bz = cbv.z + o.z;
+                if (!valid_coord(cb, bx, by, bz)) continue;
+                const uint32_t vb = voxel_at(cs, cb, bx, by, bz);
+                const uint32_t tb = vtype(vb);
+                if (tb == kEmpty) continue;
+                ++checked;
+                if (!type_filter(ta, tb)) continue;
+                const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, bx, by, bz));
+                const F3 diff = wb - wa;
+                const float d2 = lensq3(diff);
+                const bool pass = d2 < c.spec;
+                if (w.cfg.dump_candidates) {
+                    const uint32_t slot = atomicAdd(&w.ctr[C_DUMP_N], 1u);
+                    if (slot < w.dump_cap) {
+                        WorldDev::Cand& r = w.dump[slot];
+                        r.pair_index = p;
+                        r.a[0] = x; r.a[1] = y; r.a[2] = z;
+                        r.b[0] = bx; r.b[1] = by; r.b[2] = bz;
+                        r.passed = pass ? 1u : 0u;
+                        r.dist_sq = d2;
+                    }
+                }
+                if (pass) {
+                    mask |= 1u << k;
+                    top4_insert(t, cand_pen(c.vs_a, ta, tb, d2));
+                }
+            }
+        }
+        if (!__syncthreads_or(mask != 0u)) continue;
+        ncand += __popc(mask);
+        // CTA-wide exclusive scan of the threads' top-4 multisets
+        Top4 inc = t;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const Top4 o = top4_shfl_up(inc, d);
+            if ((int)lane >= d) inc = top4_merge(o, inc);
+        }
+        if (lane == 31) s_top[wid] = inc;
+        __syncthreads();
+        if (wid == 0) {
+            Top4 wi = lane < nwarps ? s_top[lane] : top4_empty();
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const Top4 o = top4_shfl_up(wi, d);
+                if ((int)lane >= d) wi = top4_merge(o, wi);
+            }
+            Top4 we = top4_shfl_up(wi, 1);
+            if (lane == 0) we = top4_empty();
+            if (lane < nwarps) s_top[lane] = we;
+        }
+        __syncthreads();
+        Top4 ex = top4_shfl_up(inc, 1);
+        if (lane == 0) ex = top4_empty();
+        Top4 run = top4_merge(state, top4_merge(s_top[wid], ex));
+        // candidates of this thread that enter the manifold
+        uint32_t enter = 0u;
+        for (uint32_t mm = mask; mm; mm &= mm - 1u) {
+            const uint32_t k = __ffs(mm) - 1;
+            const I3 o = probe_offset(k);
+            const int32_t bx = cbv.x + o.x, by = cbv.y + o.y, bz = cbv.z + o.z;
+            const uint32_t vb = voxel_at(cs, cb, bx, by, bz);
+            const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, bx, by, bz));
+            const float d2 = lensq3(wb - wa);
+            const float pen = cand_pen(c.vs_a, ta, vtype(vb), d2);
+            if (pen > run.v[3]) {
+                enter |= 1u << k;
+                top4_insert(run, pen);
+            }
+        }
+        // entering candidates in (voxel, probe) order, replayed by thread 0
+        uint32_t total = 0;
+        const uint32_t off = block_excl_scan((uint32_t)__popc(enter), &total);
+        for (uint32_t lo = 0; lo < total; lo += kReplayList) {
+            uint32_t e = off;
+            for (uint32_t mm = enter; mm; mm &= mm - 1u, ++e)
+                if (e >= lo && e < lo + kReplayList) s_list[e - lo] = ((uint32_t)(l - base) << 5) | (__ffs(mm) - 1);
+            __syncthreads();
+            if (tid == 0) {
+                const uint32_t cnt = min(kReplayList, total - lo);
+                for (uint32_t i = 0; i < cnt; ++i) {
+                    const uint32_t li = (uint32_t)base + (s_list[i] >> 5), k = s_list[i] & 31u;
+                    const int32_t rx = pi.rmin[0] + (int32_t)(li % (uint32_t)nx);
+                    const int32_t ry = pi.rmin[1] + (int32_t)((li / (uint32_t)nx) % (uint32_t)ny);
+                    const int32_t rz = pi.rmin[2] + (int32_t)(li / ((uint32_t)nx * (uint32_t)ny));
+                    const uint32_t rva = voxel_at(cs, ca, rx, ry, rz);
+                    const F3 rwa = transform_point_n(c.pa, c.qna, voxel_to_local(c.vs_a, rx, ry, rz));
+                    const I3 rcb = local_to_voxel(c.vs_b, inverse_transform_point(c.pb, c.qb, rwa));
+                    const I3 o = probe_offset(k);
+                    const I3 ibv{rcb.x + o.x, rcb.y + o.y, rcb.z + o.z};
+                    const uint32_t vb = voxel_at(cs, cb, ibv.x, ibv.y, ibv.z);
+                    const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
+                    ContactRec rec;
+                    generate_contact(c, rva, I3{rx, ry, rz}, rwa, vb, ibv, wb, &rec);
+                    add_contact(sm, rec);
+                }
+            }
+            __syncthreads();
+        }
+        // manifold penetration multiset -> state
+        if (tid == 0) {
+            Top4 st = top4_empty();
+            for (uint32_t i = 0; i < sm.n; ++i) top4_insert(st, sm.c[i].penetration);
+            sm.pens[0] = st.v[0];
+            sm.pens[1] = st.v[1];
+            sm.pens[2] = st.v[2];
+            sm.pens[3] = st.v[3];
+        }
+        __syncthreads();
+        state.v[0] = sm.pens[0];
+        state.v[1] = sm.pens[1];
+        state.v[2] = sm.pens[2];
+        state.v[3] = sm.pens[3];
+    }
+    checked = block_sum(checked);
+    ncand = block_sum(ncand);
+    ManifoldRec& out = w.man[cur][p];
+    if (tid == 0) {
+        pi.voxels_checked = checked;
+        pi.candidates = ncand;
+        out.a = prA.id;
+        out.b = prB.id;
+        out.n = sm.n;
+        out.friction = sqrtf(prA.friction * prB.friction);
+        out.restitution = fmaxf(prA.restitution, prB.restitution);
+        out._pad = 0u;
+    }
+    __syncthreads();
+    const uint32_t words = sm.n * (uint32_t)(sizeof(ContactRec) / 4);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(sm.c);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(out.c);
+    for (uint32_t i = tid; i < words; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+}
+
 template <class G>
 __device__ bool phase_probe(G& g, WorldDev& w, const ColliderSet& cs, uint32_t cur, WarpManifold* warp_sm,
                             const CacheSmem& csm) {
@@ -1107,13 +1323,26 @@ __device__ bool phase_probe(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
     WarpManifold& sm = warp_sm[threadIdx.x >> 5];
     // one warp replays the cache lookups, the others start detecting at once
     if (w.cfg.use_cache && g.rank() < 32u) cache_replay(w, csm);
+    // large regions first, one CTA each, then the rest one warp each
+    const uint32_t nh = *(volatile uint32_t*)&w.ctr[C_NHEAVY];
+    if (nh) {
+        __shared__ uint32_t s_h;
+        for (;;) {
+            __syncthreads();
+            if (threadIdx.x == 0) s_h = atomicAdd(&w.ctr[C_HWORK], 1u);
+            __syncthreads();
+            const uint32_t h = s_h;
+            if (h >= nh) break;
+            probe_pair_block(w, cs, cur, w.cons[h], warp_sm[0]);
+        }
+    }
     for (;;) {
         uint32_t p = 0;
         if (lane == 0) p = atomicAdd(&w.ctr[C_WORK], 1u);
         p = __shfl_sync(0xffffffffu, p, 0);
         if (p >= w.n_pairs) break;
         const uint32_t fl = w.pinfo[p].flags;
-        if ((fl & (PF_DETECT | PF_CACHE)) && (fl & PF_REGION)) probe_pair(w, cs, cur, p, sm);
+        if ((fl & (PF_DETECT | PF_CACHE)) && (fl & PF_REGION) && !(fl & PF_HEAVY)) probe_pair(w, cs, cur, p, sm);
     }
     return g.sync();
 }

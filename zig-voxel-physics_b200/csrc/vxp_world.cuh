@@ -73,6 +73,7 @@ enum : uint32_t {
     PF_DETECT = 1u << 7,    // detectVoxelCollisions runs
     PF_REGION = 1u << 8,    // overlap region non-empty
     PF_TESTED = 1u << 9,    // processPair was called
+    PF_HEAVY = 1u << 10,    // overlap region large enough to be probed by a whole CTA
 };
 
 struct PairInfo {
@@ -149,6 +150,7 @@ struct StepCfg {
     uint32_t solver_flow;     // 1: sweeps ordered by per-body event counters, 0: colour barriers
     uint32_t flow_smem_chunks;  // constraint chunks per block the launch's shared memory holds
     uint32_t record_substeps;   // 1: write every body's state after each substep to subrec
+    uint32_t heavy_voxels;      // overlap regions of at least this many voxels are probed by a CTA (0: never)
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 
@@ -180,6 +182,8 @@ enum : uint32_t {
     C_KIN_CONTACT,   // constraints touching an awake kinematic body
     C_SOLVE_GO,      // set by the narrow part of a step when its solve part may run
     C_SUBREC,        // substeps recorded in subrec by the last solve
+    C_NHEAVY,        // pairs in the CTA-probed list (w.cons during the probe)
+    C_HWORK,         // work counter over that list
     C_ERROR = 31,    // sticky error bits (not cleared per step)
     C_NCTR = 32
 };

@@ -135,6 +135,10 @@ class VoxelPhysicsSystem:
         after every colour batch.  Worlds stepped by one CTA always use 0."""
         self._check(self.lib.vxp_set_solver_mode(self.ctx, int(mode)))
 
+    def set_heavy_pair_voxels(self, n: int) -> None:
+        """Pairs with at least n overlap-region voxels are probed by a whole CTA (0: never)."""
+        self._check(self.lib.vxp_set_heavy_pair_voxels(self.ctx, int(n)))
+
     def set_substep_record(self, on: bool = True) -> None:
         self._check(self.lib.vxp_snapshot_substeps(self.ctx, 1 if on else 0))
 
