@@ -890,6 +890,59 @@ __device__ void generate_contact(const ProbeCtx& c, uint32_t va, I3 ia, F3 wa, u
     out->feature_id = feature_id(ia, ib);
 }
 
+// checkNeighborhood (narrow_phase.zig:796-857) for one A voxel: its 27
+// probes in dz, dy, dx order, clipped to B's voxel bounds first (a probe
+// outside them is skipped, isValidCoord); for each non-empty B voxel the
+// type filter, the distance test and, for a pass, the candidate's penetration
+// into the lane's top-4 and its bit (dz*9 + dy*3 + dx, offsets from -1) into
+// the mask.
+__device__ __forceinline__ int32_t clip_lo(int32_t bound, int32_t centre) {
+    const long long d = (long long)bound - (long long)centre;
+    return d > -1 ? (d > 2 ? 2 : (int32_t)d) : -1;
+}
+__device__ __forceinline__ int32_t clip_hi(int32_t bound_excl, int32_t centre) {
+    const long long d = (long long)bound_excl - 1ll - (long long)centre;
+    return d < 1 ? (d < -2 ? -2 : (int32_t)d) : 1;
+}
+__device__ __forceinline__ void probe_neighbourhood(WorldDev& w, const ColliderSet& cs, const ProbeCtx& c, uint32_t p,
+                                                    uint32_t ta, int32_t x, int32_t y, int32_t z, F3 wa, I3 cbv,
+                                                    uint32_t* mask, Top4* t, uint32_t* checked) {
+    const DCollider& cb = *c.cb;
+    const int32_t lx = clip_lo(cb.min_bound[0], cbv.x), hx = clip_hi(cb.max_bound[0], cbv.x);
+    const int32_t ly = clip_lo(cb.min_bound[1], cbv.y), hy = clip_hi(cb.max_bound[1], cbv.y);
+    const int32_t lz = clip_lo(cb.min_bound[2], cbv.z), hz = clip_hi(cb.max_bound[2], cbv.z);
+    for (int32_t dz = lz; dz <= hz; ++dz)
+        for (int32_t dy = ly; dy <= hy; ++dy)
+            for (int32_t dx = lx; dx <= hx; ++dx) {
+                const uint32_t k = (uint32_t)((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1));
+                const int32_t bx = cbv.x + dx, by = cbv.y + dy, bz = cbv.z + dz;
+                const uint32_t vb = voxel_at(cs, cb, bx, by, bz);
+                const uint32_t tb = vtype(vb);
+                if (tb == kEmpty) continue;
+                ++*checked;
+                if (!type_filter(ta, tb)) continue;
+                const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, bx, by, bz));
+                const F3 diff = wb - wa;
+                const float d2 = lensq3(diff);
+                const bool pass = d2 < c.spec;
+                if (w.cfg.dump_candidates) {
+                    const uint32_t slot = atomicAdd(&w.ctr[C_DUMP_N], 1u);
+                    if (slot < w.dump_cap) {
+                        WorldDev::Cand& r = w.dump[slot];
+                        r.pair_index = p;
+                        r.a[0] = x; r.a[1] = y; r.a[2] = z;
+                        r.b[0] = bx; r.b[1] = by; r.b[2] = bz;
+                        r.passed = pass ? 1u : 0u;
+                        r.dist_sq = d2;
+                    }
+                }
+                if (pass) {
+                    *mask |= 1u << k;
+                    top4_insert(*t, cand_pen(c.vs_a, ta, tb, d2));
+                }
+            }
+}
+
 // Per-warp shared state of phase_probe.
 struct WarpManifold {
     ContactRec c[4];
@@ -995,35 +1048,7 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
         if (ta != kEmpty) {
             wa = transform_point_n(c.pa, c.qna, voxel_to_local(c.vs_a, x, y, z));
             cbv = local_to_voxel(c.vs_b, inverse_transform_point(c.pb, c.qb, wa));
-            for (uint32_t k = 0; k < 27u; ++k) {
-                const I3 o = probe_offset(k);
-                const int32_t bx = cbv.x + o.x, by = cbv.y + o.y, bz = cbv.z + o.z;
-                if (!valid_coord(cb, bx, by, bz)) continue;
-                const uint32_t vb = voxel_at(cs, cb, bx, by, bz);
-                const uint32_t tb = vtype(vb);
-                if (tb == kEmpty) continue;
-                ++checked;
-                if (!type_filter(ta, tb)) continue;
-                const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, bx, by, bz));
-                const F3 diff = wb - wa;
-                const float d2 = lensq3(diff);
-                const bool pass = d2 < c.spec;
-                if (w.cfg.dump_candidates) {
-                    const uint32_t slot = atomicAdd(&w.ctr[C_DUMP_N], 1u);
-                    if (slot < w.dump_cap) {
-                        WorldDev::Cand& r = w.dump[slot];
-                        r.pair_index = p;
-                        r.a[0] = x; r.a[1] = y; r.a[2] = z;
-                        r.b[0] = bx; r.b[1] = by; r.b[2] = bz;
-                        r.passed = pass ? 1u : 0u;
-                        r.dist_sq = d2;
-                    }
-                }
-                if (pass) {
-                    mask |= 1u << k;
-                    top4_insert(t, cand_pen(c.vs_a, ta, tb, d2));
-                }
-            }
+            probe_neighbourhood(w, cs, c, p, ta, x, y, z, wa, cbv, &mask, &t, &checked);
         }
         if (__ballot_sync(0xffffffffu, mask != 0u) == 0u) continue;
         ncand += __popc(mask);
@@ -1180,35 +1205,7 @@ __device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cu
         if (ta != kEmpty) {
             wa = transform_point_n(c.pa, c.qna, voxel_to_local(c.vs_a, x, y, z));
             cbv = local_to_voxel(c.vs_b, inverse_transform_point(c.pb, c.qb, wa));
-            for (uint32_t k = 0; k < 27u; ++k) {
-                const I3 o = probe_offset(k);
-                const int32_t bx = cbv.x + o.x, by = cbv.y + o.y, bz = cbv.z + o.z;
-                if (!valid_coord(cb, bx, by, bz)) continue;
-                const uint32_t vb = voxel_at(cs, cb, bx, by, bz);
-                const uint32_t tb = vtype(vb);
-                if (tb == kEmpty) continue;
-                ++checked;
-                if (!type_filter(ta, tb)) continue;
-                const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, bx, by, bz));
-                const F3 diff = wb - wa;
-                const float d2 = lensq3(diff);
-                const bool pass = d2 < c.spec;
-                if (w.cfg.dump_candidates) {
-                    const uint32_t slot = atomicAdd(&w.ctr[C_DUMP_N], 1u);
-                    if (slot < w.dump_cap) {
-                        WorldDev::Cand& r = w.dump[slot];
-                        r.pair_index = p;
-                        r.a[0] = x; r.a[1] = y; r.a[2] = z;
-                        r.b[0] = bx; r.b[1] = by; r.b[2] = bz;
-                        r.passed = pass ? 1u : 0u;
-                        r.dist_sq = d2;
-                    }
-                }
-                if (pass) {
-                    mask |= 1u << k;
-                    top4_insert(t, cand_pen(c.vs_a, ta, tb, d2));
-                }
-            }
+            probe_neighbourhood(w, cs, c, p, ta, x, y, z, wa, cbv, &mask, &t, &checked);
         }
         if (!__syncthreads_or(mask != 0u)) continue;
         ncand += __popc(mask);
