@@ -50,8 +50,8 @@ SOLVER_V, SOLVER_Q = 1, 2
 # pile, keyed by (workload, kernel), from one ncu capture of the same
 # workload; re-captured when a kernel changes.
 PROFILED_TRAFFIC = {
-    ("config2_pile_4096", "k_step_grid"): (24_773_888, "profiles/k_step_grid_k_solve_grid_config2_pile.md"),
-    ("config2_pile_4096", "k_solve_grid"): (8_487_936, "profiles/k_step_grid_k_solve_grid_config2_pile.md"),
+    ("config2_pile_4096", "k_step_grid"): (25_673_472, "profiles/k_step_grid_k_solve_grid_config2_pile.md"),
+    ("config2_pile_4096", "k_solve_grid"): (8_729_088, "profiles/k_step_grid_k_solve_grid_config2_pile.md"),
 }
 
 
