@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-mode", type=int, default=-1)
+    ap.add_argument("--solver", type=int, default=-1, help="grid solver mode (-1: the library default)")
     ap.add_argument("--workload", default="pile", choices=["pile", "batched", "serving"],
                     help="pile: the 4096-body pile (the headline); batched: 256 independent worlds; "
                          "serving: Poisson-arriving jobs through the continuous-batching server")
@@ -266,6 +267,8 @@ def ours(args):
                                   max_pairs=max(65536, 16 * n_dyn), max_bodies=len(scene.bodies))
     sysm.load_scene(scene)
     sysm.set_launch_mode(args.launch_mode)
+    if args.solver >= 0:
+        sysm.set_solver_mode(args.solver)
     dt = np.float32(scene.dt)
     if args.state_in:
         sysm.set_bodies(np.load(args.state_in))

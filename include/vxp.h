@@ -312,14 +312,30 @@ int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n);
 
 /* Order of the solver's sweeps (ContactSolver.solve, src/solver.zig:494-561)
  * when a world is stepped by the cooperative grid (vxp_set_launch_mode).
- * 1 (default): each manifold waits only for the earlier manifolds of its own
+ * 2 (default where the device schedules the cluster, see vxp_cluster_size):
+ * the constraints and colouring on the grid, then the sweeps and the store on
+ * one thread-block cluster (16 CTAs, or 8) with a hardware cluster barrier
+ * after every colour batch and the bodies and constraint rows in the
+ * cluster's shared memory (in L2 when they do not fit); 1 (the default
+ * otherwise): each manifold waits only for the earlier manifolds of its own
  * two bodies (per-body event counters), so colour batches and sweeps overlap;
- * 0: a barrier after every colour batch.  Both give bit-identical results; a
- * step with a kinematic body in a constraint always uses 0, and so does every
- * world stepped by a single CTA (small worlds, batches). */
+ * 0: a software grid barrier after every colour batch.  All give
+ * bit-identical results; a step with a kinematic body in a constraint uses 0
+ * under mode 1, and every world stepped by a single CTA (small worlds,
+ * batches) sweeps with CTA barriers.  Mode 2 where no cluster can be
+ * scheduled returns VXP_ERR_STATE. */
 #define VXP_SOLVER_BARRIERS 0u
 #define VXP_SOLVER_EVENTS 1u
+#define VXP_SOLVER_CLUSTER 2u
 int vxp_set_solver_mode(vxp_ctx* ctx, uint32_t mode);
+
+/* CTAs of the cluster that mode VXP_SOLVER_CLUSTER runs on (0: none). */
+int vxp_cluster_size(vxp_ctx* ctx, uint32_t* n);
+
+/* Device time (ms) of the last step's solve part split by kernel under
+ * VXP_SOLVER_CLUSTER: [constraints and colouring (k_solve_grid), sweeps and
+ * store (k_solve_cluster)]; zeros for a step that ran otherwise. */
+int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]);
 
 /* Diagnostics: ns from the start of the last step kernel to the end of each
  * of its phases: [start, begin, pairs, cache, probe, finalize, constraints,

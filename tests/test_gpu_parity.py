@@ -26,11 +26,14 @@ def _first_diff(g, r):
     return ["raw"]
 
 
-def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, **cfg):
-    """Steps GPU and oracle together; returns the GPU system (open)."""
+def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=None, **cfg):
+    """Steps GPU and oracle together; returns the GPU system (open).
+    solver: the grid solver mode (0 grid barriers, 1 event order, 2 cluster)."""
     g = vxp.VoxelPhysicsSystem(**cfg)
     g.load_scene(scene)
     g.set_launch_mode(mode)
+    if solver is not None:
+        g.set_solver_mode(solver)
     r = O.OracleWorld(**cfg)
     r.load_scene(scene)
     dt = np.float32(scene.dt)
@@ -77,10 +80,28 @@ def test_config1_modes(vxp, cfg):
     lockstep(vxp, sc, 90, **cfg).close()
 
 
-def test_config2_pile_subset(vxp):
-    """216 boxes of the config-2 pile, 8 substeps at 1/120 s, grid launch."""
+@pytest.mark.parametrize("solver", [0, 1, 2])
+def test_config2_pile_subset(vxp, solver):
+    """216 boxes of the config-2 pile, 8 substeps at 1/120 s, grid launch,
+    each grid solver mode."""
     sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
-    lockstep(vxp, sc, 200, mode=1, check_every=10, substeps=8).close()
+    lockstep(vxp, sc, 200, mode=1, check_every=10, solver=solver, substeps=8).close()
+
+
+def test_cluster_available(vxp):
+    """The B200 schedules a cluster for the sweeps (16 CTAs, or 8)."""
+    g = vxp.VoxelPhysicsSystem()
+    assert g.cluster_size() in (8, 16)
+    g.close()
+
+
+@pytest.mark.parametrize("solver", [0, 2])
+@pytest.mark.parametrize("cfg", [dict(), dict(colouring=1), dict(velocity_iterations=2, position_iterations=4),
+                                 dict(enable_warm_starting=0, warm_starting=0)])
+def test_config1_grid_solver_modes(vxp, solver, cfg):
+    """The 64-cube scene on the grid with the barrier and cluster sweeps."""
+    sc = vxp.scenes.config1(mass_fn=O.mass_fn, seed=5)
+    lockstep(vxp, sc, 90, mode=1, solver=solver, **cfg).close()
 
 
 def test_config4_noise_subset(vxp):

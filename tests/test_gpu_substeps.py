@@ -1,7 +1,7 @@
 """Per-substep parity: every body's position, rotation and velocities after
 each substep (before the position sweeps and writeBack), device against the
 oracle, with the reference's own colouring (GraphColoring.build order) and
-with the project colouring, in both launch modes.  Bit for bit; the 1e-5
+with the project colouring, in both launch modes (and the cluster sweeps).  Bit for bit; the 1e-5
 relative bound of the float results is asserted too, for the record."""
 import numpy as np
 import pytest
@@ -11,14 +11,16 @@ import oracle_api as O
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode,solver", [(0, None), (1, None), (1, 2)])
 @pytest.mark.parametrize("colouring", [1, 0])
-def test_substep_states_match_oracle(vxp, mode, colouring):
+def test_substep_states_match_oracle(vxp, mode, solver, colouring):
     sc = vxp.scenes.config1(O.mass_fn)
     cfg = dict(substeps=4, colouring=colouring)
     g = vxp.VoxelPhysicsSystem(**cfg)
     g.load_scene(sc)
     g.set_launch_mode(mode)
+    if solver is not None:
+        g.set_solver_mode(solver)
     g.set_substep_record(True)
     r = O.OracleWorld(**cfg)
     r.load_scene(sc)

@@ -213,6 +213,8 @@ SIGNATURES = {
     "vxp_pairs_from_bodies": (_I, [_VP, _F, _VP, _U32, _PU32]),
     "vxp_last_step_ms": (_I, [_VP, _VP]),
     "vxp_last_kernel_ms": (_I, [_VP, _VP]),
+    "vxp_last_solve_split_ms": (_I, [_VP, _VP]),
+    "vxp_cluster_size": (_I, [_VP, _VP]),
     "vxp_snapshot_substeps": (_I, [_VP, _I]),
     "vxp_substeps_get": (_I, [_VP, _VP, _U32, _VP]),
     "vxp_synchronize": (_I, [_VP]),

@@ -64,11 +64,25 @@ __global__ void __launch_bounds__(512, 1) k_step_grid(const WorldDev* world, Col
     world_step_narrow(g, w, cs, wsm, csm);
 }
 __global__ void __launch_bounds__(256, 1) k_solve_grid(const WorldDev* world, GridBar* bar,
-                                                       unsigned long long timeout_ns) {
+                                                       unsigned long long timeout_ns, uint32_t part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WorldDev w = *world;
     GridGroup g{bar, &w.ctr[C_ERROR], timeout_ns, gridDim.x};
-    world_step_solve(g, w, reinterpret_cast<float*>(smem_raw), true);
+    world_step_solve(g, w, reinterpret_cast<float*>(smem_raw), true, part);
+}
+// The solver's sweeps and the store after k_solve_grid(..., SOLVE_CONSTRAINTS),
+// on one thread-block cluster (the whole grid).
+__global__ void __launch_bounds__(256, 1) k_solve_cluster(const WorldDev* world, uint32_t smem_bytes) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t ncta;
+    asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
+    WorldDev w = *world;
+    if (ncta != gridDim.x) {  // launch constants: the same verdict in every block
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&w.ctr[C_ERROR], ERR_BOUNDS);
+        return;
+    }
+    ClusterGroup g;
+    world_step_sweeps(g, w, smem_raw, smem_bytes);
 }
 
 // Pair source: world AABB of each body's collider (AABB.transform,
@@ -822,7 +836,11 @@ struct vxp_ctx {
     DBuf<uint32_t> pair_counts, pair_offsets;
     uint32_t grid_blocks = 0;
     uint32_t last_pairs = 0;
-    cudaEvent_t ev_start = nullptr, ev0 = nullptr, ev1 = nullptr, ev_count = nullptr, ev_mid = nullptr;
+    cudaEvent_t ev_start = nullptr, ev0 = nullptr, ev1 = nullptr, ev_count = nullptr, ev_mid = nullptr,
+                ev_cons = nullptr;
+    uint32_t cluster_size = 0;  // CTAs of the cluster that runs the sweeps (0: no cluster launch here)
+    uint32_t cluster_smem = 0;  // dynamic shared memory of each of its CTAs
+    bool last_cluster = false;
     bool last_grid = false;
     uint32_t* h_count = nullptr;  // pinned mirror of the device pair count
     bool count_pending = false;
@@ -853,11 +871,29 @@ int fail(vxp_ctx* c, int code, const char* f, ...) {
         if (e_ != cudaSuccess) return fail(ctx, VXP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
+// Launch configuration of k_solve_cluster: one cluster of n CTAs with smem
+// bytes of dynamic shared memory each.
+static void cluster_config(cudaLaunchConfig_t* lc, cudaLaunchAttribute* at, uint32_t n, uint32_t smem,
+                           cudaStream_t stream) {
+    lc->gridDim = dim3(n);
+    lc->blockDim = dim3(kSolveThreads);
+    lc->dynamicSmemBytes = smem;
+    lc->stream = stream;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = n;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc->attrs = at;
+    lc->numAttrs = 1;
+}
+
 // Runs the step kernel.  device_pairs: the kernel builds the pair list itself.
 int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, float margin) {
     if (int rc = ctx->cols.sync(ctx->err)) return rc;
-    WorldDev w = ctx->w.make(ctx->cfg, dt, phases, ctx->solver_div, device_pairs, margin, ctx->solver_flow);
     const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
+    const bool cluster = grid && ctx->solver_flow == VXP_SOLVER_CLUSTER && ctx->cluster_size > 0;
+    const uint32_t flow = ctx->solver_flow == VXP_SOLVER_EVENTS ? 1u : 0u;
+    WorldDev w = ctx->w.make(ctx->cfg, dt, phases, ctx->solver_div, device_pairs, margin, flow);
     const size_t smem = grid ? grid_smem(w.cache_cap) : step_smem(kBlockThreads, w.cache_cap);
     w.cfg.flow_smem_chunks = grid ? flow_chunks(solve_smem()) : 0u;
     w.cfg.heavy_voxels = ctx->heavy_voxels;
@@ -879,15 +915,24 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
         CK(cudaLaunchCooperativeKernel((const void*)k_step_grid, dim3(ctx->grid_blocks), dim3(kGridThreads), args,
                                        smem, ctx->stream));
         CK(cudaEventRecord(ctx->ev_mid, ctx->stream));
-        void* sargs[] = {(void*)&wp, (void*)&bp, (void*)&timeout};
+        uint32_t part = cluster ? SOLVE_CONSTRAINTS : SOLVE_ALL;
+        void* sargs[] = {(void*)&wp, (void*)&bp, (void*)&timeout, (void*)&part};
         CK(cudaLaunchCooperativeKernel((const void*)k_solve_grid, dim3(ctx->grid_blocks), dim3(kSolveThreads), sargs,
                                        solve_smem(), ctx->stream));
+        if (cluster) {
+            CK(cudaEventRecord(ctx->ev_cons, ctx->stream));
+            cudaLaunchConfig_t lc = {};
+            cudaLaunchAttribute at[1];
+            cluster_config(&lc, at, ctx->cluster_size, ctx->cluster_smem, ctx->stream);
+            CK(cudaLaunchKernelEx(&lc, k_solve_cluster, wp, ctx->cluster_smem));
+        }
     } else {
         k_step_block<kBlockThreads><<<1, kBlockThreads, smem, ctx->stream>>>(ctx->d_world.p, cs);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->last_grid = grid;
+    ctx->last_cluster = cluster;
     if (device_pairs && !ctx->count_pending) {
         CK(cudaMemcpyAsync(ctx->h_count, ctx->w.n_pairs_dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                            ctx->stream));
@@ -1141,6 +1186,7 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     if (cudaStreamCreate(&ctx->stream) != cudaSuccess) return bail(VXP_ERR_CUDA);
     if (cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev0) != cudaSuccess ||
         cudaEventCreate(&ctx->ev1) != cudaSuccess || cudaEventCreate(&ctx->ev_mid) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev_cons) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_count, cudaEventDisableTiming) != cudaSuccess)
         return bail(VXP_ERR_CUDA);
     if (cudaMallocHost(&ctx->h_count, sizeof(uint32_t)) != cudaSuccess) return bail(VXP_ERR_OOM);
@@ -1157,6 +1203,29 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
         per_sm_solve < 1)
         return bail(VXP_ERR_CUDA);
     ctx->grid_blocks = (uint32_t)smc;  // one CTA per SM for both grid kernels
+    // the largest cluster the device schedules for the sweeps: 16 CTAs (a
+    // non-portable size), else 8; none leaves the grid solver in charge
+    // each of its CTAs takes all the shared memory one block may have (the
+    // state of the sweeps lives there)
+    int optin = 0;
+    cudaFuncAttributes fa = {};
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) == cudaSuccess &&
+        cudaFuncGetAttributes(&fa, k_solve_cluster) == cudaSuccess && optin > (int)fa.sharedSizeBytes)
+        ctx->cluster_smem = (uint32_t)(optin - (int)fa.sharedSizeBytes);
+    cudaFuncSetAttribute(k_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(k_solve_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->cluster_smem);
+    for (uint32_t n : {16u, 8u}) {
+        cudaLaunchConfig_t lc = {};
+        cudaLaunchAttribute at[1];
+        cluster_config(&lc, at, n, ctx->cluster_smem, ctx->stream);
+        int active = 0;
+        if (cudaOccupancyMaxActiveClusters(&active, k_solve_cluster, &lc) == cudaSuccess && active >= 1) {
+            ctx->cluster_size = n;
+            break;
+        }
+    }
+    cudaGetLastError();  // a refused size is not an error of this context
+    ctx->solver_flow = ctx->cluster_size ? VXP_SOLVER_CLUSTER : VXP_SOLVER_EVENTS;
     if (ctx->w.init(cache_cap, ctx->grid_blocks, ctx->err)) return bail(VXP_ERR_OOM);
     if (ctx->d_world.reserve(1) != cudaSuccess || ctx->bar.reserve(2) != cudaSuccess) return bail(VXP_ERR_OOM);
     if (ctx->w.ensure_pairs(std::max<uint32_t>(cfg->max_pairs, 1024), ctx->err)) return bail(VXP_ERR_OOM);
@@ -1173,6 +1242,7 @@ void vxp_destroy(vxp_ctx* ctx) {
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ev_mid) cudaEventDestroy(ctx->ev_mid);
+    if (ctx->ev_cons) cudaEventDestroy(ctx->ev_cons);
     if (ctx->ev_count) cudaEventDestroy(ctx->ev_count);
     if (ctx->h_count) cudaFreeHost(ctx->h_count);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1485,6 +1555,25 @@ int vxp_last_kernel_ms(vxp_ctx* ctx, float out[2]) {
     return VXP_OK;
 }
 
+int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]) {
+    if (!ctx || !out) return VXP_ERR_ARG;
+    CK(cudaEventSynchronize(ctx->ev1));
+    if (ctx->last_cluster) {
+        CK(cudaEventElapsedTime(&out[0], ctx->ev_mid, ctx->ev_cons));
+        CK(cudaEventElapsedTime(&out[1], ctx->ev_cons, ctx->ev1));
+    } else {
+        out[0] = 0.0f;
+        out[1] = 0.0f;
+    }
+    return VXP_OK;
+}
+
+int vxp_cluster_size(vxp_ctx* ctx, uint32_t* n) {
+    if (!ctx || !n) return VXP_ERR_ARG;
+    *n = ctx->cluster_size;
+    return VXP_OK;
+}
+
 int vxp_synchronize(vxp_ctx* ctx) {
     if (!ctx) return VXP_ERR_ARG;
     return check_device_error(ctx);
@@ -1509,7 +1598,8 @@ int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n) {
 }
 
 int vxp_set_solver_mode(vxp_ctx* ctx, uint32_t mode) {
-    if (!ctx || mode > 1u) return VXP_ERR_ARG;
+    if (!ctx || mode > VXP_SOLVER_CLUSTER) return VXP_ERR_ARG;
+    if (mode == VXP_SOLVER_CLUSTER && ctx->cluster_size == 0) return VXP_ERR_STATE;
     ctx->solver_flow = mode;
     return VXP_OK;
 }

@@ -107,6 +107,28 @@ struct GridGroup {
     }
 };
 
+// The CTAs of one thread-block cluster (the grid is exactly one cluster).
+// sync() is the hardware cluster barrier (release / acquire at cluster scope,
+// about 0.2 us for 16 CTAs against about 0.8 us for one flag handed between
+// two SMs through L2).  That barrier cannot time out, so only code whose
+// every block passes the same sequence of sync() calls runs on this group:
+// the solver's colour sweeps and the store, whose barrier count depends only
+// on values every block reads before the first barrier (see
+// world_step_sweeps).  sync() never fails.
+struct ClusterGroup {
+    static constexpr bool kEventSweeps = false;
+    __device__ uint32_t rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+    __device__ uint32_t size() const { return gridDim.x * blockDim.x; }
+    __device__ uint32_t block() const { return blockIdx.x; }
+    __device__ uint32_t nblocks() const { return gridDim.x; }
+    __device__ bool member() const { return true; }
+    __device__ ClusterGroup subgroup(uint32_t) const { return *this; }
+    __device__ bool sync() {
+        asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+        return true;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Block-level primitives (blockDim.x <= 1024, multiple of 32)
 // ---------------------------------------------------------------------------
@@ -1868,15 +1890,17 @@ __device__ __forceinline__ void st3(const CPV& v, uint32_t f, uint32_t s, F3 x) 
 
 // prepareConstraints for one point (solver.zig:608-699), from the two
 // bodies' state after applyGravity.
-__device__ void prepare_point_s(const SolveFlags sf, const CPV v, float restitution, uint32_t i, const Soft& soft,
-                                float hinv, const BV& a, Qt qa, const BV& b, Qt qb) {
-    const F3 n = ld3(v, CP_NX, i);
-    const F3 wa = qrotate(qa, ld3(v, CP_LAX, i)) + a.p;
-    const F3 wb = qrotate(qb, ld3(v, CP_LBX, i)) + b.p;
+// vin: the point's inputs (normal, local anchors, base separation); v: where
+// its velocity-sweep fields go (the same rows, or a copy in shared memory).
+__device__ void prepare_point_s(const SolveFlags sf, const CPV vin, const CPV v, float restitution, uint32_t i,
+                                const Soft& soft, float hinv, const BV& a, Qt qa, const BV& b, Qt qb) {
+    const F3 n = ld3(vin, CP_NX, i);
+    const F3 wa = qrotate(qa, ld3(vin, CP_LAX, i)) + a.p;
+    const F3 wb = qrotate(qb, ld3(vin, CP_LBX, i)) + b.p;
     const F3 ra = wa - a.p, rb = wb - b.p;
     const F3 pt = (wa + wb) * 0.5f;
     const F3 ad = wb - wa;
-    const float sep = cpr(v, CP_BASE, i) + dot3(ad, n);
+    const float sep = cpr(vin, CP_BASE, i) + dot3(ad, n);
     const F3 rna = cross3(ra, n), rnb = cross3(rb, n);
     float k = a.im + b.im;
     k += dot3(rna, mat3_mul_vec(a.I, rna));
@@ -1914,7 +1938,8 @@ __device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft&
     const uint4 cmv = w.cm[pos];
     const BV a = load_bv(w, cmv.x), b = load_bv(w, cmv.y);
     const Qt qa = qof(w.body[cmv.x].q), qb = qof(w.body[cmv.y].q);
-    prepare_point_s(solve_flags(w.cfg), cpv_global(w, pos), w.cfr[pos].y, i, soft, hinv, a, qa, b, qb);
+    const CPV v = cpv_global(w, pos);
+    prepare_point_s(solve_flags(w.cfg), v, v, w.cfr[pos].y, i, soft, hinv, a, qa, b, qb);
 }
 
 // warmStart for one manifold (solver.zig:702-729).
@@ -2441,7 +2466,7 @@ __device__ __noinline__ void flow_prepare(const FlowCtx fc, uint32_t s, uint32_t
     const BV sa = bv_of(SA, wa), sb = bv_of(SB, wb);
     const float rest = fc.cfr[pos].y;
     for (uint32_t i = 0; i < cmv.z; ++i)
-        prepare_point_s(fc.sf, v, rest, i, fc.soft, fc.hinv, sa, qof(SA.q), sb, qof(SB.q));
+        prepare_point_s(fc.sf, v, v, rest, i, fc.soft, fc.hinv, sa, qof(SA.q), sb, qof(SB.q));
 }
 
 // One manifold in one sweep, once its bodies are ready.
@@ -2683,6 +2708,273 @@ __device__ bool phase_solve_flow(G& g, WorldDev& w, float* fsm, uint32_t M, uint
 }
 
 // ---------------------------------------------------------------------------
+// Phase: solve on one thread-block cluster, state in shared memory
+// ---------------------------------------------------------------------------
+// ContactSolver.solve with a barrier after every colour batch, as in
+// phase_solve, with the state the sweeps pass from SM to SM held in the
+// cluster's shared memory instead of L2: body i lives in CTA i % C (slot
+// i / C) and is read and written by the other CTAs through distributed
+// shared memory; the manifolds of each colour are dealt round-robin to the
+// CTAs (position lo + k + C j to CTA k), and each CTA prepares and solves its
+// own manifolds with their velocity-sweep fields (CP_NVEL per point) in its
+// shared memory.  The position sweeps read the fields that do not change
+// during the solve from the packed rows.  Every operation and its order per
+// body is that of phase_solve, so the results are bit-identical.
+//
+// Returns false, before any barrier and in every block alike, when the state
+// does not fit the shared memory given (smem_bytes); the caller then runs
+// phase_solve.
+template <class T>
+__device__ __forceinline__ T* cluster_map(T* p, uint32_t rank) {
+    unsigned long long r;
+    asm("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(p), "r"(rank));
+    return reinterpret_cast<T*>(r);
+}
+
+struct ClusterSolveSmem {
+    DBody* body;     // bcap records
+    uint4* man;      // per local slot: body a, body b, points, flags
+    float2* fr;      // per local slot: friction, restitution
+    float* row;      // CP_NVEL x 4 x scap floats, field-major
+    uint32_t* pos;   // per local slot: packed position
+    uint32_t* base;  // per colour: first local slot of this CTA; [ncol]: its slot count
+    uint32_t bcap, scap;
+};
+enum : uint32_t { CM_WA = 1u, CM_WB = 2u, CM_STATIC = 4u, CM_BAD = 8u };
+
+// Bytes of the layout for bcap bodies and scap manifold slots.
+__device__ __forceinline__ size_t cluster_smem_bytes(uint32_t bcap, uint32_t scap, uint32_t ncol) {
+    return (size_t)bcap * sizeof(DBody) + (size_t)scap * (sizeof(uint4) + sizeof(float2) + sizeof(uint32_t) +
+                                                          CP_NVEL * 4u * sizeof(float)) +
+           (size_t)(ncol + 1u) * sizeof(uint32_t);
+}
+
+__device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, uint32_t ncol, unsigned char* smem,
+                                    uint32_t smem_bytes) {
+    const StepCfg& cf = w.cfg;
+    const uint32_t C = g.nblocks(), k = g.block(), t = threadIdx.x, T = blockDim.x;
+    const uint32_t N = w.n_bodies;
+    if (ncol > 256u || M > w.pair_cap) return false;
+    // CTA 0 holds the most slots: sum over colours of ceil(n_c / C)
+    uint32_t need = 0;
+    for (uint32_t c = 0; c < ncol; ++c) {
+        const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
+        if (hi < lo || hi > M) return false;
+        need += (hi - lo + C - 1u) / C;
+    }
+    ClusterSolveSmem sm;
+    sm.bcap = (N + C - 1u) / C;
+    sm.scap = max(need, 1u);
+    if (cluster_smem_bytes(sm.bcap, sm.scap, ncol) > smem_bytes) return false;
+    {
+        unsigned char* p = smem;
+        sm.body = reinterpret_cast<DBody*>(p);
+        p += (size_t)sm.bcap * sizeof(DBody);
+        sm.man = reinterpret_cast<uint4*>(p);
+        p += (size_t)sm.scap * sizeof(uint4);
+        sm.fr = reinterpret_cast<float2*>(p);
+        p += (size_t)sm.scap * sizeof(float2);
+        sm.row = reinterpret_cast<float*>(p);
+        p += (size_t)sm.scap * CP_NVEL * 4u * sizeof(float);
+        sm.pos = reinterpret_cast<uint32_t*>(p);
+        p += (size_t)sm.scap * sizeof(uint32_t);
+        sm.base = reinterpret_cast<uint32_t*>(p);
+    }
+    // this CTA's first slot per colour
+    if (t == 0) {
+        uint32_t run = 0;
+        for (uint32_t c = 0; c < ncol; ++c) {
+            sm.base[c] = run;
+            const uint32_t n = w.colour_cnt[c + 1u] - w.colour_cnt[c];
+            run += n > k ? (n - 1u - k) / C + 1u : 0u;
+        }
+        sm.base[ncol] = run;
+    }
+    // this CTA's bodies
+    for (uint32_t s = t; s < sm.bcap; s += T) {
+        const uint32_t i = s * C + k;
+        if (i < N) sm.body[s] = w.body[i];
+    }
+    __syncthreads();
+    // this CTA's manifolds: bodies, flags, friction, normals and impulses
+    for (uint32_t c = 0; c < ncol; ++c) {
+        const uint32_t lo = w.colour_cnt[c], b0 = sm.base[c], cnt = sm.base[c + 1u] - b0;
+        for (uint32_t j = t; j < cnt; j += T) {
+            const uint32_t slot = b0 + j, pos = lo + k + C * j;
+            uint4 mv = w.cm[pos];
+            uint32_t fl = 0u;
+            if (mv.x >= N || mv.y >= N || mv.z > 4u) {
+                atomicOr(&w.ctr[C_ERROR], ERR_BOUNDS);
+                mv = make_uint4(0u, 0u, 0u, CM_BAD);
+            } else {
+                const DBodyProp pa = w.prop[mv.x], pb = w.prop[mv.y];
+                fl = (writable(pa) ? CM_WA : 0u) | (writable(pb) ? CM_WB : 0u) |
+                     (pa.type == 0u && pb.type == 0u ? CM_STATIC : 0u);
+                mv.w = fl;
+            }
+            sm.man[slot] = mv;
+            sm.fr[slot] = w.cfr[pos];
+            sm.pos[slot] = pos;
+            const CPV vg = cpv_global(w, pos), vs{sm.row + slot, sm.scap};
+            for (uint32_t i = 0; i < mv.z; ++i) {
+                st3(vs, CP_NX, i, ld3(vg, CP_NX, i));
+                cpr(vs, CP_NI, i) = cpr(vg, CP_NI, i);
+                cpr(vs, CP_TI0, i) = cpr(vg, CP_TI0, i);
+                cpr(vs, CP_TI1, i) = cpr(vg, CP_TI1, i);
+            }
+        }
+    }
+    g.sync();  // every block's bodies are in place (and every block has started)
+    const SolveFlags sf = solve_flags(cf);
+    const float h = cf.dt / (float)cf.substeps;
+    const Soft soft = soft_params(cf.hertz, cf.damping_ratio, h);
+    const float hinv = h > kEpsilon ? 1.0f / h : 0.0f;
+    const Soft hard{0.f, 1.f, 1.f};
+    const F3 grav{cf.gravity[0], cf.gravity[1], cf.gravity[2]};
+    const bool has = M > 0u;
+    const uint32_t nslot = sm.base[ncol];
+    auto body_of = [&](uint32_t i) { return cluster_map(sm.body + i / C, i % C); };
+    // one manifold of a velocity-type sweep: 0 warm start, 1 velocity, 2 relax
+    auto vel_item = [&](uint32_t slot, uint32_t kind) {
+        const uint4 mv = sm.man[slot];
+        if (mv.w & CM_BAD) return;
+        if (kind != 0u && mv.z == 0u) return;
+        DBody* pa = body_of(mv.x);
+        DBody* pb = body_of(mv.y);
+        const DBody A = *pa, B = *pb;
+        BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
+        const CPV v{sm.row + slot, sm.scap};
+        if (kind == 0u)
+            warm_points(v, mv.z, cf.warm_scale, a, b);
+        else
+            velocity_points_near(sf.friction, v, mv.z, sm.fr[slot].x, kind == 1u ? soft : hard, kind == 1u, a, b);
+        if (a.wr) {
+            pa->v = make_float4(a.v.x, a.v.y, a.v.z, 0.f);
+            pa->w = make_float4(a.w.x, a.w.y, a.w.z, 0.f);
+        }
+        if (b.wr) {
+            pb->v = make_float4(b.v.x, b.v.y, b.v.z, 0.f);
+            pb->w = make_float4(b.w.x, b.w.y, b.w.z, 0.f);
+        }
+    };
+    auto sweep = [&](uint32_t kind) {
+        for (uint32_t c = 0; c < ncol; ++c) {
+            const uint32_t b0 = sm.base[c], cnt = sm.base[c + 1u] - b0;
+            for (uint32_t j = t; j < cnt; j += T) vel_item(b0 + j, kind);
+            g.sync();
+        }
+    };
+    for (uint32_t s = 0; s < cf.substeps; ++s) {
+        // applyGravity (solver.zig:564-605)
+        for (uint32_t q = t; q < sm.bcap; q += T) {
+            const uint32_t i = q * C + k;
+            if (i >= N) break;
+            const DBodyProp& pr = w.prop[i];
+            if (!(pr.type == 2u && pr.sleeping == 0u)) continue;
+            DBody& b = sm.body[q];
+            float4 v = b.v, av = b.w;
+            body_gravity(v, av, pr, grav, h);
+            b.v = v;
+            b.w = av;
+        }
+        g.sync();
+        if (has) {
+            // prepareConstraints: one thread per (slot, point)
+            for (uint32_t it = t; it < 4u * nslot; it += T) {
+                const uint32_t slot = it >> 2, i = it & 3u;
+                const uint4 mv = sm.man[slot];
+                if (i >= mv.z || (mv.w & CM_BAD)) continue;
+                const DBody A = *body_of(mv.x), B = *body_of(mv.y);
+                const BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
+                prepare_point_s(sf, cpv_global(w, sm.pos[slot]), CPV{sm.row + slot, sm.scap}, sm.fr[slot].y, i, soft,
+                                hinv, a, qof(A.q), b, qof(B.q));
+            }
+            g.sync();
+            if (cf.warm_starting && s == 0u) sweep(0u);
+            for (uint32_t vi = 0; vi < cf.vel_iters; ++vi) sweep(1u);
+        }
+        // integratePositions (solver.zig:841-845, 341-356)
+        for (uint32_t q = t; q < sm.bcap; q += T) {
+            const uint32_t i = q * C + k;
+            if (i >= N) break;
+            const DBodyProp& pr = w.prop[i];
+            if (pr.type == 0u || pr.sleeping) continue;
+            DBody b = sm.body[q];
+            body_integrate(b, pr, h, cf.disable_rotation != 0u);
+            sm.body[q] = b;
+        }
+        g.sync();
+        if (has) sweep(2u);
+        // test hook: every body's state after this substep
+        if (cf.record_substeps && w.subrec) {
+            for (uint32_t q = t; q < sm.bcap; q += T) {
+                const uint32_t i = q * C + k;
+                if (i >= N) break;
+                const DBody b = sm.body[q];
+                float* r = w.subrec + ((size_t)s * N + i) * 13u;
+                r[0] = b.p.x; r[1] = b.p.y; r[2] = b.p.z;
+                r[3] = b.q.x; r[4] = b.q.y; r[5] = b.q.z; r[6] = b.q.w;
+                r[7] = b.v.x; r[8] = b.v.y; r[9] = b.v.z;
+                r[10] = b.w.x; r[11] = b.w.y; r[12] = b.w.z;
+            }
+            if (g.rank() == 0) w.ctr[C_SUBREC] = s + 1u;
+        }
+    }
+    if (has) {
+        for (uint32_t it = 0; it < cf.pos_iters; ++it) {
+            float mn = 0.0f, mx = -__int_as_float(0x7f800000);
+            for (uint32_t c = 0; c < ncol; ++c) {
+                const uint32_t b0 = sm.base[c], cnt = sm.base[c + 1u] - b0;
+                for (uint32_t j = t; j < cnt; j += T) {
+                    const uint32_t slot = b0 + j;
+                    const uint4 mv = sm.man[slot];
+                    if (mv.w & (CM_BAD | CM_STATIC)) continue;
+                    DBody* pa = body_of(mv.x);
+                    DBody* pb = body_of(mv.y);
+                    const DBody A = *pa, B = *pb;
+                    PB a = pb_of(A.p, A.q, A.i0, A.i1, A.i2, (mv.w & CM_WA) != 0u);
+                    PB b = pb_of(B.p, B.q, B.i0, B.i1, B.i2, (mv.w & CM_WB) != 0u);
+                    position_points(sf, cpv_global(w, sm.pos[slot]), mv.z, a, b, &mn, &mx);
+                    if (a.wr) {
+                        pa->p = make_float4(a.x.x, a.x.y, a.x.z, a.im);
+                        pa->q = f4of(a.q);
+                    }
+                    if (b.wr) {
+                        pb->p = make_float4(b.x.x, b.x.y, b.x.z, b.im);
+                        pb->q = f4of(b.q);
+                    }
+                }
+                g.sync();
+            }
+            bool brk = false;
+            pos_sweep_end(g, w, it, mn, mx, &brk);
+            if (brk) break;
+        }
+    }
+    g.sync();
+    // bodies back to the world, impulses and masses back to the packed rows
+    // (storeImpulses reads them)
+    for (uint32_t q = t; q < sm.bcap; q += T) {
+        const uint32_t i = q * C + k;
+        if (i >= N) break;
+        if (w.prop[i].type != 0u) w.body[i] = sm.body[q];
+    }
+    for (uint32_t slot = t; slot < nslot; slot += T) {
+        const uint4 mv = sm.man[slot];
+        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + slot, sm.scap};
+        for (uint32_t i = 0; i < mv.z; ++i) {
+            cpr(vg, CP_NM, i) = cpr(vs, CP_NM, i);
+            cpr(vg, CP_TM0, i) = cpr(vs, CP_TM0, i);
+            cpr(vg, CP_TM1, i) = cpr(vs, CP_TM1, i);
+            cpr(vg, CP_NI, i) = cpr(vs, CP_NI, i);
+            cpr(vg, CP_TI0, i) = cpr(vs, CP_TI0, i);
+            cpr(vg, CP_TI1, i) = cpr(vs, CP_TI1, i);
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Phase: store (writeBack, storeImpulses, updateSleepStates)
 // ---------------------------------------------------------------------------
 template <class G>
@@ -2812,11 +3104,18 @@ __device__ bool world_step_narrow(G& g, WorldDev& w, const ColliderSet& cs, Warp
     return g.sync();
 }
 
+// How much of the solve part one launch runs.
+enum : uint32_t {
+    SOLVE_ALL = 0,          // constraints, colouring, sweeps, store
+    SOLVE_CONSTRAINTS = 1,  // constraints and colouring; world_step_sweeps runs the rest
+};
+
 // The solve part of one step: constraints, colouring, ContactSolver.solve,
 // store and sleep.  check_go: read the narrow part's verdict from C_SOLVE_GO
-// (the parts run as two kernels).
+// (the parts run as two kernels).  part SOLVE_CONSTRAINTS stops after the
+// colouring and leaves M, ncol and C_SOLVE_GO = 2 for world_step_sweeps.
 template <class G>
-__device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go) {
+__device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go, uint32_t part = SOLVE_ALL) {
     const uint32_t ph = w.cfg.phases;
     if (!(ph & PH_SOLVE) || w.n_bodies == 0u) return;
     if (check_go && *(volatile uint32_t*)&w.ctr[C_SOLVE_GO] == 0u) return;
@@ -2836,6 +3135,15 @@ __device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go) {
     uint32_t M = 0, ncol = 0;
     if (!phase_constraints(s, w, cur, &M, &ncol)) return;
     stamp(s, w, TS_CONSTRAINTS);
+    if (part == SOLVE_CONSTRAINTS) {
+        if (s.rank() == 0) {
+            w.ctr[C_CONS_M] = M;
+            w.ctr[C_CONS_NCOL] = ncol;
+            __threadfence();
+            w.ctr[C_SOLVE_GO] = 2u;
+        }
+        return;
+    }
     const bool solved = w.cfg.dt > 0.0f && w.n_bodies > 0u;
     // event-ordered sweeps unless a kinematic body (moved every substep,
     // written by nobody) sits in a constraint
@@ -2856,6 +3164,34 @@ __device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go) {
     stamp(s, w, TS_SOLVE);
     if (!phase_store(s, w, cur, M, solved)) return;
     stamp(s, w, TS_END);
+}
+
+// The rest of the solve part after world_step_solve(..., SOLVE_CONSTRAINTS):
+// ContactSolver.solve with a barrier after every colour batch (phase_solve),
+// then store and sleep, on one thread-block cluster.  Every block reads the
+// go flag, M and ncol (written by the previous kernel) before its first
+// barrier and passes the same barriers: their number follows from those
+// values, the configuration and the position sweeps' early-break test, which
+// every block reads from a slot that no block writes again before the next
+// barrier.
+__device__ __forceinline__ void world_step_sweeps(ClusterGroup& g, WorldDev& w, unsigned char* smem,
+                                                  uint32_t smem_bytes) {
+    const uint32_t ph = w.cfg.phases;
+    if (!(ph & PH_SOLVE) || w.n_bodies == 0u) return;
+    if (*(volatile uint32_t*)&w.ctr[C_SOLVE_GO] != 2u) return;
+    w.n_pairs = *(volatile uint32_t*)w.n_pairs_dev;
+    const uint32_t cur = *(volatile uint32_t*)&w.frame[0] & 1u;
+    const uint32_t M = *(volatile uint32_t*)&w.ctr[C_CONS_M];
+    const uint32_t ncol = *(volatile uint32_t*)&w.ctr[C_CONS_NCOL];
+    // the position sweeps' min-separation slots at this group's offset
+    if (g.rank() < 16u) w.scan[g.nblocks() + 4u + g.rank()] = 0u;
+    g.sync();
+    const bool solved = w.cfg.dt > 0.0f;
+    if (solved && !phase_solve_cluster(g, w, M, ncol, smem, smem_bytes)) phase_solve(g, w, M, ncol);
+    g.sync();
+    stamp(g, w, TS_SOLVE);
+    phase_store(g, w, cur, M, solved);
+    stamp(g, w, TS_END);
 }
 
 // One whole step (VoxelPhysicsSystem.step with the pairs given) in one

@@ -131,9 +131,18 @@ class VoxelPhysicsSystem:
 
     # -------------------------------------------------------------- outputs
     def set_solver_mode(self, mode: int) -> None:
-        """Grid-stepped worlds: 1 event-ordered sweeps (default), 0 a barrier
-        after every colour batch.  Worlds stepped by one CTA always use 0."""
+        """Grid-stepped worlds: 2 sweeps on one thread-block cluster with a
+        cluster barrier after every colour batch and the state in shared
+        memory (the default where cluster_size() > 0), 1 event-ordered sweeps
+        (the default otherwise), 0 a grid barrier after every colour batch.
+        Worlds stepped by one CTA use CTA barriers."""
         self._check(self.lib.vxp_set_solver_mode(self.ctx, int(mode)))
+
+    def cluster_size(self) -> int:
+        """CTAs of the cluster that solver mode 2 runs on (0: not available)."""
+        n = ctypes.c_uint32(0)
+        self._check(self.lib.vxp_cluster_size(self.ctx, ctypes.byref(n)))
+        return int(n.value)
 
     def set_heavy_pair_voxels(self, n: int) -> None:
         """Pairs with at least n overlap-region voxels are probed by a whole CTA (0: never)."""
