@@ -289,7 +289,7 @@ def ours(args):
         pg.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    step_ms, kern_ms, pair_ms, stats, part_ms = [], [], [], [], []
+    step_ms, kern_ms, pair_ms, stats, part_ms, split_ms = [], [], [], [], [], []
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -302,6 +302,9 @@ def ours(args):
         parts = np.zeros(2, dtype=np.float32)
         sysm._check(sysm.lib.vxp_last_kernel_ms(sysm.ctx, abi.ptr(parts)))
         part_ms.append((float(parts[0]), float(parts[1])))
+        split = np.zeros(2, dtype=np.float32)
+        sysm._check(sysm.lib.vxp_last_solve_split_ms(sysm.ctx, abi.ptr(split)))
+        split_ms.append((float(split[0]), float(split[1])))
         stats.append(sysm.stats())
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -315,18 +318,32 @@ def ours(args):
     nb = [sum(alg_bytes(s, 8, n_dyn_awake, n_nonstatic)) for s in stats]
     peak, peak_kind = peaks()
     achieved = sum(nb) / (sum(kern_ms) / 1e3) / 1e9
-    # per kernel of the step: narrow part (k_step_grid) and solve part
-    # (k_solve_grid), each its algorithmic bytes over its own event time
+    # per kernel of the step, each its algorithmic bytes over its own event
+    # time: narrow part (k_step_grid), then the solve part, one kernel
+    # (k_solve_grid) or, with the sweeps on a cluster, the constraint table
+    # and colouring (k_solve_grid: no per-unit byte count, time only) and the
+    # sweeps and store (k_solve_cluster: the solver's bytes)
     nb_parts = [alg_bytes(s, 8, n_dyn_awake, n_nonstatic) for s in stats]
     grid = n_dyn >= 512
+    cluster = grid and all(x[1] > 0.0 for x in split_ms)
     kernels = {}
     if grid:
-        for j, name in ((0, "k_step_grid"), (1, "k_solve_grid")):
-            t = sum(x[j] for x in part_ms) / 1e3
-            b = sum(x[j] for x in nb_parts)
-            kernels[name] = {"ms_mean": 1e3 * t / len(part_ms), "alg_bytes_per_launch": b / len(nb_parts),
-                             "achieved": b / t / 1e9, "frac": b / t / 1e9 / peak}
-        dominant = max(kernels, key=lambda k: kernels[k]["ms_mean"])
+        names = [("k_step_grid", [x[0] for x in part_ms], [x[0] for x in nb_parts])]
+        if cluster:
+            names += [("k_solve_grid", [x[0] for x in split_ms], None),
+                      ("k_solve_cluster", [x[1] for x in split_ms], [x[1] for x in nb_parts])]
+        else:
+            names += [("k_solve_grid", [x[1] for x in part_ms], [x[1] for x in nb_parts])]
+        for name, tl, bl in names:
+            t = sum(tl) / 1e3
+            kernels[name] = {"ms_mean": 1e3 * t / len(tl)}
+            if bl is None:
+                kernels[name].update({"alg_bytes_per_launch": None, "achieved": None, "frac": None})
+            else:
+                b = sum(bl)
+                kernels[name].update({"alg_bytes_per_launch": b / len(bl), "achieved": b / t / 1e9,
+                                      "frac": b / t / 1e9 / peak})
+        dominant = max((k for k in kernels if kernels[k]["achieved"] is not None), key=lambda k: kernels[k]["ms_mean"])
     else:
         dominant = "k_step_block"
         kernels[dominant] = {"ms_mean": statistics.mean(kern_ms), "alg_bytes_per_launch": statistics.mean(nb),
@@ -392,7 +409,7 @@ def ours(args):
             "e2e": {"value": e2e_value, "unit": "body-substeps/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
                     "d2h_bytes_per_step": d2h // max(1, args.steps)},
             "clocks": clk,
-            "gpu_launches": args.steps * (2 if grid else 1),
+            "gpu_launches": args.steps * ((3 if cluster else 2) if grid else 1),
         }
         print(json.dumps(line), flush=True)
     if pg:

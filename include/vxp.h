@@ -332,6 +332,12 @@ int vxp_set_solver_mode(vxp_ctx* ctx, uint32_t mode);
 /* CTAs of the cluster that mode VXP_SOLVER_CLUSTER runs on (0: none). */
 int vxp_cluster_size(vxp_ctx* ctx, uint32_t* n);
 
+/* Shared memory (bytes per CTA) that the cluster's sweeps may hold their state
+ * in: the bodies and the velocity-sweep fields of the constraint rows.  A step
+ * whose state does not fit sweeps with that state in L2 instead (same
+ * results).  Default: all a block can have; 0: always in L2. */
+int vxp_set_cluster_shared_bytes(vxp_ctx* ctx, uint32_t bytes);
+
 /* Device time (ms) of the last step's solve part split by kernel under
  * VXP_SOLVER_CLUSTER: [constraints and colouring (k_solve_grid), sweeps and
  * store (k_solve_cluster)]; zeros for a step that ran otherwise. */

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-@pytest.mark.parametrize("mode,solver", [(0, None), (1, None), (1, 2)])
+@pytest.mark.parametrize("mode,solver", [(0, None), (1, 1), (1, 2)])
 def test_device_path_matches_golden(vxp, mode, solver):
     gold = np.load(os.path.join(GOLD, "config1_bodies.npz"))
     gman = np.load(os.path.join(GOLD, "config1_manifolds.npy"))

@@ -26,14 +26,17 @@ def _first_diff(g, r):
     return ["raw"]
 
 
-def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=None, **cfg):
+def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=None, cluster_smem=None, **cfg):
     """Steps GPU and oracle together; returns the GPU system (open).
-    solver: the grid solver mode (0 grid barriers, 1 event order, 2 cluster)."""
+    solver: the grid solver mode (0 grid barriers, 1 event order, 2 cluster);
+    cluster_smem: shared memory the cluster sweeps may use (0: state in L2)."""
     g = vxp.VoxelPhysicsSystem(**cfg)
     g.load_scene(scene)
     g.set_launch_mode(mode)
     if solver is not None:
         g.set_solver_mode(solver)
+    if cluster_smem is not None:
+        g.set_cluster_shared_bytes(cluster_smem)
     r = O.OracleWorld(**cfg)
     r.load_scene(scene)
     dt = np.float32(scene.dt)
@@ -80,12 +83,13 @@ def test_config1_modes(vxp, cfg):
     lockstep(vxp, sc, 90, **cfg).close()
 
 
-@pytest.mark.parametrize("solver", [0, 1, 2])
-def test_config2_pile_subset(vxp, solver):
+@pytest.mark.parametrize("solver,smem", [(0, None), (1, None), (2, None), (2, 0)])
+def test_config2_pile_subset(vxp, solver, smem):
     """216 boxes of the config-2 pile, 8 substeps at 1/120 s, grid launch,
-    each grid solver mode."""
+    each grid solver mode (the cluster one with its state in shared memory and
+    in L2)."""
     sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
-    lockstep(vxp, sc, 200, mode=1, check_every=10, solver=solver, substeps=8).close()
+    lockstep(vxp, sc, 200, mode=1, check_every=10, solver=solver, cluster_smem=smem, substeps=8).close()
 
 
 def test_cluster_available(vxp):
@@ -95,11 +99,11 @@ def test_cluster_available(vxp):
     g.close()
 
 
-@pytest.mark.parametrize("solver", [0, 2])
+@pytest.mark.parametrize("solver", [0, 1, 2])
 @pytest.mark.parametrize("cfg", [dict(), dict(colouring=1), dict(velocity_iterations=2, position_iterations=4),
                                  dict(enable_warm_starting=0, warm_starting=0)])
 def test_config1_grid_solver_modes(vxp, solver, cfg):
-    """The 64-cube scene on the grid with the barrier and cluster sweeps."""
+    """The 64-cube scene on the grid with each solver mode."""
     sc = vxp.scenes.config1(mass_fn=O.mass_fn, seed=5)
     lockstep(vxp, sc, 90, mode=1, solver=solver, **cfg).close()
 

@@ -840,6 +840,7 @@ struct vxp_ctx {
                 ev_cons = nullptr;
     uint32_t cluster_size = 0;  // CTAs of the cluster that runs the sweeps (0: no cluster launch here)
     uint32_t cluster_smem = 0;  // dynamic shared memory of each of its CTAs
+    uint32_t cluster_state_cap = 0xFFFFFFFFu;  // of which the sweeps' state may use at most this
     bool last_cluster = false;
     bool last_grid = false;
     uint32_t* h_count = nullptr;  // pinned mirror of the device pair count
@@ -924,7 +925,7 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
             cudaLaunchConfig_t lc = {};
             cudaLaunchAttribute at[1];
             cluster_config(&lc, at, ctx->cluster_size, ctx->cluster_smem, ctx->stream);
-            CK(cudaLaunchKernelEx(&lc, k_solve_cluster, wp, ctx->cluster_smem));
+            CK(cudaLaunchKernelEx(&lc, k_solve_cluster, wp, std::min(ctx->cluster_smem, ctx->cluster_state_cap)));
         }
     } else {
         k_step_block<kBlockThreads><<<1, kBlockThreads, smem, ctx->stream>>>(ctx->d_world.p, cs);
@@ -1565,6 +1566,12 @@ int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]) {
         out[0] = 0.0f;
         out[1] = 0.0f;
     }
+    return VXP_OK;
+}
+
+int vxp_set_cluster_shared_bytes(vxp_ctx* ctx, uint32_t bytes) {
+    if (!ctx) return VXP_ERR_ARG;
+    ctx->cluster_state_cap = bytes;
     return VXP_OK;
 }
 

@@ -1892,6 +1892,9 @@ __device__ __forceinline__ void st3(const CPV& v, uint32_t f, uint32_t s, F3 x) 
 // bodies' state after applyGravity.
 // vin: the point's inputs (normal, local anchors, base separation); v: where
 // its velocity-sweep fields go (the same rows, or a copy in shared memory).
+// kTangents: v holds the tangents too (else the sweeps recompute them from
+// the normal, point_tangents).
+template <bool kTangents = true>
 __device__ void prepare_point_s(const SolveFlags sf, const CPV vin, const CPV v, float restitution, uint32_t i,
                                 const Soft& soft, float hinv, const BV& a, Qt qa, const BV& b, Qt qb) {
     const F3 n = ld3(vin, CP_NX, i);
@@ -1928,8 +1931,10 @@ __device__ void prepare_point_s(const SolveFlags sf, const CPV vin, const CPV v,
         float k2 = a.im + b.im;
         k2 += dot3(r2a, mat3_mul_vec(a.I, r2a));
         k2 += dot3(r2b, mat3_mul_vec(b.I, r2b));
-        st3(v, CP_T1X, i, t1);
-        st3(v, CP_T2X, i, t2);
+        if (kTangents) {
+            st3(v, CP_T1X, i, t1);
+            st3(v, CP_T2X, i, t2);
+        }
         cpr(v, CP_TM0, i) = k1 > kEpsilon ? 1.0f / k1 : 0.0f;
         cpr(v, CP_TM1, i) = k2 > kEpsilon ? 1.0f / k2 : 0.0f;
     }
@@ -1942,13 +1947,36 @@ __device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft&
     prepare_point_s(solve_flags(w.cfg), v, v, w.cfr[pos].y, i, soft, hinv, a, qa, b, qb);
 }
 
-// warmStart for one manifold (solver.zig:702-729).
-__device__ void warm_points(const CPV& v, uint32_t n, float scale, BV& a, BV& b) {
+// The tangents of a point as prepare leaves them in the rows: t1 =
+// computeOrthogonal(n), t2 = n x t1 with friction on, zero without (the
+// constraint table starts them at zero and prepare does not write them).
+__device__ __forceinline__ void point_tangents(bool friction, F3 n, F3* t1, F3* t2) {
+    if (friction) {
+        *t1 = compute_orthogonal(n);
+        *t2 = cross3(n, *t1);
+    } else {
+        *t1 = F3{0.f, 0.f, 0.f};
+        *t2 = F3{0.f, 0.f, 0.f};
+    }
+}
+
+// warmStart for one manifold (solver.zig:702-729).  kTangents: the rows hold
+// the tangents; else they are recomputed (friction: the step's friction flag).
+template <bool kTangents = true>
+__device__ void warm_points(const CPV& v, uint32_t n, float scale, BV& a, BV& b, bool friction = true) {
     for (uint32_t i = 0; i < n; ++i) {
         const float sn = cpr(v, CP_NI, i) * scale;
         const float s1 = cpr(v, CP_TI0, i) * scale;
         const float s2 = cpr(v, CP_TI1, i) * scale;
-        const F3 imp = (ld3(v, CP_NX, i) * sn + ld3(v, CP_T1X, i) * s1) + ld3(v, CP_T2X, i) * s2;
+        const F3 nv = ld3(v, CP_NX, i);
+        F3 t1, t2;
+        if (kTangents) {
+            t1 = ld3(v, CP_T1X, i);
+            t2 = ld3(v, CP_T2X, i);
+        } else {
+            point_tangents(friction, nv, &t1, &t2);
+        }
+        const F3 imp = (nv * sn + t1 * s1) + t2 * s2;
         apply_impulse(a, -imp, ld3(v, CP_RAX, i));
         apply_impulse(b, imp, ld3(v, CP_RBX, i));
         cpr(v, CP_NI, i) = sn;
@@ -1969,14 +1997,17 @@ struct PtV {
     F3 pt, n, ra, rb, t1, t2;
     float nm, bias, tm0, tm1, ni, ti0, ti1;
 };
+template <bool kTangents = true>
 __device__ __forceinline__ PtV load_ptv(const CPV& v, uint32_t i) {
     PtV r;
     r.pt = ld3(v, CP_PX, i);
     r.n = ld3(v, CP_NX, i);
     r.ra = ld3(v, CP_RAX, i);
     r.rb = ld3(v, CP_RBX, i);
-    r.t1 = ld3(v, CP_T1X, i);
-    r.t2 = ld3(v, CP_T2X, i);
+    if (kTangents) {
+        r.t1 = ld3(v, CP_T1X, i);
+        r.t2 = ld3(v, CP_T2X, i);
+    }
     r.nm = cpr(v, CP_NM, i);
     r.bias = cpr(v, CP_BIAS, i);
     r.tm0 = cpr(v, CP_TM0, i);
@@ -2046,10 +2077,12 @@ __device__ void velocity_points(const WorldDev& w, const CPV& v, uint32_t n, flo
 // The same sweep without look-ahead: each point's fields are read when the
 // point starts, which keeps fewer registers live (the event-ordered sweeps
 // mostly read their rows from shared memory, where look-ahead gains little).
+template <bool kTangents = true>
 __device__ void velocity_points_near(bool friction, const CPV v, uint32_t n, float fr, const Soft& soft,
                                      bool use_bias, BV& a, BV& b) {
     for (uint32_t i = 0; i < n; ++i) {
-        const PtV c = load_ptv(v, i);
+        PtV c = load_ptv<kTangents>(v, i);
+        if (!kTangents) point_tangents(friction, c.n, &c.t1, &c.t2);
         const F3 rv = point_vel(b, c.pt) - point_vel(a, c.pt);
         const float vn = dot3(rv, c.n);
         float imp;
@@ -2716,8 +2749,8 @@ __device__ bool phase_solve_flow(G& g, WorldDev& w, float* fsm, uint32_t M, uint
 // i / C) and is read and written by the other CTAs through distributed
 // shared memory; the manifolds of each colour are dealt round-robin to the
 // CTAs (position lo + k + C j to CTA k), and each CTA prepares and solves its
-// own manifolds with their velocity-sweep fields (CP_NVEL per point) in its
-// shared memory.  The position sweeps read the fields that do not change
+// own manifolds with their velocity-sweep fields (CP_NVEL per point; the
+// tangents are recomputed from the normal) in its shared memory.  The position sweeps read the fields that do not change
 // during the solve from the packed rows.  Every operation and its order per
 // body is that of phase_solve, so the results are bit-identical.
 //
@@ -2845,9 +2878,10 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
         const CPV v{sm.row + slot, sm.scap};
         if (kind == 0u)
-            warm_points(v, mv.z, cf.warm_scale, a, b);
+            warm_points<false>(v, mv.z, cf.warm_scale, a, b, sf.friction);
         else
-            velocity_points_near(sf.friction, v, mv.z, sm.fr[slot].x, kind == 1u ? soft : hard, kind == 1u, a, b);
+            velocity_points_near<false>(sf.friction, v, mv.z, sm.fr[slot].x, kind == 1u ? soft : hard, kind == 1u,
+                                        a, b);
         if (a.wr) {
             pa->v = make_float4(a.v.x, a.v.y, a.v.z, 0.f);
             pa->w = make_float4(a.w.x, a.w.y, a.w.z, 0.f);
@@ -2886,8 +2920,8 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
                 if (i >= mv.z || (mv.w & CM_BAD)) continue;
                 const DBody A = *body_of(mv.x), B = *body_of(mv.y);
                 const BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
-                prepare_point_s(sf, cpv_global(w, sm.pos[slot]), CPV{sm.row + slot, sm.scap}, sm.fr[slot].y, i, soft,
-                                hinv, a, qof(A.q), b, qof(B.q));
+                prepare_point_s<false>(sf, cpv_global(w, sm.pos[slot]), CPV{sm.row + slot, sm.scap}, sm.fr[slot].y, i,
+                                       soft, hinv, a, qof(A.q), b, qof(B.q));
             }
             g.sync();
             if (cf.warm_starting && s == 0u) sweep(0u);

@@ -138,6 +138,11 @@ class VoxelPhysicsSystem:
         Worlds stepped by one CTA use CTA barriers."""
         self._check(self.lib.vxp_set_solver_mode(self.ctx, int(mode)))
 
+    def set_cluster_shared_bytes(self, n: int) -> None:
+        """Shared memory per CTA the cluster sweeps may keep their state in
+        (0: always L2).  Results do not depend on it."""
+        self._check(self.lib.vxp_set_cluster_shared_bytes(self.ctx, int(n)))
+
     def cluster_size(self) -> int:
         """CTAs of the cluster that solver mode 2 runs on (0: not available)."""
         n = ctypes.c_uint32(0)
