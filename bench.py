@@ -319,10 +319,10 @@ def ours(args):
     peak, peak_kind = peaks()
     achieved = sum(nb) / (sum(kern_ms) / 1e3) / 1e9
     # per kernel of the step, each its algorithmic bytes over its own event
-    # time: narrow part (k_step_grid), then the solve part, one kernel
-    # (k_solve_grid) or, with the sweeps on a cluster, the constraint table
-    # and colouring (k_solve_grid: no per-unit byte count, time only) and the
-    # sweeps and store (k_solve_cluster: the solver's bytes)
+    # time: narrow part (k_step_grid), then the solve part: one grid kernel
+    # (k_solve_grid), or the cluster kernel (k_solve_cluster: the solver's
+    # bytes), after the grid's constraint table and colouring when those do
+    # not run on the cluster (k_solve_grid: no per-unit byte count, time only)
     nb_parts = [alg_bytes(s, 8, n_dyn_awake, n_nonstatic) for s in stats]
     grid = n_dyn >= 512
     cluster = grid and all(x[1] > 0.0 for x in split_ms)
@@ -330,8 +330,9 @@ def ours(args):
     if grid:
         names = [("k_step_grid", [x[0] for x in part_ms], [x[0] for x in nb_parts])]
         if cluster:
-            names += [("k_solve_grid", [x[0] for x in split_ms], None),
-                      ("k_solve_cluster", [x[1] for x in split_ms], [x[1] for x in nb_parts])]
+            if statistics.mean(x[0] for x in split_ms) > 0.005:
+                names += [("k_solve_grid", [x[0] for x in split_ms], None)]
+            names += [("k_solve_cluster", [x[1] for x in split_ms], [x[1] for x in nb_parts])]
         else:
             names += [("k_solve_grid", [x[1] for x in part_ms], [x[1] for x in nb_parts])]
         for name, tl, bl in names:
@@ -409,7 +410,7 @@ def ours(args):
             "e2e": {"value": e2e_value, "unit": "body-substeps/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
                     "d2h_bytes_per_step": d2h // max(1, args.steps)},
             "clocks": clk,
-            "gpu_launches": args.steps * ((3 if cluster else 2) if grid else 1),
+            "gpu_launches": args.steps * (len(kernels) if grid else 1),
         }
         print(json.dumps(line), flush=True)
     if pg:

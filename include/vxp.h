@@ -338,9 +338,16 @@ int vxp_cluster_size(vxp_ctx* ctx, uint32_t* n);
  * results).  Default: all a block can have; 0: always in L2. */
 int vxp_set_cluster_shared_bytes(vxp_ctx* ctx, uint32_t bytes);
 
+/* Under VXP_SOLVER_CLUSTER: 0 (default) the grid builds the constraint table
+ * and colours it (k_solve_grid), then the cluster sweeps; 1 the cluster does
+ * all of the solve part (one kernel; slower on large worlds, where the
+ * colouring wants more SMs).  Same results. */
+int vxp_set_cluster_constraints(vxp_ctx* ctx, int on);
+
 /* Device time (ms) of the last step's solve part split by kernel under
- * VXP_SOLVER_CLUSTER: [constraints and colouring (k_solve_grid), sweeps and
- * store (k_solve_cluster)]; zeros for a step that ran otherwise. */
+ * VXP_SOLVER_CLUSTER: [constraints and colouring on the grid (k_solve_grid;
+ * 0 when the cluster does them), the cluster kernel (k_solve_cluster)];
+ * zeros for a step that ran otherwise. */
 int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]);
 
 /* Diagnostics: ns from the start of the last step kernel to the end of each

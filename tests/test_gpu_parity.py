@@ -26,10 +26,12 @@ def _first_diff(g, r):
     return ["raw"]
 
 
-def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=None, cluster_smem=None, **cfg):
+def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=None, cluster_smem=None,
+             cluster_cons=None, **cfg):
     """Steps GPU and oracle together; returns the GPU system (open).
     solver: the grid solver mode (0 grid barriers, 1 event order, 2 cluster);
-    cluster_smem: shared memory the cluster sweeps may use (0: state in L2)."""
+    cluster_smem: shared memory the cluster sweeps may use (0: state in L2);
+    cluster_cons: 1 to build and colour the constraint table on the cluster too."""
     g = vxp.VoxelPhysicsSystem(**cfg)
     g.load_scene(scene)
     g.set_launch_mode(mode)
@@ -37,6 +39,8 @@ def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=
         g.set_solver_mode(solver)
     if cluster_smem is not None:
         g.set_cluster_shared_bytes(cluster_smem)
+    if cluster_cons is not None:
+        g.set_cluster_constraints(bool(cluster_cons))
     r = O.OracleWorld(**cfg)
     r.load_scene(scene)
     dt = np.float32(scene.dt)
@@ -83,13 +87,15 @@ def test_config1_modes(vxp, cfg):
     lockstep(vxp, sc, 90, **cfg).close()
 
 
-@pytest.mark.parametrize("solver,smem", [(0, None), (1, None), (2, None), (2, 0)])
-def test_config2_pile_subset(vxp, solver, smem):
+@pytest.mark.parametrize("solver,smem,cons", [(0, None, None), (1, None, None), (2, None, None), (2, 0, None),
+                                              (2, None, 1)])
+def test_config2_pile_subset(vxp, solver, smem, cons):
     """216 boxes of the config-2 pile, 8 substeps at 1/120 s, grid launch,
     each grid solver mode (the cluster one with its state in shared memory and
-    in L2)."""
+    in L2, and with the colouring on the cluster and on the grid)."""
     sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
-    lockstep(vxp, sc, 200, mode=1, check_every=10, solver=solver, cluster_smem=smem, substeps=8).close()
+    lockstep(vxp, sc, 200, mode=1, check_every=10, solver=solver, cluster_smem=smem, cluster_cons=cons,
+             substeps=8).close()
 
 
 def test_cluster_available(vxp):

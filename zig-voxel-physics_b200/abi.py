@@ -216,6 +216,7 @@ SIGNATURES = {
     "vxp_last_solve_split_ms": (_I, [_VP, _VP]),
     "vxp_cluster_size": (_I, [_VP, _VP]),
     "vxp_set_cluster_shared_bytes": (_I, [_VP, _U32]),
+    "vxp_set_cluster_constraints": (_I, [_VP, _I]),
     "vxp_snapshot_substeps": (_I, [_VP, _I]),
     "vxp_substeps_get": (_I, [_VP, _VP, _U32, _VP]),
     "vxp_synchronize": (_I, [_VP]),

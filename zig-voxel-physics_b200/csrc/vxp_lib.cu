@@ -70,9 +70,10 @@ __global__ void __launch_bounds__(256, 1) k_solve_grid(const WorldDev* world, Gr
     GridGroup g{bar, &w.ctr[C_ERROR], timeout_ns, gridDim.x};
     world_step_solve(g, w, reinterpret_cast<float*>(smem_raw), true, part);
 }
-// The solver's sweeps and the store after k_solve_grid(..., SOLVE_CONSTRAINTS),
-// on one thread-block cluster (the whole grid).
-__global__ void __launch_bounds__(256, 1) k_solve_cluster(const WorldDev* world, uint32_t smem_bytes) {
+// The solve part on one thread-block cluster (the whole grid): all of it
+// (whole) or the sweeps and the store after k_solve_grid(...,
+// SOLVE_CONSTRAINTS).
+__global__ void __launch_bounds__(256, 1) k_solve_cluster(const WorldDev* world, uint32_t smem_bytes, uint32_t whole) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t ncta;
     asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(256, 1) k_solve_cluster(const WorldDev* world,
         return;
     }
     ClusterGroup g;
-    world_step_sweeps(g, w, smem_raw, smem_bytes);
+    world_step_sweeps(g, w, smem_raw, smem_bytes, whole != 0u);
 }
 
 // Pair source: world AABB of each body's collider (AABB.transform,
@@ -841,6 +842,7 @@ struct vxp_ctx {
     uint32_t cluster_size = 0;  // CTAs of the cluster that runs the sweeps (0: no cluster launch here)
     uint32_t cluster_smem = 0;  // dynamic shared memory of each of its CTAs
     uint32_t cluster_state_cap = 0xFFFFFFFFu;  // of which the sweeps' state may use at most this
+    bool cluster_whole = false;  // the cluster also builds the constraint table and colours it
     bool last_cluster = false;
     bool last_grid = false;
     uint32_t* h_count = nullptr;  // pinned mirror of the device pair count
@@ -916,16 +918,20 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
         CK(cudaLaunchCooperativeKernel((const void*)k_step_grid, dim3(ctx->grid_blocks), dim3(kGridThreads), args,
                                        smem, ctx->stream));
         CK(cudaEventRecord(ctx->ev_mid, ctx->stream));
-        uint32_t part = cluster ? SOLVE_CONSTRAINTS : SOLVE_ALL;
-        void* sargs[] = {(void*)&wp, (void*)&bp, (void*)&timeout, (void*)&part};
-        CK(cudaLaunchCooperativeKernel((const void*)k_solve_grid, dim3(ctx->grid_blocks), dim3(kSolveThreads), sargs,
-                                       solve_smem(), ctx->stream));
+        const uint32_t whole = cluster && ctx->cluster_whole ? 1u : 0u;
+        if (!whole) {
+            uint32_t part = cluster ? SOLVE_CONSTRAINTS : SOLVE_ALL;
+            void* sargs[] = {(void*)&wp, (void*)&bp, (void*)&timeout, (void*)&part};
+            CK(cudaLaunchCooperativeKernel((const void*)k_solve_grid, dim3(ctx->grid_blocks), dim3(kSolveThreads),
+                                           sargs, solve_smem(), ctx->stream));
+        }
         if (cluster) {
             CK(cudaEventRecord(ctx->ev_cons, ctx->stream));
             cudaLaunchConfig_t lc = {};
             cudaLaunchAttribute at[1];
             cluster_config(&lc, at, ctx->cluster_size, ctx->cluster_smem, ctx->stream);
-            CK(cudaLaunchKernelEx(&lc, k_solve_cluster, wp, std::min(ctx->cluster_smem, ctx->cluster_state_cap)));
+            CK(cudaLaunchKernelEx(&lc, k_solve_cluster, wp, std::min(ctx->cluster_smem, ctx->cluster_state_cap),
+                                  whole));
         }
     } else {
         k_step_block<kBlockThreads><<<1, kBlockThreads, smem, ctx->stream>>>(ctx->d_world.p, cs);
@@ -1566,6 +1572,12 @@ int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]) {
         out[0] = 0.0f;
         out[1] = 0.0f;
     }
+    return VXP_OK;
+}
+
+int vxp_set_cluster_constraints(vxp_ctx* ctx, int on) {
+    if (!ctx) return VXP_ERR_ARG;
+    ctx->cluster_whole = on != 0;
     return VXP_OK;
 }
 

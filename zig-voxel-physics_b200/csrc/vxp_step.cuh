@@ -1892,8 +1892,8 @@ __device__ __forceinline__ void st3(const CPV& v, uint32_t f, uint32_t s, F3 x) 
 // bodies' state after applyGravity.
 // vin: the point's inputs (normal, local anchors, base separation); v: where
 // its velocity-sweep fields go (the same rows, or a copy in shared memory).
-// kTangents: v holds the tangents too (else the sweeps recompute them from
-// the normal, point_tangents).
+// kTangents: v holds tangent2 too (else the sweeps recompute it as normal x
+// tangent1, point_tangents).
 template <bool kTangents = true>
 __device__ void prepare_point_s(const SolveFlags sf, const CPV vin, const CPV v, float restitution, uint32_t i,
                                 const Soft& soft, float hinv, const BV& a, Qt qa, const BV& b, Qt qb) {
@@ -1931,10 +1931,8 @@ __device__ void prepare_point_s(const SolveFlags sf, const CPV vin, const CPV v,
         float k2 = a.im + b.im;
         k2 += dot3(r2a, mat3_mul_vec(a.I, r2a));
         k2 += dot3(r2b, mat3_mul_vec(b.I, r2b));
-        if (kTangents) {
-            st3(v, CP_T1X, i, t1);
-            st3(v, CP_T2X, i, t2);
-        }
+        st3(v, CP_T1X, i, t1);
+        if (kTangents) st3(v, CP_T2X, i, t2);
         cpr(v, CP_TM0, i) = k1 > kEpsilon ? 1.0f / k1 : 0.0f;
         cpr(v, CP_TM1, i) = k2 > kEpsilon ? 1.0f / k2 : 0.0f;
     }
@@ -1947,12 +1945,13 @@ __device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft&
     prepare_point_s(solve_flags(w.cfg), v, v, w.cfr[pos].y, i, soft, hinv, a, qa, b, qb);
 }
 
-// The tangents of a point as prepare leaves them in the rows: t1 =
-// computeOrthogonal(n), t2 = n x t1 with friction on, zero without (the
-// constraint table starts them at zero and prepare does not write them).
-__device__ __forceinline__ void point_tangents(bool friction, F3 n, F3* t1, F3* t2) {
+// The tangents of a point as prepare leaves them in the rows, from the rows
+// without tangent2: with friction on, prepare wrote t1 = computeOrthogonal(n)
+// and t2 = n x t1; without, both stay zero as the constraint table set them
+// (and the rows in shared memory never got tangent1).
+__device__ __forceinline__ void point_tangents(bool friction, const CPV& v, uint32_t i, F3 n, F3* t1, F3* t2) {
     if (friction) {
-        *t1 = compute_orthogonal(n);
+        *t1 = ld3(v, CP_T1X, i);
         *t2 = cross3(n, *t1);
     } else {
         *t1 = F3{0.f, 0.f, 0.f};
@@ -1974,7 +1973,7 @@ __device__ void warm_points(const CPV& v, uint32_t n, float scale, BV& a, BV& b,
             t1 = ld3(v, CP_T1X, i);
             t2 = ld3(v, CP_T2X, i);
         } else {
-            point_tangents(friction, nv, &t1, &t2);
+            point_tangents(friction, v, i, nv, &t1, &t2);
         }
         const F3 imp = (nv * sn + t1 * s1) + t2 * s2;
         apply_impulse(a, -imp, ld3(v, CP_RAX, i));
@@ -2082,7 +2081,7 @@ __device__ void velocity_points_near(bool friction, const CPV v, uint32_t n, flo
                                      bool use_bias, BV& a, BV& b) {
     for (uint32_t i = 0; i < n; ++i) {
         PtV c = load_ptv<kTangents>(v, i);
-        if (!kTangents) point_tangents(friction, c.n, &c.t1, &c.t2);
+        if (!kTangents) point_tangents(friction, v, i, c.n, &c.t1, &c.t2);
         const F3 rv = point_vel(b, c.pt) - point_vel(a, c.pt);
         const float vn = dot3(rv, c.n);
         float imp;
@@ -2749,8 +2748,8 @@ __device__ bool phase_solve_flow(G& g, WorldDev& w, float* fsm, uint32_t M, uint
 // i / C) and is read and written by the other CTAs through distributed
 // shared memory; the manifolds of each colour are dealt round-robin to the
 // CTAs (position lo + k + C j to CTA k), and each CTA prepares and solves its
-// own manifolds with their velocity-sweep fields (CP_NVEL per point; the
-// tangents are recomputed from the normal) in its shared memory.  The position sweeps read the fields that do not change
+// own manifolds with their velocity-sweep fields (CP_NVEL per point; tangent2
+// is recomputed from the normal and tangent1) in its shared memory.  The position sweeps read the fields that do not change
 // during the solve from the packed rows.  Every operation and its order per
 // body is that of phase_solve, so the results are bit-identical.
 //
@@ -3200,26 +3199,34 @@ __device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go, u
     stamp(s, w, TS_END);
 }
 
-// The rest of the solve part after world_step_solve(..., SOLVE_CONSTRAINTS):
-// ContactSolver.solve with a barrier after every colour batch (phase_solve),
-// then store and sleep, on one thread-block cluster.  Every block reads the
-// go flag, M and ncol (written by the previous kernel) before its first
-// barrier and passes the same barriers: their number follows from those
-// values, the configuration and the position sweeps' early-break test, which
-// every block reads from a slot that no block writes again before the next
-// barrier.
+// The solve part on one thread-block cluster.  whole: all of it (constraints,
+// colouring, sweeps, store and sleep) right after the narrow part; else the
+// part after world_step_solve(..., SOLVE_CONSTRAINTS) on the grid.  The
+// sweeps run by phase_solve_cluster (state in shared memory) or, when that
+// does not fit, phase_solve.  Every block reads the go flag, M and ncol
+// (written by the previous kernel, or by this one before a barrier) and
+// passes the same barriers: their number follows from those values, the
+// configuration, the colouring's round count and the position sweeps' early
+// break, which every block reads from a slot that no block writes again
+// before the next barrier.
 __device__ __forceinline__ void world_step_sweeps(ClusterGroup& g, WorldDev& w, unsigned char* smem,
-                                                  uint32_t smem_bytes) {
+                                                  uint32_t smem_bytes, bool whole) {
     const uint32_t ph = w.cfg.phases;
     if (!(ph & PH_SOLVE) || w.n_bodies == 0u) return;
-    if (*(volatile uint32_t*)&w.ctr[C_SOLVE_GO] != 2u) return;
+    if (*(volatile uint32_t*)&w.ctr[C_SOLVE_GO] != (whole ? 1u : 2u)) return;
     w.n_pairs = *(volatile uint32_t*)w.n_pairs_dev;
     const uint32_t cur = *(volatile uint32_t*)&w.frame[0] & 1u;
-    const uint32_t M = *(volatile uint32_t*)&w.ctr[C_CONS_M];
-    const uint32_t ncol = *(volatile uint32_t*)&w.ctr[C_CONS_NCOL];
-    // the position sweeps' min-separation slots at this group's offset
-    if (g.rank() < 16u) w.scan[g.nblocks() + 4u + g.rank()] = 0u;
-    g.sync();
+    uint32_t M, ncol;
+    if (whole) {
+        phase_constraints(g, w, cur, &M, &ncol);
+        stamp(g, w, TS_CONSTRAINTS);
+    } else {
+        M = *(volatile uint32_t*)&w.ctr[C_CONS_M];
+        ncol = *(volatile uint32_t*)&w.ctr[C_CONS_NCOL];
+        // the position sweeps' min-separation slots at this group's offset
+        if (g.rank() < 16u) w.scan[g.nblocks() + 4u + g.rank()] = 0u;
+        g.sync();
+    }
     const bool solved = w.cfg.dt > 0.0f;
     if (solved && !phase_solve_cluster(g, w, M, ncol, smem, smem_bytes)) phase_solve(g, w, M, ncol);
     g.sync();

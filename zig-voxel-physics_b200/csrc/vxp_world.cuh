@@ -269,20 +269,20 @@ struct WorldDev {
 
 // Packed constraint-point fields (ConstraintPoint, solver.zig:122-168).  The
 // first CP_NVEL are the ones the velocity-type sweeps (warm start, velocity,
-// relax) read or write besides the tangents, which are a function of the
-// normal (prepareConstraints' computeOrthogonal); prepare and the position
-// sweeps also read the rest, which do not change during the solve.
+// relax) read or write besides tangent2, which is normal x tangent1
+// (prepareConstraints); prepare and the position sweeps also read the rest,
+// which do not change during the solve.
 enum : uint32_t {
     CP_NX, CP_NY, CP_NZ,            // normal
     CP_PX, CP_PY, CP_PZ,            // point
     CP_RAX, CP_RAY, CP_RAZ,         // r_a
     CP_RBX, CP_RBY, CP_RBZ,         // r_b
+    CP_T1X, CP_T1Y, CP_T1Z,         // tangent1
     CP_NM, CP_TM0, CP_TM1,          // effective masses
     CP_BIAS,                        // velocity bias
     CP_NI, CP_TI0, CP_TI1,          // accumulated impulses
     CP_NVEL,
-    CP_T1X = CP_NVEL, CP_T1Y, CP_T1Z,  // tangent1
-    CP_T2X, CP_T2Y, CP_T2Z,            // tangent2
+    CP_T2X = CP_NVEL, CP_T2Y, CP_T2Z,  // tangent2
     CP_LAX, CP_LAY, CP_LAZ,            // local anchor a
     CP_LBX, CP_LBY, CP_LBZ,            // local anchor b
     CP_BASE,                           // base separation

@@ -138,6 +138,11 @@ class VoxelPhysicsSystem:
         Worlds stepped by one CTA use CTA barriers."""
         self._check(self.lib.vxp_set_solver_mode(self.ctx, int(mode)))
 
+    def set_cluster_constraints(self, on: bool = True) -> None:
+        """Solver mode 2: the cluster also builds and colours the constraint
+        table, or (default) the grid does that first.  Same results."""
+        self._check(self.lib.vxp_set_cluster_constraints(self.ctx, 1 if on else 0))
+
     def set_cluster_shared_bytes(self, n: int) -> None:
         """Shared memory per CTA the cluster sweeps may keep their state in
         (0: always L2).  Results do not depend on it."""
