@@ -338,6 +338,13 @@ int vxp_cluster_size(vxp_ctx* ctx, uint32_t* n);
  * results).  Default: all a block can have; 0: always in L2. */
 int vxp_set_cluster_shared_bytes(vxp_ctx* ctx, uint32_t bytes);
 
+/* Traffic accounting: with on, each step counts the voxel bricks its probed
+ * pairs touch (vxp_stats.bricks_touched: A's bricks in the overlap region plus
+ * B's bricks in B's region), for the narrow phase's algorithmic-byte figure.
+ * It costs time in the narrow phase, so it is off by default (the count reads
+ * 0); results do not depend on it. */
+int vxp_set_traffic_accounting(vxp_ctx* ctx, int on);
+
 /* Under VXP_SOLVER_CLUSTER: 0 (default) the grid builds the constraint table
  * and colours it (k_solve_grid), then the cluster sweeps; 1 the cluster does
  * all of the solve part (one kernel; slower on large worlds, where the

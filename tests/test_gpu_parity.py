@@ -297,3 +297,31 @@ def test_heavy_pair_split_keeps_results(vxp, mode, heavy):
         assert g.get_bodies().tobytes() == r.get_bodies().tobytes(), f"step {s}: bodies differ"
     g.close()
     r.close()
+
+
+@pytest.mark.parametrize("heavy", [0, 1024])
+def test_traffic_accounting_changes_only_the_brick_count(vxp, heavy):
+    """With traffic accounting on, every step counts the bricks its probed
+    pairs touch; the manifolds, counters and bodies stay those of the run
+    without it (and the count reads 0 there)."""
+    sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
+    runs = []
+    for on in (False, True):
+        g = vxp.VoxelPhysicsSystem(substeps=8)
+        g.load_scene(sc)
+        g.set_launch_mode(1)
+        g.set_heavy_pair_voxels(heavy)
+        g.set_traffic_accounting(on)
+        dt = np.float32(sc.dt)
+        rows = []
+        for _ in range(40):
+            g.step(dt)
+            st = g.stats()
+            rows.append((g.manifolds().tobytes(), g.get_bodies().tobytes(), st["bricks_touched"],
+                         tuple(st[k] for k in STAT_KEYS)))
+        runs.append(rows)
+        g.close()
+    for s, (off, on) in enumerate(zip(*runs)):
+        assert off[0] == on[0] and off[1] == on[1] and off[3] == on[3], f"step {s}: results differ"
+        assert off[2] == 0, f"step {s}: bricks counted with accounting off"
+    assert sum(r[2] for r in runs[1]) > 0

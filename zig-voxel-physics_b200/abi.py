@@ -217,6 +217,7 @@ SIGNATURES = {
     "vxp_cluster_size": (_I, [_VP, _VP]),
     "vxp_set_cluster_shared_bytes": (_I, [_VP, _U32]),
     "vxp_set_cluster_constraints": (_I, [_VP, _I]),
+    "vxp_set_traffic_accounting": (_I, [_VP, _I]),
     "vxp_snapshot_substeps": (_I, [_VP, _I]),
     "vxp_substeps_get": (_I, [_VP, _VP, _U32, _VP]),
     "vxp_synchronize": (_I, [_VP]),

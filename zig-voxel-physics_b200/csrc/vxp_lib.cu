@@ -455,6 +455,7 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
     s.margin = 0.1f;
     s.solver_flow = 1;
     s.heavy_voxels = 1024;
+    s.count_bricks = 0;
     return s;
 }
 
@@ -851,6 +852,7 @@ struct vxp_ctx {
     uint32_t solver_div = 128;
     uint32_t solver_flow = 1;
     uint32_t heavy_voxels = 1024;
+    bool count_bricks = false;  // traffic accounting (C_BRICKS)
     bool record_substeps = false;
     DBuf<float> subrec;
 };
@@ -900,6 +902,7 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
     const size_t smem = grid ? grid_smem(w.cache_cap) : step_smem(kBlockThreads, w.cache_cap);
     w.cfg.flow_smem_chunks = grid ? flow_chunks(solve_smem()) : 0u;
     w.cfg.heavy_voxels = ctx->heavy_voxels;
+    w.cfg.count_bricks = ctx->count_bricks ? 1u : 0u;
     if (ctx->record_substeps) {
         const size_t need = (size_t)std::max(1u, ctx->cfg.substeps) * std::max(1u, ctx->w.n_bodies) * 13u;
         if (ctx->subrec.reserve(need) != cudaSuccess) return fail(ctx, VXP_ERR_OOM, "substep record buffer");
@@ -1572,6 +1575,12 @@ int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]) {
         out[0] = 0.0f;
         out[1] = 0.0f;
     }
+    return VXP_OK;
+}
+
+int vxp_set_traffic_accounting(vxp_ctx* ctx, int on) {
+    if (!ctx) return VXP_ERR_ARG;
+    ctx->count_bricks = on != 0;
     return VXP_OK;
 }
 

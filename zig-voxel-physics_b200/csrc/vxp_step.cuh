@@ -723,8 +723,10 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
     }
     __syncwarp();
     uint32_t hits = 0, misses = 0, evictions = 0;
+    // keys 32 at a time, one per lane, each with its window start; the
+    // lookups themselves run one after another
     for (uint32_t k0 = 0; k0 < n; k0 += 32u) {
-        uint32_t my_p = 0, my_a = 0, my_b = 0;
+        uint32_t my_p = 0, my_a = 0, my_b = 0, my_start = 0;
         unsigned long long my_th = 0;
         if (k0 + lane < n) {
             my_p = w.clist[k0 + lane];
@@ -732,13 +734,14 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
             my_a = pi.key_a;
             my_b = pi.key_b;
             my_th = pi.th;
+            my_start = (uint32_t)(cache_key_hash(my_a, my_b, my_th) % (unsigned long long)cap);
         }
         const uint32_t cnt = min(32u, n - k0);
         for (uint32_t j = 0; j < cnt; ++j) {
             const uint32_t p = __shfl_sync(0xffffffffu, my_p, j);
             const uint32_t ka = __shfl_sync(0xffffffffu, my_a, j), kb = __shfl_sync(0xffffffffu, my_b, j);
             const unsigned long long th = __shfl_sync(0xffffffffu, my_th, j);
-            const uint32_t start = (uint32_t)(cache_key_hash(ka, kb, th) % (unsigned long long)cap);
+            const uint32_t start = __shfl_sync(0xffffffffu, my_start, j);
             uint32_t slot = start + lane;
             if (slot >= cap) slot -= cap;
             bool valid = false, match = false;
@@ -761,18 +764,8 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
                 tl = fi;
             } else {
                 // first least-recently-used entry of the window
-                uint32_t best = lane < maxp ? lu : 0xFFFFFFFFu;
-                uint32_t bl = lane < maxp ? lane : 32u;
-#pragma unroll
-                for (int d = 16; d > 0; d >>= 1) {
-                    const uint32_t ob = __shfl_xor_sync(0xffffffffu, best, d);
-                    const uint32_t ol = __shfl_xor_sync(0xffffffffu, bl, d);
-                    if (ob < best || (ob == best && ol < bl)) {
-                        best = ob;
-                        bl = ol;
-                    }
-                }
-                tl = bl;
+                const uint32_t m = __reduce_min_sync(0xffffffffu, lane < maxp ? lu : 0xFFFFFFFFu);
+                tl = (uint32_t)(__ffs(__ballot_sync(0xffffffffu, lane < maxp && lu == m)) - 1);
                 ++evictions;
             }
             uint32_t target = start + tl;
@@ -965,10 +958,13 @@ __device__ __forceinline__ void probe_neighbourhood(WorldDev& w, const ColliderS
             }
 }
 
+// Entering candidates a warp generates at once before lane 0 applies them.
+constexpr uint32_t kWarpReplay = 8;
+
 // Per-warp shared state of phase_probe.
 struct WarpManifold {
     ContactRec c[4];
-    ContactRec stage;
+    ContactRec list[kWarpReplay];
     float pens[4];
     uint32_t n;
     uint32_t pad[3];
@@ -1042,7 +1038,7 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
     if (lane == 0) sm.n = 0u;
     Top4 state = top4_empty();
     uint32_t checked = 0, ncand = 0;
-    {
+    if (w.cfg.count_bricks) {
         // traffic accounting: A bricks in the region, B bricks in B's region
         uint32_t nb = warp_count_bricks(cs, ca, I3{pi.rmin[0], pi.rmin[1], pi.rmin[2]},
                                         I3{pi.rmax[0], pi.rmax[1], pi.rmax[2]});
@@ -1099,26 +1095,28 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
                 top4_insert(run, pen);
             }
         }
-        // replay entering candidates in canonical order
-        uint32_t lanes = __ballot_sync(0xffffffffu, enter != 0u);
-        while (lanes) {
-            const uint32_t L = __ffs(lanes) - 1;
-            lanes &= lanes - 1u;
-            uint32_t em = __shfl_sync(0xffffffffu, enter, L);
-            while (em) {
-                const uint32_t k = __ffs(em) - 1;
-                em &= em - 1u;
-                if (lane == L) {
-                    const I3 o = probe_offset(k);
-                    const I3 ibv{cbv.x + o.x, cbv.y + o.y, cbv.z + o.z};
-                    const uint32_t vb = voxel_at(cs, cb, ibv.x, ibv.y, ibv.z);
-                    const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
-                    generate_contact(c, va, I3{x, y, z}, wa, vb, ibv, wb, &sm.stage);
-                }
-                __syncwarp();
-                if (lane == 0) add_contact(sm, sm.stage);
-                __syncwarp();
+        // entering candidates in canonical order (lane = voxel order, then
+        // probe order): the lanes generate them at once, kWarpReplay at a
+        // time, into the warp's list; lane 0 applies them in list order
+        const uint32_t ne = (uint32_t)__popc(enter);
+        const uint32_t ninc = warp_incl_scan(ne);
+        const uint32_t total = __shfl_sync(0xffffffffu, ninc, 31);
+        for (uint32_t lo = 0; lo < total; lo += kWarpReplay) {
+            uint32_t e = ninc - ne;
+            for (uint32_t mm = enter; mm; mm &= mm - 1u, ++e) {
+                if (e < lo || e >= lo + kWarpReplay) continue;
+                const I3 o = probe_offset(__ffs(mm) - 1);
+                const I3 ibv{cbv.x + o.x, cbv.y + o.y, cbv.z + o.z};
+                const uint32_t vb = voxel_at(cs, cb, ibv.x, ibv.y, ibv.z);
+                const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
+                generate_contact(c, va, I3{x, y, z}, wa, vb, ibv, wb, &sm.list[e - lo]);
             }
+            __syncwarp();
+            if (lane == 0) {
+                const uint32_t cnt = min(kWarpReplay, total - lo);
+                for (uint32_t i = 0; i < cnt; ++i) add_contact(sm, sm.list[i]);
+            }
+            __syncwarp();
         }
         // manifold penetration multiset -> state (at most four finite values,
         // so every insert lands)
@@ -1197,7 +1195,7 @@ __device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cu
                   nz = pi.rmax[2] - pi.rmin[2] + 1;
     const unsigned long long V = (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
     if (tid == 0) sm.n = 0u;
-    if (wid == 0) {
+    if (wid == 0 && w.cfg.count_bricks) {
         // traffic accounting: A bricks in the region, B bricks in B's region
         uint32_t nb = warp_count_bricks(cs, ca, I3{pi.rmin[0], pi.rmin[1], pi.rmin[2]},
                                         I3{pi.rmax[0], pi.rmax[1], pi.rmax[2]});

@@ -151,6 +151,7 @@ struct StepCfg {
     uint32_t flow_smem_chunks;  // constraint chunks per block the launch's shared memory holds
     uint32_t record_substeps;   // 1: write every body's state after each substep to subrec
     uint32_t heavy_voxels;      // overlap regions of at least this many voxels are probed by a CTA (0: never)
+    uint32_t count_bricks;      // count the bricks each probed pair touches (C_BRICKS; traffic accounting only)
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 

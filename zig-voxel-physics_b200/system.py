@@ -138,6 +138,11 @@ class VoxelPhysicsSystem:
         Worlds stepped by one CTA use CTA barriers."""
         self._check(self.lib.vxp_set_solver_mode(self.ctx, int(mode)))
 
+    def set_traffic_accounting(self, on: bool = True) -> None:
+        """Count the bricks the probed pairs touch (stats bricks_touched; off by
+        default, it costs narrow-phase time).  Results do not depend on it."""
+        self._check(self.lib.vxp_set_traffic_accounting(self.ctx, 1 if on else 0))
+
     def set_cluster_constraints(self, on: bool = True) -> None:
         """Solver mode 2: the cluster also builds and colours the constraint
         table, or (default) the grid does that first.  Same results."""
