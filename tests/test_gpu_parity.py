@@ -325,3 +325,15 @@ def test_traffic_accounting_changes_only_the_brick_count(vxp, heavy):
         assert off[0] == on[0] and off[1] == on[1] and off[3] == on[3], f"step {s}: results differ"
         assert off[2] == 0, f"step {s}: bricks counted with accounting off"
     assert sum(r[2] for r in runs[1]) > 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("cache", [32, 48, 64, 200])
+def test_small_brick_pair_cache(vxp, mode, cache):
+    """A brick-pair cache of a few dozen slots: nearly every lookup evicts and
+    consecutive lookups' 16-slot windows often overlap, so the device replay
+    of the lookups (two at a time when their windows are disjoint) is checked
+    against the oracle's sequential one through the hit / miss / eviction
+    counters and the manifolds, every step."""
+    sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
+    lockstep(vxp, sc, 60, mode=mode, brick_pair_cache_size=cache, substeps=8).close()

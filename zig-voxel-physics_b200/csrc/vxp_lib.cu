@@ -454,7 +454,7 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
     s.device_pairs = 0;
     s.margin = 0.1f;
     s.solver_flow = 1;
-    s.heavy_voxels = 1024;
+    s.heavy_voxels = 768;
     s.count_bricks = 0;
     return s;
 }
@@ -851,7 +851,7 @@ struct vxp_ctx {
     int use_grid = -1;  // -1 auto, 0 block, 1 grid
     uint32_t solver_div = 128;
     uint32_t solver_flow = 1;
-    uint32_t heavy_voxels = 1024;
+    uint32_t heavy_voxels = 768;
     bool count_bricks = false;  // traffic accounting (C_BRICKS)
     bool record_substeps = false;
     DBuf<float> subrec;

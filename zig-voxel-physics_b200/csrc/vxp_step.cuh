@@ -73,23 +73,31 @@ struct GridGroup {
     // than one over the whole grid.  The other blocks leave the kernel.
     __device__ GridGroup subgroup(uint32_t k) const { return GridGroup{bar + 1, err, timeout_ns, k}; }
     // Bounded grid barrier: a waiting block gives up after timeout_ns, sets
-    // ERR_TIMEOUT and every later sync() of every block returns false.
+    // ERR_TIMEOUT and every later sync() of every block returns false.  The
+    // block's threads meet at __syncthreads, then thread 0 arrives with an
+    // acquire-release add on the count (the last to arrive resets it and
+    // bumps the generation with a release add) and waits with acquire loads
+    // of the generation: release / acquire at GPU scope, no full fence (a
+    // sequentially consistent fence here was seen to stall one block for
+    // hundreds of microseconds behind the memory traffic of a busy phase).
     __device__ bool sync() {
         __shared__ int s_ok;
         __syncthreads();
         if (threadIdx.x == 0) {
             int ok = 1;
-            volatile unsigned int* vgen = &bar->gen;
-            const unsigned int g = *vgen;
-            __threadfence();
-            const unsigned int arrived = atomicAdd(&bar->count, 1u);
+            unsigned int g;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(&bar->gen) : "memory");
+            unsigned int arrived;
+            asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(&bar->count) : "memory");
             if (arrived == nb - 1) {
-                atomicExch(&bar->count, 0u);
-                __threadfence();
-                atomicAdd(&bar->gen, 1u);
+                asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(&bar->count) : "memory");
+                asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&bar->gen) : "memory");
             } else {
                 const unsigned long long t0 = global_ns();
-                while (*vgen == g) {
+                for (;;) {
+                    unsigned int v;
+                    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&bar->gen) : "memory");
+                    if (v != g) break;
                     __nanosleep(64);
                     if (global_ns() - t0 > timeout_ns) {
                         atomicOr(err, ERR_TIMEOUT);
@@ -98,8 +106,9 @@ struct GridGroup {
                     }
                 }
             }
-            __threadfence();
-            if (*(volatile uint32_t*)err & ERR_TIMEOUT) ok = 0;
+            unsigned int e;
+            asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(e) : "l"(err) : "memory");
+            if (e & ERR_TIMEOUT) ok = 0;
             s_ok = ok;
         }
         __syncthreads();
@@ -723,8 +732,17 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
     }
     __syncwarp();
     uint32_t hits = 0, misses = 0, evictions = 0;
-    // keys 32 at a time, one per lane, each with its window start; the
-    // lookups themselves run one after another
+    // Keys 32 at a time, one per lane, each with its window start.  Two
+    // consecutive lookups whose windows share no slot cannot see each other's
+    // write, so they run together (lanes 0-15 hold the window of the first,
+    // lanes 16-31 that of the second); otherwise one runs alone.  Which
+    // lookups pair up follows from the window starts only.  The windows of
+    // the next round are read while this round is decided, then patched with
+    // this round's writes (the slots it touches, if in those windows); a
+    // patch stores what the writing lane stores, so it does not matter
+    // whether the read saw that store.
+    const bool pairs_ok = cap >= 32u && maxp == 16u;
+    const uint32_t half = lane >> 4, hl = lane & 15u;
     for (uint32_t k0 = 0; k0 < n; k0 += 32u) {
         uint32_t my_p = 0, my_a = 0, my_b = 0, my_start = 0;
         unsigned long long my_th = 0;
@@ -737,40 +755,106 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
             my_start = (uint32_t)(cache_key_hash(my_a, my_b, my_th) % (unsigned long long)cap);
         }
         const uint32_t cnt = min(32u, n - k0);
-        for (uint32_t j = 0; j < cnt; ++j) {
-            const uint32_t p = __shfl_sync(0xffffffffu, my_p, j);
-            const uint32_t ka = __shfl_sync(0xffffffffu, my_a, j), kb = __shfl_sync(0xffffffffu, my_b, j);
-            const unsigned long long th = __shfl_sync(0xffffffffu, my_th, j);
-            const uint32_t start = __shfl_sync(0xffffffffu, my_start, j);
-            uint32_t slot = start + lane;
-            if (slot >= cap) slot -= cap;
-            bool valid = false, match = false;
-            uint32_t lu = 0xFFFFFFFFu;
-            if (lane < maxp) {
-                lu = t.lu[slot];
-                valid = lu != 0u;
-                match = valid && t.ab[slot].x == ka && t.ab[slot].y == kb && t.th[slot] == th;
+        // round starting at lookup j: 2 lookups when j + 1 is in the batch and
+        // the two windows are disjoint, else 1
+        auto round_size = [&](uint32_t j) -> uint32_t {
+            if (!pairs_ok || j + 1u >= cnt) return 1u;
+            const uint32_t s0 = __shfl_sync(0xffffffffu, my_start, j), s1 = __shfl_sync(0xffffffffu, my_start, j + 1u);
+            const uint32_t d = s1 >= s0 ? s1 - s0 : s1 + cap - s0;
+            return (d >= 16u && d <= cap - 16u) ? 2u : 1u;
+        };
+        // this lane's lookup of a round at j: lanes 0-15 the first, lanes
+        // 16-31 the second (none when the round has one lookup); slot held
+        auto lane_lookup = [&](uint32_t j, uint32_t rs, uint32_t* sl) -> bool {
+            const uint32_t q = j + half;
+            const uint32_t st = __shfl_sync(0xffffffffu, my_start, q < cnt ? q : j);
+            uint32_t x = st + hl;
+            if (x >= cap) x -= cap;
+            *sl = x;
+            return half < rs && hl < maxp;
+        };
+        uint32_t j = 0, rs = round_size(0), c_sl = 0;
+        bool c_on = lane_lookup(0, rs, &c_sl);
+        uint32_t c_lu = 0xFFFFFFFFu, c_a = 0, c_b = 0;
+        unsigned long long c_th = 0;
+        if (c_on) {
+            c_lu = t.lu[c_sl];
+            const uint2 ab = t.ab[c_sl];
+            c_a = ab.x;
+            c_b = ab.y;
+            c_th = t.th[c_sl];
+        }
+        while (j < cnt) {
+            // this lane's key: the lookup its half of the warp decides
+            const uint32_t q = j + (half < rs ? half : 0u);
+            const uint32_t p = __shfl_sync(0xffffffffu, my_p, q);
+            const uint32_t ka = __shfl_sync(0xffffffffu, my_a, q), kb = __shfl_sync(0xffffffffu, my_b, q);
+            const unsigned long long th = __shfl_sync(0xffffffffu, my_th, q);
+            const uint32_t start = __shfl_sync(0xffffffffu, my_start, q);
+            // the next round's windows, read ahead
+            const uint32_t nj = j + rs;
+            const bool more = nj < cnt;
+            const uint32_t nrs = more ? round_size(nj) : 1u;
+            uint32_t n_sl = 0;
+            const bool n_on = lane_lookup(more ? nj : j, nrs, &n_sl) && more;
+            uint32_t n_lu = 0xFFFFFFFFu, n_a = 0, n_b = 0;
+            unsigned long long n_th = 0;
+            if (n_on) {
+                n_lu = t.lu[n_sl];
+                const uint2 ab = t.ab[n_sl];
+                n_a = ab.x;
+                n_b = ab.y;
+                n_th = t.th[n_sl];
             }
-            const uint32_t inv_m = __ballot_sync(0xffffffffu, lane < maxp && !valid);
-            const uint32_t mat_m = __ballot_sync(0xffffffffu, match);
+            // get: stop at the first empty slot (miss) or at the key (hit)
+            const bool valid = c_on && c_lu != 0u;
+            const bool match = valid & (c_a == ka) & (c_b == kb) & (c_th == th);
+            const uint32_t sh = half * 16u;
+            const uint32_t inv_m = (__ballot_sync(0xffffffffu, c_on && !valid) >> sh) & 0xFFFFu;
+            const uint32_t mat_m = (__ballot_sync(0xffffffffu, match) >> sh) & 0xFFFFu;
+            // first least-recently-used entry of the window (used when the
+            // window is full and the key is not in it)
+            const uint32_t m0 = __reduce_min_sync(0xffffffffu, (c_on && half == 0u) ? c_lu : 0xFFFFFFFFu);
+            const uint32_t m1 = __reduce_min_sync(0xffffffffu, (c_on && half == 1u) ? c_lu : 0xFFFFFFFFu);
+            const uint32_t lru_m = (__ballot_sync(0xffffffffu, c_on && c_lu == (half ? m1 : m0)) >> sh) & 0xFFFFu;
             const uint32_t fi = inv_m ? (uint32_t)(__ffs(inv_m) - 1) : 32u;
             const uint32_t fm = mat_m ? (uint32_t)(__ffs(mat_m) - 1) : 32u;
             uint32_t tl;
-            bool hit = false;
+            bool hit = false, evict = false;
             if (fm < fi) {
                 hit = true;
                 tl = fm;
             } else if (fi < 32u) {
                 tl = fi;
             } else {
-                // first least-recently-used entry of the window
-                const uint32_t m = __reduce_min_sync(0xffffffffu, lane < maxp ? lu : 0xFFFFFFFFu);
-                tl = (uint32_t)(__ffs(__ballot_sync(0xffffffffu, lane < maxp && lu == m)) - 1);
-                ++evictions;
+                tl = (uint32_t)(__ffs(lru_m) - 1);
+                evict = true;
             }
             uint32_t target = start + tl;
             if (target >= cap) target -= cap;
-            if (lane == 0) {
+            // the other half's decision (the second lookup of the round)
+            const uint32_t o_target = __shfl_xor_sync(0xffffffffu, target, 16);
+            const bool o_hit = __shfl_xor_sync(0xffffffffu, hit ? 1u : 0u, 16) != 0u;
+            const uint32_t o_a = __shfl_xor_sync(0xffffffffu, ka, 16), o_b = __shfl_xor_sync(0xffffffffu, kb, 16);
+            const unsigned long long o_th = __shfl_xor_sync(0xffffffffu, th, 16);
+            if (n_on) {
+                if (n_sl == target && half < rs) {
+                    n_lu = frame;
+                    if (!hit) {
+                        n_a = ka;
+                        n_b = kb;
+                        n_th = th;
+                    }
+                } else if ((half ^ 1u) < rs && n_sl == o_target) {
+                    n_lu = frame;
+                    if (!o_hit) {
+                        n_a = o_a;
+                        n_b = o_b;
+                        n_th = o_th;
+                    }
+                }
+            }
+            if (hl == 0u && half < rs) {
                 PairInfo& pi = w.pinfo[p];
                 t.lu[target] = frame;
                 if (hit) {
@@ -782,10 +866,19 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
                     w.cwriter[target] = p;
                     pi.hit = 2u;
                     ++misses;
+                    if (evict) ++evictions;
                 }
                 pi.cache_slot = target;
             }
             __syncwarp();
+            j = nj;
+            rs = nrs;
+            c_on = n_on;
+            c_sl = n_sl;
+            c_lu = n_lu;
+            c_a = n_a;
+            c_b = n_b;
+            c_th = n_th;
         }
     }
     for (uint32_t i = lane; i < cap; i += 32u) {
@@ -798,6 +891,9 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
         k._pad = 0u;
         w.ckey[i] = k;
     }
+    hits = warp_sum(hits);
+    misses = warp_sum(misses);
+    evictions = warp_sum(evictions);
     if (lane == 0) {
         w.ctr[C_CACHE_HITS] += hits;
         w.ctr[C_CACHE_MISSES] += misses;
@@ -1160,13 +1256,12 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
 // whole CTA: each pass covers blockDim.x consecutive voxels of the inclusive
 // z, y, x loop (one per thread).  The manifold's order-dependent reduction is
 // reproduced as in probe_pair, with a CTA-wide exclusive scan of the
-// threads' top-4 multisets in voxel order; the candidates that enter are
-// listed in that order and replayed by one thread, which rebuilds each
-// contact from its A voxel and probe alone.
-constexpr uint32_t kReplayList = 256;
+// threads' top-4 multisets in voxel order; the threads build the contacts
+// that enter, and one thread adds them to the manifold in that order.
+constexpr uint32_t kBlockReplay = 64;
 __device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cur, uint32_t p, WarpManifold& sm) {
     __shared__ Top4 s_top[32];
-    __shared__ uint32_t s_list[kReplayList];
+    __shared__ ContactRec s_rec[kBlockReplay];
     const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
     PairInfo& pi = w.pinfo[p];
     const uint32_t ia = pi.ia, ib = pi.ib;
@@ -1268,32 +1363,25 @@ __device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cu
                 top4_insert(run, pen);
             }
         }
-        // entering candidates in (voxel, probe) order, replayed by thread 0
+        // entering candidates in (voxel, probe) order: the threads generate
+        // them at once, kBlockReplay at a time, into s_rec; thread 0 applies
+        // them in that order
         uint32_t total = 0;
         const uint32_t off = block_excl_scan((uint32_t)__popc(enter), &total);
-        for (uint32_t lo = 0; lo < total; lo += kReplayList) {
+        for (uint32_t lo = 0; lo < total; lo += kBlockReplay) {
             uint32_t e = off;
-            for (uint32_t mm = enter; mm; mm &= mm - 1u, ++e)
-                if (e >= lo && e < lo + kReplayList) s_list[e - lo] = ((uint32_t)(l - base) << 5) | (__ffs(mm) - 1);
+            for (uint32_t mm = enter; mm; mm &= mm - 1u, ++e) {
+                if (e < lo || e >= lo + kBlockReplay) continue;
+                const I3 o = probe_offset(__ffs(mm) - 1);
+                const I3 ibv{cbv.x + o.x, cbv.y + o.y, cbv.z + o.z};
+                const uint32_t vb = voxel_at(cs, cb, ibv.x, ibv.y, ibv.z);
+                const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
+                generate_contact(c, va, I3{x, y, z}, wa, vb, ibv, wb, &s_rec[e - lo]);
+            }
             __syncthreads();
             if (tid == 0) {
-                const uint32_t cnt = min(kReplayList, total - lo);
-                for (uint32_t i = 0; i < cnt; ++i) {
-                    const uint32_t li = (uint32_t)base + (s_list[i] >> 5), k = s_list[i] & 31u;
-                    const int32_t rx = pi.rmin[0] + (int32_t)(li % (uint32_t)nx);
-                    const int32_t ry = pi.rmin[1] + (int32_t)((li / (uint32_t)nx) % (uint32_t)ny);
-                    const int32_t rz = pi.rmin[2] + (int32_t)(li / ((uint32_t)nx * (uint32_t)ny));
-                    const uint32_t rva = voxel_at(cs, ca, rx, ry, rz);
-                    const F3 rwa = transform_point_n(c.pa, c.qna, voxel_to_local(c.vs_a, rx, ry, rz));
-                    const I3 rcb = local_to_voxel(c.vs_b, inverse_transform_point(c.pb, c.qb, rwa));
-                    const I3 o = probe_offset(k);
-                    const I3 ibv{rcb.x + o.x, rcb.y + o.y, rcb.z + o.z};
-                    const uint32_t vb = voxel_at(cs, cb, ibv.x, ibv.y, ibv.z);
-                    const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
-                    ContactRec rec;
-                    generate_contact(c, rva, I3{rx, ry, rz}, rwa, vb, ibv, wb, &rec);
-                    add_contact(sm, rec);
-                }
+                const uint32_t cnt = min(kBlockReplay, total - lo);
+                for (uint32_t i = 0; i < cnt; ++i) add_contact(sm, s_rec[i]);
             }
             __syncthreads();
         }
@@ -1340,8 +1428,13 @@ __device__ bool phase_probe(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
     WarpManifold& sm = warp_sm[threadIdx.x >> 5];
     // one warp replays the cache lookups, the others start detecting at once
     if (w.cfg.use_cache && g.rank() < 32u) cache_replay(w, csm);
-    // large regions first, one CTA each, then the rest one warp each
+    // large regions first, one CTA each, then the rest one warp each.  On a
+    // grid, the CTA whose warp replays the cache detects nothing: the replay
+    // is a chain of dependent lookups, and other warps on its SM slow it down
+    // more than their work is worth.
     const uint32_t nh = *(volatile uint32_t*)&w.ctr[C_NHEAVY];
+    const bool replay_cta = w.cfg.use_cache && g.nblocks() > 1u && g.block() == 0u;
+    if (replay_cta) return g.sync();
     if (nh) {
         __shared__ uint32_t s_h;
         for (;;) {
