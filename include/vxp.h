@@ -306,8 +306,8 @@ int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div);
 
 /* Narrow-phase work split: a pair whose overlap region holds at least n
  * voxels is probed by a whole CTA before the other pairs, which are probed one
- * warp each (default 768; 0: every pair by one warp).  Results do not depend
- * on it. */
+ * warp each (default 768; 0: every pair by one warp; the worlds of a batch,
+ * one CTA each, use 1024).  Results do not depend on it. */
 int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n);
 
 /* Order of the solver's sweeps (ContactSolver.solve, src/solver.zig:494-561)
@@ -379,13 +379,19 @@ int vxp_batch_last_error(const vxp_batch* b, char* buf, size_t n);
 int vxp_batch_collider_upload(vxp_batch* b, uint32_t collider_id, float voxel_size, const vxp_brick* bricks,
                               uint32_t n_bricks);
 /* (Re)starts world slot `world` with these bodies: empty contact manager and
- * brick-pair cache.  pair_capacity 0 = 16 x n (grown on demand). */
+ * brick-pair cache.  pair_capacity 0 = 16 x n (grown on demand).  A slot
+ * that held a world before reuses its device buffers (zeroed, grown when too
+ * small): no allocation, and the same results as a new slot. */
 int vxp_batch_world_set(vxp_batch* b, uint32_t world, const vxp_body* bodies, uint32_t n, uint32_t pair_capacity);
-/* Empties the slot and frees its device memory. */
+/* Empties the slot; its device memory stays with it for the next world set
+ * there (vxp_batch_world_release frees it). */
 int vxp_batch_world_clear(vxp_batch* b, uint32_t world);
+/* Empties the slot and frees its device memory (which waits for the device). */
+int vxp_batch_world_release(vxp_batch* b, uint32_t world);
 int vxp_batch_world_get(vxp_batch* b, uint32_t world, vxp_body* bodies, uint32_t n);
 int vxp_batch_world_stats(vxp_batch* b, uint32_t world, vxp_stats* out);
-/* Device bytes held by a world slot (admission accounting). */
+/* Device bytes held by a world slot, occupied or cleared (admission
+ * accounting). */
 uint64_t vxp_batch_world_bytes(vxp_batch* b, uint32_t world);
 /* Every occupied slot advances n_steps steps of dt (queued, not waited for). */
 int vxp_batch_step(vxp_batch* b, float dt, uint32_t n_steps);

@@ -111,3 +111,35 @@ def test_worlds_join_and_leave(vxp):
     got1["collider_id"] -= 5000
     assert got1.tobytes() == run_alone(vxp, scenes[3], 30, dt).tobytes()
     b.close()
+
+
+def test_reused_slot_matches_new_slot(vxp):
+    """A cleared slot keeps its device buffers: a small world set into a slot
+    that held a larger one (larger pair and body capacities, a used contact
+    manager and cache) steps exactly as the small world alone; so does one
+    set after the slot's memory was released."""
+    scenes = small_mix(vxp, [120, 20, 30], seed=11)
+    dt = np.float32(1.0 / 60.0)
+    b = vxp.VoxelWorldBatch(1, substeps=4)
+    b.load_scene(0, scenes[0], collider_offset=1000)
+    b.step(dt, 15)
+    b.synchronize()
+    held = b.world_bytes(0)
+    b.clear_world(0)
+    assert b.world_bytes(0) == held
+    b.load_scene(0, scenes[1], collider_offset=3000)
+    assert b.world_bytes(0) == held
+    b.step(dt, 25)
+    b.synchronize()
+    got = b.get_world(0)
+    got["collider_id"] -= 3000
+    assert got.tobytes() == run_alone(vxp, scenes[1], 25, dt).tobytes()
+    b.release_world(0)
+    assert b.world_bytes(0) == 0
+    b.load_scene(0, scenes[2], collider_offset=5000)
+    b.step(dt, 10)
+    b.synchronize()
+    got = b.get_world(0)
+    got["collider_id"] -= 5000
+    assert got.tobytes() == run_alone(vxp, scenes[2], 10, dt).tobytes()
+    b.close()

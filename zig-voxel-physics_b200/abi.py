@@ -233,6 +233,7 @@ SIGNATURES = {
     "vxp_batch_collider_upload": (_I, [_VP, _U32, _F, _VP, _U32]),
     "vxp_batch_world_set": (_I, [_VP, _U32, _VP, _U32, _U32]),
     "vxp_batch_world_clear": (_I, [_VP, _U32]),
+    "vxp_batch_world_release": (_I, [_VP, _U32]),
     "vxp_batch_world_get": (_I, [_VP, _U32, _VP, _U32]),
     "vxp_batch_world_stats": (_I, [_VP, _U32, _VP]),
     "vxp_batch_world_bytes": (ctypes.c_uint64, [_VP, _U32]),

@@ -454,7 +454,7 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
     s.device_pairs = 0;
     s.margin = 0.1f;
     s.solver_flow = 1;
-    s.heavy_voxels = 768;
+    s.heavy_voxels = 1024;  // batches of small worlds: one CTA per world
     s.count_bricks = 0;
     return s;
 }
@@ -463,6 +463,7 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
 // constraint arrays and scratch.
 struct WorldBuffers {
     uint32_t n_bodies = 0, body_cap = 0, pair_cap = 0, ht_cap = 0, cache_cap = 1024, dump_cap = 0, scan_blocks = 1;
+    bool live = true;  // a batch slot whose world was cleared keeps its buffers with live = false
     std::vector<uint32_t> collider_public;
     DBuf<DBody> body;
     DBuf<DBodyProp> prop;
@@ -746,6 +747,20 @@ struct WorldBuffers {
         w.ts = ts.p;
         w.dump = dump.p;
         return w;
+    }
+
+    // Every device buffer back to zero, as a new allocation is: a batch slot
+    // reused for another world starts from exactly the state of a new one.
+    cudaError_t zero_all(cudaStream_t s) {
+        cudaError_t e = cudaSuccess;
+        auto z = [&](auto& b) {
+            if (b.p && e == cudaSuccess) e = cudaMemsetAsync(b.p, 0, b.bytes(), s);
+        };
+        z(body); z(prop); z(p0); z(qn); z(aabb_mn); z(aabb_mx); z(ids); z(pcount); z(poff); z(adj_off); z(adj_cur);
+        z(bmask); z(pairs); z(n_pairs_dev); z(pinfo); z(man0); z(man1); z(ht0); z(ht1); z(frame); z(cons); z(colour);
+        z(pos_of); z(packed_pair); z(adj); z(flag); z(clist); z(cp); z(cm); z(rk); z(cfr); z(ev); z(snap); z(chunk);
+        z(colour_cnt); z(colour_cur); z(scan); z(ctr); z(cwriter); z(ts); z(cframe); z(ckey); z(cval); z(dump);
+        return e;
     }
 
     size_t device_bytes() const {
@@ -1823,8 +1838,18 @@ int vxp_batch_world_set(vxp_batch* bt, uint32_t world, const vxp_body* bodies, u
     if (!bt || world >= bt->slots.size()) return bfail(bt, VXP_ERR_ARG, "world index out of range");
     BK(cudaStreamSynchronize(bt->stream));
     auto& slot = bt->slots[world];
-    // a fresh world starts with an empty contact manager and cache
-    slot.reset(new WorldBuffers);
+    // a fresh world starts with an empty contact manager and cache; a slot
+    // that held an earlier world keeps its buffers (no allocation, no free,
+    // which would wait for the whole device) and starts from them zeroed
+    if (slot) {
+        BK(slot->zero_all(bt->stream));
+        BK(cudaStreamSynchronize(bt->stream));
+        slot->n_bodies = 0;
+        slot->collider_public.clear();
+    } else {
+        slot.reset(new WorldBuffers);
+    }
+    slot->live = true;
     if (int rc = slot->init(bt->cache_cap, 1, bt->err)) return rc;
     if (int rc = slot->set_bodies(bodies, n, bt->cols, bt->err)) return rc;
     const uint32_t want = pair_capacity ? pair_capacity : std::max<uint32_t>(1024, 16u * n);
@@ -1838,6 +1863,15 @@ int vxp_batch_world_set(vxp_batch* bt, uint32_t world, const vxp_body* bodies, u
 int vxp_batch_world_clear(vxp_batch* bt, uint32_t world) {
     if (!bt || world >= bt->slots.size()) return bfail(bt, VXP_ERR_ARG, "world index out of range");
     BK(cudaStreamSynchronize(bt->stream));
+    if (bt->slots[world]) bt->slots[world]->live = false;
+    bt->active[world] = 0;
+    bt->rebuild = true;
+    return VXP_OK;
+}
+
+int vxp_batch_world_release(vxp_batch* bt, uint32_t world) {
+    if (!bt || world >= bt->slots.size()) return bfail(bt, VXP_ERR_ARG, "world index out of range");
+    BK(cudaStreamSynchronize(bt->stream));
     bt->slots[world].reset();
     bt->active[world] = 0;
     bt->rebuild = true;
@@ -1845,13 +1879,15 @@ int vxp_batch_world_clear(vxp_batch* bt, uint32_t world) {
 }
 
 int vxp_batch_world_get(vxp_batch* bt, uint32_t world, vxp_body* bodies, uint32_t n) {
-    if (!bt || world >= bt->slots.size() || !bt->slots[world]) return bfail(bt, VXP_ERR_ARG, "no such world");
+    if (!bt || world >= bt->slots.size() || !bt->slots[world] || !bt->slots[world]->live)
+        return bfail(bt, VXP_ERR_ARG, "no such world");
     BK(cudaStreamSynchronize(bt->stream));
     return bt->slots[world]->get_bodies(bodies, n, bt->stream, bt->err);
 }
 
 int vxp_batch_world_stats(vxp_batch* bt, uint32_t world, vxp_stats* s) {
-    if (!bt || !s || world >= bt->slots.size() || !bt->slots[world]) return bfail(bt, VXP_ERR_ARG, "no such world");
+    if (!bt || !s || world >= bt->slots.size() || !bt->slots[world] || !bt->slots[world]->live)
+        return bfail(bt, VXP_ERR_ARG, "no such world");
     BK(cudaStreamSynchronize(bt->stream));
     uint32_t np = 0;
     BK(cudaMemcpy(&np, bt->slots[world]->n_pairs_dev.p, sizeof(np), cudaMemcpyDeviceToHost));

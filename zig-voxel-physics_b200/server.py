@@ -6,7 +6,9 @@ VoxelWorldBatch and advances all of them with one launch per step; a job
 that arrives while others run is admitted at the next step boundary as soon
 as a slot is free and its device memory fits the budget, and its steps then
 overlap with everyone else's on the GPU.  A finished job's final bodies are
-read back and its slot and memory released.
+read back and its slot freed; the slot keeps its device buffers for the next
+job admitted there (no allocation or free while serving), and those buffers
+stay counted against the budget.
 
 Every world's arithmetic is independent of the batch it runs in, so a job's
 result is bit-identical alone and in any mix.
@@ -64,7 +66,8 @@ class SimulationServer:
         self.max_slots = int(max_slots)
         self.budget = int(budget_bytes)
         self.clock = clock
-        self.free_slots = collections.deque(range(self.max_slots))
+        self.free_slots = list(range(self.max_slots))
+        self.held = [0] * self.max_slots  # device bytes each slot holds, running or not
         self.running: dict[int, Job] = {}
         self.waiting: collections.deque[Job] = collections.deque()
         self.finished: list[Job] = []
@@ -85,15 +88,23 @@ class SimulationServer:
                 kept.append(job)
                 continue
             need = estimate_bytes(len(job.bodies))
-            if not self.free_slots or self.used_bytes + need > self.budget:
+            if not self.free_slots:
                 kept.append(job)
                 continue
-            slot = self.free_slots.popleft()
+            # the free slot whose buffers already fit with the least to spare,
+            # else the one holding the most
+            fits = [s for s in self.free_slots if self.held[s] >= need]
+            slot = min(fits, key=lambda s: self.held[s]) if fits else max(self.free_slots, key=lambda s: self.held[s])
+            if self.used_bytes + max(0, need - self.held[slot]) > self.budget:
+                kept.append(job)
+                continue
+            self.free_slots.remove(slot)
             self.batch.set_world(slot, job.bodies)
             job.slot = slot
             job.admitted_at = now
-            job.device_bytes = max(need, self.batch.world_bytes(slot))
-            self.used_bytes += job.device_bytes
+            job.device_bytes = max(need, self.held[slot], self.batch.world_bytes(slot))
+            self.used_bytes += job.device_bytes - self.held[slot]
+            self.held[slot] = job.device_bytes
             self.running[slot] = job
         self.waiting = kept
 
@@ -103,7 +114,6 @@ class SimulationServer:
             job.result = self.batch.get_world(slot)
             job.finished_at = now
             self.batch.clear_world(slot)
-            self.used_bytes -= job.device_bytes
             self.free_slots.append(slot)
             self.finished.append(job)
 

@@ -275,7 +275,13 @@ class VoxelWorldBatch:
         self.set_world(world, bodies)
 
     def clear_world(self, world: int) -> None:
+        """Empties the slot; its device memory stays for the next world set there."""
         self._check(self.lib.vxp_batch_world_clear(self.b, int(world)))
+        self.sizes.pop(int(world), None)
+
+    def release_world(self, world: int) -> None:
+        """Empties the slot and frees its device memory."""
+        self._check(self.lib.vxp_batch_world_release(self.b, int(world)))
         self.sizes.pop(int(world), None)
 
     def get_world(self, world: int) -> np.ndarray:
