@@ -1733,19 +1733,29 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
                 const PairInfo& pi = w.pinfo[w.cons[k]];
                 uint32_t used[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 bool ready = true;
-                const uint32_t bodies[2] = {pi.ia, pi.ib};
-                for (int s = 0; s < 2 && ready; ++s) {
-                    const uint32_t b = bodies[s];
-                    if (!writable(w.prop[b])) continue;
-                    for (uint32_t e = w.adj_off[b]; e < w.adj_off[b + 1u]; ++e) {
-                        const uint32_t j = w.adj[e];
-                        if (j == k) continue;
-                        const uint32_t cj = vc[j];
+                // both bodies' neighbours as one list (the bodies the solver
+                // writes), their colours sixteen at a time, every load of a
+                // batch issued before any is used (the colours were written
+                // by other SMs in the last round: each load is a long one)
+                const bool wa = writable(w.prop[pi.ia]), wb = writable(w.prop[pi.ib]);
+                const uint32_t a0 = wa ? w.adj_off[pi.ia] : 0u, a1 = wa ? w.adj_off[pi.ia + 1u] : 0u;
+                const uint32_t b0 = wb ? w.adj_off[pi.ib] : 0u, b1 = wb ? w.adj_off[pi.ib + 1u] : 0u;
+                const uint32_t na = a1 - a0, nt = na + (b1 - b0);
+                for (uint32_t t0 = 0; t0 < nt && ready; t0 += 16u) {
+                    uint32_t jj[16], cc[16];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const uint32_t t = t0 + (uint32_t)q;
+                        jj[q] = t < nt ? w.adj[t < na ? a0 + t : b0 + (t - na)] : k;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) cc[q] = jj[q] != k ? vc[jj[q]] : 0xFFFFFFFEu;
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        if (jj[q] == k) continue;
+                        const uint32_t cj = cc[q];
                         if (cj == 0xFFFFFFFFu) {
-                            if (jp_before(j, k)) {
-                                ready = false;
-                                break;
-                            }
+                            if (jp_before(jj[q], k)) ready = false;
                         } else if (cj < 256u) {
                             used[cj >> 5] |= 1u << (cj & 31);
                         }
