@@ -514,7 +514,10 @@ template <class G>
 __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool* overflow) {
     const uint32_t N = w.n_bodies;
     const float m = w.cfg.margin;
-    for (uint32_t i = g.rank(); i < N; i += g.size()) {
+    // inflated world AABBs in id order (position s holds body ids[s]), w = 1
+    // for a static body, so that the sweep below reads them coalesced
+    for (uint32_t s = g.rank(); s < N; s += g.size()) {
+        const uint32_t i = w.ids[s].y;
         const DBody b = w.body[i];
         const F3 x = f3of(b.p);
         const Qt q = qof(b.q);
@@ -538,8 +541,8 @@ __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool*
         }
         lo = lo - F3{m, m, m};
         hi = hi + F3{m, m, m};
-        w.aabb_mn[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
-        w.aabb_mx[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
+        w.aabb_mn[s] = make_float4(lo.x, lo.y, lo.z, w.prop[i].type == 0u ? 1.f : 0.f);
+        w.aabb_mx[s] = make_float4(hi.x, hi.y, hi.z, 0.f);
     }
     if (!g.sync()) return false;
     const uint32_t lane = threadIdx.x & 31, wid = g.rank() >> 5, nw = g.size() >> 5;
@@ -555,30 +558,43 @@ __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool*
             if (g.rank() == 0) *w.n_pairs_dev = total;
             if (*overflow) return true;
         }
-        for (uint32_t s = wid; s < N; s += nw) {
-            const uint2 is = w.ids[s];
-            const float4 a0 = w.aabb_mn[is.y], a1 = w.aabb_mx[is.y];
-            const bool si = w.prop[is.y].type == 0u;
-            uint32_t o = pass ? w.poff[s] : 0u;
-            uint32_t cnt = 0;
-            for (uint32_t t0 = s + 1; t0 < N; t0 += 32u) {
-                const uint32_t t = t0 + lane;
-                bool hit = false;
-                uint2 it = make_uint2(0u, 0u);
-                if (t < N) {
-                    it = w.ids[t];
-                    if (!(si && w.prop[it.y].type == 0u)) {
-                        const float4 b0 = w.aabb_mn[it.y], b1 = w.aabb_mx[it.y];
-                        hit = a0.x <= b1.x && a1.x >= b0.x && a0.y <= b1.y && a1.y >= b0.y && a0.z <= b1.z &&
-                              a1.z >= b0.z;
+        // a warp takes rows r and N - 1 - r (about N columns in all)
+        for (uint32_t r = wid; r < (N + 1u) / 2u; r += nw) {
+            for (uint32_t h = 0; h < 2u; ++h) {
+                const uint32_t s = h ? N - 1u - r : r;
+                if (h && s == r) break;
+                const float4 a0 = w.aabb_mn[s], a1 = w.aabb_mx[s];
+                const bool si = a0.w != 0.f;
+                uint32_t o = pass ? w.poff[s] : 0u;
+                uint32_t cnt = 0;
+                auto test = [&](uint32_t t) {
+                    bool hit = false;
+                    if (t < N) {
+                        const float4 b0 = __ldg(w.aabb_mn + t), b1 = __ldg(w.aabb_mx + t);
+                        hit = !(si && b0.w != 0.f) && a0.x <= b1.x && a1.x >= b0.x && a0.y <= b1.y &&
+                              a1.y >= b0.y && a0.z <= b1.z && a1.z >= b0.z;
                     }
+                    return hit;
+                };
+                auto emit = [&](bool hit, uint32_t t) {
+                    const uint32_t mk = __ballot_sync(0xffffffffu, hit);
+                    if (pass && hit)
+                        w.pairs[o + __popc(mk & ((1u << lane) - 1u))] = make_uint2(w.ids[s].x, w.ids[t].x);
+                    o += __popc(mk);
+                    cnt += __popc(mk);
+                };
+                // four chunks of 32 columns per iteration, all tested before
+                // any is counted
+                for (uint32_t t0 = s + 1; t0 < N; t0 += 128u) {
+                    const bool h0 = test(t0 + lane), h1 = test(t0 + 32u + lane), h2 = test(t0 + 64u + lane),
+                               h3 = test(t0 + 96u + lane);
+                    emit(h0, t0 + lane);
+                    if (t0 + 32u < N) emit(h1, t0 + 32u + lane);
+                    if (t0 + 64u < N) emit(h2, t0 + 64u + lane);
+                    if (t0 + 96u < N) emit(h3, t0 + 96u + lane);
                 }
-                const uint32_t mk = __ballot_sync(0xffffffffu, hit);
-                if (pass && hit) w.pairs[o + __popc(mk & ((1u << lane) - 1u))] = make_uint2(is.x, it.x);
-                o += __popc(mk);
-                cnt += __popc(mk);
+                if (!pass && lane == 0) w.pcount[s] = cnt;
             }
-            if (!pass && lane == 0) w.pcount[s] = cnt;
         }
         if (!g.sync()) return false;
     }

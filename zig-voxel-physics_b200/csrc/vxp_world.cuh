@@ -212,7 +212,7 @@ struct WorldDev {
     float4* qn;                   // normalised rotation per body (transformPoint)
     uint2* ids;                   // (id, index) sorted by id
     // pair source
-    float4* aabb_mn;              // inflated world AABB per body
+    float4* aabb_mn;              // inflated world AABB per body (the step's broad phase: in id order)
     float4* aabb_mx;
     uint32_t* pcount;             // pairs per id-sorted row
     uint32_t* poff;               // their exclusive prefix
