@@ -456,6 +456,7 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
     s.solver_flow = 1;
     s.heavy_voxels = 1024;  // batches of small worlds: one CTA per world
     s.count_bricks = 0;
+    s.owner_groups = 1;
     return s;
 }
 
@@ -483,7 +484,8 @@ struct WorldBuffers {
     DBuf<uint32_t> ev;
     DBuf<DBody> snap;
     DBuf<uint2> chunk;
-    DBuf<uint32_t> colour_cnt, colour_cur, scan, ctr, cwriter;
+    DBuf<uint32_t> colour_cnt, colour_cur, scan, ctr, cwriter, ocnt, ocur, stat;
+    uint32_t n_static = 0;
     DBuf<unsigned long long> ts, cframe;
     DBuf<CacheKeyRec> ckey;
     DBuf<CacheValRec> cval;
@@ -497,6 +499,8 @@ struct WorldBuffers {
         ok &= frame.reserve(2) == cudaSuccess;
         ok &= colour_cnt.reserve(257) == cudaSuccess;
         ok &= colour_cur.reserve(256) == cudaSuccess;
+        ok &= ocnt.reserve(256 * kMaxOwnerGroups + 1) == cudaSuccess;
+        ok &= ocur.reserve(256 * kMaxOwnerGroups) == cudaSuccess;
         ok &= scan.reserve(blocks + 64) == cudaSuccess;
         ok &= ctr.reserve(C_NCTR) == cudaSuccess;
         ok &= ts.reserve(TS_N) == cudaSuccess;
@@ -646,6 +650,17 @@ struct WorldBuffers {
             err = "body upload failed";
             return VXP_ERR_CUDA;
         }
+        // the static bodies (never moved by a step), ascending
+        std::vector<uint32_t> st;
+        for (uint32_t i = 0; i < n; ++i)
+            if (dp[i].type == 0u) st.push_back(i);
+        if (stat.reserve(std::max<size_t>(st.size(), 1)) != cudaSuccess ||
+            (!st.empty() && cudaMemcpy(stat.p, st.data(), st.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+                                cudaSuccess)) {
+            err = "static body list upload failed";
+            return VXP_ERR_CUDA;
+        }
+        n_static = (uint32_t)st.size();
         n_bodies = n;
         return VXP_OK;
     }
@@ -733,6 +748,10 @@ struct WorldBuffers {
         w.adj_cur = adj_cur.p;
         w.colour_cnt = colour_cnt.p;
         w.colour_cur = colour_cur.p;
+        w.ocnt = ocnt.p;
+        w.ocur = ocur.p;
+        w.stat_idx = stat.p;
+        w.n_static = n_static;
         w.bmask = bmask.p;
         w.cp = cp.p;
         w.cm = cm.p;
@@ -760,6 +779,7 @@ struct WorldBuffers {
         z(bmask); z(pairs); z(n_pairs_dev); z(pinfo); z(man0); z(man1); z(ht0); z(ht1); z(frame); z(cons); z(colour);
         z(pos_of); z(packed_pair); z(adj); z(flag); z(clist); z(cp); z(cm); z(rk); z(cfr); z(ev); z(snap); z(chunk);
         z(colour_cnt); z(colour_cur); z(scan); z(ctr); z(cwriter); z(ts); z(cframe); z(ckey); z(cval); z(dump);
+        z(ocnt); z(ocur); z(stat);
         return e;
     }
 
@@ -770,7 +790,8 @@ struct WorldBuffers {
                cons.bytes() + colour.bytes() + pos_of.bytes() + packed_pair.bytes() + adj.bytes() + flag.bytes() +
                clist.bytes() + cp.bytes() + cm.bytes() + rk.bytes() + ev.bytes() + snap.bytes() + chunk.bytes() + cfr.bytes() +
                ckey.bytes() + cval.bytes() +
-               cwriter.bytes() + scan.bytes() + ctr.bytes() + ts.bytes() + dump.bytes();
+               cwriter.bytes() + scan.bytes() + ctr.bytes() + ts.bytes() + dump.bytes() + ocnt.bytes() + ocur.bytes() +
+               stat.bytes();
     }
 
     // Counters -> vxp_stats.
@@ -918,6 +939,7 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
     w.cfg.flow_smem_chunks = grid ? flow_chunks(solve_smem()) : 0u;
     w.cfg.heavy_voxels = ctx->heavy_voxels;
     w.cfg.count_bricks = ctx->count_bricks ? 1u : 0u;
+    w.cfg.owner_groups = cluster ? ctx->cluster_size : 1u;
     if (ctx->record_substeps) {
         const size_t need = (size_t)std::max(1u, ctx->cfg.substeps) * std::max(1u, ctx->w.n_bodies) * 13u;
         if (ctx->subrec.reserve(need) != cudaSuccess) return fail(ctx, VXP_ERR_OOM, "substep record buffer");

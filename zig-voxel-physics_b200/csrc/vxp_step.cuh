@@ -1650,10 +1650,16 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
         w.adj_off[i] = 0u;
         if (i < N) w.adj_cur[i] = 0u;
     }
+    const uint32_t NG = w.cfg.owner_groups > 1u ? min(w.cfg.owner_groups, kMaxOwnerGroups) : 1u;
     for (uint32_t i = g.rank(); i < 257u; i += g.size()) {
         w.colour_cnt[i] = 0u;
         if (i < 256u) w.colour_cur[i] = 0u;
     }
+    if (NG > 1u)
+        for (uint32_t i = g.rank(); i <= 256u * NG; i += g.size()) {
+            w.ocnt[i] = 0u;
+            if (i < 256u * NG) w.ocur[i] = 0u;
+        }
     // colouring round counters (3) and position-sweep min separations (16)
     // live after the per-block scan partials
     if (g.rank() < 20u) w.scan[g.nblocks() + g.rank()] = 0u;
@@ -1800,12 +1806,34 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
             if (r == 0u) break;
         }
     }
-    // 4. colour-major packing + ContactSolver.addManifold (solver.zig:449-491)
+    // 4. colour-major packing + ContactSolver.addManifold (solver.zig:449-491).
+    // With owner groups, each colour is packed group by group: group =
+    // home body mod NG, the home body being a if the solver writes it, else b
+    // (the order inside a colour does not change any result).
+    auto owner = [&](uint32_t k) -> uint32_t {
+        const PairInfo& pi = w.pinfo[w.cons[k]];
+        return (writable(w.prop[pi.ia]) ? pi.ia : pi.ib) % NG;
+    };
     for (uint32_t k = g.rank(); k < M; k += g.size()) {
         if (w.colour[k] > 255u) w.colour[k] = 255u;  // only after ERR_COLOURS
         atomicAdd(&w.colour_cnt[w.colour[k]], 1u);
+        if (NG > 1u) atomicAdd(&w.ocnt[w.colour[k] * NG + owner(k)], 1u);
     }
     if (!g.sync()) return false;
+    if (NG > 1u && g.block() == 0u) {
+        // exclusive scan of the (colour, group) counts, colour-major, by block 0
+        const uint32_t E = 256u * NG, per = (E + blockDim.x - 1u) / blockDim.x, lo = threadIdx.x * per;
+        uint32_t sum = 0;
+        for (uint32_t i = lo; i < min(E, lo + per); ++i) sum += w.ocnt[i];
+        uint32_t total = 0;
+        uint32_t run = block_excl_scan(sum, &total);
+        for (uint32_t i = lo; i < min(E, lo + per); ++i) {
+            const uint32_t v = w.ocnt[i];
+            w.ocnt[i] = run;
+            run += v;
+        }
+        if (threadIdx.x == 0) w.ocnt[E] = total;
+    }
     if (g.rank() < 32u) {
         const uint32_t lane = threadIdx.x & 31;
         uint32_t carry = 0, last = 0;
@@ -1827,7 +1855,13 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
     *ncol_out = *(volatile uint32_t*)&w.ctr[C_COLOURS];
     for (uint32_t k = g.rank(); k < M; k += g.size()) {
         const uint32_t c = w.colour[k];
-        const uint32_t pos = w.colour_cnt[c] + atomicAdd(&w.colour_cur[c], 1u);
+        uint32_t pos;
+        if (NG > 1u) {
+            const uint32_t og = c * NG + owner(k);
+            pos = w.ocnt[og] + atomicAdd(&w.ocur[og], 1u);
+        } else {
+            pos = w.colour_cnt[c] + atomicAdd(&w.colour_cur[c], 1u);
+        }
         const uint32_t p = w.cons[k];
         w.pos_of[k] = pos;
         w.packed_pair[pos] = p;
@@ -2863,12 +2897,16 @@ __device__ bool phase_solve_flow(G& g, WorldDev& w, float* fsm, uint32_t M, uint
 // phase_solve, with the state the sweeps pass from SM to SM held in the
 // cluster's shared memory instead of L2: body i lives in CTA i % C (slot
 // i / C) and is read and written by the other CTAs through distributed
-// shared memory; the manifolds of each colour are dealt round-robin to the
-// CTAs (position lo + k + C j to CTA k), and each CTA prepares and solves its
-// own manifolds with their velocity-sweep fields (CP_NVEL per point; tangent2
-// is recomputed from the normal and tangent1) in its shared memory.  The position sweeps read the fields that do not change
-// during the solve from the packed rows.  Every operation and its order per
-// body is that of phase_solve, so the results are bit-identical.
+// shared memory.  Each CTA prepares and solves its own manifolds with their
+// velocity-sweep fields (CP_NVEL per point; tangent2 is recomputed from the
+// normal and tangent1) in its shared memory: with the packing grouped by
+// owner (owner_groups == C), the manifolds of each colour whose home body it
+// holds, so that most manifold steps touch local bodies only; else the
+// colour's manifolds dealt round-robin (position lo + k + C j to CTA k).
+// Static bodies (up to kMaxStaticReplicas) are copied into every CTA.  The
+// position sweeps read the fields that do not change during the solve from
+// the packed rows.  Every operation and its order per body is that of
+// phase_solve, so the results are bit-identical.
 //
 // Returns false, before any barrier and in every block alike, when the state
 // does not fit the shared memory given (smem_bytes); the caller then runs
@@ -2880,22 +2918,29 @@ __device__ __forceinline__ T* cluster_map(T* p, uint32_t rank) {
     return reinterpret_cast<T*>(r);
 }
 
+constexpr uint32_t kMaxStaticReplicas = 32;
+
 struct ClusterSolveSmem {
     DBody* body;     // bcap records
+    DBody* rep;      // copies of the static bodies (nrep)
+    uint32_t* stat;  // their body indices, ascending
     uint4* man;      // per local slot: body a, body b, points, flags
     float2* fr;      // per local slot: friction, restitution
     float* row;      // CP_NVEL x 4 x scap floats, field-major
     uint32_t* pos;   // per local slot: packed position
     uint32_t* base;  // per colour: first local slot of this CTA; [ncol]: its slot count
-    uint32_t bcap, scap;
+    uint32_t bcap, scap, nrep;
 };
-enum : uint32_t { CM_WA = 1u, CM_WB = 2u, CM_STATIC = 4u, CM_BAD = 8u };
+// manifold flags; a body read from a static copy has its copy's index at
+// bits 8-15 (a) or 16-23 (b)
+enum : uint32_t { CM_WA = 1u, CM_WB = 2u, CM_STATIC = 4u, CM_BAD = 8u, CM_RA = 16u, CM_RB = 32u };
 
-// Bytes of the layout for bcap bodies and scap manifold slots.
-__device__ __forceinline__ size_t cluster_smem_bytes(uint32_t bcap, uint32_t scap, uint32_t ncol) {
-    return (size_t)bcap * sizeof(DBody) + (size_t)scap * (sizeof(uint4) + sizeof(float2) + sizeof(uint32_t) +
-                                                          CP_NVEL * 4u * sizeof(float)) +
-           (size_t)(ncol + 1u) * sizeof(uint32_t);
+// Bytes of the layout for bcap bodies, nrep static copies and scap manifold
+// slots.
+__device__ __forceinline__ size_t cluster_smem_bytes(uint32_t bcap, uint32_t nrep, uint32_t scap, uint32_t ncol) {
+    return (size_t)(bcap + nrep) * sizeof(DBody) +
+           (size_t)scap * (sizeof(uint4) + sizeof(float2) + sizeof(uint32_t) + CP_NVEL * 4u * sizeof(float)) +
+           (size_t)(ncol + 1u) * sizeof(uint32_t) + (size_t)kMaxStaticReplicas * sizeof(uint32_t);
 }
 
 __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, uint32_t ncol, unsigned char* smem,
@@ -2904,21 +2949,44 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     const uint32_t C = g.nblocks(), k = g.block(), t = threadIdx.x, T = blockDim.x;
     const uint32_t N = w.n_bodies;
     if (ncol > 256u || M > w.pair_cap) return false;
-    // CTA 0 holds the most slots: sum over colours of ceil(n_c / C)
+    // by owner when the packing is grouped so and the fullest CTA's share
+    // fits; else round-robin over the same positions (any order inside a
+    // colour will do), which balances the CTAs exactly
+    bool by_owner = w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
+    // this CTA's manifolds of colour c: positions [first(c), first(c) + count(c))
+    // by owner, else every C-th from lo + k
+    auto count_of = [&](uint32_t c, uint32_t cta) -> uint32_t {
+        if (by_owner) return w.ocnt[c * C + cta + 1u] - w.ocnt[c * C + cta];
+        const uint32_t n = w.colour_cnt[c + 1u] - w.colour_cnt[c];
+        return n > cta ? (n - 1u - cta) / C + 1u : 0u;
+    };
+    // the most slots any CTA holds (the same verdict in every block)
     uint32_t need = 0;
     for (uint32_t c = 0; c < ncol; ++c) {
         const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
         if (hi < lo || hi > M) return false;
-        need += (hi - lo + C - 1u) / C;
     }
     ClusterSolveSmem sm;
     sm.bcap = (N + C - 1u) / C;
+    sm.nrep = w.n_static <= kMaxStaticReplicas ? w.n_static : 0u;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        need = 0;
+        for (uint32_t cta = 0; cta < C; ++cta) {
+            uint32_t n = 0;
+            for (uint32_t c = 0; c < ncol; ++c) n += count_of(c, cta);
+            need = max(need, n);
+        }
+        if (!by_owner || cluster_smem_bytes(sm.bcap, sm.nrep, max(need, 1u), ncol) <= smem_bytes) break;
+        by_owner = false;
+    }
     sm.scap = max(need, 1u);
-    if (cluster_smem_bytes(sm.bcap, sm.scap, ncol) > smem_bytes) return false;
+    if (cluster_smem_bytes(sm.bcap, sm.nrep, sm.scap, ncol) > smem_bytes) return false;
     {
         unsigned char* p = smem;
         sm.body = reinterpret_cast<DBody*>(p);
         p += (size_t)sm.bcap * sizeof(DBody);
+        sm.rep = reinterpret_cast<DBody*>(p);
+        p += (size_t)sm.nrep * sizeof(DBody);
         sm.man = reinterpret_cast<uint4*>(p);
         p += (size_t)sm.scap * sizeof(uint4);
         sm.fr = reinterpret_cast<float2*>(p);
@@ -2928,28 +2996,45 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         sm.pos = reinterpret_cast<uint32_t*>(p);
         p += (size_t)sm.scap * sizeof(uint32_t);
         sm.base = reinterpret_cast<uint32_t*>(p);
+        p += (size_t)(ncol + 1u) * sizeof(uint32_t);
+        sm.stat = reinterpret_cast<uint32_t*>(p);
     }
     // this CTA's first slot per colour
     if (t == 0) {
         uint32_t run = 0;
         for (uint32_t c = 0; c < ncol; ++c) {
             sm.base[c] = run;
-            const uint32_t n = w.colour_cnt[c + 1u] - w.colour_cnt[c];
-            run += n > k ? (n - 1u - k) / C + 1u : 0u;
+            run += count_of(c, k);
         }
         sm.base[ncol] = run;
     }
-    // this CTA's bodies
+    // this CTA's bodies, and a copy of every static body
     for (uint32_t s = t; s < sm.bcap; s += T) {
         const uint32_t i = s * C + k;
         if (i < N) sm.body[s] = w.body[i];
     }
+    for (uint32_t r = t; r < sm.nrep; r += T) {
+        const uint32_t i = w.stat_idx[r];
+        sm.stat[r] = i < N ? i : 0xFFFFFFFFu;
+        if (i < N) sm.rep[r] = w.body[i];
+    }
     __syncthreads();
+    // the static copy holding body i, or -1
+    auto rep_of = [&](uint32_t i) -> int32_t {
+        uint32_t lo = 0, hi = sm.nrep;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sm.stat[mid] < i) lo = mid + 1u;
+            else hi = mid;
+        }
+        return lo < sm.nrep && sm.stat[lo] == i ? (int32_t)lo : -1;
+    };
     // this CTA's manifolds: bodies, flags, friction, normals and impulses
     for (uint32_t c = 0; c < ncol; ++c) {
-        const uint32_t lo = w.colour_cnt[c], b0 = sm.base[c], cnt = sm.base[c + 1u] - b0;
+        const uint32_t b0 = sm.base[c], cnt = sm.base[c + 1u] - b0;
+        const uint32_t first = by_owner ? w.ocnt[c * C + k] : w.colour_cnt[c] + k, stride = by_owner ? 1u : C;
         for (uint32_t j = t; j < cnt; j += T) {
-            const uint32_t slot = b0 + j, pos = lo + k + C * j;
+            const uint32_t slot = b0 + j, pos = first + stride * j;
             uint4 mv = w.cm[pos];
             uint32_t fl = 0u;
             if (mv.x >= N || mv.y >= N || mv.z > 4u) {
@@ -2959,6 +3044,14 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
                 const DBodyProp pa = w.prop[mv.x], pb = w.prop[mv.y];
                 fl = (writable(pa) ? CM_WA : 0u) | (writable(pb) ? CM_WB : 0u) |
                      (pa.type == 0u && pb.type == 0u ? CM_STATIC : 0u);
+                if (pa.type == 0u) {
+                    const int32_t r = rep_of(mv.x);
+                    if (r >= 0) fl |= CM_RA | ((uint32_t)r << 8);
+                }
+                if (pb.type == 0u) {
+                    const int32_t r = rep_of(mv.y);
+                    if (r >= 0) fl |= CM_RB | ((uint32_t)r << 16);
+                }
                 mv.w = fl;
             }
             sm.man[slot] = mv;
@@ -2982,14 +3075,20 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     const F3 grav{cf.gravity[0], cf.gravity[1], cf.gravity[2]};
     const bool has = M > 0u;
     const uint32_t nslot = sm.base[ncol];
-    auto body_of = [&](uint32_t i) { return cluster_map(sm.body + i / C, i % C); };
+    // body a (or b) of a manifold: its static copy here, else its home CTA's record
+    auto body_a = [&](const uint4& mv) {
+        return (mv.w & CM_RA) ? sm.rep + ((mv.w >> 8) & 0xFFu) : cluster_map(sm.body + mv.x / C, mv.x % C);
+    };
+    auto body_b = [&](const uint4& mv) {
+        return (mv.w & CM_RB) ? sm.rep + ((mv.w >> 16) & 0xFFu) : cluster_map(sm.body + mv.y / C, mv.y % C);
+    };
     // one manifold of a velocity-type sweep: 0 warm start, 1 velocity, 2 relax
     auto vel_item = [&](uint32_t slot, uint32_t kind) {
         const uint4 mv = sm.man[slot];
         if (mv.w & CM_BAD) return;
         if (kind != 0u && mv.z == 0u) return;
-        DBody* pa = body_of(mv.x);
-        DBody* pb = body_of(mv.y);
+        DBody* pa = body_a(mv);
+        DBody* pb = body_b(mv);
         const DBody A = *pa, B = *pb;
         BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
         const CPV v{sm.row + slot, sm.scap};
@@ -3034,7 +3133,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
                 const uint32_t slot = it >> 2, i = it & 3u;
                 const uint4 mv = sm.man[slot];
                 if (i >= mv.z || (mv.w & CM_BAD)) continue;
-                const DBody A = *body_of(mv.x), B = *body_of(mv.y);
+                const DBody A = *body_a(mv), B = *body_b(mv);
                 const BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
                 prepare_point_s<false>(sf, cpv_global(w, sm.pos[slot]), CPV{sm.row + slot, sm.scap}, sm.fr[slot].y, i,
                                        soft, hinv, a, qof(A.q), b, qof(B.q));
@@ -3079,8 +3178,8 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
                     const uint32_t slot = b0 + j;
                     const uint4 mv = sm.man[slot];
                     if (mv.w & (CM_BAD | CM_STATIC)) continue;
-                    DBody* pa = body_of(mv.x);
-                    DBody* pb = body_of(mv.y);
+                    DBody* pa = body_a(mv);
+                    DBody* pb = body_b(mv);
                     const DBody A = *pa, B = *pb;
                     PB a = pb_of(A.p, A.q, A.i0, A.i1, A.i2, (mv.w & CM_WA) != 0u);
                     PB b = pb_of(B.p, B.q, B.i0, B.i1, B.i2, (mv.w & CM_WB) != 0u);

@@ -152,6 +152,7 @@ struct StepCfg {
     uint32_t record_substeps;   // 1: write every body's state after each substep to subrec
     uint32_t heavy_voxels;      // overlap regions of at least this many voxels are probed by a CTA (0: never)
     uint32_t count_bricks;      // count the bricks each probed pair touches (C_BRICKS; traffic accounting only)
+    uint32_t owner_groups;      // > 1: pack each colour by owner group (home body mod this; the sweep cluster's size)
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 
@@ -240,6 +241,10 @@ struct WorldDev {
     uint32_t* adj_cur;            // fill cursors (n_bodies)
     uint32_t* colour_cnt;         // 257: counts, then offsets
     uint32_t* colour_cur;         // 256 cursors
+    uint32_t* ocnt;               // 256 x owner_groups + 1: counts, then offsets of (colour, owner) groups
+    uint32_t* ocur;               // 256 x owner_groups cursors
+    const uint32_t* stat_idx;     // the static bodies, ascending
+    uint32_t n_static;
     uint32_t* bmask;              // reference colouring: 8 words per body
     // event-ordered sweeps: per packed manifold (rank on body a, degree of a,
     // rank on body b, degree of b), ~0u for a body the solver never writes;
@@ -267,6 +272,10 @@ struct WorldDev {
         float dist_sq;
     } * dump;
 };
+
+// Owner groups the packing can sort each colour into (the largest sweep
+// cluster).
+constexpr uint32_t kMaxOwnerGroups = 16;
 
 // Packed constraint-point fields (ConstraintPoint, solver.zig:122-168).  The
 // first CP_NVEL are the ones the velocity-type sweeps (warm start, velocity,
