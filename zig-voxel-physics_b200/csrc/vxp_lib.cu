@@ -499,7 +499,7 @@ struct WorldBuffers {
         ok &= frame.reserve(2) == cudaSuccess;
         ok &= colour_cnt.reserve(257) == cudaSuccess;
         ok &= colour_cur.reserve(256) == cudaSuccess;
-        ok &= ocnt.reserve(256 * kMaxOwnerGroups + 1) == cudaSuccess;
+        ok &= ocnt.reserve(kOwnerPoints + 2 * kMaxOwnerGroups) == cudaSuccess;
         ok &= ocur.reserve(256 * kMaxOwnerGroups) == cudaSuccess;
         ok &= scan.reserve(blocks + 64) == cudaSuccess;
         ok &= ctr.reserve(C_NCTR) == cudaSuccess;

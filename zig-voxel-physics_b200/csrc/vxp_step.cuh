@@ -1655,11 +1655,13 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
         w.colour_cnt[i] = 0u;
         if (i < 256u) w.colour_cur[i] = 0u;
     }
-    if (NG > 1u)
+    if (NG > 1u) {
         for (uint32_t i = g.rank(); i <= 256u * NG; i += g.size()) {
             w.ocnt[i] = 0u;
             if (i < 256u * NG) w.ocur[i] = 0u;
         }
+        for (uint32_t i = g.rank(); i < 2u * kMaxOwnerGroups; i += g.size()) w.ocnt[kOwnerPoints + i] = 0u;
+    }
     // colouring round counters (3) and position-sweep min separations (16)
     // live after the per-block scan partials
     if (g.rank() < 20u) w.scan[g.nblocks() + g.rank()] = 0u;
@@ -1857,8 +1859,12 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
         const uint32_t c = w.colour[k];
         uint32_t pos;
         if (NG > 1u) {
-            const uint32_t og = c * NG + owner(k);
+            const uint32_t o = owner(k), og = c * NG + o;
             pos = w.ocnt[og] + atomicAdd(&w.ocur[og], 1u);
+            // points each sweep CTA would hold: by owner, and dealt round-robin
+            const uint32_t np = w.man[cur][w.cons[k]].n;
+            atomicAdd(&w.ocnt[kOwnerPoints + o], np);
+            atomicAdd(&w.ocnt[kOwnerPoints + kMaxOwnerGroups + (pos - w.colour_cnt[c]) % NG], np);
         } else {
             pos = w.colour_cnt[c] + atomicAdd(&w.colour_cur[c], 1u);
         }
@@ -2019,16 +2025,21 @@ __device__ __forceinline__ SolveFlags solve_flags(const StepCfg& c) {
     return SolveFlags{c.friction_on != 0u, c.restitution_on != 0u, c.slop, c.pos_rate, c.max_pos_corr};
 }
 
-// The constraint-point fields of one manifold: field f of point slot s is
-// b[(f * 4 + s) * st].  In global memory b = cp + position, st = pair
-// capacity; a chunk held in shared memory has b = chunk + lane, st = 32.
+// The constraint-point fields of one manifold: field f of point s is
+// b[f * sf + s * si].  In global memory b = cp + position, si = pair
+// capacity, sf = 4 si; a chunk of the event-ordered sweeps held in shared
+// memory has b = chunk + lane, si = 32, sf = 128; the cluster sweeps keep a
+// CTA's points one after another (b = rows + first point, si = 1, sf = point
+// capacity).
 struct CPV {
     float* b;
-    uint32_t st;
+    uint32_t sf, si;
 };
-__device__ __forceinline__ CPV cpv_global(const WorldDev& w, uint32_t pos) { return CPV{w.cp + pos, w.pair_cap}; }
+__device__ __forceinline__ CPV cpv_global(const WorldDev& w, uint32_t pos) {
+    return CPV{w.cp + pos, 4u * w.pair_cap, w.pair_cap};
+}
 __device__ __forceinline__ float& cpr(const CPV& v, uint32_t f, uint32_t s) {
-    return v.b[(size_t)(f * 4u + s) * v.st];
+    return v.b[(size_t)f * v.sf + (size_t)s * v.si];
 }
 __device__ __forceinline__ F3 ld3(const CPV& v, uint32_t f, uint32_t s) {
     return F3{cpr(v, f, s), cpr(v, f + 1, s), cpr(v, f + 2, s)};
@@ -2747,7 +2758,8 @@ __device__ bool flow_run(G& g, WorldDev& w, const FlowCtx& fc, float* fsm, uint3
             const uint32_t pos = ch.x + lane;
             bool valid = pos < ch.y && ch.y <= w.pair_cap;
             const uint32_t L = (threadIdx.x >> 5) + j * nwb;
-            const CPV v = L < fc.smem_chunks ? CPV{fsm + (size_t)L * kChunkFloats + lane, 32u} : cpv_global(w, pos);
+            const CPV v =
+                L < fc.smem_chunks ? CPV{fsm + (size_t)L * kChunkFloats + lane, 128u, 32u} : cpv_global(w, pos);
             uint4 cmv = make_uint4(0u, 0u, 0u, 0u), rkv = make_uint4(0xFFFFFFFFu, 0u, 0xFFFFFFFFu, 0u);
             if (valid) {
                 cmv = w.cm[pos];
@@ -2926,21 +2938,24 @@ struct ClusterSolveSmem {
     uint32_t* stat;  // their body indices, ascending
     uint4* man;      // per local slot: body a, body b, points, flags
     float2* fr;      // per local slot: friction, restitution
-    float* row;      // CP_NVEL x 4 x scap floats, field-major
+    float* row;      // CP_NVEL x pcap floats, field-major, the slots' points one after another
     uint32_t* pos;   // per local slot: packed position
+    uint32_t* po;    // per local slot: its first point in row
     uint32_t* base;  // per colour: first local slot of this CTA; [ncol]: its slot count
-    uint32_t bcap, scap, nrep;
+    uint32_t bcap, scap, pcap, nrep;
 };
 // manifold flags; a body read from a static copy has its copy's index at
 // bits 8-15 (a) or 16-23 (b)
 enum : uint32_t { CM_WA = 1u, CM_WB = 2u, CM_STATIC = 4u, CM_BAD = 8u, CM_RA = 16u, CM_RB = 32u };
 
-// Bytes of the layout for bcap bodies, nrep static copies and scap manifold
-// slots.
-__device__ __forceinline__ size_t cluster_smem_bytes(uint32_t bcap, uint32_t nrep, uint32_t scap, uint32_t ncol) {
+// Bytes of the layout for bcap bodies, nrep static copies, scap manifold
+// slots and pcap points.
+__device__ __forceinline__ size_t cluster_smem_bytes(uint32_t bcap, uint32_t nrep, uint32_t scap, uint32_t pcap,
+                                                     uint32_t ncol) {
     return (size_t)(bcap + nrep) * sizeof(DBody) +
-           (size_t)scap * (sizeof(uint4) + sizeof(float2) + sizeof(uint32_t) + CP_NVEL * 4u * sizeof(float)) +
-           (size_t)(ncol + 1u) * sizeof(uint32_t) + (size_t)kMaxStaticReplicas * sizeof(uint32_t);
+           (size_t)scap * (sizeof(uint4) + sizeof(float2) + 2u * sizeof(uint32_t)) +
+           (size_t)pcap * CP_NVEL * sizeof(float) + (size_t)(ncol + 1u) * sizeof(uint32_t) +
+           (size_t)kMaxStaticReplicas * sizeof(uint32_t);
 }
 
 __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, uint32_t ncol, unsigned char* smem,
@@ -2969,18 +2984,27 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     ClusterSolveSmem sm;
     sm.bcap = (N + C - 1u) / C;
     sm.nrep = w.n_static <= kMaxStaticReplicas ? w.n_static : 0u;
+    // points: the packing's tallies when it grouped for this cluster, else
+    // four per slot
+    const bool tallied = w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
+    uint32_t needp = 0;
     for (int attempt = 0; attempt < 2; ++attempt) {
         need = 0;
+        needp = 0;
         for (uint32_t cta = 0; cta < C; ++cta) {
             uint32_t n = 0;
             for (uint32_t c = 0; c < ncol; ++c) n += count_of(c, cta);
             need = max(need, n);
+            needp = max(needp, tallied ? w.ocnt[kOwnerPoints + (by_owner ? 0u : kMaxOwnerGroups) + cta] : 4u * n);
         }
-        if (!by_owner || cluster_smem_bytes(sm.bcap, sm.nrep, max(need, 1u), ncol) <= smem_bytes) break;
+        if (!by_owner ||
+            cluster_smem_bytes(sm.bcap, sm.nrep, max(need, 1u), max(needp, 1u), ncol) <= smem_bytes)
+            break;
         by_owner = false;
     }
     sm.scap = max(need, 1u);
-    if (cluster_smem_bytes(sm.bcap, sm.nrep, sm.scap, ncol) > smem_bytes) return false;
+    sm.pcap = max(needp, 1u);
+    if (cluster_smem_bytes(sm.bcap, sm.nrep, sm.scap, sm.pcap, ncol) > smem_bytes) return false;
     {
         unsigned char* p = smem;
         sm.body = reinterpret_cast<DBody*>(p);
@@ -2992,8 +3016,10 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         sm.fr = reinterpret_cast<float2*>(p);
         p += (size_t)sm.scap * sizeof(float2);
         sm.row = reinterpret_cast<float*>(p);
-        p += (size_t)sm.scap * CP_NVEL * 4u * sizeof(float);
+        p += (size_t)sm.pcap * CP_NVEL * sizeof(float);
         sm.pos = reinterpret_cast<uint32_t*>(p);
+        p += (size_t)sm.scap * sizeof(uint32_t);
+        sm.po = reinterpret_cast<uint32_t*>(p);
         p += (size_t)sm.scap * sizeof(uint32_t);
         sm.base = reinterpret_cast<uint32_t*>(p);
         p += (size_t)(ncol + 1u) * sizeof(uint32_t);
@@ -3057,13 +3083,40 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
             sm.man[slot] = mv;
             sm.fr[slot] = w.cfr[pos];
             sm.pos[slot] = pos;
-            const CPV vg = cpv_global(w, pos), vs{sm.row + slot, sm.scap};
-            for (uint32_t i = 0; i < mv.z; ++i) {
-                st3(vs, CP_NX, i, ld3(vg, CP_NX, i));
-                cpr(vs, CP_NI, i) = cpr(vg, CP_NI, i);
-                cpr(vs, CP_TI0, i) = cpr(vg, CP_TI0, i);
-                cpr(vs, CP_TI1, i) = cpr(vg, CP_TI1, i);
-            }
+            sm.po[slot] = mv.z;
+        }
+    }
+    __syncthreads();
+    // each slot's first point: exclusive scan of the point counts in slot order
+    const uint32_t nsl = sm.base[ncol];
+    uint32_t carry = 0;
+    for (uint32_t lo = 0; lo < nsl; lo += T) {
+        const uint32_t slot = lo + t;
+        const uint32_t v = slot < nsl ? sm.po[slot] : 0u;
+        uint32_t tile = 0;
+        const uint32_t ex = block_excl_scan(v, &tile);
+        if (slot < nsl) sm.po[slot] = carry + ex;
+        carry += tile;
+    }
+    const bool points_fit = carry <= sm.pcap;  // the same in every thread of this block
+    if (!points_fit && t == 0) atomicOr(&w.ctr[C_ERROR], ERR_BOUNDS);
+    __syncthreads();
+    for (uint32_t slot = t; slot < nsl; slot += T) {
+        uint4 mv = sm.man[slot];
+        if (!points_fit) {
+            // never with the packing's own tallies; skip every manifold here
+            // rather than write past the rows
+            mv.w |= CM_BAD;
+            mv.z = 0u;
+            sm.man[slot] = mv;
+            continue;
+        }
+        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + sm.po[slot], sm.pcap, 1u};
+        for (uint32_t i = 0; i < mv.z; ++i) {
+            st3(vs, CP_NX, i, ld3(vg, CP_NX, i));
+            cpr(vs, CP_NI, i) = cpr(vg, CP_NI, i);
+            cpr(vs, CP_TI0, i) = cpr(vg, CP_TI0, i);
+            cpr(vs, CP_TI1, i) = cpr(vg, CP_TI1, i);
         }
     }
     g.sync();  // every block's bodies are in place (and every block has started)
@@ -3091,7 +3144,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         DBody* pb = body_b(mv);
         const DBody A = *pa, B = *pb;
         BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
-        const CPV v{sm.row + slot, sm.scap};
+        const CPV v{sm.row + sm.po[slot], sm.pcap, 1u};
         if (kind == 0u)
             warm_points<false>(v, mv.z, cf.warm_scale, a, b, sf.friction);
         else
@@ -3135,7 +3188,8 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
                 if (i >= mv.z || (mv.w & CM_BAD)) continue;
                 const DBody A = *body_a(mv), B = *body_b(mv);
                 const BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
-                prepare_point_s<false>(sf, cpv_global(w, sm.pos[slot]), CPV{sm.row + slot, sm.scap}, sm.fr[slot].y, i,
+                prepare_point_s<false>(sf, cpv_global(w, sm.pos[slot]), CPV{sm.row + sm.po[slot], sm.pcap, 1u},
+                                       sm.fr[slot].y, i,
                                        soft, hinv, a, qof(A.q), b, qof(B.q));
             }
             g.sync();
@@ -3210,7 +3264,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     }
     for (uint32_t slot = t; slot < nslot; slot += T) {
         const uint4 mv = sm.man[slot];
-        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + slot, sm.scap};
+        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + sm.po[slot], sm.pcap, 1u};
         for (uint32_t i = 0; i < mv.z; ++i) {
             cpr(vg, CP_NM, i) = cpr(vs, CP_NM, i);
             cpr(vg, CP_TM0, i) = cpr(vs, CP_TM0, i);

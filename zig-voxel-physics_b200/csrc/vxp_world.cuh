@@ -241,7 +241,7 @@ struct WorldDev {
     uint32_t* adj_cur;            // fill cursors (n_bodies)
     uint32_t* colour_cnt;         // 257: counts, then offsets
     uint32_t* colour_cur;         // 256 cursors
-    uint32_t* ocnt;               // 256 x owner_groups + 1: counts, then offsets of (colour, owner) groups
+    uint32_t* ocnt;               // 256 x owner_groups + 1: counts, then offsets of (colour, owner) groups; points at kOwnerPoints
     uint32_t* ocur;               // 256 x owner_groups cursors
     const uint32_t* stat_idx;     // the static bodies, ascending
     uint32_t n_static;
@@ -276,6 +276,9 @@ struct WorldDev {
 // Owner groups the packing can sort each colour into (the largest sweep
 // cluster).
 constexpr uint32_t kMaxOwnerGroups = 16;
+// After the (colour, owner) offsets in ocnt: the points each sweep CTA holds
+// by owner (kMaxOwnerGroups), then dealt round-robin (kMaxOwnerGroups).
+constexpr uint32_t kOwnerPoints = 256u * kMaxOwnerGroups + 1u;
 
 // Packed constraint-point fields (ConstraintPoint, solver.zig:122-168).  The
 // first CP_NVEL are the ones the velocity-type sweeps (warm start, velocity,
