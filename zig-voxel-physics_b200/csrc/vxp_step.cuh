@@ -2028,9 +2028,9 @@ __device__ __forceinline__ SolveFlags solve_flags(const StepCfg& c) {
 // The constraint-point fields of one manifold: field f of point s is
 // b[f * sf + s * si].  In global memory b = cp + position, si = pair
 // capacity, sf = 4 si; a chunk of the event-ordered sweeps held in shared
-// memory has b = chunk + lane, si = 32, sf = 128; the cluster sweeps keep a
-// CTA's points one after another (b = rows + first point, si = 1, sf = point
-// capacity).
+// memory has b = chunk + lane, si = 32, sf = 128; the cluster sweeps keep
+// each point's fields together and a CTA's points one after another (b =
+// rows + CP_NVEL x first point, sf = 1, si = CP_NVEL).
 struct CPV {
     float* b;
     uint32_t sf, si;
@@ -2286,6 +2286,104 @@ __device__ void velocity_points_near(bool friction, const CPV v, uint32_t n, flo
         cpr(v, CP_NI, i) = ni;
         cpr(v, CP_TI0, i) = ti0;
         cpr(v, CP_TI1, i) = ti1;
+    }
+}
+// The velocity-sweep fields of one point held contiguously (CP_NVEL floats,
+// 8-byte aligned, the cluster sweeps' rows in shared memory): eleven 8-byte
+// loads from one base address instead of one load and one address per field.
+static_assert(CP_NX == 0 && CP_PX == 3 && CP_RAX == 6 && CP_RBX == 9 && CP_T1X == 12 && CP_NM == 15 &&
+                  CP_TM0 == 16 && CP_TM1 == 17 && CP_BIAS == 18 && CP_NI == 19 && CP_TI0 == 20 && CP_TI1 == 21 &&
+                  CP_NVEL == 22,
+              "contiguous point rows pair the fields as (NX NY) (NZ PX) (PY PZ) ... (TI0 TI1)");
+__device__ __forceinline__ PtV load_pt_row(const float* r, bool friction) {
+    const float2* q = reinterpret_cast<const float2*>(r);
+    const float2 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6], q7 = q[7], q8 = q[8],
+                 q9 = q[9], q10 = q[10];
+    PtV c;
+    c.n = F3{q0.x, q0.y, q1.x};
+    c.pt = F3{q1.y, q2.x, q2.y};
+    c.ra = F3{q3.x, q3.y, q4.x};
+    c.rb = F3{q4.y, q5.x, q5.y};
+    // tangents as point_tangents forms them
+    if (friction) {
+        c.t1 = F3{q6.x, q6.y, q7.x};
+        c.t2 = cross3(c.n, c.t1);
+    } else {
+        c.t1 = F3{0.f, 0.f, 0.f};
+        c.t2 = F3{0.f, 0.f, 0.f};
+    }
+    c.nm = q7.y;
+    c.tm0 = q8.x;
+    c.tm1 = q8.y;
+    c.bias = q9.x;
+    c.ni = q9.y;
+    c.ti0 = q10.x;
+    c.ti1 = q10.y;
+    return c;
+}
+// warm_points and velocity_points_near over contiguous point rows (rows =
+// the manifold's first point); the same operations in the same order.
+__device__ __forceinline__ void warm_points_rows(float* rows, uint32_t n, float scale, BV& a, BV& b,
+                                                 bool friction) {
+    for (uint32_t i = 0; i < n; ++i) {
+        float* r = rows + (size_t)i * CP_NVEL;
+        const PtV c = load_pt_row(r, friction);
+        const float sn = c.ni * scale;
+        const float s1 = c.ti0 * scale;
+        const float s2 = c.ti1 * scale;
+        const F3 imp = (c.n * sn + c.t1 * s1) + c.t2 * s2;
+        apply_impulse(a, -imp, c.ra);
+        apply_impulse(b, imp, c.rb);
+        r[CP_NI] = sn;
+        *reinterpret_cast<float2*>(r + CP_TI0) = make_float2(s1, s2);
+    }
+}
+__device__ __forceinline__ void velocity_points_rows(bool friction, float* rows, uint32_t n, float fr,
+                                                     const Soft& soft, bool use_bias, BV& a, BV& b) {
+    for (uint32_t i = 0; i < n; ++i) {
+        float* r = rows + (size_t)i * CP_NVEL;
+        const PtV c = load_pt_row(r, friction);
+        const F3 rv = point_vel(b, c.pt) - point_vel(a, c.pt);
+        const float vn = dot3(rv, c.n);
+        float imp;
+        if (use_bias)
+            imp = -soft.mass_coeff * c.nm * (vn + c.bias) - soft.impulse_coeff * c.ni;
+        else
+            imp = -c.nm * vn;
+        const float nn = fmaxf(c.ni + imp, 0.0f);
+        imp = nn - c.ni;
+        const float ni = nn;
+        const F3 P = c.n * imp;
+        apply_impulse(a, -P, c.ra);
+        apply_impulse(b, P, c.rb);
+        float ti0 = c.ti0, ti1 = c.ti1;
+        if (friction && fr > 0.0f) {
+            const float mf = fr * ni;
+            {
+                const F3 rv1 = point_vel(b, c.pt) - point_vel(a, c.pt);
+                const float vt1 = dot3(rv1, c.t1);
+                float f1 = -c.tm0 * vt1;
+                const float o1 = ti0;
+                ti0 = clampf_ref(o1 + f1, -mf, mf);
+                f1 = ti0 - o1;
+                const F3 I1 = c.t1 * f1;
+                apply_impulse(a, -I1, c.ra);
+                apply_impulse(b, I1, c.rb);
+            }
+            {
+                const F3 rv2 = point_vel(b, c.pt) - point_vel(a, c.pt);
+                const float vt2 = dot3(rv2, c.t2);
+                float f2 = -c.tm1 * vt2;
+                const float o2 = ti1;
+                ti1 = clampf_ref(o2 + f2, -mf, mf);
+                f2 = ti1 - o2;
+                const F3 I2 = c.t2 * f2;
+                apply_impulse(a, -I2, c.ra);
+                apply_impulse(b, I2, c.rb);
+            }
+        }
+        r[CP_NI] = ni;
+        *reinterpret_cast<float2*>(r + CP_TI0) = make_float2(ti0, ti1);
     }
 }
 __device__ void velocity_manifold(WorldDev& w, uint32_t pos, const Soft& soft, bool use_bias) {
@@ -2938,7 +3036,7 @@ struct ClusterSolveSmem {
     uint32_t* stat;  // their body indices, ascending
     uint4* man;      // per local slot: body a, body b, points, flags
     float2* fr;      // per local slot: friction, restitution
-    float* row;      // CP_NVEL x pcap floats, field-major, the slots' points one after another
+    float* row;      // pcap x CP_NVEL floats, point-major, the slots' points one after another
     uint32_t* pos;   // per local slot: packed position
     uint32_t* po;    // per local slot: its first point in row
     uint32_t* base;  // per colour: first local slot of this CTA; [ncol]: its slot count
@@ -3111,7 +3209,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
             sm.man[slot] = mv;
             continue;
         }
-        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + sm.po[slot], sm.pcap, 1u};
+        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + (size_t)sm.po[slot] * CP_NVEL, 1u, CP_NVEL};
         for (uint32_t i = 0; i < mv.z; ++i) {
             st3(vs, CP_NX, i, ld3(vg, CP_NX, i));
             cpr(vs, CP_NI, i) = cpr(vg, CP_NI, i);
@@ -3128,12 +3226,17 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     const F3 grav{cf.gravity[0], cf.gravity[1], cf.gravity[2]};
     const bool has = M > 0u;
     const uint32_t nslot = sm.base[ncol];
+    // body i's home CTA and its slot there (shift and mask for the usual
+    // power-of-two cluster)
+    const uint32_t csh = (C & (C - 1u)) == 0u ? (uint32_t)(__ffs(C) - 1) : 32u;
+    auto home = [&](uint32_t i) { return csh < 32u ? i & (C - 1u) : i % C; };
+    auto home_slot = [&](uint32_t i) { return csh < 32u ? i >> csh : i / C; };
     // body a (or b) of a manifold: its static copy here, else its home CTA's record
     auto body_a = [&](const uint4& mv) {
-        return (mv.w & CM_RA) ? sm.rep + ((mv.w >> 8) & 0xFFu) : cluster_map(sm.body + mv.x / C, mv.x % C);
+        return (mv.w & CM_RA) ? sm.rep + ((mv.w >> 8) & 0xFFu) : cluster_map(sm.body + home_slot(mv.x), home(mv.x));
     };
     auto body_b = [&](const uint4& mv) {
-        return (mv.w & CM_RB) ? sm.rep + ((mv.w >> 16) & 0xFFu) : cluster_map(sm.body + mv.y / C, mv.y % C);
+        return (mv.w & CM_RB) ? sm.rep + ((mv.w >> 16) & 0xFFu) : cluster_map(sm.body + home_slot(mv.y), home(mv.y));
     };
     // one manifold of a velocity-type sweep: 0 warm start, 1 velocity, 2 relax
     auto vel_item = [&](uint32_t slot, uint32_t kind) {
@@ -3144,12 +3247,12 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         DBody* pb = body_b(mv);
         const DBody A = *pa, B = *pb;
         BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
-        const CPV v{sm.row + sm.po[slot], sm.pcap, 1u};
+        float* rows = sm.row + (size_t)sm.po[slot] * CP_NVEL;
         if (kind == 0u)
-            warm_points<false>(v, mv.z, cf.warm_scale, a, b, sf.friction);
+            warm_points_rows(rows, mv.z, cf.warm_scale, a, b, sf.friction);
         else
-            velocity_points_near<false>(sf.friction, v, mv.z, sm.fr[slot].x, kind == 1u ? soft : hard, kind == 1u,
-                                        a, b);
+            velocity_points_rows(sf.friction, rows, mv.z, sm.fr[slot].x, kind == 1u ? soft : hard, kind == 1u, a,
+                                 b);
         if (a.wr) {
             pa->v = make_float4(a.v.x, a.v.y, a.v.z, 0.f);
             pa->w = make_float4(a.w.x, a.w.y, a.w.z, 0.f);
@@ -3188,7 +3291,8 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
                 if (i >= mv.z || (mv.w & CM_BAD)) continue;
                 const DBody A = *body_a(mv), B = *body_b(mv);
                 const BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
-                prepare_point_s<false>(sf, cpv_global(w, sm.pos[slot]), CPV{sm.row + sm.po[slot], sm.pcap, 1u},
+                prepare_point_s<false>(sf, cpv_global(w, sm.pos[slot]),
+                                       CPV{sm.row + (size_t)sm.po[slot] * CP_NVEL, 1u, CP_NVEL},
                                        sm.fr[slot].y, i,
                                        soft, hinv, a, qof(A.q), b, qof(B.q));
             }
@@ -3264,7 +3368,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     }
     for (uint32_t slot = t; slot < nslot; slot += T) {
         const uint4 mv = sm.man[slot];
-        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + sm.po[slot], sm.pcap, 1u};
+        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + (size_t)sm.po[slot] * CP_NVEL, 1u, CP_NVEL};
         for (uint32_t i = 0; i < mv.z; ++i) {
             cpr(vg, CP_NM, i) = cpr(vs, CP_NM, i);
             cpr(vg, CP_TM0, i) = cpr(vs, CP_TM0, i);
