@@ -1038,12 +1038,22 @@ __device__ __forceinline__ void probe_neighbourhood(WorldDev& w, const ColliderS
     const int32_t lx = clip_lo(cb.min_bound[0], cbv.x), hx = clip_hi(cb.max_bound[0], cbv.x);
     const int32_t ly = clip_lo(cb.min_bound[1], cbv.y), hy = clip_hi(cb.max_bound[1], cbv.y);
     const int32_t lz = clip_lo(cb.min_bound[2], cbv.z), hz = clip_hi(cb.max_bound[2], cbv.z);
+    if (lx > hx || ly > hy || lz > hz) return;
+    // the brick holding the centre voxel (every probe is inside B's voxel
+    // bounds, so inside its brick grid): probes in the same brick read their
+    // byte at a fixed offset from the centre's, the others look their brick up
+    const int32_t cx = cbv.x & 7, cy = cbv.y & 7, cz = cbv.z & 7;
+    const int32_t cslot = brick_slot(cs, cb, cbv.x >> 3, cbv.y >> 3, cbv.z >> 3);
+    const uint8_t* cvox = cs.vox + (size_t)(cb.brick_off + (uint32_t)max(cslot, 0)) * 512u +
+                          (uint32_t)(cx + 8 * cy + 64 * cz);
     for (int32_t dz = lz; dz <= hz; ++dz)
         for (int32_t dy = ly; dy <= hy; ++dy)
             for (int32_t dx = lx; dx <= hx; ++dx) {
                 const uint32_t k = (uint32_t)((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1));
                 const int32_t bx = cbv.x + dx, by = cbv.y + dy, bz = cbv.z + dz;
-                const uint32_t vb = voxel_at(cs, cb, bx, by, bz);
+                const bool same = (uint32_t)(cx + dx) < 8u && (uint32_t)(cy + dy) < 8u && (uint32_t)(cz + dz) < 8u;
+                const uint32_t vb = same ? (cslot >= 0 ? (uint32_t)__ldg(cvox + (dx + 8 * dy + 64 * dz)) : 0u)
+                                         : voxel_at(cs, cb, bx, by, bz);
                 const uint32_t tb = vtype(vb);
                 if (tb == kEmpty) continue;
                 ++*checked;
