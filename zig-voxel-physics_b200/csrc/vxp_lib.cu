@@ -307,7 +307,11 @@ struct ColliderStore {
     DBuf<DCollider> d_col;
     DBuf<int32_t> d_grid;
     DBuf<uint8_t> d_vox;
+    DBuf<uint4> d_nb;
     uint32_t n_dev = 0;
+    // neighbourhood-mask tables: colliders with at most kNbMaxCentres probe
+    // centres get one, while the pool stays within kNbMaxTotal entries
+    static constexpr uint64_t kNbMaxCentres = 1ull << 23, kNbMaxTotal = 1ull << 25;
 
     int upload(uint32_t id, float vs, const vxp_brick* bricks, uint32_t n, std::string& err) {
         if (!bricks && n) {
@@ -354,6 +358,7 @@ struct ColliderStore {
         std::vector<int32_t> grid;
         std::vector<uint8_t> vox;
         uint32_t brick_total = 0;
+        uint64_t nb_total = 0;
         for (size_t ci = 0; ci < colliders.size(); ++ci) {
             const HostCollider& h = colliders[ci];
             DCollider& d = dc[ci];
@@ -403,6 +408,14 @@ struct ColliderStore {
                     }
             vox.insert(vox.end(), h.vox.begin(), h.vox.end());
             brick_total += (uint32_t)nb;
+            uint64_t centres = 1;
+            for (int k = 0; k < 3; ++k) centres *= (uint64_t)((int64_t)h.max_bound[k] - h.min_bound[k] + 2);
+            if (centres <= kNbMaxCentres && nb_total + centres <= kNbMaxTotal) {
+                d.nb_off = (uint32_t)nb_total;
+                nb_total += centres;
+            } else {
+                d.nb_off = kNoTable;
+            }
         }
         if (d_col.reserve(dc.size()) != cudaSuccess || d_grid.reserve(grid.size()) != cudaSuccess ||
             d_vox.reserve(vox.size()) != cudaSuccess) {
@@ -418,10 +431,22 @@ struct ColliderStore {
             return VXP_ERR_CUDA;
         }
         n_dev = (uint32_t)dc.size();
+        if (nb_total) {
+            if (d_nb.reserve(nb_total) != cudaSuccess) {
+                err = "collider upload: device allocation failed";
+                return VXP_ERR_OOM;
+            }
+            const dim3 grid_dims(64, std::min<uint32_t>(n_dev, 65535u));
+            k_nbhd_build<<<grid_dims, 256>>>(set(), d_nb.p);
+            if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(0) != cudaSuccess) {
+                err = "collider upload: neighbourhood tables failed";
+                return VXP_ERR_CUDA;
+            }
+        }
         dirty = false;
         return VXP_OK;
     }
-    ColliderSet set() const { return ColliderSet{d_col.p, d_grid.p, d_vox.p, n_dev}; }
+    ColliderSet set() const { return ColliderSet{d_col.p, d_grid.p, d_vox.p, n_dev, d_nb.p}; }
 };
 
 StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) {

@@ -221,6 +221,7 @@ struct ColliderSet {
     const int32_t* grid;
     const uint8_t* vox;
     uint32_t n;
+    const uint4* nb;  // neighbourhood masks (DCollider::nb_off)
 };
 
 __device__ __forceinline__ uint32_t voxel_at(const ColliderSet& cs, const DCollider& c, int32_t x, int32_t y,
@@ -233,6 +234,36 @@ __device__ __forceinline__ uint32_t voxel_at(const ColliderSet& cs, const DColli
     if (slot < 0) return 0u;
     return (uint32_t)__ldg(&cs.vox[(size_t)(c.brick_off + (uint32_t)slot) * 512u + (uint32_t)((x & 7) + 8 * (y & 7) +
                                                                                                  64 * (z & 7))]);
+}
+// The neighbourhood masks of collider ci's probe centres (DCollider::nb_off):
+// one thread per centre, the same 27 lookups and clipping as a probe.
+__global__ void k_nbhd_build(ColliderSet cs, uint4* nb) {
+    for (uint32_t ci = blockIdx.y; ci < cs.n; ci += gridDim.y) {
+        const DCollider& c = cs.c[ci];
+        if (c.nb_off == kNoTable) continue;
+        const uint32_t ex = (uint32_t)(c.max_bound[0] - c.min_bound[0]) + 2u,
+                       ey = (uint32_t)(c.max_bound[1] - c.min_bound[1]) + 2u,
+                       ez = (uint32_t)(c.max_bound[2] - c.min_bound[2]) + 2u;
+        const uint32_t total = ex * ey * ez;
+        for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+            const int32_t x = c.min_bound[0] - 1 + (int32_t)(e % ex), y = c.min_bound[1] - 1 + (int32_t)((e / ex) % ey),
+                          z = c.min_bound[2] - 1 + (int32_t)(e / (ex * ey));
+            uint32_t ne = 0u, co = 0u, ec = 0u, in = 0u;
+            for (uint32_t k = 0; k < 27u; ++k) {
+                const int32_t bx = x + (int32_t)(k % 3u) - 1, by = y + (int32_t)((k / 3u) % 3u) - 1,
+                              bz = z + (int32_t)(k / 9u) - 1;
+                if (bx < c.min_bound[0] || bx >= c.max_bound[0] || by < c.min_bound[1] || by >= c.max_bound[1] ||
+                    bz < c.min_bound[2] || bz >= c.max_bound[2])
+                    continue;
+                const uint32_t tb = vtype(voxel_at(cs, c, bx, by, bz));
+                ne |= (uint32_t)(tb != kEmpty) << k;
+                co |= (uint32_t)(tb == kCorner) << k;
+                ec |= (uint32_t)(tb == kCorner || tb == kEdge) << k;
+                in |= (uint32_t)(tb == kInside) << k;
+            }
+            nb[c.nb_off + e] = make_uint4(ne, co, ec, in);
+        }
+    }
 }
 // Slot of the brick at brick coordinates (bx, by, bz), or -1.
 __device__ __forceinline__ int32_t brick_slot(const ColliderSet& cs, const DCollider& c, int32_t bx, int32_t by,
@@ -1035,6 +1066,47 @@ __device__ __forceinline__ void probe_neighbourhood(WorldDev& w, const ColliderS
                                                     uint32_t ta, int32_t x, int32_t y, int32_t z, F3 wa, I3 cbv,
                                                     uint32_t* mask, Top4* t, uint32_t* checked) {
     const DCollider& cb = *c.cb;
+    if (cb.nb_off != kNoTable) {
+        // one lookup gives the non-empty probes (counted as checked) and those
+        // passing type_filter(ta, tb) (ta is never empty here); only the
+        // latter are transformed and distance-tested, in probe order.  A
+        // centre outside [min_bound - 1, max_bound] has no neighbour in bounds.
+        const uint32_t ex = (uint32_t)(cb.max_bound[0] - cb.min_bound[0]) + 2u,
+                       ey = (uint32_t)(cb.max_bound[1] - cb.min_bound[1]) + 2u,
+                       ez = (uint32_t)(cb.max_bound[2] - cb.min_bound[2]) + 2u;
+        const uint32_t tx = (uint32_t)cbv.x - ((uint32_t)cb.min_bound[0] - 1u),
+                       ty = (uint32_t)cbv.y - ((uint32_t)cb.min_bound[1] - 1u),
+                       tz = (uint32_t)cbv.z - ((uint32_t)cb.min_bound[2] - 1u);
+        if (tx >= ex || ty >= ey || tz >= ez) return;
+        const uint4 nm = __ldg(cs.nb + cb.nb_off + (tx + ex * (ty + ey * tz)));
+        *checked += (uint32_t)__popc(nm.x);
+        const uint32_t ps = ta == kCorner ? nm.x : (ta == kEdge ? nm.z : nm.y);
+        for (uint32_t m = ps; m; m &= m - 1u) {
+            const uint32_t k = __ffs(m) - 1;
+            const I3 o = probe_offset(k);
+            const int32_t bx = cbv.x + o.x, by = cbv.y + o.y, bz = cbv.z + o.z;
+            const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, bx, by, bz));
+            const F3 diff = wb - wa;
+            const float d2 = lensq3(diff);
+            const bool pass = d2 < c.spec;
+            if (w.cfg.dump_candidates) {
+                const uint32_t slot = atomicAdd(&w.ctr[C_DUMP_N], 1u);
+                if (slot < w.dump_cap) {
+                    WorldDev::Cand& r = w.dump[slot];
+                    r.pair_index = p;
+                    r.a[0] = x; r.a[1] = y; r.a[2] = z;
+                    r.b[0] = bx; r.b[1] = by; r.b[2] = bz;
+                    r.passed = pass ? 1u : 0u;
+                    r.dist_sq = d2;
+                }
+            }
+            if (pass) {
+                *mask |= 1u << k;
+                top4_insert(*t, cand_pen(c.vs_a, ta, ((nm.w >> k) & 1u) ? (uint32_t)kInside : (uint32_t)kCorner, d2));
+            }
+        }
+        return;
+    }
     const int32_t lx = clip_lo(cb.min_bound[0], cbv.x), hx = clip_hi(cb.max_bound[0], cbv.x);
     const int32_t ly = clip_lo(cb.min_bound[1], cbv.y), hy = clip_hi(cb.max_bound[1], cbv.y);
     const int32_t lz = clip_lo(cb.min_bound[2], cbv.z), hz = clip_hi(cb.max_bound[2], cbv.z);

@@ -42,7 +42,14 @@ struct DCollider {
     uint32_t brick_off;                   // first brick in the voxel pool
     uint32_t n_bricks;
     uint32_t solid_count;
+    // Neighbourhood masks (kNoTable: none): for every probe centre c in
+    // [min_bound - 1, max_bound] per axis (x fastest), a uint4 of 27-bit masks
+    // over the centre's 3 x 3 x 3 neighbours inside [min_bound, max_bound)
+    // (bit dz*9 + dy*3 + dx, offsets from -1): non-empty, corner, corner or
+    // edge, inside.  Built once from the voxels when the colliders upload.
+    uint32_t nb_off;
 };
+constexpr uint32_t kNoTable = 0xFFFFFFFFu;
 
 // Solver / narrow-phase state of one body (BodyState, solver.zig:203-229).
 struct __align__(16) DBody {
