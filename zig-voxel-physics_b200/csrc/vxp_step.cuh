@@ -1152,44 +1152,82 @@ __device__ __forceinline__ void probe_neighbourhood(WorldDev& w, const ColliderS
             }
 }
 
-// Entering candidates a warp generates at once before lane 0 applies them.
-constexpr uint32_t kWarpReplay = 8;
+// A candidate entering the manifold during detection: penetration, feature
+// id, and where it came from (A voxel li of the region in loop order, probe
+// k).  Its contact is built only if it is still in the manifold when the pair
+// ends: a contact's fields are a function of (li, k), and the impulses of
+// every contact added during detection are zero.
+struct CandRec {
+    unsigned long long fid;
+    float pen;
+    uint32_t li, k, _pad;
+};
+
+// Entering candidates a warp lists at once before lane 0 applies them.
+constexpr uint32_t kWarpReplay = 16;
 
 // Per-warp shared state of phase_probe.
 struct WarpManifold {
-    ContactRec c[4];
-    ContactRec list[kWarpReplay];
+    ContactRec c[4];              // the pair's contacts, built when it ends
+    CandRec k[4];                 // the manifold during detection
+    CandRec list[kWarpReplay];
     float pens[4];
     uint32_t n;
     uint32_t pad[3];
 };
 
-// ContactManifold.addContact (narrow_phase.zig:451-481), executed by one lane.
-__device__ __forceinline__ void add_contact(WarpManifold& m, const ContactRec& k) {
+// ContactManifold.addContact (narrow_phase.zig:451-481) on candidate
+// records, executed by one lane: a contact with the same feature id is
+// replaced (keeping its impulses, all zero here), else appended while fewer
+// than four, else the first contact of least penetration below the new one
+// is replaced.
+__device__ __forceinline__ void add_cand(WarpManifold& m, const CandRec& r) {
     for (uint32_t i = 0; i < m.n; ++i) {
-        if (m.c[i].feature_id == k.feature_id) {
-            const float ni = m.c[i].normal_impulse, t0 = m.c[i].tangent_impulse[0], t1 = m.c[i].tangent_impulse[1];
-            m.c[i] = k;
-            m.c[i].normal_impulse = ni;
-            m.c[i].tangent_impulse[0] = t0;
-            m.c[i].tangent_impulse[1] = t1;
+        if (m.k[i].fid == r.fid) {
+            m.k[i] = r;
             return;
         }
     }
     if (m.n < 4u) {
-        m.c[m.n] = k;
+        m.k[m.n] = r;
         m.n += 1u;
         return;
     }
-    float mp = k.penetration;
+    float mp = r.pen;
     int mi = -1;
     for (uint32_t i = 0; i < m.n; ++i) {
-        if (m.c[i].penetration < mp) {
-            mp = m.c[i].penetration;
+        if (m.k[i].pen < mp) {
+            mp = m.k[i].pen;
             mi = (int)i;
         }
     }
-    if (mi >= 0) m.c[mi] = k;
+    if (mi >= 0) m.k[mi] = r;
+}
+// The manifold's penetration multiset (at most four finite values, so every
+// insert lands), by one lane, into m.pens.
+__device__ __forceinline__ void cand_pens(WarpManifold& m) {
+    Top4 s = top4_empty();
+    for (uint32_t i = 0; i < m.n; ++i) top4_insert(s, m.k[i].pen);
+    m.pens[0] = s.v[0];
+    m.pens[1] = s.v[1];
+    m.pens[2] = s.v[2];
+    m.pens[3] = s.v[3];
+}
+// generateContact for candidate r of the pair probed with c over the region
+// starting at rmin, nx x ny voxels per z layer: the same lookups and
+// transforms as the detection loop.
+__device__ void build_contact(const ColliderSet& cs, const ProbeCtx& c, const int32_t* rmin, uint32_t nx,
+                              uint32_t ny, const CandRec& r, ContactRec* out) {
+    const int32_t x = rmin[0] + (int32_t)(r.li % nx), y = rmin[1] + (int32_t)((r.li / nx) % ny),
+                  z = rmin[2] + (int32_t)(r.li / (nx * ny));
+    const uint32_t va = voxel_at(cs, *c.ca, x, y, z);
+    const F3 wa = transform_point_n(c.pa, c.qna, voxel_to_local(c.vs_a, x, y, z));
+    const I3 cbv = local_to_voxel(c.vs_b, inverse_transform_point(c.pb, c.qb, wa));
+    const I3 o = probe_offset(r.k);
+    const I3 ibv{cbv.x + o.x, cbv.y + o.y, cbv.z + o.z};
+    const uint32_t vb = voxel_at(cs, *c.cb, ibv.x, ibv.y, ibv.z);
+    const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
+    generate_contact(c, va, I3{x, y, z}, wa, vb, ibv, wb, out);
 }
 
 // One warp runs detectVoxelCollisions for pair p.  The inclusive z, y, x loop
@@ -1290,8 +1328,8 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
             }
         }
         // entering candidates in canonical order (lane = voxel order, then
-        // probe order): the lanes generate them at once, kWarpReplay at a
-        // time, into the warp's list; lane 0 applies them in list order
+        // probe order): the lanes list them at once, kWarpReplay at a time;
+        // lane 0 applies them in list order
         const uint32_t ne = (uint32_t)__popc(enter);
         const uint32_t ninc = warp_incl_scan(ne);
         const uint32_t total = __shfl_sync(0xffffffffu, ninc, 31);
@@ -1299,29 +1337,27 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
             uint32_t e = ninc - ne;
             for (uint32_t mm = enter; mm; mm &= mm - 1u, ++e) {
                 if (e < lo || e >= lo + kWarpReplay) continue;
-                const I3 o = probe_offset(__ffs(mm) - 1);
+                const uint32_t k = __ffs(mm) - 1;
+                const I3 o = probe_offset(k);
                 const I3 ibv{cbv.x + o.x, cbv.y + o.y, cbv.z + o.z};
                 const uint32_t vb = voxel_at(cs, cb, ibv.x, ibv.y, ibv.z);
                 const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
-                generate_contact(c, va, I3{x, y, z}, wa, vb, ibv, wb, &sm.list[e - lo]);
+                CandRec& r = sm.list[e - lo];
+                r.fid = feature_id(I3{x, y, z}, ibv);
+                r.pen = cand_pen(c.vs_a, ta, vtype(vb), lensq3(wb - wa));
+                r.li = (uint32_t)l;
+                r.k = k;
+                r._pad = 0u;
             }
             __syncwarp();
             if (lane == 0) {
                 const uint32_t cnt = min(kWarpReplay, total - lo);
-                for (uint32_t i = 0; i < cnt; ++i) add_contact(sm, sm.list[i]);
+                for (uint32_t i = 0; i < cnt; ++i) add_cand(sm, sm.list[i]);
             }
             __syncwarp();
         }
-        // manifold penetration multiset -> state (at most four finite values,
-        // so every insert lands)
-        if (lane == 0) {
-            Top4 s = top4_empty();
-            for (uint32_t i = 0; i < sm.n; ++i) top4_insert(s, sm.c[i].penetration);
-            sm.pens[0] = s.v[0];
-            sm.pens[1] = s.v[1];
-            sm.pens[2] = s.v[2];
-            sm.pens[3] = s.v[3];
-        }
+        // manifold penetration multiset -> state
+        if (lane == 0) cand_pens(sm);
         __syncwarp();
         state.v[0] = sm.pens[0];
         state.v[1] = sm.pens[1];
@@ -1330,6 +1366,9 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
     }
     checked = warp_sum(checked);
     ncand = warp_sum(ncand);
+    // the contacts left in the manifold
+    if (lane < sm.n) build_contact(cs, c, pi.rmin, (uint32_t)nx, (uint32_t)ny, sm.k[lane], &sm.c[lane]);
+    __syncwarp();
     ManifoldRec& out = w.man[cur][p];
     if (lane == 0) {
         pi.voxels_checked = checked;
@@ -1359,7 +1398,7 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
 constexpr uint32_t kBlockReplay = 64;
 __device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cur, uint32_t p, WarpManifold& sm) {
     __shared__ Top4 s_top[32];
-    __shared__ ContactRec s_rec[kBlockReplay];
+    __shared__ CandRec s_rec[kBlockReplay];
     const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
     PairInfo& pi = w.pinfo[p];
     const uint32_t ia = pi.ia, ib = pi.ib;
@@ -1461,37 +1500,36 @@ __device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cu
                 top4_insert(run, pen);
             }
         }
-        // entering candidates in (voxel, probe) order: the threads generate
-        // them at once, kBlockReplay at a time, into s_rec; thread 0 applies
-        // them in that order
+        // entering candidates in (voxel, probe) order: the threads list them
+        // at once, kBlockReplay at a time, into s_rec; thread 0 applies them
+        // in that order
         uint32_t total = 0;
         const uint32_t off = block_excl_scan((uint32_t)__popc(enter), &total);
         for (uint32_t lo = 0; lo < total; lo += kBlockReplay) {
             uint32_t e = off;
             for (uint32_t mm = enter; mm; mm &= mm - 1u, ++e) {
                 if (e < lo || e >= lo + kBlockReplay) continue;
-                const I3 o = probe_offset(__ffs(mm) - 1);
+                const uint32_t k = __ffs(mm) - 1;
+                const I3 o = probe_offset(k);
                 const I3 ibv{cbv.x + o.x, cbv.y + o.y, cbv.z + o.z};
                 const uint32_t vb = voxel_at(cs, cb, ibv.x, ibv.y, ibv.z);
                 const F3 wb = transform_point_n(c.pb, c.qnb, voxel_to_local(c.vs_b, ibv.x, ibv.y, ibv.z));
-                generate_contact(c, va, I3{x, y, z}, wa, vb, ibv, wb, &s_rec[e - lo]);
+                CandRec& r = s_rec[e - lo];
+                r.fid = feature_id(I3{x, y, z}, ibv);
+                r.pen = cand_pen(c.vs_a, ta, vtype(vb), lensq3(wb - wa));
+                r.li = (uint32_t)l;
+                r.k = k;
+                r._pad = 0u;
             }
             __syncthreads();
             if (tid == 0) {
                 const uint32_t cnt = min(kBlockReplay, total - lo);
-                for (uint32_t i = 0; i < cnt; ++i) add_contact(sm, s_rec[i]);
+                for (uint32_t i = 0; i < cnt; ++i) add_cand(sm, s_rec[i]);
             }
             __syncthreads();
         }
         // manifold penetration multiset -> state
-        if (tid == 0) {
-            Top4 st = top4_empty();
-            for (uint32_t i = 0; i < sm.n; ++i) top4_insert(st, sm.c[i].penetration);
-            sm.pens[0] = st.v[0];
-            sm.pens[1] = st.v[1];
-            sm.pens[2] = st.v[2];
-            sm.pens[3] = st.v[3];
-        }
+        if (tid == 0) cand_pens(sm);
         __syncthreads();
         state.v[0] = sm.pens[0];
         state.v[1] = sm.pens[1];
@@ -1500,6 +1538,9 @@ __device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cu
     }
     checked = block_sum(checked);
     ncand = block_sum(ncand);
+    // the contacts left in the manifold
+    if (tid < sm.n) build_contact(cs, c, pi.rmin, (uint32_t)nx, (uint32_t)ny, sm.k[tid], &sm.c[tid]);
+    __syncthreads();
     ManifoldRec& out = w.man[cur][p];
     if (tid == 0) {
         pi.voxels_checked = checked;
