@@ -1302,6 +1302,9 @@ __device__ void probe_pair(WorldDev& w, const ColliderSet& cs, uint32_t cur, uin
         }
         if (__ballot_sync(0xffffffffu, mask != 0u) == 0u) continue;
         ncand += __popc(mask);
+        // a candidate enters only above the running 4th penetration, which is
+        // at least the manifold's: when no lane's best beats that, none does
+        if (__ballot_sync(0xffffffffu, t.v[0] > state.v[3]) == 0u) continue;
         // exclusive warp scan of the lanes' top-4 multisets
         Top4 inc = t;
 #pragma unroll
@@ -1461,6 +1464,9 @@ __device__ void probe_pair_block(WorldDev& w, const ColliderSet& cs, uint32_t cu
         }
         if (!__syncthreads_or(mask != 0u)) continue;
         ncand += __popc(mask);
+        // a candidate enters only above the running 4th penetration, which is
+        // at least the manifold's: when no thread's best beats that, none does
+        if (!__syncthreads_or(t.v[0] > state.v[3])) continue;
         // CTA-wide exclusive scan of the threads' top-4 multisets
         Top4 inc = t;
 #pragma unroll
