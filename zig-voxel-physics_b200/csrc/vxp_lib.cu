@@ -502,7 +502,8 @@ struct WorldBuffers {
     DBuf<ManifoldRec> man0, man1;
     DBuf<HashSlot> ht0, ht1;
     DBuf<uint32_t> frame;
-    DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag, clist;
+    DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag;
+    DBuf<CacheLook> clist;
     DBuf<float> cp;
     DBuf<uint4> cm, rk;
     DBuf<float2> cfr;

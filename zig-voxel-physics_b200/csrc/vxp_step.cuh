@@ -736,12 +736,22 @@ __device__ bool phase_pairs(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
     if ((threadIdx.x & 31) == 0 && tested) atomicAdd(&w.ctr[C_PAIRS_TESTED], tested);
     if (!g.sync()) return false;
     if (w.cfg.use_cache) {
-        // pairs consulting the cache, in pair order, for the replay warp
+        // the lookups of the pairs consulting the cache, in pair order, for
+        // the replay warp (window starts computed here, off its chain)
         uint32_t nc = 0;
         if (!group_scan(
                 g, P, [&](uint32_t i) { return (w.pinfo[i].flags & PF_CACHE) ? 1u : 0u; },
                 [&](uint32_t i, uint32_t pre) {
-                    if (w.pinfo[i].flags & PF_CACHE) w.clist[pre] = i;
+                    const PairInfo& pi = w.pinfo[i];
+                    if (pi.flags & PF_CACHE) {
+                        CacheLook r;
+                        r.p = i;
+                        r.a = pi.key_a;
+                        r.b = pi.key_b;
+                        r.th = pi.th;
+                        r.start = (uint32_t)(cache_key_hash(r.a, r.b, r.th) % (unsigned long long)w.cache_cap);
+                        w.clist[pre] = r;
+                    }
                 },
                 w.scan, &nc))
             return false;
@@ -760,11 +770,35 @@ __device__ bool phase_pairs(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
 // or at the key = hit, which refreshes last_used) and, after a miss, a put
 // (the first empty slot of the window, else evict its least recently used
 // entry).  One warp replays the keys of this step in pair order on a
-// shared-memory copy of the table, 16 lanes probing a window at once, while
-// the other warps already detect every cache-consulting pair; a hit later
-// discards that detection and replays the cached contacts instead.  Values
-// are written after detection (phase_finalize), the last writer of a slot
-// winning, as the sequential puts would leave them.
+// shared-memory copy of the table while the other warps already detect every
+// cache-consulting pair; a hit later discards that detection and replays the
+// cached contacts instead.  Values are written after detection
+// (phase_finalize), the last writer of a slot winning, as the sequential puts
+// would leave them.
+//
+// A lookup reads and writes only its window, so it sees the state the
+// sequential replay gives it once every earlier lookup whose window overlaps
+// its own has run.  The warp keeps up to 32 pending lookups in order, one per
+// lane; each round every pending lookup whose window overlaps no earlier
+// pending one runs (their windows are disjoint), the rest move up in order
+// and new ones fill the free lanes.  Keys stream in 32 at a time, one batch
+// ahead.
+
+// Position of the n-th (from 0) set bit of m; n < popc(m).
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t n) {
+    uint32_t r = 0;
+#pragma unroll
+    for (uint32_t wd = 16; wd; wd >>= 1) {
+        const uint32_t c = (uint32_t)__popc(m & ((1u << wd) - 1u));
+        if (n >= c) {
+            n -= c;
+            m >>= wd;
+            r += wd;
+        }
+    }
+    return r;
+}
+
 __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t cap = w.cache_cap;
@@ -779,154 +813,129 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
     }
     __syncwarp();
     uint32_t hits = 0, misses = 0, evictions = 0;
-    // Keys 32 at a time, one per lane, each with its window start.  Two
-    // consecutive lookups whose windows share no slot cannot see each other's
-    // write, so they run together (lanes 0-15 hold the window of the first,
-    // lanes 16-31 that of the second); otherwise one runs alone.  Which
-    // lookups pair up follows from the window starts only.  The windows of
-    // the next round are read while this round is decided, then patched with
-    // this round's writes (the slots it touches, if in those windows); a
-    // patch stores what the writing lane stores, so it does not matter
-    // whether the read saw that store.
-    const bool pairs_ok = cap >= 32u && maxp == 16u;
-    const uint32_t half = lane >> 4, hl = lane & 15u;
-    for (uint32_t k0 = 0; k0 < n; k0 += 32u) {
-        uint32_t my_p = 0, my_a = 0, my_b = 0, my_start = 0;
-        unsigned long long my_th = 0;
-        if (k0 + lane < n) {
-            my_p = w.clist[k0 + lane];
-            const PairInfo& pi = w.pinfo[my_p];
-            my_a = pi.key_a;
-            my_b = pi.key_b;
-            my_th = pi.th;
-            my_start = (uint32_t)(cache_key_hash(my_a, my_b, my_th) % (unsigned long long)cap);
+    // the lookups stream into this SM's L1 ahead of use (nothing else runs
+    // here): their 128-byte lines, all requests in flight at once
+    {
+        const char* base = reinterpret_cast<const char*>(w.clist);
+        const uint32_t lines = (uint32_t)(((size_t)n * sizeof(CacheLook) + 127u) / 128u);
+        for (uint32_t i = lane; i < lines; i += 32u)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(base + (size_t)i * 128u));
+    }
+    using Look = CacheLook;
+    auto load = [&](uint32_t idx) {
+        Look r{0u, 0u, 0u, 0u, 0ull};
+        if (idx < n) r = w.clist[idx];
+        return r;
+    };
+    auto shfl = [&](const Look& x, uint32_t src) {
+        Look r;
+        r.p = __shfl_sync(0xffffffffu, x.p, src);
+        r.a = __shfl_sync(0xffffffffu, x.a, src);
+        r.b = __shfl_sync(0xffffffffu, x.b, src);
+        r.start = __shfl_sync(0xffffffffu, x.start, src);
+        r.th = __shfl_sync(0xffffffffu, x.th, src);
+        return r;
+    };
+    // the windows starting at s0 and s1 (maxp slots each, mod cap) overlap
+    auto overlap = [&](uint32_t s0, uint32_t s1) {
+        const uint32_t d = s1 >= s0 ? s1 - s0 : s1 + cap - s0;
+        return d < maxp || cap - d < maxp;
+    };
+    const bool coarse = cap >= 64u * maxp;
+    Look cur = load(lane), nxt = load(32u + lane);  // keys [cb, cb + 32) and the batch after
+    uint32_t cb = 0, taken = 0, np = 0;
+    Look mine{0u, 0u, 0u, 0u, 0ull};
+    for (;;) {
+        // fill lanes np.. with the next keys, in order
+        const uint32_t take = min(32u - np, n - taken);
+        {
+            const bool fill = lane >= np && lane < np + take;
+            const uint32_t rc = fill ? taken + (lane - np) - cb : 0u;  // relative to cb, < 64
+            const Look fc = shfl(cur, rc < 32u ? rc : 0u), fn = shfl(nxt, rc >= 32u ? rc - 32u : 0u);
+            if (fill) mine = rc < 32u ? fc : fn;
         }
-        const uint32_t cnt = min(32u, n - k0);
-        // round starting at lookup j: 2 lookups when j + 1 is in the batch and
-        // the two windows are disjoint, else 1
-        auto round_size = [&](uint32_t j) -> uint32_t {
-            if (!pairs_ok || j + 1u >= cnt) return 1u;
-            const uint32_t s0 = __shfl_sync(0xffffffffu, my_start, j), s1 = __shfl_sync(0xffffffffu, my_start, j + 1u);
-            const uint32_t d = s1 >= s0 ? s1 - s0 : s1 + cap - s0;
-            return (d >= 16u && d <= cap - 16u) ? 2u : 1u;
-        };
-        // this lane's lookup of a round at j: lanes 0-15 the first, lanes
-        // 16-31 the second (none when the round has one lookup); slot held
-        auto lane_lookup = [&](uint32_t j, uint32_t rs, uint32_t* sl) -> bool {
-            const uint32_t q = j + half;
-            const uint32_t st = __shfl_sync(0xffffffffu, my_start, q < cnt ? q : j);
-            uint32_t x = st + hl;
-            if (x >= cap) x -= cap;
-            *sl = x;
-            return half < rs && hl < maxp;
-        };
-        uint32_t j = 0, rs = round_size(0), c_sl = 0;
-        bool c_on = lane_lookup(0, rs, &c_sl);
-        uint32_t c_lu = 0xFFFFFFFFu, c_a = 0, c_b = 0;
-        unsigned long long c_th = 0;
-        if (c_on) {
-            c_lu = t.lu[c_sl];
-            const uint2 ab = t.ab[c_sl];
-            c_a = ab.x;
-            c_b = ab.y;
-            c_th = t.th[c_sl];
+        taken += take;
+        np += take;
+        if (np == 0u) break;
+        while (taken >= cb + 32u && cb + 32u < n) {
+            cur = nxt;
+            cb += 32u;
+            nxt = load(cb + 32u + lane);
         }
-        while (j < cnt) {
-            // this lane's key: the lookup its half of the warp decides
-            const uint32_t q = j + (half < rs ? half : 0u);
-            const uint32_t p = __shfl_sync(0xffffffffu, my_p, q);
-            const uint32_t ka = __shfl_sync(0xffffffffu, my_a, q), kb = __shfl_sync(0xffffffffu, my_b, q);
-            const unsigned long long th = __shfl_sync(0xffffffffu, my_th, q);
-            const uint32_t start = __shfl_sync(0xffffffffu, my_start, q);
-            // the next round's windows, read ahead
-            const uint32_t nj = j + rs;
-            const bool more = nj < cnt;
-            const uint32_t nrs = more ? round_size(nj) : 1u;
-            uint32_t n_sl = 0;
-            const bool n_on = lane_lookup(more ? nj : j, nrs, &n_sl) && more;
-            uint32_t n_lu = 0xFFFFFFFFu, n_a = 0, n_b = 0;
-            unsigned long long n_th = 0;
-            if (n_on) {
-                n_lu = t.lu[n_sl];
-                const uint2 ab = t.ab[n_sl];
-                n_a = ab.x;
-                n_b = ab.y;
-                n_th = t.th[n_sl];
+        // ready: no earlier pending window overlaps this one.  With at least
+        // 64 x maxp slots, overlapping windows start in the same or adjacent
+        // sixty-fourths of the table, which a prefix OR over the lanes checks
+        // (a conservative test); else every earlier window is compared.
+        const bool pending = lane < np;
+        bool ready = pending;
+        if (coarse) {
+            const uint32_t bk = (uint32_t)(((unsigned long long)mine.start * 64ull) / cap);
+            const unsigned long long m = pending ? 1ull << bk : 0ull;
+            unsigned long long inc = m;
+#pragma unroll
+            for (uint32_t d = 1; d < 32u; d <<= 1) {
+                const unsigned long long o = __shfl_up_sync(0xffffffffu, inc, d);
+                if (lane >= d) inc |= o;
             }
-            // get: stop at the first empty slot (miss) or at the key (hit)
-            const bool valid = c_on && c_lu != 0u;
-            const bool match = valid & (c_a == ka) & (c_b == kb) & (c_th == th);
-            const uint32_t sh = half * 16u;
-            const uint32_t inv_m = (__ballot_sync(0xffffffffu, c_on && !valid) >> sh) & 0xFFFFu;
-            const uint32_t mat_m = (__ballot_sync(0xffffffffu, match) >> sh) & 0xFFFFu;
-            // first least-recently-used entry of the window (used when the
-            // window is full and the key is not in it)
-            const uint32_t m0 = __reduce_min_sync(0xffffffffu, (c_on && half == 0u) ? c_lu : 0xFFFFFFFFu);
-            const uint32_t m1 = __reduce_min_sync(0xffffffffu, (c_on && half == 1u) ? c_lu : 0xFFFFFFFFu);
-            const uint32_t lru_m = (__ballot_sync(0xffffffffu, c_on && c_lu == (half ? m1 : m0)) >> sh) & 0xFFFFu;
-            const uint32_t fi = inv_m ? (uint32_t)(__ffs(inv_m) - 1) : 32u;
-            const uint32_t fm = mat_m ? (uint32_t)(__ffs(mat_m) - 1) : 32u;
-            uint32_t tl;
-            bool hit = false, evict = false;
-            if (fm < fi) {
-                hit = true;
-                tl = fm;
-            } else if (fi < 32u) {
-                tl = fi;
-            } else {
-                tl = (uint32_t)(__ffs(lru_m) - 1);
-                evict = true;
+            unsigned long long ex = __shfl_up_sync(0xffffffffu, inc, 1);
+            if (lane == 0u) ex = 0ull;
+            const unsigned long long near = m | (m << 1) | (m >> 1) | (bk == 0u ? 1ull << 63 : 0ull) |
+                                            (bk == 63u ? 1ull : 0ull);
+            if (ex & near) ready = false;
+        } else {
+            for (uint32_t i = 0; i + 1u < np; ++i) {
+                const uint32_t si = __shfl_sync(0xffffffffu, mine.start, i);
+                if (i < lane && overlap(si, mine.start)) ready = false;
             }
-            uint32_t target = start + tl;
-            if (target >= cap) target -= cap;
-            // the other half's decision (the second lookup of the round)
-            const uint32_t o_target = __shfl_xor_sync(0xffffffffu, target, 16);
-            const bool o_hit = __shfl_xor_sync(0xffffffffu, hit ? 1u : 0u, 16) != 0u;
-            const uint32_t o_a = __shfl_xor_sync(0xffffffffu, ka, 16), o_b = __shfl_xor_sync(0xffffffffu, kb, 16);
-            const unsigned long long o_th = __shfl_xor_sync(0xffffffffu, th, 16);
-            if (n_on) {
-                if (n_sl == target && half < rs) {
-                    n_lu = frame;
-                    if (!hit) {
-                        n_a = ka;
-                        n_b = kb;
-                        n_th = th;
-                    }
-                } else if ((half ^ 1u) < rs && n_sl == o_target) {
-                    n_lu = frame;
-                    if (!o_hit) {
-                        n_a = o_a;
-                        n_b = o_b;
-                        n_th = o_th;
-                    }
-                }
-            }
-            if (hl == 0u && half < rs) {
-                PairInfo& pi = w.pinfo[p];
-                t.lu[target] = frame;
-                if (hit) {
-                    pi.hit = 1u;
-                    ++hits;
+        }
+        if (ready) {
+            // get: the first empty slot (miss) or the key (hit), whichever
+            // comes first; put after a miss: that empty slot, else the first
+            // least recently used one
+            uint32_t fi = maxp, fm = maxp, mn = 0xFFFFFFFFu, mi = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 16u; ++i) {
+                if (i >= maxp) break;
+                uint32_t x = mine.start + i;
+                if (x >= cap) x -= cap;
+                const uint32_t lu = t.lu[x];
+                const uint2 ab = t.ab[x];
+                const unsigned long long th = t.th[x];
+                if (lu == 0u) {
+                    if (fi == maxp) fi = i;
                 } else {
-                    t.ab[target] = make_uint2(ka, kb);
-                    t.th[target] = th;
-                    w.cwriter[target] = p;
-                    pi.hit = 2u;
-                    ++misses;
-                    if (evict) ++evictions;
+                    if (fm == maxp && ab.x == mine.a && ab.y == mine.b && th == mine.th) fm = i;
+                    if (lu < mn) {
+                        mn = lu;
+                        mi = i;
+                    }
                 }
-                pi.cache_slot = target;
             }
-            __syncwarp();
-            j = nj;
-            rs = nrs;
-            c_on = n_on;
-            c_sl = n_sl;
-            c_lu = n_lu;
-            c_a = n_a;
-            c_b = n_b;
-            c_th = n_th;
+            const bool hit = fm < fi;
+            const bool evict = !hit && fi == maxp;
+            uint32_t target = mine.start + (hit ? fm : (evict ? mi : fi));
+            if (target >= cap) target -= cap;
+            PairInfo& pi = w.pinfo[mine.p];
+            t.lu[target] = frame;
+            if (hit) {
+                pi.hit = 1u;
+                ++hits;
+            } else {
+                t.ab[target] = make_uint2(mine.a, mine.b);
+                t.th[target] = mine.th;
+                w.cwriter[target] = mine.p;
+                pi.hit = 2u;
+                ++misses;
+                if (evict) ++evictions;
+            }
+            pi.cache_slot = target;
         }
+        __syncwarp();
+        // the lookups left move up, in order
+        const uint32_t rm = __ballot_sync(0xffffffffu, pending && !ready);
+        np = (uint32_t)__popc(rm);
+        const Look moved = shfl(mine, lane < np ? nth_set_bit(rm, lane) : 0u);
+        if (lane < np) mine = moved;
     }
     for (uint32_t i = lane; i < cap; i += 32u) {
         CacheKeyRec k;

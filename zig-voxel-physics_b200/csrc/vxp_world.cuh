@@ -204,6 +204,13 @@ enum : uint32_t {
 };
 enum : uint32_t { ERR_TIMEOUT = 1u, ERR_CAP = 2u, ERR_COLOURS = 4u, ERR_OVERFLOW = 8u, ERR_BOUNDS = 16u };
 
+// A brick-pair cache lookup of the step: the pair, its key and the start of
+// its probe window (hash % capacity).
+struct CacheLook {
+    uint32_t p, a, b, start;
+    unsigned long long th;
+};
+
 struct WorldDev {
     StepCfg cfg;
     uint32_t n_bodies;
@@ -236,7 +243,7 @@ struct WorldDev {
     CacheKeyRec* ckey;
     CacheValRec* cval;
     uint32_t* cwriter;            // last pair writing each slot this frame
-    uint32_t* clist;              // pairs consulting the cache, in pair order
+    CacheLook* clist;             // lookups of the pairs consulting the cache, in pair order
     unsigned long long* cframe;   // cache frame counter
     // constraints
     uint32_t* cons;               // constraint -> pair index (pair order)
