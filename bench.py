@@ -50,9 +50,9 @@ SOLVER_V, SOLVER_Q = 1, 2
 # pile, keyed by (workload, kernel), from one ncu capture of the same
 # workload; re-captured when a kernel changes.
 PROFILED_TRAFFIC = {
-    ("config2_pile_4096", "k_step_grid"): (26_672_384, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
-    ("config2_pile_4096", "k_solve_grid"): (6_090_752, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
-    ("config2_pile_4096", "k_solve_cluster"): (3_659_264,
+    ("config2_pile_4096", "k_step_grid"): (41_747_968, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
+    ("config2_pile_4096", "k_solve_grid"): (5_913_856, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
+    ("config2_pile_4096", "k_solve_cluster"): (3_658_752,
                                                "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
 }
 
