@@ -310,6 +310,13 @@ int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div);
  * one CTA each, use 1024).  Results do not depend on it. */
 int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n);
 
+/* Narrow-phase probe tables: with enable (the default) every collider of at
+ * most 2^23 probe centres gets a table of its voxels' 27-neighbour type masks
+ * when the colliders upload, and a probe centre costs one lookup instead of
+ * 27; with 0 every probe looks its voxels up.  Takes effect at the next step.
+ * Results do not depend on it. */
+int vxp_set_probe_tables(vxp_ctx* ctx, int enable);
+
 /* Order of the solver's sweeps (ContactSolver.solve, src/solver.zig:494-561)
  * when a world is stepped by the cooperative grid (vxp_set_launch_mode).
  * 2 (default where the device schedules the cluster, see vxp_cluster_size):

@@ -27,11 +27,12 @@ def _first_diff(g, r):
 
 
 def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=None, cluster_smem=None,
-             cluster_cons=None, **cfg):
+             cluster_cons=None, probe_tables=None, **cfg):
     """Steps GPU and oracle together; returns the GPU system (open).
     solver: the grid solver mode (0 grid barriers, 1 event order, 2 cluster);
     cluster_smem: shared memory the cluster sweeps may use (0: state in L2);
-    cluster_cons: 1 to build and colour the constraint table on the cluster too."""
+    cluster_cons: 1 to build and colour the constraint table on the cluster too;
+    probe_tables: False to probe without the neighbourhood-mask tables."""
     g = vxp.VoxelPhysicsSystem(**cfg)
     g.load_scene(scene)
     g.set_launch_mode(mode)
@@ -41,6 +42,8 @@ def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=
         g.set_cluster_shared_bytes(cluster_smem)
     if cluster_cons is not None:
         g.set_cluster_constraints(bool(cluster_cons))
+    if probe_tables is not None:
+        g.set_probe_tables(bool(probe_tables))
     r = O.OracleWorld(**cfg)
     r.load_scene(scene)
     dt = np.float32(scene.dt)
@@ -112,6 +115,15 @@ def test_config1_grid_solver_modes(vxp, solver, cfg):
     """The 64-cube scene on the grid with each solver mode."""
     sc = vxp.scenes.config1(mass_fn=O.mass_fn, seed=5)
     lockstep(vxp, sc, 90, mode=1, solver=solver, **cfg).close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_probes_without_tables(vxp, mode):
+    """The narrow phase's 27 voxel lookups per probe centre (the path of
+    colliders too large for a neighbourhood-mask table), on one CTA and on
+    the grid, bit-exact against the oracle."""
+    sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=3)
+    lockstep(vxp, sc, 40, mode=mode, substeps=8, probe_tables=False).close()
 
 
 def test_config4_noise_subset(vxp):
@@ -334,6 +346,8 @@ def test_small_brick_pair_cache(vxp, mode, cache):
     consecutive lookups' 16-slot windows often overlap, so the device replay
     of the lookups (two at a time when their windows are disjoint) is checked
     against the oracle's sequential one through the hit / miss / eviction
-    counters and the manifolds, every step."""
+    counters and the manifolds, every step.  Tables this small compare the
+    windows of the pending lookups pairwise; the 64-slot and larger ones also
+    exercise the wrap-around."""
     sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
     lockstep(vxp, sc, 60, mode=mode, brick_pair_cache_size=cache, substeps=8).close()

@@ -312,6 +312,7 @@ struct ColliderStore {
     // neighbourhood-mask tables: colliders with at most kNbMaxCentres probe
     // centres get one, while the pool stays within kNbMaxTotal entries
     static constexpr uint64_t kNbMaxCentres = 1ull << 23, kNbMaxTotal = 1ull << 25;
+    bool tables = true;  // build neighbourhood-mask tables at all
 
     int upload(uint32_t id, float vs, const vxp_brick* bricks, uint32_t n, std::string& err) {
         if (!bricks && n) {
@@ -410,7 +411,7 @@ struct ColliderStore {
             brick_total += (uint32_t)nb;
             uint64_t centres = 1;
             for (int k = 0; k < 3; ++k) centres *= (uint64_t)((int64_t)h.max_bound[k] - h.min_bound[k] + 2);
-            if (centres <= kNbMaxCentres && nb_total + centres <= kNbMaxTotal) {
+            if (tables && centres <= kNbMaxCentres && nb_total + centres <= kNbMaxTotal) {
                 d.nb_off = (uint32_t)nb_total;
                 nb_total += centres;
             } else {
@@ -1685,6 +1686,15 @@ int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div) {
 int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n) {
     if (!ctx) return VXP_ERR_ARG;
     ctx->heavy_voxels = n;
+    return VXP_OK;
+}
+
+int vxp_set_probe_tables(vxp_ctx* ctx, int enable) {
+    if (!ctx) return VXP_ERR_ARG;
+    if (ctx->cols.tables != (enable != 0)) {
+        ctx->cols.tables = enable != 0;
+        ctx->cols.dirty = true;
+    }
     return VXP_OK;
 }
 

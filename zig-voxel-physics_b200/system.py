@@ -163,6 +163,10 @@ class VoxelPhysicsSystem:
         """Pairs with at least n overlap-region voxels are probed by a whole CTA (0: never)."""
         self._check(self.lib.vxp_set_heavy_pair_voxels(self.ctx, int(n)))
 
+    def set_probe_tables(self, on: bool = True) -> None:
+        """Neighbourhood-mask tables for the narrow phase's probes (on by default)."""
+        self._check(self.lib.vxp_set_probe_tables(self.ctx, 1 if on else 0))
+
     def set_substep_record(self, on: bool = True) -> None:
         self._check(self.lib.vxp_snapshot_substeps(self.ctx, 1 if on else 0))
 
