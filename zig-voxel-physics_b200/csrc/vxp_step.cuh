@@ -1764,6 +1764,8 @@ __device__ __forceinline__ bool jp_before(uint32_t i, uint32_t j) {
     const uint32_t pi = jp_priority(i), pj = jp_priority(j);
     return pi != pj ? pi > pj : i < j;
 }
+// Bound on the polling colouring's wait for higher-priority neighbours.
+constexpr unsigned long long kColourTimeoutNs = 2000000000ull;
 
 __device__ __forceinline__ size_t cpi(const WorldDev& w, uint32_t field, uint32_t slot, uint32_t pos) {
     return ((size_t)(field * 4u + slot)) * w.pair_cap + pos;
@@ -1880,14 +1882,22 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
         if (!g.sync()) return false;
     } else {
         // Jones-Plassmann over writable bodies == greedy in priority order.
-        // rounds; three rotating counters at scan[nblocks .. nblocks+3)
+        // A manifold is coloured once every higher-priority neighbour is
+        // (then no lower-priority one is yet).  On one CTA: rounds, a barrier
+        // after each.  On several, no barrier: each thread polls its
+        // manifolds until all are coloured (the highest-priority uncoloured
+        // manifold can always be coloured by its thread, so this ends; the
+        // wait is bounded by kColourTimeoutNs, ERR_TIMEOUT).
+        const bool polling = g.nblocks() > 1u;
+        const unsigned long long t_start = polling ? global_ns() : 0ull;
+        // rounds: three rotating counters at scan[nblocks .. nblocks+3)
         uint32_t* rem = w.scan + g.nblocks();
         for (uint32_t round = 0;; ++round) {
-            if (round > M + 1u) {
+            if (!polling && round > M + 1u) {
                 if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_COLOURS);
                 break;
             }
-            if (g.rank() == 0) rem[(round + 1u) % 3u] = 0u;
+            if (!polling && g.rank() == 0) rem[(round + 1u) % 3u] = 0u;
             uint32_t left = 0;
             for (uint32_t k = g.rank(); k < M; k += g.size()) {
                 volatile uint32_t* vc = w.colour;
@@ -1939,12 +1949,22 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
                 }
                 vc[k] = c;
             }
+            if (polling) {
+                if (left == 0u) break;
+                if (global_ns() - t_start > kColourTimeoutNs) {
+                    atomicOr(&w.ctr[C_ERROR], ERR_TIMEOUT);
+                    break;
+                }
+                if ((*(volatile uint32_t*)&w.ctr[C_ERROR] & ERR_TIMEOUT) != 0u) break;
+                continue;
+            }
             left = warp_sum(left);
             if ((threadIdx.x & 31) == 0 && left) atomicAdd(&rem[round % 3u], left);
             if (!g.sync()) return false;
             const uint32_t r = *(volatile uint32_t*)&rem[round % 3u];
             if (r == 0u) break;
         }
+        if (polling && !g.sync()) return false;
     }
     // 4. colour-major packing + ContactSolver.addManifold (solver.zig:449-491).
     // With owner groups, each colour is packed group by group: group =
