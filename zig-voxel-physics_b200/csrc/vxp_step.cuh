@@ -3281,14 +3281,12 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         p += (size_t)(ncol + 1u) * sizeof(uint32_t);
         sm.stat = reinterpret_cast<uint32_t*>(p);
     }
-    // this CTA's first slot per colour
-    if (t == 0) {
-        uint32_t run = 0;
-        for (uint32_t c = 0; c < ncol; ++c) {
-            sm.base[c] = run;
-            run += count_of(c, k);
-        }
-        sm.base[ncol] = run;
+    // this CTA's first slot per colour (ncol <= 256 <= T): a block scan
+    {
+        uint32_t total = 0;
+        const uint32_t ex = block_excl_scan(t < ncol ? count_of(t, k) : 0u, &total);
+        if (t < ncol) sm.base[t] = ex;
+        if (t == 0) sm.base[ncol] = total;
     }
     // this CTA's bodies, and a copy of every static body
     for (uint32_t s = t; s < sm.bcap; s += T) {
@@ -3311,12 +3309,20 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         }
         return lo < sm.nrep && sm.stat[lo] == i ? (int32_t)lo : -1;
     };
-    // this CTA's manifolds: bodies, flags, friction, normals and impulses
-    for (uint32_t c = 0; c < ncol; ++c) {
-        const uint32_t b0 = sm.base[c], cnt = sm.base[c + 1u] - b0;
-        const uint32_t first = by_owner ? w.ocnt[c * C + k] : w.colour_cnt[c] + k, stride = by_owner ? 1u : C;
-        for (uint32_t j = t; j < cnt; j += T) {
-            const uint32_t slot = b0 + j, pos = first + stride * j;
+    // this CTA's manifolds: bodies, flags, friction, normals and impulses,
+    // every slot at once (its colour by binary search over the slot bases)
+    const uint32_t nsl0 = sm.base[ncol];
+    for (uint32_t slot = t; slot < nsl0; slot += T) {
+        {
+            uint32_t lo = 0, hi = ncol;  // the last colour whose base is <= slot
+            while (hi - lo > 1u) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (sm.base[mid] <= slot) lo = mid;
+                else hi = mid;
+            }
+            const uint32_t c = lo, j = slot - sm.base[c];
+            const uint32_t first = by_owner ? w.ocnt[c * C + k] : w.colour_cnt[c] + k, stride = by_owner ? 1u : C;
+            const uint32_t pos = first + stride * j;
             uint4 mv = w.cm[pos];
             uint32_t fl = 0u;
             if (mv.x >= N || mv.y >= N || mv.z > 4u) {
