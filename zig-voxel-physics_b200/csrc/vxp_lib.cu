@@ -496,7 +496,11 @@ struct WorldBuffers {
     DBuf<DBodyProp> prop;
     DBuf<float4> p0, qn, aabb_mn, aabb_mx;
     DBuf<uint2> ids;
-    DBuf<uint32_t> pcount, poff, adj_off, adj_cur, bmask;
+    DBuf<uint32_t> pcount, poff, adj_off, adj_cur, bmask, bpmask;
+    uint32_t bp_stride = 0, bp_rows = 0;
+    // worlds of at most this many bodies keep the broad phase's hit masks
+    // (rows x rows / 32 words) and sweep their AABBs once
+    static constexpr uint32_t kMaskBodies = 8192;
     DBuf<uint2> pairs;
     DBuf<uint32_t> n_pairs_dev;
     DBuf<PairInfo> pinfo;
@@ -619,6 +623,14 @@ struct WorldBuffers {
         ok &= adj_off.reserve((size_t)cap + 1) == cudaSuccess;
         ok &= adj_cur.reserve(cap) == cudaSuccess;
         ok &= bmask.reserve((size_t)cap * 8) == cudaSuccess;
+        if (cap <= kMaskBodies) {
+            ok &= bpmask.reserve((size_t)cap * ((cap + 31u) / 32u)) == cudaSuccess;
+            bp_stride = (cap + 31u) / 32u;
+            bp_rows = cap;
+        } else {
+            bpmask.release();
+            bp_stride = bp_rows = 0;
+        }
         ok &= ev.reserve(cap) == cudaSuccess;
         ok &= snap.reserve((size_t)cap * 2) == cudaSuccess;
         if (!ok) {
@@ -754,6 +766,9 @@ struct WorldBuffers {
         w.aabb_mx = aabb_mx.p;
         w.pcount = pcount.p;
         w.poff = poff.p;
+        w.bpmask = bp_rows ? bpmask.p : nullptr;
+        w.bp_stride = bp_stride;
+        w.bp_rows = bp_rows;
         w.pairs = pairs.p;
         w.pinfo = pinfo.p;
         w.man[0] = man0.p;
@@ -806,7 +821,7 @@ struct WorldBuffers {
         z(bmask); z(pairs); z(n_pairs_dev); z(pinfo); z(man0); z(man1); z(ht0); z(ht1); z(frame); z(cons); z(colour);
         z(pos_of); z(packed_pair); z(adj); z(flag); z(clist); z(cp); z(cm); z(rk); z(cfr); z(ev); z(snap); z(chunk);
         z(colour_cnt); z(colour_cur); z(scan); z(ctr); z(cwriter); z(ts); z(cframe); z(ckey); z(cval); z(dump);
-        z(ocnt); z(ocur); z(stat);
+        z(ocnt); z(ocur); z(stat); z(bpmask);
         return e;
     }
 
@@ -818,7 +833,7 @@ struct WorldBuffers {
                clist.bytes() + cp.bytes() + cm.bytes() + rk.bytes() + ev.bytes() + snap.bytes() + chunk.bytes() + cfr.bytes() +
                ckey.bytes() + cval.bytes() +
                cwriter.bytes() + scan.bytes() + ctr.bytes() + ts.bytes() + dump.bytes() + ocnt.bytes() + ocur.bytes() +
-               stat.bytes();
+               stat.bytes() + bpmask.bytes();
     }
 
     // Counters -> vxp_stats.

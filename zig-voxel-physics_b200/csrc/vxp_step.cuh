@@ -539,8 +539,11 @@ __device__ bool phase_begin(G& g, WorldDev& w, bool skip_test, bool* skipped) {
 // pair, not both static, whose world AABBs (AABB.transform of the collider's
 // local AABB, math.zig:686-693) inflated by `margin` overlap, sorted by
 // (body_a, body_b): one warp per id-sorted row, lanes sweeping the later
-// rows, a ballot keeping them in order.  *overflow: the list does not fit
-// pair_cap (nothing is written; the host grows the buffers).
+// rows, a ballot keeping them in order.  The sweep counts each row's pairs;
+// after a scan of the counts the pairs are written from the hit masks the
+// sweep kept (worlds with mask room), else by sweeping again.  *overflow:
+// the list does not fit pair_cap (nothing is written; the host grows the
+// buffers).
 template <class G>
 __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool* overflow) {
     const uint32_t N = w.n_bodies;
@@ -577,6 +580,7 @@ __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool*
     }
     if (!g.sync()) return false;
     const uint32_t lane = threadIdx.x & 31, wid = g.rank() >> 5, nw = g.size() >> 5;
+    const bool masks = w.bpmask != nullptr && N <= w.bp_rows;
     for (int pass = 0; pass < 2; ++pass) {
         if (pass == 1) {
             uint32_t total = 0;
@@ -594,6 +598,24 @@ __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool*
             for (uint32_t h = 0; h < 2u; ++h) {
                 const uint32_t s = h ? N - 1u - r : r;
                 if (h && s == r) break;
+                if (pass && masks) {
+                    // the row's pairs from its masks, 32 mask words at a time
+                    const uint32_t nj = (N - 1u - s + 31u) / 32u;
+                    const uint32_t* mrow = w.bpmask + (size_t)s * w.bp_stride;
+                    uint32_t o = w.poff[s];
+                    const uint32_t ida = w.ids[s].x;
+                    for (uint32_t jb = 0; jb < nj; jb += 32u) {
+                        const uint32_t j = jb + lane;
+                        uint32_t mk = j < nj ? mrow[j] : 0u;
+                        const uint32_t c = (uint32_t)__popc(mk);
+                        const uint32_t inc = warp_incl_scan(c);
+                        uint32_t q = o + inc - c;
+                        for (; mk; mk &= mk - 1u)
+                            w.pairs[q++] = make_uint2(ida, w.ids[s + 1u + 32u * j + (uint32_t)(__ffs(mk) - 1)].x);
+                        o += __shfl_sync(0xffffffffu, inc, 31);
+                    }
+                    continue;
+                }
                 const float4 a0 = w.aabb_mn[s], a1 = w.aabb_mx[s];
                 const bool si = a0.w != 0.f;
                 uint32_t o = pass ? w.poff[s] : 0u;
@@ -609,6 +631,7 @@ __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool*
                 };
                 auto emit = [&](bool hit, uint32_t t) {
                     const uint32_t mk = __ballot_sync(0xffffffffu, hit);
+                    if (masks && lane == 0) w.bpmask[(size_t)s * w.bp_stride + (t - lane - s - 1u) / 32u] = mk;
                     if (pass && hit)
                         w.pairs[o + __popc(mk & ((1u << lane) - 1u))] = make_uint2(w.ids[s].x, w.ids[t].x);
                     o += __popc(mk);

@@ -230,6 +230,8 @@ struct WorldDev {
     float4* aabb_mn;              // inflated world AABB per body (the step's broad phase: in id order)
     float4* aabb_mx;
     uint32_t* pcount;             // pairs per id-sorted row
+    uint32_t* bpmask;             // broad-phase hit masks: row s, 32 columns from s + 1 + 32 j at s * bp_stride + j
+    uint32_t bp_stride, bp_rows;  // words per row; rows it holds (0: no masks, the sweep runs twice)
     uint32_t* poff;               // their exclusive prefix
     // pairs
     uint2* pairs;                 // (body_a id, body_b id)
