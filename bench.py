@@ -50,9 +50,9 @@ SOLVER_V, SOLVER_Q = 1, 2
 # pile, keyed by (workload, kernel), from one ncu capture of the same
 # workload; re-captured when a kernel changes.
 PROFILED_TRAFFIC = {
-    ("config2_pile_4096", "k_step_grid"): (41_747_968, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
-    ("config2_pile_4096", "k_solve_grid"): (5_913_856, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
-    ("config2_pile_4096", "k_solve_cluster"): (3_658_752,
+    ("config2_pile_4096", "k_step_grid"): (43_096_576, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
+    ("config2_pile_4096", "k_solve_grid"): (5_917_184, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
+    ("config2_pile_4096", "k_solve_cluster"): (3_659_008,
                                                "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
 }
 
