@@ -122,12 +122,32 @@ __global__ void k_body_aabbs(const DBody* body, const DBodyProp* prop, uint32_t 
 // both static.  One warp per row s; lanes sweep t in strides of 32 and a
 // ballot keeps the row's pairs in t order.  Pass 0 counts per row, pass 1
 // writes at the scanned offsets (clamped to cap).
+// masks (row stride mstride words, or null): the count pass keeps each row's
+// 32-column hit masks there and the write pass reads them instead of testing
+// the boxes again.
 __global__ void k_pairs(const uint2* ids, const DBodyProp* prop, uint32_t n, const float4* mn, const float4* mx,
-                        uint32_t* counts, const uint32_t* offsets, uint2* out, uint32_t cap, int pass) {
+                        uint32_t* counts, const uint32_t* offsets, uint2* out, uint32_t cap, int pass,
+                        uint32_t* masks, uint32_t mstride) {
     const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
     if (s >= n) return;
     const uint2 is = ids[s];
+    if (pass && masks) {
+        const uint32_t nj = (n - 1u - s + 31u) / 32u;
+        const uint32_t* mrow = masks + (size_t)s * mstride;
+        uint32_t o = offsets[s];
+        for (uint32_t jb = 0; jb < nj; jb += 32u) {
+            const uint32_t j = jb + lane;
+            uint32_t mk = j < nj ? mrow[j] : 0u;
+            const uint32_t c = (uint32_t)__popc(mk);
+            const uint32_t inc = warp_incl_scan(c);
+            uint32_t q = o + inc - c;
+            for (; mk; mk &= mk - 1u, ++q)
+                if (q < cap) out[q] = make_uint2(is.x, ids[s + 1u + 32u * j + (uint32_t)(__ffs(mk) - 1)].x);
+            o += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        return;
+    }
     const float4 a0 = mn[is.y], a1 = mx[is.y];
     const bool si = prop[is.y].type == 0u;
     uint32_t o = pass ? offsets[s] : 0u;
@@ -144,6 +164,7 @@ __global__ void k_pairs(const uint2* ids, const DBodyProp* prop, uint32_t n, con
             }
         }
         const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (masks && lane == 0) masks[(size_t)s * mstride + (t0 - s - 1u) / 32u] = m;
         if (pass && hit) {
             const uint32_t slot = o + __popc(m & ((1u << lane) - 1u));
             if (slot < cap) out[slot] = make_uint2(is.x, it.x);
@@ -1051,8 +1072,9 @@ int compute_device_pairs(vxp_ctx* ctx, float margin, uint32_t* n_out) {
     const uint32_t tb = 256, nb = (n + tb - 1) / tb;
     const uint32_t wb = (n * 32u + tb - 1) / tb;
     k_body_aabbs<<<nb, tb, 0, ctx->stream>>>(w.body.p, w.prop.p, n, cs, margin, w.aabb_mn.p, w.aabb_mx.p);
+    uint32_t* masks = n <= w.bp_rows ? w.bpmask.p : nullptr;
     k_pairs<<<wb, tb, 0, ctx->stream>>>(w.ids.p, w.prop.p, n, w.aabb_mn.p, w.aabb_mx.p, ctx->pair_counts.p, nullptr,
-                                        nullptr, 0, 0);
+                                        nullptr, 0, 0, masks, w.bp_stride);
     k_scan1<<<1, 1024, 0, ctx->stream>>>(ctx->pair_counts.p, ctx->pair_offsets.p, n, w.n_pairs_dev.p);
     CK(cudaGetLastError());
     uint32_t total = 0;
@@ -1060,7 +1082,7 @@ int compute_device_pairs(vxp_ctx* ctx, float margin, uint32_t* n_out) {
     CK(cudaStreamSynchronize(ctx->stream));
     if (int rc = w.ensure_pairs(total, ctx->err)) return rc;
     k_pairs<<<wb, tb, 0, ctx->stream>>>(w.ids.p, w.prop.p, n, w.aabb_mn.p, w.aabb_mx.p, nullptr, ctx->pair_offsets.p,
-                                        w.pairs.p, w.pair_cap, 1);
+                                        w.pairs.p, w.pair_cap, 1, masks, w.bp_stride);
     CK(cudaGetLastError());
     *n_out = total;
     return VXP_OK;
