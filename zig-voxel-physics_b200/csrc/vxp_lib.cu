@@ -1077,13 +1077,23 @@ int compute_device_pairs(vxp_ctx* ctx, float margin, uint32_t* n_out) {
                                         nullptr, 0, 0, masks, w.bp_stride);
     k_scan1<<<1, 1024, 0, ctx->stream>>>(ctx->pair_counts.p, ctx->pair_offsets.p, n, w.n_pairs_dev.p);
     CK(cudaGetLastError());
+    // the write pass runs at once into the pair buffers as they are (it
+    // writes no pair past their capacity); only when the total does not fit
+    // are they grown and the pass run again
+    auto write_pass = [&]() {
+        k_pairs<<<wb, tb, 0, ctx->stream>>>(w.ids.p, w.prop.p, n, w.aabb_mn.p, w.aabb_mx.p, nullptr,
+                                            ctx->pair_offsets.p, w.pairs.p, w.pair_cap, 1, masks, w.bp_stride);
+        return cudaGetLastError();
+    };
+    const bool early = w.pairs.p != nullptr && w.pair_cap > 0u;
+    if (early) CK(write_pass());
     uint32_t total = 0;
     CK(cudaMemcpyAsync(&total, w.n_pairs_dev.p, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (int rc = w.ensure_pairs(total, ctx->err)) return rc;
-    k_pairs<<<wb, tb, 0, ctx->stream>>>(w.ids.p, w.prop.p, n, w.aabb_mn.p, w.aabb_mx.p, nullptr, ctx->pair_offsets.p,
-                                        w.pairs.p, w.pair_cap, 1, masks, w.bp_stride);
-    CK(cudaGetLastError());
+    if (!early || total > w.pair_cap) {
+        if (int rc = w.ensure_pairs(total, ctx->err)) return rc;
+        CK(write_pass());
+    }
     *n_out = total;
     return VXP_OK;
 }
