@@ -344,7 +344,7 @@ def test_traffic_accounting_changes_only_the_brick_count(vxp, heavy):
 def test_small_brick_pair_cache(vxp, mode, cache):
     """A brick-pair cache of a few dozen slots: nearly every lookup evicts and
     consecutive lookups' 16-slot windows often overlap, so the device replay
-    of the lookups (two at a time when their windows are disjoint) is checked
+    of the lookups (in rounds of lookups whose windows are disjoint) is checked
     against the oracle's sequential one through the hit / miss / eviction
     counters and the manifolds, every step.  Tables this small compare the
     windows of the pending lookups pairwise; the 64-slot and larger ones also
