@@ -347,7 +347,7 @@ def test_small_brick_pair_cache(vxp, mode, cache):
     of the lookups (in rounds of lookups whose windows are disjoint) is checked
     against the oracle's sequential one through the hit / miss / eviction
     counters and the manifolds, every step.  Tables this small compare the
-    windows of the pending lookups pairwise; the 64-slot and larger ones also
-    exercise the wrap-around."""
+    windows of the pending lookups pairwise (larger ones by table
+    sixty-fourths)."""
     sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
     lockstep(vxp, sc, 60, mode=mode, brick_pair_cache_size=cache, substeps=8).close()
