@@ -2236,7 +2236,7 @@ __device__ __forceinline__ void st3(const CPV& v, uint32_t f, uint32_t s, F3 x) 
 // vin: the point's inputs (normal, local anchors, base separation); v: where
 // its velocity-sweep fields go (the same rows, or a copy in shared memory).
 // kTangents: v holds tangent2 too (else the sweeps recompute it as normal x
-// tangent1, point_tangents).
+// tangent1, load_pt_row).
 template <bool kTangents = true>
 __device__ void prepare_point_s(const SolveFlags sf, const CPV vin, const CPV v, float restitution, uint32_t i,
                                 const Soft& soft, float hinv, const BV& a, Qt qa, const BV& b, Qt qb) {
@@ -2288,36 +2288,14 @@ __device__ void prepare_point(WorldDev& w, uint32_t pos, uint32_t i, const Soft&
     prepare_point_s(solve_flags(w.cfg), v, v, w.cfr[pos].y, i, soft, hinv, a, qa, b, qb);
 }
 
-// The tangents of a point as prepare leaves them in the rows, from the rows
-// without tangent2: with friction on, prepare wrote t1 = computeOrthogonal(n)
-// and t2 = n x t1; without, both stay zero as the constraint table set them
-// (and the rows in shared memory never got tangent1).
-__device__ __forceinline__ void point_tangents(bool friction, const CPV& v, uint32_t i, F3 n, F3* t1, F3* t2) {
-    if (friction) {
-        *t1 = ld3(v, CP_T1X, i);
-        *t2 = cross3(n, *t1);
-    } else {
-        *t1 = F3{0.f, 0.f, 0.f};
-        *t2 = F3{0.f, 0.f, 0.f};
-    }
-}
-
-// warmStart for one manifold (solver.zig:702-729).  kTangents: the rows hold
-// the tangents; else they are recomputed (friction: the step's friction flag).
-template <bool kTangents = true>
-__device__ void warm_points(const CPV& v, uint32_t n, float scale, BV& a, BV& b, bool friction = true) {
+// warmStart for one manifold (solver.zig:702-729), rows holding the tangents.
+__device__ void warm_points(const CPV& v, uint32_t n, float scale, BV& a, BV& b) {
     for (uint32_t i = 0; i < n; ++i) {
         const float sn = cpr(v, CP_NI, i) * scale;
         const float s1 = cpr(v, CP_TI0, i) * scale;
         const float s2 = cpr(v, CP_TI1, i) * scale;
         const F3 nv = ld3(v, CP_NX, i);
-        F3 t1, t2;
-        if (kTangents) {
-            t1 = ld3(v, CP_T1X, i);
-            t2 = ld3(v, CP_T2X, i);
-        } else {
-            point_tangents(friction, v, i, nv, &t1, &t2);
-        }
+        const F3 t1 = ld3(v, CP_T1X, i), t2 = ld3(v, CP_T2X, i);
         const F3 imp = (nv * sn + t1 * s1) + t2 * s2;
         apply_impulse(a, -imp, ld3(v, CP_RAX, i));
         apply_impulse(b, imp, ld3(v, CP_RBX, i));
@@ -2339,17 +2317,14 @@ struct PtV {
     F3 pt, n, ra, rb, t1, t2;
     float nm, bias, tm0, tm1, ni, ti0, ti1;
 };
-template <bool kTangents = true>
 __device__ __forceinline__ PtV load_ptv(const CPV& v, uint32_t i) {
     PtV r;
     r.pt = ld3(v, CP_PX, i);
     r.n = ld3(v, CP_NX, i);
     r.ra = ld3(v, CP_RAX, i);
     r.rb = ld3(v, CP_RBX, i);
-    if (kTangents) {
-        r.t1 = ld3(v, CP_T1X, i);
-        r.t2 = ld3(v, CP_T2X, i);
-    }
+    r.t1 = ld3(v, CP_T1X, i);
+    r.t2 = ld3(v, CP_T2X, i);
     r.nm = cpr(v, CP_NM, i);
     r.bias = cpr(v, CP_BIAS, i);
     r.tm0 = cpr(v, CP_TM0, i);
@@ -2419,12 +2394,10 @@ __device__ void velocity_points(const WorldDev& w, const CPV& v, uint32_t n, flo
 // The same sweep without look-ahead: each point's fields are read when the
 // point starts, which keeps fewer registers live (the event-ordered sweeps
 // mostly read their rows from shared memory, where look-ahead gains little).
-template <bool kTangents = true>
 __device__ void velocity_points_near(bool friction, const CPV v, uint32_t n, float fr, const Soft& soft,
                                      bool use_bias, BV& a, BV& b) {
     for (uint32_t i = 0; i < n; ++i) {
-        PtV c = load_ptv<kTangents>(v, i);
-        if (!kTangents) point_tangents(friction, v, i, c.n, &c.t1, &c.t2);
+        const PtV c = load_ptv(v, i);
         const F3 rv = point_vel(b, c.pt) - point_vel(a, c.pt);
         const float vn = dot3(rv, c.n);
         float imp;
@@ -2485,7 +2458,9 @@ __device__ __forceinline__ PtV load_pt_row(const float* r, bool friction) {
     c.pt = F3{q1.y, q2.x, q2.y};
     c.ra = F3{q3.x, q3.y, q4.x};
     c.rb = F3{q4.y, q5.x, q5.y};
-    // tangents as point_tangents forms them
+    // tangents as prepare leaves them: with friction, tangent1 =
+    // computeOrthogonal(n) and tangent2 = n x tangent1; without, both zero as
+    // the constraint table set them (the rows here never get tangent1)
     if (friction) {
         c.t1 = F3{q6.x, q6.y, q7.x};
         c.t2 = cross3(c.n, c.t1);
