@@ -117,3 +117,25 @@ def test_product_package_has_no_oracle_imports():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
                 src = open(os.path.join(dirpath, f)).read()
                 assert not any(b in src for b in banned), f
+
+
+def test_tuning_setters_reject_a_null_context(vxp):
+    """Every tuning setter checks its context before touching the device, so
+    a null context is an argument error on any machine."""
+    lib = vxp.abi.load()
+    calls = {
+        "vxp_set_candidate_dump": (0,),
+        "vxp_set_traffic_accounting": (1,),
+        "vxp_set_cluster_constraints": (1,),
+        "vxp_set_cluster_shared_bytes": (0,),
+        "vxp_set_launch_mode": (0,),
+        "vxp_set_solver_blocks_divisor": (128,),
+        "vxp_set_heavy_pair_voxels": (768,),
+        "vxp_set_probe_tables": (0,),
+        "vxp_set_solver_mode": (0,),
+        "vxp_synchronize": (),
+    }
+    for name, args in calls.items():
+        assert getattr(lib, name)(None, *args) == vxp.abi.VXP_ERR_ARG, name
+    n = ctypes.c_uint32(7)
+    assert lib.vxp_cluster_size(None, ctypes.byref(n)) == vxp.abi.VXP_ERR_ARG
