@@ -565,6 +565,17 @@ void vxo_mat3_inverse(const float* m, float* out) {
     const M3<float> r = minverse(a);
     for (int i = 0; i < 9; ++i) out[i] = r.m[i / 3][i % 3];
 }
+// VoxelBody.getWorldInvInertia (body.zig:386-392) of a dynamic body with
+// rotation q and local inverse inertia inv_local (row-major 3x3).
+void vxo_world_inv_inertia(const float* q, const float* inv_local, float* out) {
+    Body<float> b;
+    b.type = B_DYNAMIC;
+    b.inv_mass = 1.0f;
+    b.rot = Q<float>{q[0], q[1], q[2], q[3]};
+    for (int i = 0; i < 9; ++i) b.inv_I_local.m[i / 3][i % 3] = inv_local[i];
+    const M3<float> r = b.worldInvInertia();
+    for (int i = 0; i < 9; ++i) out[i] = r.m[i / 3][i % 3];
+}
 float vxo_sinf(float x) { return sincos_f32(x, 0); }
 float vxo_cosf(float x) { return sincos_f32(x, 1); }
 

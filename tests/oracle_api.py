@@ -68,6 +68,7 @@ for name, res, args in [
     ("vxo_inverse_transform_point", None, [_VP, _VP, _VP, _VP]),
     ("vxo_quat_rotate", None, [_VP, _VP, _VP]),
     ("vxo_mat3_inverse", None, [_VP, _VP]),
+    ("vxo_world_inv_inertia", None, [_VP, _VP, _VP]),
     ("vxo_sinf", _F, [_F]),
     ("vxo_cosf", _F, [_F]),
     ("vxo_manifold_replay", _I, [_VP, _VP, _U32, _VP, _PU32]),

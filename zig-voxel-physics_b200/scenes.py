@@ -11,7 +11,42 @@ Voxel classification follows the reference:
   * readme_box: the cube classification of the README quick start
     (README.md:84-116) with the boundary test at the cube's first and last
     voxel;
-  * example_ground: the ground-slab convention of examples/basic.zig:91-122.
+  * example_ground / ground_slab: the ground-slab convention of
+    examples/basic.zig:91-122 (face voxels with a +y normal, edge rims,
+    corner corners);
+  * example_box: the 3x3x3 box of examples/basic.zig:125-156.
+
+Two rules of the reference decide how a one-voxel-thick ground slab must be
+built for its bodies to rest on it:
+  * the brick map is keyed by hashBrickPos alone (src/collider.zig:153,
+    187-192, 232-238), and that hash collides for small brick positions of
+    mixed sign, e.g. (-4,0,1) and (2,0,-1): the second brick's voxels are
+    written into the first, which keeps its own position.  A 64x64 slab at
+    voxels [-32,32) keeps only 40 of its 64 bricks and loses the strip
+    z >= 1.6 m (local), AABB included.  Slabs here therefore sit at
+    non-negative voxel coordinates (no merges up to 512x512), and the body
+    is placed to centre them;
+  * classifyFromNeighbors (src/collision_voxel.zig:103-130, 194-235) types a
+    voxel with two empty faces as an edge and sums the empty faces'
+    directions; a one-voxel slab's +y and -y cancel to (0,0,0), which
+    findClosestNormalIndex (src/collision_voxel.zig:85-99) maps to index 0,
+    +x.  Contacts on such a slab get a horizontal normal whenever the
+    voxel pair's direction leans towards +x (generateContact,
+    src/narrow_phase.zig:860-922), and boxes sink through it.  Ground slabs
+    therefore use the example's explicit classification.
+
+Boxes are placed by their centres and rotated about them
+(origin_for_centre): the body position is the collider's voxel origin, a
+corner of the box, so a rotation applied there could put a box into the
+ground before the first step, and only corner voxels ever meet the ground's
+face voxels (src/narrow_phase.zig:701-709).
+
+One rule is the reference's and no scene avoids it: Quat.toMat3
+(src/math.zig:350-372) is the transpose of the rotation Quat.rotate applies,
+so the world inverse inertia (src/body.zig:386-392, src/solver.zig:351-354)
+is R^T I^-1 R.  Cubes do not notice; a long box's contacts can get a normal
+mass an order of magnitude too small, so long boxes under load in the pile
+sink slowly into the ground.
 
 Bodies are VoxelBody records (src/body.zig:177-263): dynamic bodies get
 BodyProperties.default damping (0.3 / 0.5) and the mass properties of
@@ -167,31 +202,67 @@ def readme_box(n: int = 8) -> np.ndarray:
     return dense_to_bricks(voxel_byte(vtype, normal))
 
 
-def example_ground(size: int) -> np.ndarray:
-    """size x 1 x size slab at x, z in [-size/2, size/2), y = 0, classified as in
-    examples/basic.zig:91-122 (face interior with +y normal, edge rims,
-    corner corners)."""
-    half = size // 2
-    idx = np.arange(-half, half)
-    x, z = np.meshgrid(idx, idx, indexing="ij")
-    on_x = (x == -half) | (x == half - 1)
-    on_z = (z == -half) | (z == half - 1)
-    vtype = np.full(x.shape, T_FACE, dtype=np.uint8)
-    normal = np.full(x.shape, 2, dtype=np.uint8)
+def _ground_voxels(nx: int, nz: int) -> np.ndarray:
+    """Voxel bytes [x, 1, z] of an nx x 1 x nz ground slab classified as in
+    examples/basic.zig:91-122: face with the +y normal (2) inside, edge rims
+    with the outward-and-up normals (-x: 8, +x: 6, -z: 15, +z: 14), corner
+    corners (-x-z: 23, +x-z: 19, -x+z: 22, +x+z: 18)."""
+    i = np.arange(nx)[:, None]
+    k = np.arange(nz)[None, :]
+    lo_x, hi_x = i == 0, i == nx - 1
+    lo_z, hi_z = k == 0, k == nz - 1
+    on_x, on_z = lo_x | hi_x, lo_z | hi_z
+    shape = (nx, nz)
+    vtype = np.full(shape, T_FACE, dtype=np.uint8)
+    normal = np.full(shape, 2, dtype=np.uint8)
     corner = on_x & on_z
     vtype[corner] = T_CORNER
-    normal[corner & (x < 0) & (z < 0)] = 23
-    normal[corner & (x > 0) & (z < 0)] = 19
-    normal[corner & (x < 0) & (z > 0)] = 22
-    normal[corner & (x > 0) & (z > 0)] = 18
+    normal[corner & lo_x & lo_z] = 23
+    normal[corner & hi_x & lo_z] = 19
+    normal[corner & lo_x & hi_z] = 22
+    normal[corner & hi_x & hi_z] = 18
     ex = on_x & ~on_z
     vtype[ex] = T_EDGE
-    normal[ex] = np.where(x[ex] < 0, 8, 6)
+    normal[ex] = np.broadcast_to(np.where(lo_x, 8, 6), shape)[ex]
     ez = on_z & ~on_x
     vtype[ez] = T_EDGE
-    normal[ez] = np.where(z[ez] < 0, 15, 14)
-    vox = voxel_byte(vtype, normal)[:, None, :]
-    return dense_to_bricks(vox, origin=(-half, 0, -half))
+    normal[ez] = np.broadcast_to(np.where(lo_z, 15, 14), shape)[ez]
+    return voxel_byte(vtype, normal)[:, None, :]
+
+
+def example_ground(size: int) -> np.ndarray:
+    """size x 1 x size slab at x, z in [-size/2, size/2), y = 0, exactly as
+    examples/basic.zig:91-122 builds it (its loops run z then x).  At size 64
+    the brick hash merges 24 of its 64 bricks (see the module docstring);
+    the reference's own example uses size 16, which merges none."""
+    half = size // 2
+    return dense_to_bricks(_ground_voxels(size, size), origin=(-half, 0, -half))
+
+
+def ground_slab(nx: int, nz: int) -> np.ndarray:
+    """nx x 1 x nz ground slab at voxels [0,nx) x 0 x [0,nz), classified as in
+    examples/basic.zig:91-122; non-negative brick positions keep every brick
+    distinct under hashBrickPos."""
+    return dense_to_bricks(_ground_voxels(nx, nz))
+
+
+def example_box() -> np.ndarray:
+    """The 3x3x3 box of examples/basic.zig:125-156: voxels (-1..1)^3 written in
+    z, y, x order, typed by the count of boundary axes, normal 0 unless a
+    boundary axis overrides it (x, then y, then z)."""
+    idx = np.arange(-1, 2)
+    x, y, z = np.meshgrid(idx, idx, idx, indexing="ij")
+    on_x, on_y, on_z = x != 0, y != 0, z != 0
+    edges = on_x.astype(np.uint8) + on_y + on_z
+    vtype = np.select([edges == 3, edges == 2, edges == 1], [T_CORNER, T_EDGE, T_FACE], T_INSIDE)
+    normal = np.zeros(x.shape, dtype=np.uint8)
+    normal[on_x & (x > 0)] = 0
+    normal[on_x & (x < 0)] = 1
+    normal[on_y & (y > 0)] = 2
+    normal[on_y & (y < 0)] = 3
+    normal[on_z & (z > 0)] = 4
+    normal[on_z & (z < 0)] = 5
+    return dense_to_bricks(voxel_byte(vtype, normal), origin=(-1, -1, -1))
 
 
 def solid_box(ex: int, ey: int, ez: int) -> np.ndarray:
@@ -209,11 +280,6 @@ def walled_bin(nx: int, ny: int, nz: int, wall: int = 2) -> np.ndarray:
     s[:, :, :wall] = True
     s[:, :, -wall:] = True
     return dense_to_bricks(classify_from_neighbors(s))
-
-
-def slab(nx: int, nz: int) -> np.ndarray:
-    """nx x 1 x nz slab at voxels [0,nx) x 0 x [0,nz), classified from neighbours."""
-    return dense_to_bricks(classify_from_neighbors(np.ones((nx, 1, nz), dtype=bool)))
 
 
 def value_noise_solid(rng: np.random.Generator, n: int = 64, lattice: int = 8, threshold: float = 0.5) -> np.ndarray:
@@ -256,6 +322,21 @@ def shoemake_quat(rng: np.random.Generator, n: int) -> np.ndarray:
         axis=1,
     )
     return q.astype(np.float32)
+
+
+def origin_for_centre(centre: np.ndarray, rot: np.ndarray, half: np.ndarray) -> np.ndarray:
+    """Body positions (the collider's voxel origin, src/body.zig:177-203) that
+    put each box's centre `half` (local) at `centre` (world) under rotation
+    `rot` (x, y, z, w): position = centre - R(rot) half.  Rotating about the
+    centre keeps a box inside the sphere of radius |half| around its lattice
+    point, so a lattice whose lowest centres sit that far above the ground
+    starts with no box in the ground."""
+    q = np.asarray(rot, dtype=np.float64)
+    u, w = q[:, :3], q[:, 3:4]
+    v = np.broadcast_to(np.asarray(half, dtype=np.float64), u.shape)
+    t = 2.0 * np.cross(u, v)
+    r = v + w * t + np.cross(u, t)
+    return (np.asarray(centre, dtype=np.float64) - r).astype(np.float32)
 
 
 # ---------------------------------------------------------------------------
@@ -338,28 +419,56 @@ def _dynamic_bodies(ids, cids, pos, rot, mass_of: dict) -> np.ndarray:
 
 
 def config1(mass_fn: MassFn | None = None, n_side: int = 4, seed: int = 1, steps: int = 300) -> Scene:
-    """64 solid 8^3 cubes (one brick each, vs 0.2, 1 kg per voxel) on a 4x4x4
-    lattice at 2 m spacing, lowest layer 3 m up, over a static 64x1x64 slab at
-    y = 0 (created first, so it is body A of every ground pair); +-0.1 m
-    position jitter, uniform random orientations; dt 1/60, 4 substeps, 300 steps."""
+    """64 solid 8^3 cubes (one brick each, vs 0.2, 1 kg per voxel), centres on
+    a 4x4x4 lattice at 2 m spacing, lowest layer 3 m up, over a static 64x1x64 slab at
+    y = 0 spanning x, z in [-6.4, 6.4) m (created first, so it is body A of
+    every ground pair; its voxels sit at [0,64) and the body at x = z = -6.4 so
+    that no brick is merged by the brick hash); +-0.1 m position jitter,
+    uniform random orientations about the cube's centre; dt 1/60, 4
+    substeps, 300 steps."""
     mass_fn = mass_fn or default_mass_fn()
     rng = np.random.default_rng(seed)
     vs = 0.2
-    ground = Collider(0, vs, example_ground(64))
+    ground = Collider(0, vs, ground_slab(64, 64))
     box = Collider(1, vs, readme_box(8))
     density = 1.0 / (vs ** 3)
     mass = {1: mass_fn(vs, box.bricks, np.float32(density))}
     n = n_side ** 3
     grid = np.array([(i, j, k) for j in range(n_side) for k in range(n_side) for i in range(n_side)], dtype=np.float64)
     off = (n_side - 1) / 2.0
-    pos = np.stack([(grid[:, 0] - off) * 2.0, 3.0 + grid[:, 1] * 2.0, (grid[:, 2] - off) * 2.0], axis=1)
-    pos += rng.uniform(-0.1, 0.1, size=pos.shape)
+    centre = np.stack([(grid[:, 0] - off) * 2.0, 3.0 + grid[:, 1] * 2.0, (grid[:, 2] - off) * 2.0], axis=1)
+    centre += rng.uniform(-0.1, 0.1, size=centre.shape)
     rot = shoemake_quat(rng, n)
+    pos = origin_for_centre(centre, rot, np.full(3, 8 * vs * 0.5))
     bodies = np.concatenate(
-        [_static_body(1, 0, (0.0, -vs * 0.5, 0.0)), _dynamic_bodies(np.arange(2, n + 2), np.ones(n, int), pos, rot, mass)]
+        [_static_body(1, 0, (-6.4, -vs * 0.5, -6.4)),
+         _dynamic_bodies(np.arange(2, n + 2), np.ones(n, int), pos, rot, mass)]
     )
     return Scene("config1_small", [ground, box], bodies, 1.0 / 60.0, steps, dict(substeps=4), 0.1,
                  notes=f"{n} cubes 8^3 vs0.2 on 64x1x64 slab, seed {seed}")
+
+
+def basic_example(mass_fn: MassFn | None = None, centred_ground: bool = True) -> Scene:
+    """The scene of examples/basic.zig:16-90: a static 16x1x16 ground slab
+    (vs 0.2) at (0, -0.1, 0) created first, then the 3x3x3 box at (0, 3, 0)
+    with density 1.0 (createDynamicBody, src/system.zig:294-320: 1 kg per m^3,
+    i.e. 0.008 kg per voxel); gravity -9.81, dt 1/60, 4 substeps, 2 velocity
+    and 4 position iterations, warm starting and sleeping on, at most 600
+    frames.  `centred_ground=False` builds the same slab at voxels [0,16)
+    placed at (-1.6, -0.1, -1.6)."""
+    mass_fn = mass_fn or default_mass_fn()
+    vs = 0.2
+    if centred_ground:
+        ground, gpos = Collider(0, vs, example_ground(16)), (0.0, -vs * 0.5, 0.0)
+    else:
+        ground, gpos = Collider(0, vs, ground_slab(16, 16)), (-1.6, -vs * 0.5, -1.6)
+    box = Collider(1, vs, example_box())
+    mass = {1: mass_fn(vs, box.bricks, np.float32(1.0))}
+    bodies = np.concatenate([_static_body(1, 0, gpos),
+                             _dynamic_bodies([2], [1], [(0.0, 3.0, 0.0)], [(0.0, 0.0, 0.0, 1.0)], mass)])
+    return Scene("basic_example", [ground, box], bodies, 1.0 / 60.0, 600,
+                 dict(substeps=4, velocity_iterations=2, position_iterations=4), 0.1,
+                 notes="examples/basic.zig: 3x3x3 box dropped from 3 m onto a 16x1x16 slab")
 
 
 _BOX_CACHE: dict = {}
@@ -396,7 +505,7 @@ def shape_library(mass_fn=None, vs: float = 0.1, lo: int = 2, hi: int = 16) -> l
     """Every config-2 box shape once, ids box_shape_id(...), plus the 64x1x64
     ground slab as id 0: a server uploads these once and jobs refer to them."""
     mass_fn = mass_fn or default_mass_fn()
-    out = [Collider(0, vs, slab(64, 64))]
+    out = [Collider(0, vs, ground_slab(64, 64))]
     for ex in range(lo, hi + 1):
         for ey in range(lo, hi + 1):
             for ez in range(lo, hi + 1):
@@ -421,33 +530,35 @@ def job_bodies(job: dict, mass_fn=None, vs: float = 0.1) -> np.ndarray:
     layer, cell = np.divmod(k, 9)
     cx, cz = np.divmod(cell, 3)
     half = ext * vs * 0.5
-    pos = np.stack([(cx - 1) * 2.2, 1.5 + layer * 2.8, (cz - 1) * 2.2], axis=1).astype(np.float64) - half
-    pos += rng.uniform(-0.1, 0.1, size=pos.shape)
+    centre = np.stack([(cx - 1) * 2.2, 1.6 + layer * 2.8, (cz - 1) * 2.2], axis=1).astype(np.float64)
+    centre += rng.uniform(-0.1, 0.1, size=centre.shape)
     rot = shoemake_quat(rng, n)
+    pos = origin_for_centre(centre, rot, half)
     return np.concatenate([_static_body(1, 0, (-3.2, -vs, -3.2)),
                            _dynamic_bodies(np.arange(2, n + 2), cids, pos, rot, mass)])
 
 
 def config2(mass_fn: MassFn | None = None, n_side: int = 16, seed: int = 2, steps: int = 600) -> Scene:
     """4096 seeded random boxes (per-axis extents U{2..16} voxels, vs 0.1, sparse
-    bricks, classified from neighbours, 1 kg per voxel) dropped from a 16^3
-    jittered lattice (2.8 m spacing, lowest layer 3 m up, random orientations)
-    over a static 128x8x128 walled bin (floor and walls 2 voxels thick) that
+    bricks, classified from neighbours, 1 kg per voxel) dropped with their
+    centres on a 16^3 jittered lattice (2.8 m spacing, lowest layer 3 m up,
+    random orientations about the centre) over a static 128x8x128 walled bin (floor and walls 2 voxels thick) that
     sits on a static 512x1x512 ground slab; dt 1/120, 8 substeps, 600 steps."""
     mass_fn = mass_fn or default_mass_fn()
     rng = np.random.default_rng(seed)
     vs = 0.1
     bin_c = Collider(0, vs, walled_bin(128, 8, 128))
-    ground = Collider(1, vs, slab(512, 512))
+    ground = Collider(1, vs, ground_slab(512, 512))
     n = n_side ** 3
     cols, mass, ext = _random_box_colliders(rng, n, 2, vs, mass_fn)
     sp = 2.8
     grid = np.array([(i, j, k) for j in range(n_side) for k in range(n_side) for i in range(n_side)], dtype=np.float64)
     off = (n_side - 1) / 2.0
     half = ext * vs * 0.5
-    pos = np.stack([(grid[:, 0] - off) * sp, 3.0 + grid[:, 1] * sp, (grid[:, 2] - off) * sp], axis=1) - half
-    pos += rng.uniform(-0.1, 0.1, size=pos.shape)
+    centre = np.stack([(grid[:, 0] - off) * sp, 3.0 + grid[:, 1] * sp, (grid[:, 2] - off) * sp], axis=1)
+    centre += rng.uniform(-0.1, 0.1, size=centre.shape)
     rot = shoemake_quat(rng, n)
+    pos = origin_for_centre(centre, rot, half)
     bodies = np.concatenate(
         [
             _static_body(1, 0, (-6.4, 0.0, -6.4)),
@@ -462,16 +573,18 @@ def config2(mass_fn: MassFn | None = None, n_side: int = 16, seed: int = 2, step
 def world_for_batch(rng, n_bodies: int, mass_fn: MassFn, vs: float = 0.1, steps: int = 300, name="world") -> Scene:
     """One world of the batched / served mixes: n bodies shaped as in config 2
     (random boxes U{2..16} voxels) in columns over the world's own static
-    64x1x64 slab (vs 0.1), 3x3 columns at 2.2 m spacing, 2.8 m per layer."""
-    ground = Collider(0, vs, slab(64, 64))
+    64x1x64 slab (vs 0.1): box centres in 3x3 columns at 2.2 m spacing, 2.8 m
+    per layer from 1.6 m up, random orientations about the centre."""
+    ground = Collider(0, vs, ground_slab(64, 64))
     cols, mass, ext = _random_box_colliders(rng, n_bodies, 1, vs, mass_fn)
     k = np.arange(n_bodies)
     layer, cell = np.divmod(k, 9)
     cx, cz = np.divmod(cell, 3)
     half = ext * vs * 0.5
-    pos = np.stack([(cx - 1) * 2.2, 1.5 + layer * 2.8, (cz - 1) * 2.2], axis=1).astype(np.float64) - half
-    pos += rng.uniform(-0.1, 0.1, size=pos.shape)
+    centre = np.stack([(cx - 1) * 2.2, 1.6 + layer * 2.8, (cz - 1) * 2.2], axis=1).astype(np.float64)
+    centre += rng.uniform(-0.1, 0.1, size=centre.shape)
     rot = shoemake_quat(rng, n_bodies)
+    pos = origin_for_centre(centre, rot, half)
     bodies = np.concatenate(
         [
             _static_body(1, 0, (-3.2, -vs, -3.2)),
