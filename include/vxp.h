@@ -317,6 +317,14 @@ int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n);
  * Results do not depend on it. */
 int vxp_set_probe_tables(vxp_ctx* ctx, int enable);
 
+/* Longest time a block of a grid-launched step waits at a grid barrier
+ * before the step gives up with VXP_ERR_TIMEOUT (0: the default, 10 s).  A
+ * failure-detection knob: a limit of a few nanoseconds makes a real step run
+ * out at its first uneven barrier, the kernels return, the call reports
+ * VXP_ERR_TIMEOUT and the context keeps working.  No counterpart in the
+ * reference, which has no bounded waits. */
+int vxp_set_wait_limit_ns(vxp_ctx* ctx, uint64_t ns);
+
 /* Order of the solver's sweeps (ContactSolver.solve, src/solver.zig:494-561)
  * when a world is stepped by the cooperative grid (vxp_set_launch_mode).
  * 2 (default where the device schedules the cluster, see vxp_cluster_size):
@@ -429,7 +437,10 @@ int vxp_batch_autotune(vxp_batch* b, float dt, uint32_t trial_steps, float* ms_o
  *   positions, rotations   n x 4 floats (x, y, z, unused) / (x, y, z, w)
  *   local_aabbs            n x 8 floats: min x, y, z, unused, max x, y, z,
  *                          unused; min > max marks a body without collider
- *   ids                    n body ids, strictly ascending
+ *   ids                    n body ids, strictly ascending (otherwise
+ *                          *count is 0 and no pair is written; with
+ *                          VXP_CHECK_ARGS=1 in the environment the call
+ *                          waits for its work and returns VXP_ERR_ARG)
  *   body_types             n VXP_BODY_* values
  *   out                    room for cap pairs; *count (device) receives the
  *                          total, which may exceed cap (the list is cut)
@@ -443,7 +454,10 @@ int vxp_batch_autotune(vxp_batch* b, float dt, uint32_t trial_steps, float* ms_o
  * first call before capturing any stream.  Every call uses the same array:
  * calls whose work overlaps on the GPU (other streams, other host threads)
  * race and must be serialised by the caller.  No scratch value carries over
- * from one call to the next.
+ * from one call to the next.  The device address is kept for the life of
+ * the process: do not reset the device while the library is loaded.  An
+ * error already pending on the calling thread is left in place and the call
+ * returns VXP_ERR_CUDA without launching.
  * ------------------------------------------------------------------------- */
 int vxp_pairs_noalloc(const float* positions, const float* rotations, const float* local_aabbs,
                       const uint32_t* ids, const uint32_t* body_types, uint32_t n, float margin,

@@ -131,6 +131,7 @@ def test_tuning_setters_reject_a_null_context(vxp):
         "vxp_set_launch_mode": (0,),
         "vxp_set_solver_blocks_divisor": (128,),
         "vxp_set_heavy_pair_voxels": (768,),
+        "vxp_set_wait_limit_ns": (0,),
         "vxp_set_probe_tables": (0,),
         "vxp_set_solver_mode": (0,),
         "vxp_synchronize": (),

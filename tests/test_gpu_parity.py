@@ -47,6 +47,7 @@ def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=
     r = O.OracleWorld(**cfg)
     r.load_scene(scene)
     dt = np.float32(scene.dt)
+    touching = 0
     for s in range(steps):
         pairs = r.pairs()
         if own_pairs:
@@ -56,6 +57,7 @@ def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=
         else:
             g.step(dt, pairs)
         r.step(dt, pairs)
+        touching += r.stats()["manifolds"] > 0
         if s % check_every and s != steps - 1:
             continue
         gm, rm = g.manifolds(), r.manifolds()
@@ -67,6 +69,8 @@ def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=
         gb, rb = g.get_bodies(), r.get_bodies()
         assert gb.tobytes() == rb.tobytes(), f"step {s}: bodies differ in {_first_diff(gb, rb)}"
     r.close()
+    # a run of 20 steps or more must have compared some contacts, not only free fall
+    assert steps < 20 or touching >= 5, f"only {touching} of {steps} steps had a manifold"
     return g
 
 

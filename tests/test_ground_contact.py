@@ -141,7 +141,7 @@ def test_lattice_boxes_start_above_the_ground(vxp):
     w = sc.world_for_batch(np.random.default_rng(9), 96, O.mass_fn)
     assert _lowest_corner(vxp, w)[1:].min() > 0.0
     s2 = sc.config2(mass_fn=O.mass_fn, n_side=6)
-    assert _lowest_corner(vxp, s2)[2:].min() > 0.2 + 1.0
+    assert _lowest_corner(vxp, s2)[2:].min() > 0.2
 
 
 def _leave_points(half, w, dt, steps, below):

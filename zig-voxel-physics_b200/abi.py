@@ -226,6 +226,7 @@ SIGNATURES = {
     "vxp_set_solver_blocks_divisor": (_I, [_VP, _U32]),
     "vxp_set_solver_mode": (_I, [_VP, _U32]),
     "vxp_set_heavy_pair_voxels": (_I, [_VP, _U32]),
+    "vxp_set_wait_limit_ns": (_I, [_VP, ctypes.c_uint64]),
     "vxp_set_probe_tables": (_I, [_VP, _I]),
     "vxp_pairs_noalloc": (_I, [_VP, _VP, _VP, _VP, _VP, _U32, _F, _VP, _U32, _VP, _VP]),
     "vxp_batch_create": (_I, [_VP, _I, _U32, ctypes.POINTER(_VP)]),

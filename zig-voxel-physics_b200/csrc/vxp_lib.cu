@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -951,6 +952,7 @@ struct vxp_ctx {
     uint32_t solver_div = 128;
     uint32_t solver_flow = 1;
     uint32_t heavy_voxels = 768;
+    unsigned long long wait_limit_ns = 0;  // grid-barrier wait limit; 0: kGridWaitNs
     bool count_bricks = false;  // traffic accounting (C_BRICKS)
     bool record_substeps = false;
     DBuf<float> subrec;
@@ -991,6 +993,9 @@ static void cluster_config(cudaLaunchConfig_t* lc, cudaLaunchAttribute* at, uint
     lc->numAttrs = 1;
 }
 
+// Longest wait of a block at a grid barrier before it gives up (ERR_TIMEOUT).
+constexpr unsigned long long kGridWaitNs = 10ull * 1000ull * 1000ull * 1000ull;
+
 // Runs the step kernel.  device_pairs: the kernel builds the pair list itself.
 int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, float margin) {
     if (int rc = ctx->cols.sync(ctx->err)) return rc;
@@ -1016,7 +1021,7 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
         CK(cudaMemsetAsync(ctx->bar.p, 0, 2 * sizeof(GridBar), ctx->stream));
         const WorldDev* wp = ctx->d_world.p;
         GridBar* bp = ctx->bar.p;
-        unsigned long long timeout = 10ull * 1000ull * 1000ull * 1000ull;  // 10 s per barrier wait
+        const unsigned long long timeout = ctx->wait_limit_ns ? ctx->wait_limit_ns : kGridWaitNs;
         void* args[] = {(void*)&wp, (void*)&cs, (void*)&bp, (void*)&timeout};
         CK(cudaLaunchCooperativeKernel((const void*)k_step_grid, dim3(ctx->grid_blocks), dim3(kGridThreads), args,
                                        smem, ctx->stream));
@@ -1121,6 +1126,7 @@ struct NoAllocScratch {
     uint32_t* counts;
     uint32_t* offsets;
     uint32_t* total;
+    uint32_t* unordered;  // set by the scan when ids are not strictly ascending
 };
 __host__ __device__ inline NoAllocScratch noalloc_layout(unsigned char* base) {
     NoAllocScratch s;
@@ -1129,6 +1135,7 @@ __host__ __device__ inline NoAllocScratch noalloc_layout(unsigned char* base) {
     s.counts = reinterpret_cast<uint32_t*>(s.mx + kNoAllocMaxBodies);
     s.offsets = s.counts + kNoAllocMaxBodies;
     s.total = s.offsets + kNoAllocMaxBodies;
+    s.unordered = s.total + 1;
     return s;
 }
 
@@ -1172,6 +1179,7 @@ __global__ void k_noalloc_pairs(const uint32_t* ids, const uint32_t* types, uint
     const uint32_t lane = threadIdx.x & 31;
     if (sidx >= n) return;
     const NoAllocScratch s = noalloc_layout(base);
+    if (pass && *s.unordered) return;  // rejected by the scan: nothing is written
     const float4 a0 = s.mn[sidx], a1 = s.mx[sidx];
     const bool si = types[sidx] == 0u;
     const uint32_t id_s = ids[sidx];
@@ -1195,29 +1203,47 @@ __global__ void k_noalloc_pairs(const uint32_t* ids, const uint32_t* types, uint
     if (!pass && lane == 0) s.counts[sidx] = cnt;
 }
 
-__global__ void __launch_bounds__(1024) k_noalloc_scan(uint32_t n, unsigned char* base, uint32_t* count_out) {
+// Exclusive scan of the per-row counts; also checks the ids' precondition
+// (strictly ascending): when it fails, the total is 0, the flag word is set
+// and the write pass writes nothing.
+__global__ void __launch_bounds__(1024) k_noalloc_scan(uint32_t n, const uint32_t* ids, unsigned char* base,
+                                                        uint32_t* count_out) {
     const NoAllocScratch s = noalloc_layout(base);
     uint32_t carry = 0;
+    int bad = 0;
     for (uint32_t t0 = 0; t0 < n; t0 += blockDim.x) {
         const uint32_t i = t0 + threadIdx.x;
         const uint32_t v = i < n ? s.counts[i] : 0u;
+        if (i + 1 < n && ids[i] >= ids[i + 1]) bad = 1;
         uint32_t tile;
         const uint32_t ex = block_excl_scan(v, &tile);
         if (i < n) s.offsets[i] = carry + ex;
         carry += tile;
     }
+    bad = __syncthreads_or(bad);
     if (threadIdx.x == 0) {
-        *s.total = carry;
-        *count_out = carry;
+        *s.unordered = bad ? 1u : 0u;
+        *s.total = bad ? 0u : carry;
+        *count_out = bad ? 0u : carry;
     }
 }
 
 namespace {
 // Device address of g_noalloc_scratch, looked up once per device with that
 // device current (a host-side mention of the array names a host stand-in,
-// not device memory).
+// not device memory).  The address is kept for the life of the process, so
+// the device must not be reset (cudaDeviceReset) while the library is loaded:
+// the next call would hand the kernels the old context's address.
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_addr[256] = {};
+
+bool check_args_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("VXP_CHECK_ARGS");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
 
 int noalloc_scratch_for_current_device(unsigned char** out) {
     int dev = 0;
@@ -1618,6 +1644,9 @@ int vxp_pairs_noalloc(const float* positions, const float* rotations, const floa
     if (n > kNoAllocMaxBodies) return VXP_ERR_CAP;
     if (!count || (n && (!positions || !rotations || !local_aabbs || !ids || !body_types)) || (cap && !out))
         return VXP_ERR_ARG;
+    // An error the caller left pending is theirs: launch nothing and leave it
+    // in place rather than report it later as this call's failure.
+    if (cudaPeekAtLastError() != cudaSuccess) return VXP_ERR_CUDA;
     unsigned char* base = nullptr;
     if (int rc = noalloc_scratch_for_current_device(&base)) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1629,9 +1658,24 @@ int vxp_pairs_noalloc(const float* positions, const float* rotations, const floa
                                        reinterpret_cast<const float4*>(rotations),
                                        reinterpret_cast<const float4*>(local_aabbs), n, margin, base);
     k_noalloc_pairs<<<wb, tb, 0, st>>>(ids, body_types, n, base, nullptr, 0, 0);
-    k_noalloc_scan<<<1, 1024, 0, st>>>(n, base, count);
+    k_noalloc_scan<<<1, 1024, 0, st>>>(n, ids, base, count);
     k_noalloc_pairs<<<wb, tb, 0, st>>>(ids, body_types, n, base, reinterpret_cast<uint2*>(out), cap, 1);
-    return cudaGetLastError() == cudaSuccess ? VXP_OK : VXP_ERR_CUDA;
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        (void)cudaGetLastError();  // this call's launch error: reported here, so cleared
+        return VXP_ERR_CUDA;
+    }
+    // With VXP_CHECK_ARGS=1 in the environment the call also waits for its
+    // work and turns ids that are not strictly ascending into VXP_ERR_ARG;
+    // otherwise such a call only leaves *count at 0 and writes no pair.
+    if (check_args_enabled()) {
+        uint32_t unordered = 0;
+        if (cudaStreamSynchronize(st) != cudaSuccess) return VXP_ERR_CUDA;
+        if (cudaMemcpy(&unordered, noalloc_layout(base).unordered, sizeof(unordered), cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+            return VXP_ERR_CUDA;
+        if (unordered) return VXP_ERR_ARG;
+    }
+    return VXP_OK;
 }
 
 // Phase boundaries of the last step, ns since its start (diagnostics).
@@ -1733,6 +1777,12 @@ int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div) {
 int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n) {
     if (!ctx) return VXP_ERR_ARG;
     ctx->heavy_voxels = n;
+    return VXP_OK;
+}
+
+int vxp_set_wait_limit_ns(vxp_ctx* ctx, uint64_t ns) {
+    if (!ctx) return VXP_ERR_ARG;
+    ctx->wait_limit_ns = ns;
     return VXP_OK;
 }
 

@@ -541,8 +541,9 @@ def job_bodies(job: dict, mass_fn=None, vs: float = 0.1) -> np.ndarray:
 def config2(mass_fn: MassFn | None = None, n_side: int = 16, seed: int = 2, steps: int = 600) -> Scene:
     """4096 seeded random boxes (per-axis extents U{2..16} voxels, vs 0.1, sparse
     bricks, classified from neighbours, 1 kg per voxel) dropped with their
-    centres on a 16^3 jittered lattice (2.8 m spacing, lowest layer 3 m up,
-    random orientations about the centre) over a static 128x8x128 walled bin (floor and walls 2 voxels thick) that
+    centres on a 16^3 jittered lattice (2.8 m spacing, lowest layer 1.7 m up,
+    so no box, whatever its rotation about its jittered centre, starts below
+    the bin floor's top at 0.2 m) over a static 128x8x128 walled bin (floor and walls 2 voxels thick) that
     sits on a static 512x1x512 ground slab; dt 1/120, 8 substeps, 600 steps."""
     mass_fn = mass_fn or default_mass_fn()
     rng = np.random.default_rng(seed)
@@ -555,7 +556,7 @@ def config2(mass_fn: MassFn | None = None, n_side: int = 16, seed: int = 2, step
     grid = np.array([(i, j, k) for j in range(n_side) for k in range(n_side) for i in range(n_side)], dtype=np.float64)
     off = (n_side - 1) / 2.0
     half = ext * vs * 0.5
-    centre = np.stack([(grid[:, 0] - off) * sp, 3.0 + grid[:, 1] * sp, (grid[:, 2] - off) * sp], axis=1)
+    centre = np.stack([(grid[:, 0] - off) * sp, 1.7 + grid[:, 1] * sp, (grid[:, 2] - off) * sp], axis=1)
     centre += rng.uniform(-0.1, 0.1, size=centre.shape)
     rot = shoemake_quat(rng, n)
     pos = origin_for_centre(centre, rot, half)

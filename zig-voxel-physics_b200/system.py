@@ -163,6 +163,11 @@ class VoxelPhysicsSystem:
         """Pairs with at least n overlap-region voxels are probed by a whole CTA (0: never)."""
         self._check(self.lib.vxp_set_heavy_pair_voxels(self.ctx, int(n)))
 
+    def set_wait_limit_ns(self, ns: int) -> None:
+        """Grid-barrier wait limit of grid-launched steps (0: the default, 10 s);
+        a step that waits longer fails with VXP_ERR_TIMEOUT."""
+        self._check(self.lib.vxp_set_wait_limit_ns(self.ctx, int(ns)))
+
     def set_probe_tables(self, on: bool = True) -> None:
         """Neighbourhood-mask tables for the narrow phase's probes (on by default)."""
         self._check(self.lib.vxp_set_probe_tables(self.ctx, 1 if on else 0))
