@@ -16,9 +16,20 @@ memory: every step copies the pair list host->device (vxp_step) and reads the
 pair list and the body table back (vxp_pairs_from_bodies, vxp_bodies_get),
 timed by the host clock.
 
+The pile's line also carries compact runs of the other two north-star
+comparisons, on the same box: "batched" (the 256-world mix under the
+autotuned schedule against the plain single-world path, 10 timed steps) and
+"serving" (150 Poisson-arriving jobs through the continuous-batching server,
+step and job latency percentiles); --no-extras leaves them out.
+
+--workload stress: the narrow-phase stress scene (512 bodies of 64^3 voxels
+filled by value noise, 10 % overlap in a walled bin; dt 1/60, 4 substeps),
+timed from its first step; the same value / roofline / e2e / CPU baseline.
+--workload batched / serving: the full versions of the two summaries.
+
 --impl reference times the reference's CPU path (the CPU restatement of the
 reference, with its thread-pooled narrow phase on every host core and the
-single-threaded solver) on the same scene.
+single-threaded solver) on the same scene (pile or stress).
 
 Multi-GPU: a single world does not shard; N ranks run N independent replicas
 ("replicas only", weak scaling) and value is the sum of their work over the
@@ -69,9 +80,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-mode", type=int, default=-1)
     ap.add_argument("--solver", type=int, default=-1, help="grid solver mode (-1: the library default)")
-    ap.add_argument("--workload", default="pile", choices=["pile", "batched", "serving"],
-                    help="pile: the 4096-body pile (the headline); batched: 256 independent worlds; "
+    ap.add_argument("--workload", default="pile", choices=["pile", "stress", "batched", "serving"],
+                    help="pile: the 4096-body pile (the headline); stress: 512 bodies of 64^3 voxels "
+                         "(narrow-phase stress); batched: 256 independent worlds; "
                          "serving: Poisson-arriving jobs through the continuous-batching server")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="pile only: skip the batched and serving summaries the pile line carries")
     ap.add_argument("--jobs", type=int, default=300)
     ap.add_argument("--state-out", default=None, help="save the body table after settling (npy)")
     ap.add_argument("--state-in", default=None, help="start from a saved body table instead of settling")
@@ -188,11 +202,23 @@ def peaks() -> tuple:
 
 
 # --------------------------------------------------------------------------
-def run_cpu(scene, oracle, args, body_state=None, steps=None, budget_s=None, threads=None):
+def single_world_workload(vxp, args, mass_fn=None):
+    """(scene, substeps, settle steps, workload name) of a single-world run:
+    the 4096-box pile (config 2, 8 substeps at dt 1/120, settled before the
+    timed steps) or the narrow-phase stress scene (config 4, 4 substeps at
+    dt 1/60, timed from its start)."""
+    if args.workload == "stress":
+        scene = vxp.scenes.config4(mass_fn=mass_fn)
+        return scene, 4, 0, f"config4_stress_{scene.dynamic_count}"
+    scene = vxp.scenes.config2(mass_fn=mass_fn, n_side=args.n_side)
+    return scene, 8, args.settle, f"config2_pile_{scene.dynamic_count}"
+
+
+def run_cpu(scene, oracle, args, body_state=None, steps=None, budget_s=None, threads=None, substeps=8):
     """Times the reference's CPU step (threaded narrow phase on every host core,
     single-threaded solver).  Returns (body_substeps_per_s, steps_timed, threads, per-step s)."""
     threads = threads or os.cpu_count() or 1
-    w = oracle.OracleWorld(substeps=8, fixed_timestep=np.float32(1.0 / 120.0))
+    w = oracle.OracleWorld(substeps=substeps, fixed_timestep=np.float32(scene.dt), reference_caps=0)
     w.load_scene(scene)
     if body_state is not None:
         w.set_bodies(body_state)
@@ -212,7 +238,7 @@ def run_cpu(scene, oracle, args, body_state=None, steps=None, budget_s=None, thr
         if budget_s is not None and time.perf_counter() - t_start > budget_s and k >= 2:
             break
     w.close()
-    return n_dyn * 8 * k / sum(times), k, threads, times
+    return n_dyn * substeps * k / sum(times), k, threads, times
 
 
 def reference_arm(args):
@@ -225,12 +251,12 @@ def reference_arm(args):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_api
 
-    scene = vxp.scenes.config2(mass_fn=oracle_api.mass_fn, n_side=args.n_side)
+    scene, substeps, settle, workload = single_world_workload(vxp, args, oracle_api.mass_fn)
     threads = os.cpu_count() or 1
-    w = oracle_api.OracleWorld(substeps=8, fixed_timestep=np.float32(1.0 / 120.0))
+    w = oracle_api.OracleWorld(substeps=substeps, fixed_timestep=np.float32(scene.dt), reference_caps=0)
     w.load_scene(scene)
     dt = np.float32(scene.dt)
-    for _ in range(args.settle + args.warmup):
+    for _ in range(settle + args.warmup):
         w.step_threaded(dt, w.pairs(), threads)
     times = []
     for _ in range(args.steps):
@@ -239,15 +265,15 @@ def reference_arm(args):
         w.step_threaded(dt, pairs, threads)
         times.append(time.perf_counter() - t0)
     n_dyn = scene.dynamic_count
-    value = n_dyn * 8 * len(times) / sum(times)
+    value = n_dyn * substeps * len(times) / sum(times)
     line = {
         "impl": "reference", "metric": "body_substeps_per_s", "value": value, "unit": "body-substeps/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"config2_pile_{n_dyn}", "bodies": n_dyn, "substeps": 8, "dt": "1/120",
-                   "settle_steps": args.settle},
+        "config": {"workload": workload, "bodies": n_dyn, "substeps": substeps,
+                   "dt": "1/120" if substeps == 8 else "1/60", "settle_steps": settle},
         "cpu_baseline": {"value": value, "unit": "body-substeps/s", "cores": threads, "kind": "port",
-                         "sample": f"{len(times)} steps after {args.settle + args.warmup} settle/warm-up steps; "
+                         "sample": f"{len(times)} steps after {settle + args.warmup} settle/warm-up steps; "
                                    "threaded narrow phase (reference partitioning) + single-threaded solver"},
         "e2e": {"value": value, "unit": "body-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -263,11 +289,11 @@ def ours(args):
     torch.cuda.set_device(local)
     vxp = importlib.import_module("zig-voxel-physics_b200")
     abi = vxp.abi
-    scene = vxp.scenes.config2(n_side=args.n_side)
+    scene, substeps, settle, workload = single_world_workload(vxp, args)
     n_dyn = scene.dynamic_count
     n_nonstatic = int((scene.bodies["body_type"] != abi.BODY_STATIC).sum())
-    sysm = vxp.VoxelPhysicsSystem(device=local, substeps=8, fixed_timestep=np.float32(1.0 / 120.0),
-                                  max_pairs=max(65536, 16 * n_dyn), max_bodies=len(scene.bodies))
+    sysm = vxp.VoxelPhysicsSystem(device=local, substeps=substeps, fixed_timestep=np.float32(scene.dt),
+                                  reference_caps=0, max_pairs=max(65536, 16 * n_dyn), max_bodies=len(scene.bodies))
     sysm.load_scene(scene)
     sysm.set_launch_mode(args.launch_mode)
     if args.solver >= 0:
@@ -276,7 +302,7 @@ def ours(args):
     if args.state_in:
         sysm.set_bodies(np.load(args.state_in))
     else:
-        for i in range(args.settle):
+        for i in range(settle):
             sysm.step(dt)
             if i % 32 == 31:
                 sysm.synchronize()
@@ -315,9 +341,9 @@ def ours(args):
     clk = clocks.stop()
     total_s = sum(step_ms) / 1e3
     total_s = max_over_ranks(pg, total_s, f"cuda:{local}")
-    value = ws * n_dyn * 8 * args.steps / total_s
+    value = ws * n_dyn * substeps * args.steps / total_s
     pts = [s["contact_points"] for s in stats]
-    contacts_per_s = ws * sum(pts) * 8 / total_s
+    contacts_per_s = ws * sum(pts) * substeps / total_s
     bodies = sysm.get_bodies()
     n_dyn_awake = int(((bodies["body_type"] == abi.BODY_DYNAMIC) & (bodies["is_sleeping"] == 0)).sum())
     # the bricks each step's probed pairs touch (the narrow phase's per-brick
@@ -329,7 +355,7 @@ def ours(args):
         sysm.step(dt)
         st["bricks_touched"] = sysm.stats()["bricks_touched"]
     sysm.set_traffic_accounting(False)
-    nb = [sum(alg_bytes(s, 8, n_dyn_awake, n_nonstatic)) for s in stats]
+    nb = [sum(alg_bytes(s, substeps, n_dyn_awake, n_nonstatic)) for s in stats]
     peak, peak_kind = peaks()
     achieved = sum(nb) / (sum(kern_ms) / 1e3) / 1e9
     # per kernel of the step, each its algorithmic bytes over its own event
@@ -337,7 +363,7 @@ def ours(args):
     # (k_solve_grid), or the cluster kernel (k_solve_cluster: the solver's
     # bytes), after the grid's constraint table and colouring when those do
     # not run on the cluster (k_solve_grid: no per-unit byte count, time only)
-    nb_parts = [alg_bytes(s, 8, n_dyn_awake, n_nonstatic) for s in stats]
+    nb_parts = [alg_bytes(s, substeps, n_dyn_awake, n_nonstatic) for s in stats]
     grid = n_dyn >= 512
     cluster = grid and all(x[1] > 0.0 for x in split_ms)
     kernels = {}
@@ -397,7 +423,7 @@ def ours(args):
         d2h += 8 * n + 128 * len(pin_bodies)
     e2e_s = max(time.perf_counter() - t0, 1e-9)
     e2e_s = max_over_ranks(pg, e2e_s, f"cuda:{local}")
-    e2e_value = None if args.no_e2e else ws * n_dyn * 8 * args.steps / e2e_s
+    e2e_value = None if args.no_e2e else ws * n_dyn * substeps * args.steps / e2e_s
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -405,19 +431,35 @@ def ours(args):
         import oracle_api
 
         state = sysm.get_bodies()
-        v, k, threads, _ = run_cpu(scene, oracle_api, args, body_state=state, budget_s=args.cpu_sample_s)
+        v, k, threads, _ = run_cpu(scene, oracle_api, args, body_state=state, budget_s=args.cpu_sample_s,
+                                   substeps=substeps)
         cpu = {"value": v, "unit": "body-substeps/s", "cores": threads, "kind": "port",
-               "sample": f"{k} steps of the same pile from the GPU's state after {args.settle + args.warmup + args.steps} "
+               "sample": f"{k} steps of the same scene from the GPU's state after {settle + args.warmup + args.steps} "
                          "steps; threaded narrow phase (reference partitioning) + single-threaded solver"}
     sysm.close()
+    extras = {}
+    if rank == 0 and ws == 1 and args.workload == "pile" and not args.no_extras:
+        # the north-star comparisons, measured on the same box in the same run
+        # (compact versions of --workload batched / serving)
+        bl = batched(args, steps=10, warmup=3, emit=False)
+        extras["batched"] = {k: bl[k] for k in ("value", "unit", "ms_per_step", "plain_single_world",
+                                                "batched_over_plain", "world_step_latency_ms", "clocks")}
+        extras["batched"]["config"] = bl["config"]
+        sl = serving(args, jobs=150, emit=False)
+        so = sl["serving"]
+        extras["serving"] = {"value": sl["value"], "unit": sl["unit"], "config": sl["config"], "clocks": sl["clocks"],
+                             **{k: so[k] for k in ("step_ms_p50", "step_ms_p99", "job_latency_s_p50",
+                                                   "job_latency_s_p99", "jobs_finished", "wall_s",
+                                                   "mean_active_jobs")}}
     if rank == 0:
         ms = statistics.mean(step_ms)
         line = {
             "metric": "body_substeps_per_s", "value": value, "unit": "body-substeps/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"config2_pile_{n_dyn}", "bodies": n_dyn, "substeps": 8, "dt": "1/120",
-                       "settle_steps": args.settle, "l2": "flushed (256 MiB write) between timed steps",
+            "config": {"workload": workload, "bodies": n_dyn, "substeps": substeps,
+                       "dt": "1/120" if substeps == 8 else "1/60",
+                       "settle_steps": settle, "l2": "flushed (256 MiB write) between timed steps",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single world",
                        "contact_points_mean": statistics.mean(pts), "pairs_mean": statistics.mean(
                            [s["pairs_tested"] for s in stats])},
@@ -426,19 +468,20 @@ def ours(args):
                                 "kernel_mean": statistics.mean(kern_ms), "pairs_mean": statistics.mean(pair_ms)},
             "roofline": {"bound": "hbm", "achieved": kernels[dominant]["achieved"], "peak": peak, "unit": "GB/s",
                          "frac": kernels[dominant]["frac"],
-                         "traffic": PROFILED_TRAFFIC.get((f"config2_pile_{n_dyn}", dominant), (None,))[0],
-                         "traffic_source": PROFILED_TRAFFIC.get((f"config2_pile_{n_dyn}", dominant), (None, None))[1],
+                         "traffic": PROFILED_TRAFFIC.get((workload, dominant), (None,))[0],
+                         "traffic_source": PROFILED_TRAFFIC.get((workload, dominant), (None, None))[1],
                          "peak_kind": peak_kind, "kernel": dominant,
                          "alg_bytes_per_launch": kernels[dominant]["alg_bytes_per_launch"],
                          "step": {"achieved": achieved, "frac": achieved / peak,
                                   "alg_bytes_per_step": statistics.mean(nb)},
-                         "kernels": {k: dict(v, traffic=PROFILED_TRAFFIC.get((f"config2_pile_{n_dyn}", k), (None,))[0])
+                         "kernels": {k: dict(v, traffic=PROFILED_TRAFFIC.get((workload, k), (None,))[0])
                                      for k, v in kernels.items()}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "body-substeps/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
                     "d2h_bytes_per_step": d2h // max(1, args.steps)},
             "clocks": clk,
             "gpu_launches": args.steps * (len(kernels) if grid else 1),
+            **extras,
         }
         print(json.dumps(line), flush=True)
     if pg:
@@ -447,31 +490,43 @@ def ours(args):
     return 0
 
 
-def batched(args):
+def batched(args, steps=None, warmup=None, emit=True, dist_ctx=(1, 0, 0, None)):
     """256 independent worlds (bodies per world floor(exp(U(ln 8, ln 2048))),
     config-2 shapes, own 64x1x64 slab, dt 1/60, 4 substeps) stepped by one
     graph-replayed launch per step under the autotuned schedule, against the
-    plain single-world path stepping the same worlds one after another."""
+    plain single-world path stepping the same worlds one after another.
+    With N ranks the worlds are sharded by estimated cost (sharding.partition,
+    the same on every rank, no exchange); times are the slowest rank's and the
+    plain path's time is the sum over ranks (one GPU stepping every world).
+    Returns the line (printed on rank 0 when emit)."""
     import torch
 
+    ws, rank, local, pg = dist_ctx
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     vxp = importlib.import_module("zig-voxel-physics_b200")
-    scenes = vxp.scenes.config3(n_worlds=args.worlds)
+    all_scenes = vxp.scenes.config3(n_worlds=args.worlds)
+    n_dyn = sum(sc.dynamic_count for sc in all_scenes)
+    parts = vxp.sharding.partition([vxp.sharding.world_cost(sc.dynamic_count) for sc in all_scenes], ws)
+    scenes = [all_scenes[i] for i in parts[rank]]
     dt = np.float32(1.0 / 60.0)
-    n_dyn = sum(sc.dynamic_count for sc in scenes)
-    b = vxp.VoxelWorldBatch(len(scenes), substeps=4)
+    b = vxp.VoxelWorldBatch(len(scenes), substeps=4, device=local)
     off = 0
     for i, sc in enumerate(scenes):
         b.load_scene(i, sc, collider_offset=off)
         off += len(sc.colliders) + 1
     choice, tune_ms = b.autotune(dt, trial_steps=2)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         b.step(dt)
         b.synchronize()
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    clocks = Clocks(0)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    clocks = Clocks(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
     clocks.start()
     step_ms, world_ms = [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
         b.step(dt)
@@ -480,23 +535,24 @@ def batched(args):
         step_ms.append(tot)
         world_ms.append(per[per > 0])
     clk = clocks.stop()
-    value = n_dyn * 4 * args.steps / (sum(step_ms) / 1e3)
+    batch_s = max_over_ranks(pg, sum(step_ms) / 1e3, f"cuda:{local}")
+    value = n_dyn * 4 * steps / batch_s
     # e2e: the same steps with every world's body table read back each step
     bufs = [np.zeros(len(sc.bodies), dtype=vxp.abi.BODY_DTYPE) for sc in scenes]
     d2h = 0
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         b.step(dt)
         b.synchronize()
         for i in range(len(scenes)):
             b._check(b.lib.vxp_batch_world_get(b.b, i, vxp.abi.ptr(bufs[i]), len(bufs[i])))
             d2h += bufs[i].nbytes
-    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(pg, time.perf_counter() - t0, f"cuda:{local}")
     b.close()
     # plain path: each world stepped alone by its own launches, one world after another
     plain_ms = 0.0
     for sc in scenes:
-        s = vxp.VoxelPhysicsSystem(substeps=4)
+        s = vxp.VoxelPhysicsSystem(substeps=4, device=local)
         s.load_scene(sc)
         for _ in range(2):
             s.step(dt)
@@ -509,13 +565,25 @@ def batched(args):
             tt.append(float(out[2]))
         plain_ms += statistics.mean(tt)
         s.close()
+    if pg:
+        import torch.distributed as dist
+
+        t = torch.tensor([plain_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        plain_ms = float(t.item())
+        gathered = [None] * ws
+        dist.all_gather_object(gathered, [float(x) for x in np.concatenate(world_ms)] if world_ms else [])
+        wm = np.array([x for g in gathered for x in g]) if any(gathered) else np.zeros(1)
+    else:
+        wm = np.concatenate(world_ms) if world_ms else np.zeros(1)
     plain_value = n_dyn * 4 / (plain_ms / 1e3)
-    wm = np.concatenate(world_ms) if world_ms else np.zeros(1)
     line = {
-        "metric": "body_substeps_per_s", "value": value, "unit": "body-substeps/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"config3_batched_{len(scenes)}", "worlds": len(scenes), "bodies": n_dyn,
+        "metric": "body_substeps_per_s", "value": value, "unit": "body-substeps/s", "n_gpus": ws,
+        "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * batch_s / steps,
+        "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"config3_batched_{len(all_scenes)}", "worlds": len(all_scenes), "bodies": n_dyn,
+                   "parallelism": f"worlds sharded over {ws} GPUs by estimated cost" if ws > 1 else "one GPU",
                    "substeps": 4, "dt": "1/60", "l2": "flushed (256 MiB write) between timed steps",
                    "schedule": {"choice": ["256/slot", "256/longest-first", "512/slot", "512/longest-first"][choice],
                                 "autotune_ms": [float(x) for x in tune_ms]}},
@@ -524,57 +592,93 @@ def batched(args):
         "batched_over_plain": value / plain_value,
         "world_step_latency_ms": {"p50": float(np.percentile(wm, 50)), "p99": float(np.percentile(wm, 99)),
                                   "max": float(wm.max())},
-        "e2e": {"value": n_dyn * 4 * args.steps / e2e_s, "unit": "body-substeps/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": d2h // args.steps},
+        "e2e": {"value": n_dyn * 4 * steps / e2e_s, "unit": "body-substeps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": d2h // steps},
         "clocks": clk,
-        "gpu_launches": args.steps,
+        "gpu_launches": steps,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    if emit and rank == 0:
+        print(json.dumps(line), flush=True)
+    return line
 
 
-def serving(args):
+def serving(args, jobs=None, emit=True, dist_ctx=(1, 0, 0, None)):
     """Jobs arrive as a Poisson process (mean 200 jobs/s), each a world of
     log-uniform 16..4096 config-2 boxes over its own slab running a uniform
     60..600 steps of dt 1/60 with 4 substeps; admitted against a 120 GB
-    device-memory budget into a continuously batched set of world slots."""
+    device-memory budget into a continuously batched set of world slots.
+    With N ranks each job goes to one rank by estimated outstanding work
+    (sharding.assign_jobs, the same on every rank, no exchange) and every rank
+    serves its jobs on its own GPU; throughput is all jobs' work over the
+    slowest rank's wall time, latency percentiles are over all jobs and steps.
+    Returns the line (printed on rank 0 when emit)."""
+    ws, rank, local, pg = dist_ctx
+    n_jobs = args.jobs if jobs is None else jobs
     vxp = importlib.import_module("zig-voxel-physics_b200")
     sc = vxp.scenes
     lib = sc.shape_library()
-    specs = sc.serving_jobs(args.jobs, seed=5)
-    jobs = [vxp.server.Job(i, j["arrival"], sc.job_bodies(j), j["steps"]) for i, j in enumerate(specs)]
-    batch = vxp.VoxelWorldBatch(args.slots, substeps=4)
+    specs = sc.serving_jobs(n_jobs, seed=5)
+    owner = vxp.sharding.assign_jobs(specs, ws)
+    jobs = [vxp.server.Job(i, j["arrival"], sc.job_bodies(j), j["steps"]) for i, j in enumerate(specs)
+            if owner[i] == rank]
+    batch = vxp.VoxelWorldBatch(args.slots, substeps=4, device=local)
     for c in lib:
         batch.add_collider(c.id, c.voxel_size, c.bricks)
     batch.set_schedule(512, 1)
     server = vxp.server.SimulationServer(batch, 1.0 / 60.0, max_slots=args.slots, budget_bytes=120 * 10**9)
-    clocks = Clocks(0)
+    clocks = Clocks(local)
+    if pg:
+        pg.barrier()
     clocks.start()
     out = server.run(jobs)
     clk = clocks.stop()
     batch.close()
+    if pg:
+        import torch.distributed as dist
+
+        mine = (out["body_substeps"], out["wall_s"], list(server.step_ms),
+                [j.finished_at - j.arrival for j in server.finished], out["jobs_finished"])
+        got = [None] * ws
+        dist.all_gather_object(got, mine)
+        wall = max(g[1] for g in got)
+        steps_ms = [x for g in got for x in g[2]]
+        lat = [x for g in got for x in g[3]]
+        out = dict(out, body_substeps=sum(g[0] for g in got), wall_s=wall,
+                   body_substeps_per_s=sum(g[0] for g in got) / wall if wall > 0 else 0.0,
+                   steps=len(steps_ms), jobs_finished=sum(g[4] for g in got), jobs_total=n_jobs,
+                   step_ms_p50=float(np.percentile(steps_ms, 50)), step_ms_p99=float(np.percentile(steps_ms, 99)),
+                   job_latency_s_p50=float(np.percentile(lat, 50)), job_latency_s_p99=float(np.percentile(lat, 99)))
     line = {
         "metric": "body_substeps_per_s", "value": out["body_substeps_per_s"], "unit": "body-substeps/s",
-        "n_gpus": 1, "steps": out["steps"], "warmup": 0, "ms_per_step": out["step_ms_p50"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "config5_serving", "jobs": args.jobs, "arrival_rate_per_s": 200,
+        "n_gpus": ws, "steps": out["steps"], "warmup": 0, "ms_per_step": out["step_ms_p50"],
+        "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "config5_serving", "jobs": n_jobs, "arrival_rate_per_s": 200,
+                   "parallelism": f"jobs sharded over {ws} GPUs by estimated work" if ws > 1 else "one GPU",
                    "bodies": "log-uniform 16..4096", "steps": "uniform 60..600", "dt": "1/60", "substeps": 4,
                    "slots": args.slots, "budget_bytes": 120 * 10**9},
         "serving": out,
         "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    if emit and rank == 0:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
-    if args.workload == "batched":
-        return batched(args)
-    if args.workload == "serving":
-        return serving(args)
+    if args.workload in ("batched", "serving"):
+        ws, rank, local, pg = dist_setup(args)
+        import torch
+
+        torch.cuda.set_device(local)
+        (batched if args.workload == "batched" else serving)(args, dist_ctx=(ws, rank, local, pg))
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return 0
     return ours(args)
 
 

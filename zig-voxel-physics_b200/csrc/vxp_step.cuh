@@ -980,6 +980,176 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
     }
 }
 
+// The same replay on a whole CTA (the grid step's CTA 0, which detects
+// nothing), for tables of at least 64 x 16 slots.  Up to kCtaReplayPending
+// lookups are pending, in order, one per thread; each round every pending
+// lookup whose window overlaps no earlier pending one is ready (the
+// sixty-fourths prefix OR of cache_replay, over the block), the ready ones run
+// at once, each scanned by sixteen lanes (a ballot finds the first empty slot
+// and the key, a min-reduction the least recently used slot), and the rest
+// move up in order.  The windows of a round are disjoint, so every lookup
+// sees the state the sequential replay gives it.  scratch: at least
+// cta_replay_scratch_bytes() bytes (the block's unused warp scratch).
+constexpr uint32_t kCtaReplayPending = 256;
+__host__ __device__ constexpr size_t cta_replay_scratch_bytes() {
+    return 2u * kCtaReplayPending * sizeof(CacheLook) + kCtaReplayPending * sizeof(uint16_t) +
+           32u * sizeof(unsigned long long) + 32u * sizeof(uint32_t) + 4u * sizeof(uint32_t);
+}
+
+__device__ void cache_replay_cta(WorldDev& w, const CacheSmem& t, unsigned char* scratch) {
+    const uint32_t tid = threadIdx.x, T = blockDim.x, lane = tid & 31u, wid = tid >> 5;
+    const uint32_t cap = w.cache_cap;
+    const uint32_t frame = (uint32_t)w.cframe[0];
+    const uint32_t n = w.ctr[C_NCACHE];
+    CacheLook* bufA = reinterpret_cast<CacheLook*>(scratch);
+    CacheLook* bufB = bufA + kCtaReplayPending;
+    uint16_t* rdy = reinterpret_cast<uint16_t*>(bufB + kCtaReplayPending);
+    unsigned long long* s_or = reinterpret_cast<unsigned long long*>(rdy + kCtaReplayPending);
+    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_or + 32);
+    uint32_t* s_tot = s_cnt + 32;
+    for (uint32_t i = tid; i < cap; i += T) {
+        const CacheKeyRec k = w.ckey[i];
+        t.ab[i] = make_uint2(k.a, k.b);
+        t.th[i] = k.th;
+        t.lu[i] = k.valid ? (uint32_t)k.last_used : 0u;
+    }
+    uint32_t hits = 0, misses = 0, evictions = 0;
+    CacheLook* P = bufA;
+    CacheLook* Q = bufB;
+    uint32_t np = 0, taken = 0;
+    const uint32_t nw = (kCtaReplayPending + 31u) / 32u;  // warps holding pending entries
+    for (;;) {
+        // fill the pending list up to its capacity, in order
+        const uint32_t take = min(kCtaReplayPending - np, n - taken);
+        for (uint32_t i = tid; i < take; i += T) P[np + i] = w.clist[taken + i];
+        taken += take;
+        np += take;
+        __syncthreads();
+        if (np == 0u) break;
+        // ready: no earlier pending window in the same or an adjacent sixty-fourth
+        const bool pending = tid < np;
+        uint32_t bk = 0;
+        unsigned long long m = 0ull;
+        if (pending) {
+            bk = (uint32_t)(((unsigned long long)P[tid].start * 64ull) / cap);
+            m = 1ull << bk;
+        }
+        unsigned long long inc = m;
+#pragma unroll
+        for (uint32_t d = 1; d < 32u; d <<= 1) {
+            const unsigned long long o = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc |= o;
+        }
+        if (lane == 31u && wid < nw) s_or[wid] = inc;
+        __syncthreads();
+        unsigned long long ex = __shfl_up_sync(0xffffffffu, inc, 1);
+        if (lane == 0u) ex = 0ull;
+        for (uint32_t k = 0; k < wid && k < nw; ++k) ex |= s_or[k];
+        const unsigned long long near =
+            m | (m << 1) | (m >> 1) | (bk == 0u ? 1ull << 63 : 0ull) | (bk == 63u ? 1ull : 0ull);
+        const bool ready = pending && !(ex & near);
+        // positions: ready ones in a list, the others moved up into Q in order
+        const uint32_t c = ready ? 1u : (pending ? 0x10000u : 0u);
+        uint32_t ci = c;
+#pragma unroll
+        for (uint32_t d = 1; d < 32u; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, ci, d);
+            if (lane >= d) ci += o;
+        }
+        if (lane == 31u && wid < nw) s_cnt[wid] = ci;
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t run = 0;
+            for (uint32_t k = 0; k < nw; ++k) {
+                const uint32_t v = s_cnt[k];
+                s_cnt[k] = run;
+                run += v;
+            }
+            *s_tot = run;
+        }
+        __syncthreads();
+        const uint32_t off = (wid < nw ? s_cnt[wid] : 0u) + ci - c;
+        if (ready) rdy[off & 0xFFFFu] = (uint16_t)tid;
+        else if (pending) Q[off >> 16] = P[tid];
+        __syncthreads();
+        const uint32_t tot = *s_tot, nready = tot & 0xFFFFu;
+        // the ready lookups, sixteen lanes each (the windows are disjoint)
+        const uint32_t l16 = tid & 15u, grp = tid >> 4, ngrp = T >> 4;
+        const uint32_t half = (lane >> 4) << 4;
+        for (uint32_t j0 = 0; j0 < nready; j0 += ngrp) {
+            const uint32_t j = j0 + grp;
+            const bool act = j < nready;
+            CacheLook L{0u, 0u, 0u, 0u, 0ull};
+            if (act) L = P[rdy[j]];
+            uint32_t x = L.start + l16;
+            if (x >= cap) x -= cap;
+            bool empty = false, match = false;
+            unsigned long long key = ~0ull;
+            if (act) {
+                const uint32_t lu = t.lu[x];
+                const uint2 ab = t.ab[x];
+                const unsigned long long th = t.th[x];
+                empty = lu == 0u;
+                match = !empty && ab.x == L.a && ab.y == L.b && th == L.th;
+                if (!empty) key = ((unsigned long long)lu << 32) | l16;
+            }
+            const uint32_t be = (__ballot_sync(0xffffffffu, empty) >> half) & 0xFFFFu;
+            const uint32_t bm = (__ballot_sync(0xffffffffu, match) >> half) & 0xFFFFu;
+#pragma unroll
+            for (uint32_t d = 8; d > 0; d >>= 1) {
+                const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, d, 16);
+                key = o < key ? o : key;
+            }
+            if (act && l16 == 0u) {
+                const uint32_t fi = be ? (uint32_t)(__ffs(be) - 1) : 16u;
+                const uint32_t fm = bm ? (uint32_t)(__ffs(bm) - 1) : 16u;
+                const uint32_t mi = (uint32_t)(key & 0xFFFFu);
+                const bool hit = fm < fi;
+                const bool evict = !hit && fi == 16u;
+                uint32_t target = L.start + (hit ? fm : (evict ? mi : fi));
+                if (target >= cap) target -= cap;
+                PairInfo& pi = w.pinfo[L.p];
+                t.lu[target] = frame;
+                if (hit) {
+                    pi.hit = 1u;
+                    ++hits;
+                } else {
+                    t.ab[target] = make_uint2(L.a, L.b);
+                    t.th[target] = L.th;
+                    w.cwriter[target] = L.p;
+                    pi.hit = 2u;
+                    ++misses;
+                    if (evict) ++evictions;
+                }
+                pi.cache_slot = target;
+            }
+        }
+        __syncthreads();
+        CacheLook* tmp = P;
+        P = Q;
+        Q = tmp;
+        np = tot >> 16;
+    }
+    for (uint32_t i = tid; i < cap; i += T) {
+        CacheKeyRec k;
+        k.a = t.ab[i].x;
+        k.b = t.ab[i].y;
+        k.th = t.th[i];
+        k.last_used = t.lu[i];
+        k.valid = t.lu[i] != 0u ? 1u : 0u;
+        k._pad = 0u;
+        w.ckey[i] = k;
+    }
+    hits = warp_sum(hits);
+    misses = warp_sum(misses);
+    evictions = warp_sum(evictions);
+    if (lane == 0 && (hits | misses | evictions)) {
+        atomicAdd(&w.ctr[C_CACHE_HITS], hits);
+        atomicAdd(&w.ctr[C_CACHE_MISSES], misses);
+        atomicAdd(&w.ctr[C_CACHE_EVICTIONS], evictions);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Phase: probe (detectVoxelCollisions + checkNeighborhood + addContact)
 // ---------------------------------------------------------------------------
@@ -1603,14 +1773,19 @@ __device__ bool phase_probe(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
                             const CacheSmem& csm) {
     const uint32_t lane = threadIdx.x & 31;
     WarpManifold& sm = warp_sm[threadIdx.x >> 5];
-    // one warp replays the cache lookups, the others start detecting at once
-    if (w.cfg.use_cache && g.rank() < 32u) cache_replay(w, csm);
-    // large regions first, one CTA each, then the rest one warp each.  On a
-    // grid, the CTA whose warp replays the cache detects nothing: the replay
-    // is a chain of dependent lookups, and other warps on its SM slow it down
-    // more than their work is worth.
-    const uint32_t nh = *(volatile uint32_t*)&w.ctr[C_NHEAVY];
+    // the cache lookups are replayed by one CTA of a grid (which detects
+    // nothing: the replay is a chain of dependent rounds, and other work on
+    // its SM would slow it more than it is worth), or by one warp of a lone
+    // CTA while its other warps start detecting at once
     const bool replay_cta = w.cfg.use_cache && g.nblocks() > 1u && g.block() == 0u;
+    if (replay_cta && w.cache_cap >= 64u * 16u &&
+        (size_t)(blockDim.x >> 5) * sizeof(WarpManifold) >= cta_replay_scratch_bytes()) {
+        cache_replay_cta(w, csm, reinterpret_cast<unsigned char*>(warp_sm));
+        return g.sync();
+    }
+    if (w.cfg.use_cache && g.rank() < 32u) cache_replay(w, csm);
+    // large regions first, one CTA each, then the rest one warp each
+    const uint32_t nh = *(volatile uint32_t*)&w.ctr[C_NHEAVY];
     if (replay_cta) return g.sync();
     if (nh) {
         __shared__ uint32_t s_h;
