@@ -80,9 +80,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-mode", type=int, default=-1)
     ap.add_argument("--solver", type=int, default=-1, help="grid solver mode (-1: the library default)")
-    ap.add_argument("--workload", default="pile", choices=["pile", "stress", "batched", "serving"],
-                    help="pile: the 4096-body pile (the headline); stress: 512 bodies of 64^3 voxels "
-                         "(narrow-phase stress); batched: 256 independent worlds; "
+    ap.add_argument("--workload", default="pile", choices=["pile", "small", "stress", "batched", "serving"],
+                    help="pile: the 4096-body pile (the headline); small: the 64 cubes of config 1 (100 steps "
+                         "in); stress: 512 bodies of 64^3 voxels (narrow-phase stress); "
+                         "batched: 256 independent worlds; "
                          "serving: Poisson-arriving jobs through the continuous-batching server")
     ap.add_argument("--no-extras", action="store_true",
                     help="pile only: skip the batched and serving summaries the pile line carries")
@@ -92,6 +93,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--slots", type=int, default=512)
     ap.add_argument("--worlds", type=int, default=256)
+    ap.add_argument("--batch-settle", type=int, default=150,
+                    help="batched: untimed steps before the autotuner and the timed steps (mid-run state)")
     return ap.parse_args()
 
 
@@ -205,11 +208,15 @@ def peaks() -> tuple:
 def single_world_workload(vxp, args, mass_fn=None):
     """(scene, substeps, settle steps, workload name) of a single-world run:
     the 4096-box pile (config 2, 8 substeps at dt 1/120, settled before the
-    timed steps) or the narrow-phase stress scene (config 4, 4 substeps at
-    dt 1/60, timed from its start)."""
+    timed steps), the 64 cubes (config 1, 4 substeps at dt 1/60, from step
+    100) or the narrow-phase stress scene (config 4, 4 substeps at dt 1/60,
+    timed from its start)."""
     if args.workload == "stress":
         scene = vxp.scenes.config4(mass_fn=mass_fn)
         return scene, 4, 0, f"config4_stress_{scene.dynamic_count}"
+    if args.workload == "small":
+        scene = vxp.scenes.config1(mass_fn=mass_fn)
+        return scene, 4, 100, f"config1_small_{scene.dynamic_count}"
     scene = vxp.scenes.config2(mass_fn=mass_fn, n_side=args.n_side)
     return scene, 8, args.settle, f"config2_pile_{scene.dynamic_count}"
 
@@ -511,10 +518,16 @@ def batched(args, steps=None, warmup=None, emit=True, dist_ctx=(1, 0, 0, None)):
     scenes = [all_scenes[i] for i in parts[rank]]
     dt = np.float32(1.0 / 60.0)
     b = vxp.VoxelWorldBatch(len(scenes), substeps=4, device=local)
-    off = 0
+    off, offs = 0, []
     for i, sc in enumerate(scenes):
         b.load_scene(i, sc, collider_offset=off)
+        offs.append(off)
         off += len(sc.colliders) + 1
+    # half-way through the configuration's 300 steps: the lower layers of
+    # every world have landed, so the timed steps carry contacts
+    if args.batch_settle:
+        b.step(dt, args.batch_settle)
+        b.synchronize()
     choice, tune_ms = b.autotune(dt, trial_steps=2)
     for _ in range(warmup):
         b.step(dt)
@@ -548,12 +561,19 @@ def batched(args, steps=None, warmup=None, emit=True, dist_ctx=(1, 0, 0, None)):
             b._check(b.lib.vxp_batch_world_get(b.b, i, vxp.abi.ptr(bufs[i]), len(bufs[i])))
             d2h += bufs[i].nbytes
     e2e_s = max_over_ranks(pg, time.perf_counter() - t0, f"cuda:{local}")
+    states = []
+    for i, sc in enumerate(scenes):
+        st = b.get_world(i)
+        st["collider_id"] -= offs[i]
+        states.append(st)
     b.close()
-    # plain path: each world stepped alone by its own launches, one world after another
+    # plain path: each world stepped alone by its own launches, one world
+    # after another, from the state the batch reached
     plain_ms = 0.0
-    for sc in scenes:
+    for sc, st in zip(scenes, states):
         s = vxp.VoxelPhysicsSystem(substeps=4, device=local)
         s.load_scene(sc)
+        s.set_bodies(st)
         for _ in range(2):
             s.step(dt)
         s.synchronize()
@@ -583,12 +603,14 @@ def batched(args, steps=None, warmup=None, emit=True, dist_ctx=(1, 0, 0, None)):
         "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"config3_batched_{len(all_scenes)}", "worlds": len(all_scenes), "bodies": n_dyn,
+                   "settle_steps": args.batch_settle,
                    "parallelism": f"worlds sharded over {ws} GPUs by estimated cost" if ws > 1 else "one GPU",
                    "substeps": 4, "dt": "1/60", "l2": "flushed (256 MiB write) between timed steps",
                    "schedule": {"choice": ["256/slot", "256/longest-first", "512/slot", "512/longest-first"][choice],
                                 "autotune_ms": [float(x) for x in tune_ms]}},
         "plain_single_world": {"value": plain_value, "ms_per_batch_step": plain_ms,
-                               "method": "each world alone, its own launches, 3 timed steps after 2, summed"},
+                               "method": "each world alone from the batch's state, its own launches, "
+                                         "3 timed steps after 2, summed"},
         "batched_over_plain": value / plain_value,
         "world_step_latency_ms": {"p50": float(np.percentile(wm, 50)), "p99": float(np.percentile(wm, 99)),
                                   "max": float(wm.max())},

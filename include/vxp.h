@@ -306,7 +306,7 @@ int vxp_set_solver_blocks_divisor(vxp_ctx* ctx, uint32_t div);
 
 /* Narrow-phase work split: a pair whose overlap region holds at least n
  * voxels is probed by a whole CTA before the other pairs, which are probed one
- * warp each (default 768; 0: every pair by one warp; the worlds of a batch,
+ * warp each (default 2048; 0: every pair by one warp; the worlds of a batch,
  * one CTA each, use 1024).  Results do not depend on it. */
 int vxp_set_heavy_pair_voxels(vxp_ctx* ctx, uint32_t n);
 

@@ -951,7 +951,7 @@ struct vxp_ctx {
     int use_grid = -1;  // -1 auto, 0 block, 1 grid
     uint32_t solver_div = 128;
     uint32_t solver_flow = 1;
-    uint32_t heavy_voxels = 768;
+    uint32_t heavy_voxels = 2048;
     unsigned long long wait_limit_ns = 0;  // grid-barrier wait limit; 0: kGridWaitNs
     bool count_bricks = false;  // traffic accounting (C_BRICKS)
     bool record_substeps = false;

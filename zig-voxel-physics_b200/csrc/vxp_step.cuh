@@ -977,6 +977,7 @@ __device__ void cache_replay(WorldDev& w, const CacheSmem& t) {
         w.ctr[C_CACHE_HITS] += hits;
         w.ctr[C_CACHE_MISSES] += misses;
         w.ctr[C_CACHE_EVICTIONS] += evictions;
+        if (w.ts) w.ts[TS_CACHE] = global_ns();  // end of the replay (diagnostics)
     }
 }
 
@@ -1148,6 +1149,7 @@ __device__ void cache_replay_cta(WorldDev& w, const CacheSmem& t, unsigned char*
         atomicAdd(&w.ctr[C_CACHE_MISSES], misses);
         atomicAdd(&w.ctr[C_CACHE_EVICTIONS], evictions);
     }
+    if (tid == 0 && w.ts) w.ts[TS_CACHE] = global_ns();  // end of the replay (diagnostics)
 }
 
 // ---------------------------------------------------------------------------
