@@ -220,6 +220,51 @@ int vxp_abi_version(void);
 int vxp_collider_upload(vxp_ctx* ctx, uint32_t collider_id, float voxel_size,
                         const vxp_brick* bricks, uint32_t n_bricks);
 
+/* Collider edits, for destructible or growing voxel bodies.  An edit batch
+ * writes n voxels of an uploaded collider (coords: 3 ints per voxel, in the
+ * collider's voxel space) and then does what the reference's caller does
+ * after setCollisionVoxel (src/collider.zig:267-273): recomputeMetadata
+ * (src/collider.zig:283-333).  Modes:
+ *   VXP_EDIT_SET        values[i] is the CollisionVoxel byte stored
+ *                       (src/collision_voxel.zig:133-167: type in bits 0-2,
+ *                       normal index in bits 3-7), as setCollisionVoxel stores it;
+ *   VXP_EDIT_OCCUPANCY  values[i] != 0 makes the voxel solid, 0 empty; then
+ *                       every listed voxel and each of its six face
+ *                       neighbours that is solid is re-typed by
+ *                       classifyFromNeighbors (src/collision_voxel.zig:213-235,
+ *                       exported by src/physics.zig:52) of the new occupancy.
+ * Writes run in list order (a voxel listed twice keeps its last value).  A
+ * voxel whose brick the collider lacks gets a new brick, as getOrCreateBrick
+ * (src/collider.zig:232-239) makes one, in the order the writes reach them.
+ * The edit is queued on the context's stream after the steps already queued,
+ * and the next step sees it; the bodies' collider ids are unchanged.  Cached
+ * brick-pair results of the bodies that use the collider stay valid until
+ * vxp_invalidate_cache_for_body drops them, as in the reference. */
+#define VXP_EDIT_SET 0
+#define VXP_EDIT_OCCUPANCY 1
+int vxp_collider_edit(vxp_ctx* ctx, uint32_t collider_id, const int32_t* coords,
+                      const uint8_t* values, uint32_t n, int mode);
+
+/* The collider as the device holds it: metadata, and up to cap bricks (in
+ * the collider's brick order: uploaded bricks first, then those that edits
+ * created).  *n_bricks gets the collider's brick count.  bricks may be null. */
+typedef struct vxp_collider_info {
+    float voxel_size;
+    int32_t min_bound[3], max_bound[3];  /* voxel coordinates, max exclusive */
+    float aabb_min[3], aabb_max[3];      /* local AABB */
+    uint32_t solid_count;
+    uint32_t n_bricks;
+    uint32_t has_table;                  /* the probes use a neighbourhood-mask table */
+} vxp_collider_info;
+int vxp_collider_read(vxp_ctx* ctx, uint32_t collider_id, vxp_collider_info* info,
+                      vxp_brick* bricks, uint32_t cap, uint32_t* n_bricks);
+
+/* NarrowPhase.invalidateCacheForBody (src/narrow_phase.zig:1399-1403): every
+ * brick-pair cache entry of the body becomes invalid.  *n_invalidated (may be
+ * null; when given, the call waits for the device) gets their number, the
+ * cache's invalidations statistic (src/narrow_phase.zig:305-312). */
+int vxp_invalidate_cache_for_body(vxp_ctx* ctx, uint32_t body_id, uint32_t* n_invalidated);
+
 /* Replaces the per-slot body state that step() reads and writes.  Bodies are
  * kept in the order given (the solver's addBody order, src/system.zig:677-681). */
 int vxp_bodies_set(vxp_ctx* ctx, const vxp_body* bodies, uint32_t n);
@@ -393,6 +438,15 @@ void vxp_batch_destroy(vxp_batch* b);
 int vxp_batch_last_error(const vxp_batch* b, char* buf, size_t n);
 int vxp_batch_collider_upload(vxp_batch* b, uint32_t collider_id, float voxel_size, const vxp_brick* bricks,
                               uint32_t n_bricks);
+/* vxp_collider_edit / vxp_collider_read on the batch's shared colliders (every
+ * world whose bodies use the collider sees the edit), and
+ * vxp_invalidate_cache_for_body on one world's cache. */
+int vxp_batch_collider_edit(vxp_batch* b, uint32_t collider_id, const int32_t* coords,
+                            const uint8_t* values, uint32_t n, int mode);
+int vxp_batch_collider_read(vxp_batch* b, uint32_t collider_id, vxp_collider_info* info,
+                            vxp_brick* bricks, uint32_t cap, uint32_t* n_bricks);
+int vxp_batch_invalidate_cache_for_body(vxp_batch* b, uint32_t world, uint32_t body_id,
+                                        uint32_t* n_invalidated);
 /* (Re)starts world slot `world` with these bodies: empty contact manager and
  * brick-pair cache.  pair_capacity 0 = 16 x n (grown on demand).  A slot
  * that held a world before reuses its device buffers (zeroed, grown when too

@@ -150,6 +150,39 @@ template <class R> void manifoldOut(const Manifold<R>& m, vxp_manifold* o) {
     }
 }
 
+template <class R>
+int readCollider(Handle<R>& h, uint32_t collider_id, vxp_collider_info* info, vxp_brick* bricks, uint32_t cap,
+                 uint32_t* n_out) {
+    auto it = h.cmap.find(collider_id);
+    if (it == h.cmap.end()) return VXP_ERR_ARG;
+    const Collider<R>& c = h.w.colliders[(size_t)it->second];
+    const uint32_t n = (uint32_t)c.bricks.size();
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->voxel_size = (float)c.voxel_size;
+        const int32_t mn[3] = {c.min_bound.x, c.min_bound.y, c.min_bound.z};
+        const int32_t mx[3] = {c.max_bound.x, c.max_bound.y, c.max_bound.z};
+        const R amn[3] = {c.local_aabb.mn.x, c.local_aabb.mn.y, c.local_aabb.mn.z};
+        const R amx[3] = {c.local_aabb.mx.x, c.local_aabb.mx.y, c.local_aabb.mx.z};
+        for (int k = 0; k < 3; ++k) {
+            info->min_bound[k] = mn[k];
+            info->max_bound[k] = mx[k];
+            info->aabb_min[k] = (float)amn[k];
+            info->aabb_max[k] = (float)amx[k];
+        }
+        info->solid_count = c.solid_count;
+        info->n_bricks = n;
+    }
+    if (n_out) *n_out = n;
+    for (uint32_t b = 0; bricks && b < std::min(cap, n); ++b) {
+        bricks[b].pos[0] = c.bricks[b].pos.x;
+        bricks[b].pos[1] = c.bricks[b].pos.y;
+        bricks[b].pos[2] = c.bricks[b].pos.z;
+        std::memcpy(bricks[b].voxels, c.bricks[b].vox, 512);
+    }
+    return VXP_OK;
+}
+
 Obb<float> obbIn(const float* a) {
     return {{a[0], a[1], a[2]}, {a[3], a[4], a[5]}, {a[6], a[7], a[8], a[9]}};
 }
@@ -190,6 +223,35 @@ int vxo_collider_add(void* p, uint32_t collider_id, float vs, const vxp_brick* b
         }
     });
     return rc;
+}
+
+int vxo_collider_edit(void* p, uint32_t collider_id, const int32_t* coords, const uint8_t* values, uint32_t n,
+                      int mode) {
+    if (mode != 0 && mode != 1) return VXP_ERR_ARG;
+    int rc = 0;
+    DISPATCH(p, {
+        auto it = h->cmap.find(collider_id);
+        if (it == h->cmap.end()) rc = VXP_ERR_ARG;
+        else h->w.colliders[(size_t)it->second].edit(coords, values, n, mode);
+    });
+    return rc;
+}
+
+int vxo_collider_read(void* p, uint32_t collider_id, vxp_collider_info* info, vxp_brick* bricks, uint32_t cap,
+                      uint32_t* n_out) {
+    int rc = 0;
+    DISPATCH(p, rc = readCollider(*h, collider_id, info, bricks, cap, n_out));
+    return rc;
+}
+
+uint32_t vxo_invalidate_cache_for_body(void* p, uint32_t body_id) {
+    uint32_t n = 0;
+    DISPATCH(p, {
+        const uint64_t before = h->w.cache.invalidations;
+        h->w.cache.invalidateBody(body_id);
+        n = (uint32_t)(h->w.cache.invalidations - before);
+    });
+    return n;
 }
 
 int vxo_bodies_set(void* p, const vxp_body* b, uint32_t n) {

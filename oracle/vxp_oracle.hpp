@@ -484,6 +484,53 @@ template <class R> struct Collider {
             max_bound = {0, 0, 0};
         }
     }
+    // setCollisionVoxel (collider.zig:267-273): getOrCreateBrick (232-239)
+    // appends a zeroed brick when no brick has the position's hash.
+    void set(IV3 v, uint8_t val) {
+        const IV3 bp{divFloor8(v.x), divFloor8(v.y), divFloor8(v.z)};
+        const uint64_t hb = hashBrickPos(bp);
+        auto it = by_hash.find(hb);
+        int32_t bi;
+        if (it == by_hash.end()) {
+            Brick b{};
+            b.pos = bp;
+            std::memset(b.vox, 0, sizeof(b.vox));
+            bi = (int32_t)bricks.size();
+            bricks.push_back(b);
+            by_hash.emplace(hb, bi);
+        } else {
+            bi = it->second;
+        }
+        bricks[(size_t)bi].vox[mod8(v.x) + 8 * mod8(v.y) + 64 * mod8(v.z)] = val;
+    }
+    // An edit batch as a host caller writes it with the reference's calls.
+    // mode 0: setCollisionVoxel(coords[i], values[i]) in list order.
+    // mode 1: each voxel in list order becomes solid (values[i] != 0; an empty
+    // voxel gets an inside byte, a solid one keeps its byte) or empty; then
+    // every listed voxel and each of its six face neighbours that is solid is
+    // set to classifyFromNeighbors (collision_voxel.zig:213-235) of the face
+    // neighbours' occupancy.  Then recomputeMetadata.
+    void edit(const int32_t* coords, const uint8_t* values, uint32_t n, int mode) {
+        for (uint32_t i = 0; i < n; ++i) {
+            const IV3 v{coords[i * 3], coords[i * 3 + 1], coords[i * 3 + 2]};
+            if (mode == 0) set(v, values[i]);
+            else if (!values[i]) set(v, 0);
+            else set(v, vtype(get(v)) == T_EMPTY ? (uint8_t)T_INSIDE : get(v));
+        }
+        if (mode == 1) {
+            const int32_t off[7][3] = {{0, 0, 0}, {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+            auto solid = [&](IV3 u) { return vtype(get(u)) != T_EMPTY; };
+            for (uint32_t i = 0; i < n; ++i)
+                for (int k = 0; k < 7; ++k) {
+                    const IV3 u{coords[i * 3] + off[k][0], coords[i * 3 + 1] + off[k][1], coords[i * 3 + 2] + off[k][2]};
+                    if (!solid(u)) continue;
+                    set(u, classifyFromNeighbors(true, solid({u.x - 1, u.y, u.z}), solid({u.x + 1, u.y, u.z}),
+                                                 solid({u.x, u.y - 1, u.z}), solid({u.x, u.y + 1, u.z}),
+                                                 solid({u.x, u.y, u.z - 1}), solid({u.x, u.y, u.z + 1})));
+                }
+        }
+        recomputeMetadata();
+    }
     V3<R> getCenterOfMass() const {  // collider.zig:376-403
         if (solid_count == 0) return {0, 0, 0};
         V3<R> sum = {0, 0, 0};

@@ -32,6 +32,9 @@ for name, res, args in [
     ("vxo_world_create", _VP, [_VP, _I]),
     ("vxo_world_destroy", None, [_VP]),
     ("vxo_collider_add", _I, [_VP, _U32, _F, _VP, _U32]),
+    ("vxo_collider_edit", _I, [_VP, _U32, _VP, _VP, _U32, _I]),
+    ("vxo_collider_read", _I, [_VP, _U32, _VP, _VP, _U32, _PU32]),
+    ("vxo_invalidate_cache_for_body", _U32, [_VP, _U32]),
     ("vxo_bodies_set", _I, [_VP, _VP, _U32]),
     ("vxo_bodies_get", _I, [_VP, _VP, _U32]),
     ("vxo_step", _I, [_VP, _F, _VP, _U32]),
@@ -124,6 +127,23 @@ class OracleWorld:
     def add_collider(self, cid, vs, bricks):
         bricks = np.ascontiguousarray(bricks, dtype=abi.BRICK_DTYPE)
         assert L.vxo_collider_add(self.h, int(cid), np.float32(vs), abi.ptr(bricks), len(bricks)) == 0
+
+    def edit_collider(self, cid, coords, values, mode="occupancy"):
+        coords = np.ascontiguousarray(coords, dtype=np.int32).reshape(-1, 3)
+        values = np.ascontiguousarray(values, dtype=np.uint8).reshape(-1)
+        mode = {"set": abi.EDIT_SET, "occupancy": abi.EDIT_OCCUPANCY}.get(mode, mode)
+        assert L.vxo_collider_edit(self.h, int(cid), abi.ptr(coords), abi.ptr(values), len(values), int(mode)) == 0
+
+    def read_collider(self, cid):
+        info = np.zeros(1, dtype=abi.COLLIDER_INFO_DTYPE)
+        n = ctypes.c_uint32(0)
+        assert L.vxo_collider_read(self.h, int(cid), abi.ptr(info), None, 0, ctypes.byref(n)) == 0
+        bricks = np.zeros(n.value, dtype=abi.BRICK_DTYPE)
+        assert L.vxo_collider_read(self.h, int(cid), abi.ptr(info), abi.ptr(bricks), len(bricks), ctypes.byref(n)) == 0
+        return info[0], bricks
+
+    def invalidate_cache_for_body(self, body_id):
+        return int(L.vxo_invalidate_cache_for_body(self.h, int(body_id)))
 
     def set_bodies(self, bodies):
         bodies = np.ascontiguousarray(bodies, dtype=abi.BODY_DTYPE)

@@ -26,6 +26,23 @@ COLOUR_PROJECT, COLOUR_REFERENCE = 0, 1
 BRICK_DTYPE = np.dtype([("pos", "<i4", (3,)), ("voxels", "u1", (512,))], align=False)
 assert BRICK_DTYPE.itemsize == 524
 
+EDIT_SET, EDIT_OCCUPANCY = 0, 1
+
+# vxp_collider_info
+COLLIDER_INFO_DTYPE = np.dtype(
+    [
+        ("voxel_size", "<f4"),
+        ("min_bound", "<i4", (3,)),
+        ("max_bound", "<i4", (3,)),
+        ("aabb_min", "<f4", (3,)),
+        ("aabb_max", "<f4", (3,)),
+        ("solid_count", "<u4"),
+        ("n_bricks", "<u4"),
+        ("has_table", "<u4"),
+    ]
+)
+assert COLLIDER_INFO_DTYPE.itemsize == 64
+
 BODY_DTYPE = np.dtype(
     [
         ("id", "<u4"),
@@ -198,6 +215,9 @@ SIGNATURES = {
     "vxp_last_error": (_I, [_VP, ctypes.c_char_p, ctypes.c_size_t]),
     "vxp_abi_version": (_I, []),
     "vxp_collider_upload": (_I, [_VP, _U32, _F, _VP, _U32]),
+    "vxp_collider_edit": (_I, [_VP, _U32, _VP, _VP, _U32, _I]),
+    "vxp_collider_read": (_I, [_VP, _U32, _VP, _VP, _U32, _VP]),
+    "vxp_invalidate_cache_for_body": (_I, [_VP, _U32, _VP]),
     "vxp_bodies_set": (_I, [_VP, _VP, _U32]),
     "vxp_bodies_get": (_I, [_VP, _VP, _U32]),
     "vxp_mass_properties": (_I, [_F, _VP, _U32, _F, ctypes.POINTER(_F), _VP]),
@@ -233,6 +253,9 @@ SIGNATURES = {
     "vxp_batch_destroy": (None, [_VP]),
     "vxp_batch_last_error": (_I, [_VP, ctypes.c_char_p, ctypes.c_size_t]),
     "vxp_batch_collider_upload": (_I, [_VP, _U32, _F, _VP, _U32]),
+    "vxp_batch_collider_edit": (_I, [_VP, _U32, _VP, _VP, _U32, _I]),
+    "vxp_batch_collider_read": (_I, [_VP, _U32, _VP, _VP, _U32, _VP]),
+    "vxp_batch_invalidate_cache_for_body": (_I, [_VP, _U32, _U32, _VP]),
     "vxp_batch_world_set": (_I, [_VP, _U32, _VP, _U32, _U32]),
     "vxp_batch_world_clear": (_I, [_VP, _U32]),
     "vxp_batch_world_release": (_I, [_VP, _U32]),

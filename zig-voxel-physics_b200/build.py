@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvxp.so")
 
 SOURCES = ["vxp_lib.cu"]
-HEADERS = ["vxp_math.cuh", "vxp_world.cuh", "vxp_step.cuh"]
+HEADERS = ["vxp_math.cuh", "vxp_world.cuh", "vxp_step.cuh", "vxp_collider.cuh"]
 
 NVCC_FLAGS = [
     "-std=c++17",

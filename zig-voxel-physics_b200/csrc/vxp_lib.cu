@@ -21,6 +21,7 @@
 
 #include "../../include/vxp.h"
 #include "vxp_math.cuh"
+#include "vxp_collider.cuh"
 #include "vxp_step.cuh"
 #include "vxp_world.cuh"
 
@@ -202,16 +203,6 @@ __global__ void k_rehash(const ManifoldRec* man, uint32_t n, HashSlot* ht, uint3
 // ===========================================================================
 namespace {
 
-struct HostCollider {
-    uint32_t id;
-    float vs;
-    std::vector<int32_t> pos;  // 3 per brick
-    std::vector<uint8_t> vox;  // 512 per brick
-    int32_t min_bound[3], max_bound[3];
-    float aabb_min[3], aabb_max[3];
-    uint32_t solid;
-};
-
 template <class T> struct DBuf {
     T* p = nullptr;
     size_t n = 0;
@@ -277,8 +268,16 @@ uint64_t hash_brick_pos(int32_t x, int32_t y, int32_t z) {  // collider.zig:187-
     return ux ^ (uy * 0x517cc1b727220a95ull) ^ (uz * 0x9e3779b97f4a7c15ull);
 }
 
-// VoxelCollider.recomputeMetadata (collider.zig:283-333), bricks in the order given.
-void collider_metadata(HostCollider& h) {
+// VoxelCollider.recomputeMetadata (collider.zig:283-333), bricks in the order
+// given: bounds over the solid voxels (max exclusive; zero when none is
+// solid), the local AABB as the merge of the bricks' solid-voxel boxes, the
+// solid count.
+struct ColliderMeta {
+    int32_t min_bound[3], max_bound[3];
+    float aabb_min[3], aabb_max[3];
+    uint32_t solid;
+};
+void collider_metadata(float vs, const int32_t* pos, const uint8_t* vox, size_t nb, ColliderMeta& h) {
     h.solid = 0;
     for (int k = 0; k < 3; ++k) {
         h.min_bound[k] = INT32_MAX;
@@ -286,10 +285,9 @@ void collider_metadata(HostCollider& h) {
     }
     const float inf = __builtin_inff();
     float amn[3] = {inf, inf, inf}, amx[3] = {-inf, -inf, -inf};
-    const size_t nb = h.pos.size() / 3;
     for (size_t b = 0; b < nb; ++b) {
-        const int32_t* bp = &h.pos[b * 3];
-        const uint8_t* v = &h.vox[b * 512];
+        const int32_t* bp = &pos[b * 3];
+        const uint8_t* v = &vox[b * 512];
         uint32_t solid = 0;
         float bmn[3] = {inf, inf, inf}, bmx[3] = {-inf, -inf, -inf};
         for (int i = 0; i < 512; ++i) {
@@ -297,9 +295,9 @@ void collider_metadata(HostCollider& h) {
             ++solid;
             const int c[3] = {i % 8, (i / 8) % 8, i / 64};
             for (int k = 0; k < 3; ++k) {
-                const float lp = ((float)bp[k] * 8.0f + (float)c[k]) * h.vs;
+                const float lp = ((float)bp[k] * 8.0f + (float)c[k]) * vs;
                 bmn[k] = std::fmin(bmn[k], lp);
-                bmx[k] = std::fmax(bmx[k], lp + h.vs);
+                bmx[k] = std::fmax(bmx[k], lp + vs);
                 const int32_t vc = bp[k] * 8 + c[k];
                 h.min_bound[k] = std::min(h.min_bound[k], vc);
                 h.max_bound[k] = std::max(h.max_bound[k], vc + 1);
@@ -320,21 +318,81 @@ void collider_metadata(HostCollider& h) {
     }
 }
 
-// The colliders of a context or batch, mirrored on the device as a dense
-// brick grid per collider over one voxel pool.
+// Floor division by the brick size (voxelToBrickPos, collider.zig:195-201).
+inline int32_t brick_of(int32_t v) { return v >= 0 ? v / 8 : -((-v + 7) / 8); }
+
+struct VoxelKey {
+    int32_t x, y, z;
+    bool operator==(const VoxelKey& o) const { return x == o.x && y == o.y && z == o.z; }
+};
+struct VoxelKeyHash {
+    size_t operator()(const VoxelKey& k) const {
+        return (size_t)(((uint64_t)(uint32_t)k.x * 0x9E3779B97F4A7C15ull) ^
+                        ((uint64_t)(uint32_t)k.y * 0xC2B2AE3D27D4EB4Full) ^ ((uint64_t)(uint32_t)k.z << 1));
+    }
+};
+
+// The colliders of a context or batch on the device.  Per collider: a dense
+// grid of brick slots (each cell resolved by hashBrickPos, as the reference's
+// brick map resolves it) over the box of its bricks plus one brick on every
+// side, its bricks' voxels and positions in two pools, and a neighbourhood-mask
+// table.  The pools grow by appending: an upload places only its own collider,
+// an edit runs in place on the device, and an edit that needs new bricks
+// places its collider again from a copy of its voxels.  Ranges left behind by
+// replaced placements are reclaimed by a full re-placement once they outweigh
+// the live ones.
 struct ColliderStore {
-    std::vector<HostCollider> colliders;
+    struct Entry {
+        uint32_t id = 0;
+        float vs = 0.0f;
+        std::vector<int32_t> pos;                        // 3 per brick, the device's brick order
+        std::unordered_map<uint64_t, uint32_t> by_hash;  // hashBrickPos -> brick
+        std::vector<int32_t> cover;                      // further brick cells the grid covers (3 each)
+        std::vector<uint8_t> staged;                     // voxels waiting for placement (512 per brick)
+        bool placed = false;
+        bool aliased = false;    // some grid cell reaches a brick of another position (shared hash)
+        DCollider d{};           // the layout as placed; the metadata then lives on the device
+        size_t grid_cells = 0;
+    };
+    std::vector<Entry> colliders;
     std::unordered_map<uint32_t, uint32_t> index;
-    bool dirty = true;
     DBuf<DCollider> d_col;
     DBuf<int32_t> d_grid;
     DBuf<uint8_t> d_vox;
+    DBuf<int4> d_bpos;
     DBuf<uint4> d_nb;
+    DBuf<uint32_t> d_list;
+    DBuf<EditScratch> d_scratch;
+    size_t grid_used = 0, brick_used = 0, nb_used = 0;
+    size_t grid_dead = 0, brick_dead = 0, nb_dead = 0;
     uint32_t n_dev = 0;
+    bool dirty = false;    // colliders wait for placement
+    bool replace = false;  // every collider is placed again (tables switched)
     // neighbourhood-mask tables: colliders with at most kNbMaxCentres probe
     // centres get one, while the pool stays within kNbMaxTotal entries
     static constexpr uint64_t kNbMaxCentres = 1ull << 23, kNbMaxTotal = 1ull << 25;
+    static constexpr size_t kMaxGridCells = (size_t)1 << 28;
     bool tables = true;  // build neighbourhood-mask tables at all
+    // pinned staging of edit lists, two in turn, each free again once the
+    // kernels of the edit that used it have run
+    struct Staging {
+        int4* host = nullptr;
+        size_t cap = 0;
+        DBuf<int4> dev;
+        cudaEvent_t done = nullptr;
+    };
+    Staging stage[2];
+    uint32_t turn = 0;
+
+    ColliderStore() = default;
+    ColliderStore(const ColliderStore&) = delete;
+    ColliderStore& operator=(const ColliderStore&) = delete;
+    ~ColliderStore() {
+        for (Staging& s : stage) {
+            if (s.done) cudaEventDestroy(s.done);
+            if (s.host) cudaFreeHost(s.host);
+        }
+    }
 
     int upload(uint32_t id, float vs, const vxp_brick* bricks, uint32_t n, std::string& err) {
         if (!bricks && n) {
@@ -345,28 +403,28 @@ struct ColliderStore {
             err = "voxel_size must be positive";
             return VXP_ERR_ARG;
         }
-        HostCollider h;
-        h.id = id;
-        h.vs = vs;
-        h.pos.resize((size_t)n * 3);
-        h.vox.resize((size_t)n * 512);
-        std::unordered_map<uint64_t, uint32_t> seen;
+        Entry e;
+        e.id = id;
+        e.vs = vs;
+        e.pos.resize((size_t)n * 3);
+        e.staged.resize((size_t)n * 512);
         for (uint32_t i = 0; i < n; ++i) {
-            for (int k = 0; k < 3; ++k) h.pos[(size_t)i * 3 + k] = bricks[i].pos[k];
-            std::memcpy(&h.vox[(size_t)i * 512], bricks[i].voxels, 512);
+            for (int k = 0; k < 3; ++k) e.pos[(size_t)i * 3 + k] = bricks[i].pos[k];
+            std::memcpy(&e.staged[(size_t)i * 512], bricks[i].voxels, 512);
             const uint64_t hb = hash_brick_pos(bricks[i].pos[0], bricks[i].pos[1], bricks[i].pos[2]);
-            auto ins = seen.emplace(hb, i);
+            auto ins = e.by_hash.emplace(hb, i);
             if (!ins.second) {
                 err = fmt("collider %u: bricks %u and %u share a hashBrickPos value", id, ins.first->second, i);
                 return VXP_ERR_ARG;
             }
         }
-        collider_metadata(h);
         auto it = index.find(id);
-        if (it != index.end()) colliders[it->second] = std::move(h);
-        else {
+        if (it != index.end()) {
+            retire(colliders[it->second]);
+            colliders[it->second] = std::move(e);
+        } else {
             index[id] = (uint32_t)colliders.size();
-            colliders.push_back(std::move(h));
+            colliders.push_back(std::move(e));
         }
         dirty = true;
         return VXP_OK;
@@ -375,18 +433,310 @@ struct ColliderStore {
         auto it = index.find(id);
         return it == index.end() ? 0xFFFFFFFFu : it->second;
     }
-    int sync(std::string& err) {
+    void set_tables(bool on) {
+        if (tables == on) return;
+        tables = on;
+        replace = dirty = true;
+    }
+    ColliderSet set() const { return ColliderSet{d_col.p, d_grid.p, d_vox.p, n_dev, d_nb.p}; }
+
+    // Places every collider that waits, on `s` (ordered after the work
+    // already there), and reclaims dead ranges when they outweigh the live.
+    int sync(cudaStream_t s, std::string& err) {
+        if (!d_col.p && (d_col.reserve(1) != cudaSuccess || d_grid.reserve(1) != cudaSuccess ||
+                         d_vox.reserve(512) != cudaSuccess || d_bpos.reserve(1) != cudaSuccess ||
+                         d_nb.reserve(1) != cudaSuccess)) {
+            err = "collider store: device allocation failed";
+            return VXP_ERR_OOM;
+        }
         if (!dirty) return VXP_OK;
-        std::vector<DCollider> dc(colliders.size());
+        const bool reclaim = (brick_dead > 4096 && brick_dead > brick_used - brick_dead) ||
+                             (nb_dead > ((size_t)1 << 20) && nb_dead > nb_used - nb_dead) ||
+                             (grid_dead > ((size_t)1 << 20) && grid_dead > grid_used - grid_dead);
+        if (replace || reclaim) {
+            if (int rc = fetch_all(s, err)) return rc;
+            grid_used = brick_used = nb_used = 0;
+            grid_dead = brick_dead = nb_dead = 0;
+            for (Entry& e : colliders) e.placed = false;
+            replace = false;
+        }
+        std::vector<uint32_t> todo;
+        for (uint32_t i = 0; i < colliders.size(); ++i)
+            if (!colliders[i].placed) todo.push_back(i);
+        if (int rc = place(todo, s, err)) return rc;
+        dirty = false;
+        return VXP_OK;
+    }
+
+    // The current metadata and bricks of collider `id`, read from the device.
+    int read(uint32_t id, vxp_collider_info* info, vxp_brick* bricks, uint32_t cap, uint32_t* n_out,
+             cudaStream_t s, std::string& err) {
+        const uint32_t ci = index_of(id);
+        if (ci == 0xFFFFFFFFu) {
+            err = fmt("collider %u was never uploaded", id);
+            return VXP_ERR_ARG;
+        }
+        if (int rc = sync(s, err)) return rc;
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            err = "collider read: stream failed";
+            return VXP_ERR_CUDA;
+        }
+        const Entry& e = colliders[ci];
+        DCollider d;
+        if (cudaMemcpy(&d, d_col.p + ci, sizeof(d), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            err = "collider read: copy failed";
+            return VXP_ERR_CUDA;
+        }
+        const uint32_t n = d.n_bricks;
+        if (info) {
+            std::memset(info, 0, sizeof(*info));
+            info->voxel_size = d.vs;
+            for (int k = 0; k < 3; ++k) {
+                info->min_bound[k] = d.min_bound[k];
+                info->max_bound[k] = d.max_bound[k];
+                info->aabb_min[k] = d.aabb_min[k];
+                info->aabb_max[k] = d.aabb_max[k];
+            }
+            info->solid_count = d.solid_count;
+            info->n_bricks = n;
+            info->has_table = d.nb_off != kNoTable ? 1u : 0u;
+        }
+        if (n_out) *n_out = n;
+        const uint32_t k = bricks ? std::min(cap, n) : 0u;
+        if (k) {
+            std::vector<uint8_t> v((size_t)k * 512);
+            if (cudaMemcpy(v.data(), d_vox.p + (size_t)d.brick_off * 512, v.size(), cudaMemcpyDeviceToHost) !=
+                cudaSuccess) {
+                err = "collider read: copy failed";
+                return VXP_ERR_CUDA;
+            }
+            for (uint32_t b = 0; b < k; ++b) {
+                for (int q = 0; q < 3; ++q) bricks[b].pos[q] = e.pos[(size_t)b * 3 + q];
+                std::memcpy(bricks[b].voxels, &v[(size_t)b * 512], 512);
+            }
+        }
+        return VXP_OK;
+    }
+
+    // An edit batch of collider `id` (vxp_collider_edit), queued on `s`.
+    int edit(uint32_t id, const int32_t* coords, const uint8_t* values, uint32_t n, uint32_t mode, cudaStream_t s,
+             std::string& err) {
+        const uint32_t ci = index_of(id);
+        if (ci == 0xFFFFFFFFu) {
+            err = fmt("collider %u was never uploaded", id);
+            return VXP_ERR_ARG;
+        }
+        if ((n && (!coords || !values)) || mode > EDIT_OCCUPANCY || n > (1u << 24)) {
+            err = "collider edit: bad arguments";
+            return VXP_ERR_ARG;
+        }
+        if (n == 0) return VXP_OK;
+        if (int rc = sync(s, err)) return rc;
+        Entry& e = colliders[ci];
+        // one entry per voxel, the last write winning; new bricks in the
+        // order the writes first reach them (getOrCreateBrick)
+        std::vector<int4> list;
+        list.reserve(n);
+        std::unordered_map<VoxelKey, uint32_t, VoxelKeyHash> seen;
+        seen.reserve((size_t)n * 2);
+        std::vector<int32_t> fresh;                   // new brick positions, 3 each
+        std::unordered_map<uint64_t, bool> fresh_at;  // by hash
+        std::vector<int32_t> extra;                   // held cells whose neighbours leave the grid
+        for (uint32_t i = 0; i < n; ++i) {
+            const int32_t x = coords[(size_t)i * 3], y = coords[(size_t)i * 3 + 1], z = coords[(size_t)i * 3 + 2];
+            const int32_t w = mode == EDIT_SET ? (int32_t)values[i] : (values[i] ? 1 : 0);
+            auto ins = seen.emplace(VoxelKey{x, y, z}, (uint32_t)list.size());
+            if (!ins.second) {
+                list[ins.first->second].w = w;
+                continue;
+            }
+            list.push_back(make_int4(x, y, z, w));
+            const int32_t bx = brick_of(x), by = brick_of(y), bz = brick_of(z);
+            const uint64_t hb = hash_brick_pos(bx, by, bz);
+            if (!e.by_hash.count(hb)) {
+                if (fresh_at.emplace(hb, true).second) {
+                    fresh.push_back(bx);
+                    fresh.push_back(by);
+                    fresh.push_back(bz);
+                }
+            } else if (!in_grid(e.d, bx - 1, by - 1, bz - 1) || !in_grid(e.d, bx + 1, by + 1, bz + 1)) {
+                extra.push_back(bx);
+                extra.push_back(by);
+                extra.push_back(bz);
+            }
+        }
+        if (!fresh.empty() || !extra.empty()) {
+            // place the collider again with the new bricks (zeroed) and a grid
+            // that covers every cell the edit reads or writes
+            if (int rc = fetch(ci, s, err)) return rc;
+            const size_t nb0 = e.pos.size() / 3;
+            for (size_t b = 0; b < fresh.size() / 3; ++b) {
+                e.by_hash.emplace(hash_brick_pos(fresh[b * 3], fresh[b * 3 + 1], fresh[b * 3 + 2]),
+                                  (uint32_t)(nb0 + b));
+                e.pos.insert(e.pos.end(), &fresh[b * 3], &fresh[b * 3] + 3);
+            }
+            e.staged.resize(e.pos.size() / 3 * 512, 0);
+            e.cover.insert(e.cover.end(), extra.begin(), extra.end());
+            retire(e);
+            std::vector<uint32_t> one{ci};
+            if (int rc = place(one, s, err)) return rc;
+        }
+        // Where one brick serves several cells of the grid (a shared
+        // hashBrickPos), distinct coordinates can reach one voxel byte: each
+        // such byte then takes the last value the list writes to it, and one
+        // re-typing, the last in the reference's order (list order, then the
+        // voxel before its -x, +x, -y, +y, -z, +z neighbours); and any table
+        // entry may read a changed byte, so the whole table is rebuilt.
+        std::vector<int4> targets;
+        const bool shared = e.aliased;
+        if (shared) {
+            auto byte_of = [&](int32_t x, int32_t y, int32_t z, uint64_t* key) {
+                auto it = e.by_hash.find(hash_brick_pos(brick_of(x), brick_of(y), brick_of(z)));
+                if (it == e.by_hash.end()) return false;
+                *key = ((uint64_t)it->second << 9) | (uint64_t)((x & 7) + 8 * (y & 7) + 64 * (z & 7));
+                return true;
+            };
+            std::unordered_map<uint64_t, int32_t> last;
+            uint64_t key = 0;
+            for (uint32_t i = 0; i < n; ++i)
+                if (byte_of(coords[(size_t)i * 3], coords[(size_t)i * 3 + 1], coords[(size_t)i * 3 + 2], &key))
+                    last[key] = mode == EDIT_SET ? (int32_t)values[i] : (values[i] ? 1 : 0);
+            for (int4& q : list)
+                if (byte_of(q.x, q.y, q.z, &key)) q.w = last[key];
+            if (mode == EDIT_OCCUPANCY) {
+                const int32_t off[7][3] = {{0, 0, 0}, {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+                std::unordered_map<uint64_t, uint32_t> who;
+                for (uint32_t i = 0; i < n; ++i)
+                    for (int k = 0; k < 7; ++k) {
+                        const int32_t x = coords[(size_t)i * 3] + off[k][0], y = coords[(size_t)i * 3 + 1] + off[k][1],
+                                      z = coords[(size_t)i * 3 + 2] + off[k][2];
+                        if (!byte_of(x, y, z, &key)) continue;
+                        auto r = who.emplace(key, (uint32_t)targets.size());
+                        if (r.second) targets.push_back(make_int4(x, y, z, 0));
+                        else targets[r.first->second] = make_int4(x, y, z, 0);
+                    }
+            }
+        }
+        // the lists through pinned staging: the writes, then the re-typings
+        const size_t total = list.size() + targets.size();
+        Staging& st = stage[turn];
+        turn ^= 1u;
+        if (st.done && cudaEventSynchronize(st.done) != cudaSuccess) {
+            err = "collider edit: stream failed";
+            return VXP_ERR_CUDA;
+        }
+        if (!st.done && cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming) != cudaSuccess) {
+            err = "collider edit: event";
+            return VXP_ERR_CUDA;
+        }
+        if (st.cap < total) {
+            if (st.host) cudaFreeHost(st.host);
+            st.host = nullptr;
+            st.cap = 0;
+            const size_t want = std::max<size_t>(total, 1024);
+            if (cudaMallocHost(&st.host, want * sizeof(int4)) != cudaSuccess || st.dev.reserve(want) != cudaSuccess) {
+                err = "collider edit: allocation failed";
+                return VXP_ERR_OOM;
+            }
+            st.cap = want;
+        }
+        if (d_scratch.reserve(1) != cudaSuccess) {
+            err = "collider edit: allocation failed";
+            return VXP_ERR_OOM;
+        }
+        std::memcpy(st.host, list.data(), list.size() * sizeof(int4));
+        if (!targets.empty()) std::memcpy(st.host + list.size(), targets.data(), targets.size() * sizeof(int4));
+        if (cudaMemcpyAsync(st.dev.p, st.host, total * sizeof(int4), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+            err = "collider edit: copy failed";
+            return VXP_ERR_CUDA;
+        }
+        const uint32_t m = (uint32_t)list.size(), t = (uint32_t)targets.size();
+        const uint32_t tb = 256;
+        k_edit_apply<<<(m + tb - 1) / tb, tb, 0, s>>>(d_col.p, ci, d_grid.p, d_vox.p, st.dev.p, m, mode);
+        if (mode == EDIT_OCCUPANCY && !shared)
+            k_edit_classify<<<(m * 7u + tb - 1) / tb, tb, 0, s>>>(d_col.p, ci, d_grid.p, d_vox.p, st.dev.p, m, 7u);
+        else if (mode == EDIT_OCCUPANCY && t)
+            k_edit_classify<<<(t + tb - 1) / tb, tb, 0, s>>>(d_col.p, ci, d_grid.p, d_vox.p, st.dev.p + m, t, 1u);
+        const uint32_t nb = e.d.n_bricks;
+        const uint32_t mb = std::max<uint32_t>(1u, std::min<uint32_t>(kMetaBlocks, (nb * 32u + kMetaThreads - 1) /
+                                                                                       kMetaThreads));
+        k_edit_meta<<<mb, kMetaThreads, 0, s>>>(d_col.p, ci, d_vox.p, d_bpos.p, d_scratch.p, shared ? 1u : 0u);
+        if (e.d.nb_cap) {
+            if (!shared)
+                k_edit_table_local<<<(m * 125u + tb - 1) / tb, tb, 0, s>>>(set(), d_nb.p, ci, st.dev.p, m,
+                                                                           d_scratch.p);
+            const uint32_t fb = std::min<uint32_t>(148u * 4u, (e.d.nb_cap + tb - 1) / tb);
+            k_edit_table_full<<<fb, tb, 0, s>>>(set(), d_nb.p, ci, d_scratch.p);
+        }
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess || cudaEventRecord(st.done, s) != cudaSuccess) {
+            err = fmt("collider edit: launch failed: %s", cudaGetErrorString(le));
+            return VXP_ERR_CUDA;
+        }
+        return VXP_OK;
+    }
+
+  private:
+    static bool in_grid(const DCollider& d, int32_t bx, int32_t by, int32_t bz) {
+        return (uint32_t)(bx - d.bmin[0]) < (uint32_t)d.bdim[0] && (uint32_t)(by - d.bmin[1]) < (uint32_t)d.bdim[1] &&
+               (uint32_t)(bz - d.bmin[2]) < (uint32_t)d.bdim[2];
+    }
+    // A placement's ranges become dead.
+    void retire(Entry& e) {
+        if (!e.placed) return;
+        grid_dead += e.grid_cells;
+        brick_dead += e.d.n_bricks;
+        nb_dead += e.d.nb_cap;
+        e.placed = false;
+        dirty = true;
+    }
+    // Collider ci's voxels as the device holds them, into its staging copy.
+    int fetch(uint32_t ci, cudaStream_t s, std::string& err) {
+        Entry& e = colliders[ci];
+        if (!e.placed) return VXP_OK;
+        e.staged.resize((size_t)e.d.n_bricks * 512);
+        if (cudaStreamSynchronize(s) != cudaSuccess ||
+            (!e.staged.empty() && cudaMemcpy(e.staged.data(), d_vox.p + (size_t)e.d.brick_off * 512,
+                                             e.staged.size(), cudaMemcpyDeviceToHost) != cudaSuccess)) {
+            err = "collider store: read-back failed";
+            return VXP_ERR_CUDA;
+        }
+        return VXP_OK;
+    }
+    int fetch_all(cudaStream_t s, std::string& err) {
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            err = "collider store: stream failed";
+            return VXP_ERR_CUDA;
+        }
+        std::vector<uint8_t> all(brick_used * 512);
+        if (!all.empty() && cudaMemcpy(all.data(), d_vox.p, all.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            err = "collider store: read-back failed";
+            return VXP_ERR_CUDA;
+        }
+        for (Entry& e : colliders) {
+            if (!e.placed) continue;
+            const size_t off = (size_t)e.d.brick_off * 512;
+            e.staged.assign(all.begin() + (ptrdiff_t)off, all.begin() + (ptrdiff_t)(off + (size_t)e.d.n_bricks * 512));
+        }
+        return VXP_OK;
+    }
+    // Appends the listed colliders (from their staging copies) to the pools,
+    // writes their records and builds their tables.
+    int place(const std::vector<uint32_t>& todo, cudaStream_t s, std::string& err) {
+        if (todo.empty()) return VXP_OK;
         std::vector<int32_t> grid;
         std::vector<uint8_t> vox;
-        uint32_t brick_total = 0;
-        uint64_t nb_total = 0;
-        for (size_t ci = 0; ci < colliders.size(); ++ci) {
-            const HostCollider& h = colliders[ci];
-            DCollider& d = dc[ci];
+        std::vector<int4> bpos;
+        std::vector<uint32_t> built;
+        const size_t g0 = grid_used, b0 = brick_used;
+        for (uint32_t ci : todo) {
+            Entry& e = colliders[ci];
+            const size_t nb = e.pos.size() / 3;
+            ColliderMeta h;
+            collider_metadata(e.vs, e.pos.data(), e.staged.data(), nb, h);
+            DCollider& d = e.d;
             std::memset(&d, 0, sizeof(d));
-            d.vs = h.vs;
+            d.vs = e.vs;
             for (int k = 0; k < 3; ++k) {
                 d.min_bound[k] = h.min_bound[k];
                 d.max_bound[k] = h.max_bound[k];
@@ -394,82 +744,121 @@ struct ColliderStore {
                 d.aabb_max[k] = h.aabb_max[k];
             }
             d.solid_count = h.solid;
-            const size_t nb = h.pos.size() / 3;
-            // The reference finds a brick through hashBrickPos (collider.zig:
-            // 187-192, 241-248), and distinct positions can share a hash.  Every
-            // voxel the step looks up lies in [min_bound, max_bound] (the overlap
-            // region is clamped to the bounds, inclusive; B probes pass
-            // isValidCoord), so the grid covers those bricks and resolves each
-            // cell by its hash.
-            std::unordered_map<uint64_t, int32_t> by_hash;
-            for (size_t b = 0; b < nb; ++b)
-                by_hash.emplace(hash_brick_pos(h.pos[b * 3], h.pos[b * 3 + 1], h.pos[b * 3 + 2]), (int32_t)b);
-            int32_t lo[3], hi[3];
+            // grid: the box of the bricks and the extra cells, one brick wider
+            // on every side; a collider without bricks gets one empty cell
+            int32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+            bool any = false;
+            auto grow = [&](const int32_t* p) {
+                for (int k = 0; k < 3; ++k) {
+                    lo[k] = any ? std::min(lo[k], p[k] - 1) : p[k] - 1;
+                    hi[k] = any ? std::max(hi[k], p[k] + 1) : p[k] + 1;
+                }
+                any = true;
+            };
+            for (size_t b = 0; b < nb; ++b) grow(&e.pos[b * 3]);
+            for (size_t c = 0; c < e.cover.size() / 3; ++c) grow(&e.cover[c * 3]);
+            size_t cells = 1;
             for (int k = 0; k < 3; ++k) {
-                lo[k] = h.min_bound[k] >> 3;
-                hi[k] = h.max_bound[k] >> 3;
                 d.bmin[k] = lo[k];
                 d.bdim[k] = hi[k] - lo[k] + 1;
+                cells *= (size_t)d.bdim[k];
             }
-            d.grid_off = (uint32_t)grid.size();
-            d.brick_off = brick_total;
-            d.n_bricks = (uint32_t)nb;
-            const size_t cells = (size_t)d.bdim[0] * d.bdim[1] * d.bdim[2];
-            if (cells > (size_t)1 << 28) {
-                err = fmt("collider %u brick grid too large", h.id);
+            if (cells > kMaxGridCells) {
+                err = fmt("collider %u brick grid too large", e.id);
                 return VXP_ERR_CAP;
             }
-            grid.resize(grid.size() + cells, -1);
+            d.grid_off = (uint32_t)(g0 + grid.size());
+            d.brick_off = (uint32_t)(b0 + bpos.size());
+            d.n_bricks = (uint32_t)nb;
+            const size_t gbase = grid.size();
+            grid.resize(gbase + cells, -1);
+            bool aliased = false;
             for (int32_t bz = lo[2]; bz <= hi[2]; ++bz)
                 for (int32_t by = lo[1]; by <= hi[1]; ++by)
                     for (int32_t bx = lo[0]; bx <= hi[0]; ++bx) {
-                        auto it = by_hash.find(hash_brick_pos(bx, by, bz));
-                        if (it == by_hash.end()) continue;
-                        grid[d.grid_off + (size_t)(bx - lo[0]) +
+                        auto it = e.by_hash.find(hash_brick_pos(bx, by, bz));
+                        if (it == e.by_hash.end()) continue;
+                        const int32_t* own = &e.pos[(size_t)it->second * 3];
+                        aliased |= own[0] != bx || own[1] != by || own[2] != bz;
+                        grid[gbase + (size_t)(bx - lo[0]) +
                              (size_t)d.bdim[0] * ((size_t)(by - lo[1]) + (size_t)d.bdim[1] * (size_t)(bz - lo[2]))] =
-                            it->second;
+                            (int32_t)it->second;
                     }
-            vox.insert(vox.end(), h.vox.begin(), h.vox.end());
-            brick_total += (uint32_t)nb;
+            e.grid_cells = cells;
+            e.aliased = aliased;
+            vox.insert(vox.end(), e.staged.begin(), e.staged.end());
+            for (size_t b = 0; b < nb; ++b) bpos.push_back(make_int4(e.pos[b * 3], e.pos[b * 3 + 1], e.pos[b * 3 + 2], 0));
             uint64_t centres = 1;
             for (int k = 0; k < 3; ++k) centres *= (uint64_t)((int64_t)h.max_bound[k] - h.min_bound[k] + 2);
-            if (tables && centres <= kNbMaxCentres && nb_total + centres <= kNbMaxTotal) {
-                d.nb_off = (uint32_t)nb_total;
-                nb_total += centres;
+            if (tables && centres <= kNbMaxCentres && nb_used + centres <= kNbMaxTotal) {
+                d.nb_base = d.nb_off = (uint32_t)nb_used;
+                d.nb_cap = (uint32_t)centres;
+                nb_used += centres;
+                built.push_back(ci);
             } else {
                 d.nb_off = kNoTable;
+                d.nb_base = d.nb_cap = 0;
             }
         }
-        if (d_col.reserve(dc.size()) != cudaSuccess || d_grid.reserve(grid.size()) != cudaSuccess ||
-            d_vox.reserve(vox.size()) != cudaSuccess) {
+        const size_t ng = g0 + grid.size(), nbk = b0 + bpos.size();
+        // growing a pool copies it and frees the old one: nothing may still read it
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            err = "collider store: stream failed";
+            return VXP_ERR_CUDA;
+        }
+        auto room = [](size_t need, size_t have) { return need <= have ? have : std::max(need, 2 * have); };
+        if (d_col.reserve(room(colliders.size(), d_col.p ? d_col.n : 0), true) != cudaSuccess ||
+            d_grid.reserve(room(ng, d_grid.p ? d_grid.n : 0), true) != cudaSuccess ||
+            d_vox.reserve(room(nbk * 512, d_vox.p ? d_vox.n : 0), true) != cudaSuccess ||
+            d_bpos.reserve(room(nbk, d_bpos.p ? d_bpos.n : 0), true) != cudaSuccess ||
+            (nb_used && d_nb.reserve(room(nb_used, d_nb.p ? d_nb.n : 0), true) != cudaSuccess) ||
+            (!built.empty() && d_list.reserve(built.size()) != cudaSuccess)) {
             err = "collider upload: device allocation failed";
             return VXP_ERR_OOM;
         }
-        if ((!dc.empty() && cudaMemcpy(d_col.p, dc.data(), dc.size() * sizeof(DCollider), cudaMemcpyHostToDevice) !=
-                                cudaSuccess) ||
-            (!grid.empty() &&
-             cudaMemcpy(d_grid.p, grid.data(), grid.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) ||
-            (!vox.empty() && cudaMemcpy(d_vox.p, vox.data(), vox.size(), cudaMemcpyHostToDevice) != cudaSuccess)) {
+        bool ok = (grid.empty() || cudaMemcpy(d_grid.p + g0, grid.data(), grid.size() * sizeof(int32_t),
+                                              cudaMemcpyHostToDevice) == cudaSuccess) &&
+                  (vox.empty() || cudaMemcpy(d_vox.p + b0 * 512, vox.data(), vox.size(), cudaMemcpyHostToDevice) ==
+                                      cudaSuccess) &&
+                  (bpos.empty() || cudaMemcpy(d_bpos.p + b0, bpos.data(), bpos.size() * sizeof(int4),
+                                              cudaMemcpyHostToDevice) == cudaSuccess);
+        // records, one copy per run of consecutive indices
+        for (size_t i = 0; ok && i < todo.size();) {
+            size_t j = i + 1;
+            while (j < todo.size() && todo[j] == todo[j - 1] + 1) ++j;
+            std::vector<DCollider> run(j - i);
+            for (size_t k = i; k < j; ++k) run[k - i] = colliders[todo[k]].d;
+            ok = cudaMemcpy(d_col.p + todo[i], run.data(), run.size() * sizeof(DCollider), cudaMemcpyHostToDevice) ==
+                 cudaSuccess;
+            i = j;
+        }
+        if (!ok) {
             err = "collider upload: copy failed";
             return VXP_ERR_CUDA;
         }
-        n_dev = (uint32_t)dc.size();
-        if (nb_total) {
-            if (d_nb.reserve(nb_total) != cudaSuccess) {
-                err = "collider upload: device allocation failed";
-                return VXP_ERR_OOM;
+        grid_used = ng;
+        brick_used = nbk;
+        n_dev = (uint32_t)colliders.size();
+        for (uint32_t ci : todo) {
+            Entry& e = colliders[ci];
+            e.placed = true;
+            std::vector<uint8_t>().swap(e.staged);
+        }
+        if (!built.empty()) {
+            if (cudaMemcpy(d_list.p, built.data(), built.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+                cudaSuccess) {
+                err = "collider upload: copy failed";
+                return VXP_ERR_CUDA;
             }
-            const dim3 grid_dims(64, std::min<uint32_t>(n_dev, 65535u));
-            k_nbhd_build<<<grid_dims, 256>>>(set(), d_nb.p);
-            if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(0) != cudaSuccess) {
+            const dim3 grid_dims(64, std::min<uint32_t>((uint32_t)built.size(), 65535u));
+            k_nbhd_build<<<grid_dims, 256, 0, s>>>(set(), d_nb.p, d_list.p, (uint32_t)built.size());
+            if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
                 err = "collider upload: neighbourhood tables failed";
                 return VXP_ERR_CUDA;
             }
         }
-        dirty = false;
         return VXP_OK;
     }
-    ColliderSet set() const { return ColliderSet{d_col.p, d_grid.p, d_vox.p, n_dev, d_nb.p}; }
 };
 
 StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) {
@@ -956,6 +1345,7 @@ struct vxp_ctx {
     bool count_bricks = false;  // traffic accounting (C_BRICKS)
     bool record_substeps = false;
     DBuf<float> subrec;
+    DBuf<uint32_t> d_word;  // a count read back by the host
 };
 
 namespace {
@@ -998,7 +1388,7 @@ constexpr unsigned long long kGridWaitNs = 10ull * 1000ull * 1000ull * 1000ull;
 
 // Runs the step kernel.  device_pairs: the kernel builds the pair list itself.
 int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, float margin) {
-    if (int rc = ctx->cols.sync(ctx->err)) return rc;
+    if (int rc = ctx->cols.sync(ctx->stream, ctx->err)) return rc;
     const bool grid = ctx->use_grid == 1 || (ctx->use_grid < 0 && ctx->w.n_bodies >= 512);
     const bool cluster = grid && ctx->solver_flow == VXP_SOLVER_CLUSTER && ctx->cluster_size > 0;
     const uint32_t flow = ctx->solver_flow == VXP_SOLVER_EVENTS ? 1u : 0u;
@@ -1064,7 +1454,7 @@ int check_device_error(vxp_ctx* ctx) {
 
 // The pair list of the current body state into ctx->w.pairs (host waits).
 int compute_device_pairs(vxp_ctx* ctx, float margin, uint32_t* n_out) {
-    if (int rc = ctx->cols.sync(ctx->err)) return rc;
+    if (int rc = ctx->cols.sync(ctx->stream, ctx->err)) return rc;
     WorldBuffers& w = ctx->w;
     const uint32_t n = w.n_bodies;
     const ColliderSet cs = ctx->cols.set();
@@ -1408,6 +1798,34 @@ int vxp_collider_upload(vxp_ctx* ctx, uint32_t collider_id, float voxel_size, co
     return ctx->cols.upload(collider_id, voxel_size, bricks, n_bricks, ctx->err);
 }
 
+int vxp_collider_edit(vxp_ctx* ctx, uint32_t collider_id, const int32_t* coords, const uint8_t* values, uint32_t n,
+                      int mode) {
+    if (!ctx) return VXP_ERR_ARG;
+    if (mode != VXP_EDIT_SET && mode != VXP_EDIT_OCCUPANCY) return fail(ctx, VXP_ERR_ARG, "unknown edit mode %d", mode);
+    return ctx->cols.edit(collider_id, coords, values, n, (uint32_t)mode, ctx->stream, ctx->err);
+}
+
+int vxp_collider_read(vxp_ctx* ctx, uint32_t collider_id, vxp_collider_info* info, vxp_brick* bricks, uint32_t cap,
+                      uint32_t* n_bricks) {
+    if (!ctx) return VXP_ERR_ARG;
+    if (int rc = check_device_error(ctx)) return rc;
+    return ctx->cols.read(collider_id, info, bricks, cap, n_bricks, ctx->stream, ctx->err);
+}
+
+int vxp_invalidate_cache_for_body(vxp_ctx* ctx, uint32_t body_id, uint32_t* n_invalidated) {
+    if (!ctx) return VXP_ERR_ARG;
+    if (ctx->d_word.reserve(1) != cudaSuccess) return fail(ctx, VXP_ERR_OOM, "device allocation failed");
+    const uint32_t cap = ctx->w.cache_cap;
+    CK(cudaMemsetAsync(ctx->d_word.p, 0, sizeof(uint32_t), ctx->stream));
+    k_cache_invalidate<<<(cap + 255) / 256, 256, 0, ctx->stream>>>(ctx->w.ckey.p, cap, body_id, ctx->d_word.p);
+    CK(cudaGetLastError());
+    if (n_invalidated) {
+        CK(cudaMemcpyAsync(n_invalidated, ctx->d_word.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return VXP_OK;
+}
+
 int vxp_bodies_set(vxp_ctx* ctx, const vxp_body* b, uint32_t n) {
     if (!ctx) return VXP_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1423,15 +1841,14 @@ int vxp_bodies_get(vxp_ctx* ctx, vxp_body* b, uint32_t n) {
 int vxp_mass_properties(float vs, const vxp_brick* bricks, uint32_t n, float density, float* inv_mass,
                         float inv_inertia[9]) {
     if ((!bricks && n) || !inv_mass || !inv_inertia) return VXP_ERR_ARG;
-    HostCollider h;
-    h.vs = vs;
-    h.pos.resize((size_t)n * 3);
-    h.vox.resize((size_t)n * 512);
+    std::vector<int32_t> pos((size_t)n * 3);
+    std::vector<uint8_t> vox((size_t)n * 512);
     for (uint32_t i = 0; i < n; ++i) {
-        for (int k = 0; k < 3; ++k) h.pos[(size_t)i * 3 + k] = bricks[i].pos[k];
-        std::memcpy(&h.vox[(size_t)i * 512], bricks[i].voxels, 512);
+        for (int k = 0; k < 3; ++k) pos[(size_t)i * 3 + k] = bricks[i].pos[k];
+        std::memcpy(&vox[(size_t)i * 512], bricks[i].voxels, 512);
     }
-    collider_metadata(h);
+    ColliderMeta h;
+    collider_metadata(vs, pos.data(), vox.data(), n, h);
     if (h.solid == 0) {
         *inv_mass = 0.0f;
         for (int k = 0; k < 9; ++k) inv_inertia[k] = 0.0f;
@@ -1446,10 +1863,10 @@ int vxp_mass_properties(float vs, const vxp_brick* bricks, uint32_t n, float den
     const float half = vs * 0.5f;
     for (uint32_t b = 0; b < n; ++b)
         for (int i = 0; i < 512; ++i) {
-            if ((h.vox[(size_t)b * 512 + i] & 7u) == 0u) continue;
+            if ((vox[(size_t)b * 512 + i] & 7u) == 0u) continue;
             const int c[3] = {i % 8, (i / 8) % 8, i / 64};
             for (int k = 0; k < 3; ++k) {
-                const float p = ((float)(h.pos[(size_t)b * 3 + k] * 8 + c[k]) * vs + half) + vs * 0.5f;
+                const float p = ((float)(pos[(size_t)b * 3 + k] * 8 + c[k]) * vs + half) + vs * 0.5f;
                 sum[k] = sum[k] + p;
             }
             ++count;
@@ -1460,11 +1877,11 @@ int vxp_mass_properties(float vs, const vxp_brick* bricks, uint32_t n, float den
     for (int k = 0; k < 9; ++k) I.m[k] = 0.0f;
     for (uint32_t b = 0; b < n; ++b)
         for (int i = 0; i < 512; ++i) {
-            if ((h.vox[(size_t)b * 512 + i] & 7u) == 0u) continue;
+            if ((vox[(size_t)b * 512 + i] & 7u) == 0u) continue;
             const int c[3] = {i % 8, (i / 8) % 8, i / 64};
             float r[3];
             for (int k = 0; k < 3; ++k) {
-                const float p = ((float)(h.pos[(size_t)b * 3 + k] * 8 + c[k]) * vs + half) + vs * 0.5f;
+                const float p = ((float)(pos[(size_t)b * 3 + k] * 8 + c[k]) * vs + half) + vs * 0.5f;
                 r[k] = p - com[k];
             }
             const float r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
@@ -1788,10 +2205,7 @@ int vxp_set_wait_limit_ns(vxp_ctx* ctx, uint64_t ns) {
 
 int vxp_set_probe_tables(vxp_ctx* ctx, int enable) {
     if (!ctx) return VXP_ERR_ARG;
-    if (ctx->cols.tables != (enable != 0)) {
-        ctx->cols.tables = enable != 0;
-        ctx->cols.dirty = true;
-    }
+    ctx->cols.set_tables(enable != 0);
     return VXP_OK;
 }
 
@@ -1832,8 +2246,10 @@ struct vxp_batch {
     bool rebuild = true;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    const void* graph_key[3] = {nullptr, nullptr, nullptr};
+    const void* graph_worlds = nullptr;  // what the graph's launch was captured with
+    ColliderSet graph_cs{};
     uint32_t graph_n = 0, graph_threads = 0;
+    DBuf<uint32_t> d_word;  // a count read back by the host
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t cache_cap = 1024;
 };
@@ -1876,7 +2292,7 @@ __global__ void k_batch_status(const WorldDev* worlds, uint32_t n, uint32_t* out
 
 // Launch order, device WorldDev array and the graph of one step.
 int batch_prepare(vxp_batch* bt, float dt) {
-    if (int rc = bt->cols.sync(bt->err)) return rc;
+    if (int rc = bt->cols.sync(bt->stream, bt->err)) return rc;
     if (bt->rebuild || dt != bt->built_dt) {
         std::vector<uint32_t> ord;
         for (uint32_t s = 0; s < bt->slots.size(); ++s)
@@ -1904,9 +2320,9 @@ int batch_prepare(vxp_batch* bt, float dt) {
         bt->rebuild = false;
     }
     const ColliderSet cs = bt->cols.set();
-    const void* key[3] = {bt->d_worlds.p, cs.c, cs.vox};
     const uint32_t n = (uint32_t)bt->order.size();
-    if (bt->exec && key[0] == bt->graph_key[0] && key[1] == bt->graph_key[1] && key[2] == bt->graph_key[2] &&
+    if (bt->exec && bt->d_worlds.p == bt->graph_worlds && cs.c == bt->graph_cs.c &&
+        cs.grid == bt->graph_cs.grid && cs.vox == bt->graph_cs.vox && cs.n == bt->graph_cs.n && cs.nb == bt->graph_cs.nb &&
         n == bt->graph_n && bt->threads == bt->graph_threads)
         return VXP_OK;
     if (bt->exec) {
@@ -1929,7 +2345,8 @@ int batch_prepare(vxp_batch* bt, float dt) {
         return bfail(bt, VXP_ERR_CUDA, "graph capture: %s / %s", cudaGetErrorString(le), cudaGetErrorString(ce));
     bt->graph = g;
     BK(cudaGraphInstantiate(&bt->exec, bt->graph, 0));
-    for (int i = 0; i < 3; ++i) bt->graph_key[i] = key[i];
+    bt->graph_worlds = bt->d_worlds.p;
+    bt->graph_cs = cs;
     bt->graph_n = n;
     bt->graph_threads = bt->threads;
     return VXP_OK;
@@ -1987,6 +2404,34 @@ int vxp_batch_collider_upload(vxp_batch* bt, uint32_t collider_id, float voxel_s
     if (!bt) return VXP_ERR_ARG;
     BK(cudaStreamSynchronize(bt->stream));
     return bt->cols.upload(collider_id, voxel_size, bricks, n_bricks, bt->err);
+}
+
+int vxp_batch_collider_edit(vxp_batch* bt, uint32_t collider_id, const int32_t* coords, const uint8_t* values,
+                            uint32_t n, int mode) {
+    if (!bt) return VXP_ERR_ARG;
+    if (mode != VXP_EDIT_SET && mode != VXP_EDIT_OCCUPANCY) return bfail(bt, VXP_ERR_ARG, "unknown edit mode %d", mode);
+    return bt->cols.edit(collider_id, coords, values, n, (uint32_t)mode, bt->stream, bt->err);
+}
+
+int vxp_batch_collider_read(vxp_batch* bt, uint32_t collider_id, vxp_collider_info* info, vxp_brick* bricks,
+                            uint32_t cap, uint32_t* n_bricks) {
+    if (!bt) return VXP_ERR_ARG;
+    return bt->cols.read(collider_id, info, bricks, cap, n_bricks, bt->stream, bt->err);
+}
+
+int vxp_batch_invalidate_cache_for_body(vxp_batch* bt, uint32_t world, uint32_t body_id, uint32_t* n_invalidated) {
+    if (!bt || world >= bt->slots.size() || !bt->slots[world]) return bfail(bt, VXP_ERR_ARG, "no such world");
+    if (bt->d_word.reserve(1) != cudaSuccess) return bfail(bt, VXP_ERR_OOM, "device allocation failed");
+    WorldBuffers& w = *bt->slots[world];
+    const uint32_t cap = w.cache_cap;
+    BK(cudaMemsetAsync(bt->d_word.p, 0, sizeof(uint32_t), bt->stream));
+    k_cache_invalidate<<<(cap + 255) / 256, 256, 0, bt->stream>>>(w.ckey.p, cap, body_id, bt->d_word.p);
+    BK(cudaGetLastError());
+    if (n_invalidated) {
+        BK(cudaMemcpyAsync(n_invalidated, bt->d_word.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, bt->stream));
+        BK(cudaStreamSynchronize(bt->stream));
+    }
+    return VXP_OK;
 }
 
 int vxp_batch_world_set(vxp_batch* bt, uint32_t world, const vxp_body* bodies, uint32_t n, uint32_t pair_capacity) {

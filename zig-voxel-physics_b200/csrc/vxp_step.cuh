@@ -235,34 +235,41 @@ __device__ __forceinline__ uint32_t voxel_at(const ColliderSet& cs, const DColli
     return (uint32_t)__ldg(&cs.vox[(size_t)(c.brick_off + (uint32_t)slot) * 512u + (uint32_t)((x & 7) + 8 * (y & 7) +
                                                                                                  64 * (z & 7))]);
 }
-// The neighbourhood masks of collider ci's probe centres (DCollider::nb_off):
-// one thread per centre, the same 27 lookups and clipping as a probe.
-__global__ void k_nbhd_build(ColliderSet cs, uint4* nb) {
-    for (uint32_t ci = blockIdx.y; ci < cs.n; ci += gridDim.y) {
-        const DCollider& c = cs.c[ci];
+// The masks of table entry e (the probe centre at offset e of [min_bound - 1,
+// max_bound], x fastest, extents ex, ey): the same 27 lookups and clipping as
+// a probe.
+__device__ __forceinline__ uint4 nbhd_entry(const ColliderSet& cs, const DCollider& c, uint32_t e, uint32_t ex,
+                                            uint32_t ey) {
+    const int32_t x = c.min_bound[0] - 1 + (int32_t)(e % ex), y = c.min_bound[1] - 1 + (int32_t)((e / ex) % ey),
+                  z = c.min_bound[2] - 1 + (int32_t)(e / (ex * ey));
+    uint32_t ne = 0u, co = 0u, ec = 0u, in = 0u;
+    for (uint32_t k = 0; k < 27u; ++k) {
+        const int32_t bx = x + (int32_t)(k % 3u) - 1, by = y + (int32_t)((k / 3u) % 3u) - 1,
+                      bz = z + (int32_t)(k / 9u) - 1;
+        if (bx < c.min_bound[0] || bx >= c.max_bound[0] || by < c.min_bound[1] || by >= c.max_bound[1] ||
+            bz < c.min_bound[2] || bz >= c.max_bound[2])
+            continue;
+        const uint32_t tb = vtype(voxel_at(cs, c, bx, by, bz));
+        ne |= (uint32_t)(tb != kEmpty) << k;
+        co |= (uint32_t)(tb == kCorner) << k;
+        ec |= (uint32_t)(tb == kCorner || tb == kEdge) << k;
+        in |= (uint32_t)(tb == kInside) << k;
+    }
+    return make_uint4(ne, co, ec, in);
+}
+// The neighbourhood masks of the listed colliders' probe centres
+// (DCollider::nb_off; every collider when list is null): one thread per centre.
+__global__ void k_nbhd_build(ColliderSet cs, uint4* nb, const uint32_t* list, uint32_t n_list) {
+    const uint32_t n = list ? n_list : cs.n;
+    for (uint32_t li = blockIdx.y; li < n; li += gridDim.y) {
+        const DCollider& c = cs.c[list ? list[li] : li];
         if (c.nb_off == kNoTable) continue;
         const uint32_t ex = (uint32_t)(c.max_bound[0] - c.min_bound[0]) + 2u,
                        ey = (uint32_t)(c.max_bound[1] - c.min_bound[1]) + 2u,
                        ez = (uint32_t)(c.max_bound[2] - c.min_bound[2]) + 2u;
         const uint32_t total = ex * ey * ez;
-        for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
-            const int32_t x = c.min_bound[0] - 1 + (int32_t)(e % ex), y = c.min_bound[1] - 1 + (int32_t)((e / ex) % ey),
-                          z = c.min_bound[2] - 1 + (int32_t)(e / (ex * ey));
-            uint32_t ne = 0u, co = 0u, ec = 0u, in = 0u;
-            for (uint32_t k = 0; k < 27u; ++k) {
-                const int32_t bx = x + (int32_t)(k % 3u) - 1, by = y + (int32_t)((k / 3u) % 3u) - 1,
-                              bz = z + (int32_t)(k / 9u) - 1;
-                if (bx < c.min_bound[0] || bx >= c.max_bound[0] || by < c.min_bound[1] || by >= c.max_bound[1] ||
-                    bz < c.min_bound[2] || bz >= c.max_bound[2])
-                    continue;
-                const uint32_t tb = vtype(voxel_at(cs, c, bx, by, bz));
-                ne |= (uint32_t)(tb != kEmpty) << k;
-                co |= (uint32_t)(tb == kCorner) << k;
-                ec |= (uint32_t)(tb == kCorner || tb == kEdge) << k;
-                in |= (uint32_t)(tb == kInside) << k;
-            }
-            nb[c.nb_off + e] = make_uint4(ne, co, ec, in);
-        }
+        for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x)
+            nb[c.nb_off + e] = nbhd_entry(cs, c, e, ex, ey);
     }
 }
 // Slot of the brick at brick coordinates (bx, by, bz), or -1.

@@ -46,8 +46,13 @@ struct DCollider {
     // [min_bound - 1, max_bound] per axis (x fastest), a uint4 of 27-bit masks
     // over the centre's 3 x 3 x 3 neighbours inside [min_bound, max_bound)
     // (bit dz*9 + dy*3 + dx, offsets from -1): non-empty, corner, corner or
-    // edge, inside.  Built once from the voxels when the colliders upload.
+    // edge, inside.  Built from the voxels when the collider reaches the
+    // device, and again after each edit of its voxels.
     uint32_t nb_off;
+    // The table's range in the pool: nb_cap entries from nb_base (nb_cap 0:
+    // none).  An edit that leaves more probe centres than nb_cap sets nb_off
+    // to kNoTable, and the probes fall back to their 27 lookups.
+    uint32_t nb_base, nb_cap;
 };
 constexpr uint32_t kNoTable = 0xFFFFFFFFu;
 

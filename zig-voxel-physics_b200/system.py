@@ -30,6 +30,26 @@ class VxpError(RuntimeError):
         self.code = code
 
 
+def _edit_args(coords, values, mode):
+    coords = np.ascontiguousarray(coords, dtype=np.int32).reshape(-1, 3)
+    values = np.ascontiguousarray(values, dtype=np.uint8).reshape(-1)
+    if len(values) != len(coords):
+        raise ValueError("one value per voxel")
+    mode = {"set": abi.EDIT_SET, "occupancy": abi.EDIT_OCCUPANCY}.get(mode, mode)
+    return coords, values, int(mode)
+
+
+def _read_collider(fn, handle, collider_id):
+    info = np.zeros(1, dtype=abi.COLLIDER_INFO_DTYPE)
+    n = ctypes.c_uint32(0)
+    rc = fn(handle, int(collider_id), abi.ptr(info), None, 0, ctypes.byref(n))
+    if rc != 0:
+        return rc, None, None
+    bricks = np.zeros(n.value, dtype=abi.BRICK_DTYPE)
+    rc = fn(handle, int(collider_id), abi.ptr(info), abi.ptr(bricks), len(bricks), ctypes.byref(n))
+    return rc, info[0], bricks
+
+
 class VoxelPhysicsSystem:
     """One simulated world on one GPU."""
 
@@ -75,6 +95,31 @@ class VoxelPhysicsSystem:
         bricks = np.ascontiguousarray(bricks, dtype=abi.BRICK_DTYPE)
         self._check(self.lib.vxp_collider_upload(self.ctx, int(collider_id), np.float32(voxel_size),
                                                  abi.ptr(bricks), len(bricks)))
+
+    def edit_collider(self, collider_id: int, coords, values, mode="occupancy") -> None:
+        """Writes voxels of an uploaded collider on the device, then recomputes
+        its metadata (vxp_collider_edit).  mode "set": values are CollisionVoxel
+        bytes, stored as setCollisionVoxel stores them; "occupancy": nonzero
+        makes the voxel solid, zero empty, and the written voxels and their
+        solid face neighbours are re-typed by classifyFromNeighbors.  Queued
+        after the steps already queued."""
+        coords, values, mode = _edit_args(coords, values, mode)
+        self._check(self.lib.vxp_collider_edit(self.ctx, int(collider_id), abi.ptr(coords), abi.ptr(values),
+                                               len(values), mode))
+
+    def read_collider(self, collider_id: int):
+        """(info, bricks) of the collider as the device holds it: info is a
+        COLLIDER_INFO_DTYPE record, bricks a BRICK_DTYPE array."""
+        rc, info, bricks = _read_collider(self.lib.vxp_collider_read, self.ctx, collider_id)
+        self._check(rc)
+        return info, bricks
+
+    def invalidate_cache_for_body(self, body_id: int) -> int:
+        """NarrowPhase.invalidateCacheForBody: drops the body's brick-pair
+        cache entries; returns how many there were."""
+        n = ctypes.c_uint32(0)
+        self._check(self.lib.vxp_invalidate_cache_for_body(self.ctx, int(body_id), ctypes.byref(n)))
+        return int(n.value)
 
     def set_bodies(self, bodies: np.ndarray) -> None:
         bodies = np.ascontiguousarray(bodies, dtype=abi.BODY_DTYPE)
@@ -269,6 +314,23 @@ class VoxelWorldBatch:
         bricks = np.ascontiguousarray(bricks, dtype=abi.BRICK_DTYPE)
         self._check(self.lib.vxp_batch_collider_upload(self.b, int(collider_id), np.float32(voxel_size),
                                                        abi.ptr(bricks), len(bricks)))
+
+    def edit_collider(self, collider_id: int, coords, values, mode="occupancy") -> None:
+        """VoxelPhysicsSystem.edit_collider on the batch's shared colliders:
+        every world whose bodies use the collider sees the edit."""
+        coords, values, mode = _edit_args(coords, values, mode)
+        self._check(self.lib.vxp_batch_collider_edit(self.b, int(collider_id), abi.ptr(coords), abi.ptr(values),
+                                                     len(values), mode))
+
+    def read_collider(self, collider_id: int):
+        rc, info, bricks = _read_collider(self.lib.vxp_batch_collider_read, self.b, collider_id)
+        self._check(rc)
+        return info, bricks
+
+    def invalidate_cache_for_body(self, world: int, body_id: int) -> int:
+        n = ctypes.c_uint32(0)
+        self._check(self.lib.vxp_batch_invalidate_cache_for_body(self.b, int(world), int(body_id), ctypes.byref(n)))
+        return int(n.value)
 
     def set_world(self, world: int, bodies: np.ndarray, pair_capacity: int = 0) -> None:
         bodies = np.ascontiguousarray(bodies, dtype=abi.BODY_DTYPE)
