@@ -469,7 +469,10 @@ def ours(args):
                        "settle_steps": settle, "l2": "flushed (256 MiB write) between timed steps",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single world",
                        "contact_points_mean": statistics.mean(pts), "pairs_mean": statistics.mean(
-                           [s["pairs_tested"] for s in stats])},
+                           [s["pairs_tested"] for s in stats]),
+                       # 1: constraint rows in the cluster's shared memory; 2: the
+                       # rows that do not fit spilled to global memory; 3: all in L2
+                       "sweep_paths": sorted({int(s["sweep_path"]) for s in stats})},
             "contacts_per_s": contacts_per_s,
             "step_latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                                 "kernel_mean": statistics.mean(kern_ms), "pairs_mean": statistics.mean(pair_ms)},

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define VXP_ABI_VERSION 1
+#define VXP_ABI_VERSION 2
 
 /* ---- status codes (Zig error unions swallowed by `catch {}` in the
  *      reference become explicit codes here; src/system.zig:577,610,637,...) */
@@ -181,6 +181,11 @@ typedef struct {
     uint32_t bricks_touched;         /* bricks of A inside the overlap region
                                         plus bricks of B inside B's, summed over
                                         the pairs detected (traffic accounting) */
+    uint32_t sweep_path;             /* how the solver's sweeps ran on the
+                                        thread-block cluster: 1 every constraint
+                                        row in shared memory, 2 the rows that did
+                                        not fit in global memory, 3 all state in
+                                        L2; 0 no cluster sweep this step      */
 } vxp_stats;
 
 /* One candidate voxel pair of the narrow phase, for parity checks of the

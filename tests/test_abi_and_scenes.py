@@ -18,7 +18,7 @@ def test_library_exports_every_header_symbol(vxp):
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) <= set(vxp.abi.SIGNATURES), set(names) - set(vxp.abi.SIGNATURES)
-    assert lib.vxp_abi_version() == 1
+    assert lib.vxp_abi_version() == 2
 
 
 def test_config_default_matches_reference(vxp):
@@ -36,7 +36,7 @@ def test_struct_sizes(vxp):
     assert a.MANIFOLD_DTYPE.itemsize == 376
     assert a.CONTACT_DTYPE.itemsize == 88
     assert ctypes.sizeof(a.Config) == 4 * 26
-    assert ctypes.sizeof(a.Stats) == 4 * 19
+    assert ctypes.sizeof(a.Stats) == 4 * 20
 
 
 def test_classification_matches_reference(vxp):

@@ -95,14 +95,19 @@ def test_config1_modes(vxp, cfg):
 
 
 @pytest.mark.parametrize("solver,smem,cons", [(0, None, None), (1, None, None), (2, None, None), (2, 0, None),
-                                              (2, None, 1)])
+                                              (2, 4096, None), (2, None, 1)])
 def test_config2_pile_subset(vxp, solver, smem, cons):
     """216 boxes of the config-2 pile, 8 substeps at 1/120 s, grid launch,
-    each grid solver mode (the cluster one with its state in shared memory and
-    in L2, and with the colouring on the cluster and on the grid)."""
+    each grid solver mode (the cluster one with its state in shared memory,
+    with 4 KiB of shared memory a CTA so that most constraint rows spill to
+    global memory, and in L2; with the colouring on the cluster and on the
+    grid).  The last step's stats say which sweep path ran."""
     sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
-    lockstep(vxp, sc, 200, mode=1, check_every=10, solver=solver, cluster_smem=smem, cluster_cons=cons,
-             substeps=8).close()
+    g = lockstep(vxp, sc, 200, mode=1, check_every=10, solver=solver, cluster_smem=smem, cluster_cons=cons,
+                 substeps=8)
+    want = {None: 1, 4096: 2, 0: 3}[smem] if solver == 2 else 0
+    assert g.stats()["sweep_path"] == want
+    g.close()
 
 
 def test_cluster_available(vxp):

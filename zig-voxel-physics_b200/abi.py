@@ -156,6 +156,7 @@ class Stats(ctypes.Structure):
         ("max_penetration", ctypes.c_float),
         ("candidates", ctypes.c_uint32),
         ("bricks_touched", ctypes.c_uint32),
+        ("sweep_path", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:

@@ -902,6 +902,9 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
 struct WorldBuffers {
     uint32_t n_bodies = 0, body_cap = 0, pair_cap = 0, ht_cap = 0, cache_cap = 1024, dump_cap = 0, scan_blocks = 1;
     bool live = true;  // a batch slot whose world was cleared keeps its buffers with live = false
+    // a context's world (swept by a cluster) keeps a global home for the
+    // constraint rows that do not fit in the cluster's shared memory
+    bool spill_rows = false;
     std::vector<uint32_t> collider_public;
     DBuf<DBody> body;
     DBuf<DBodyProp> prop;
@@ -920,7 +923,7 @@ struct WorldBuffers {
     DBuf<uint32_t> frame;
     DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag;
     DBuf<CacheLook> clist;
-    DBuf<float> cp;
+    DBuf<float> cp, crow;
     DBuf<uint4> cm, rk;
     DBuf<float2> cfr;
     DBuf<uint32_t> ev;
@@ -978,6 +981,7 @@ struct WorldBuffers {
         ok &= flag.reserve(cap) == cudaSuccess;
         ok &= clist.reserve(cap) == cudaSuccess;
         ok &= cp.reserve((size_t)CP_NFIELDS * 4 * cap) == cudaSuccess;
+        if (spill_rows) ok &= crow.reserve((size_t)CP_NVEL * 4 * cap) == cudaSuccess;
         ok &= cm.reserve(cap) == cudaSuccess;
         ok &= rk.reserve(cap) == cudaSuccess;
         ok &= chunk.reserve((size_t)cap / 32 + 257) == cudaSuccess;
@@ -1207,6 +1211,7 @@ struct WorldBuffers {
         w.n_static = n_static;
         w.bmask = bmask.p;
         w.cp = cp.p;
+        w.crow = crow.p;
         w.cm = cm.p;
         w.rk = rk.p;
         w.ev = ev.p;
@@ -1277,6 +1282,7 @@ struct WorldBuffers {
         std::memcpy(&s->max_penetration, &bits, 4);
         s->candidates = c[C_CANDIDATES];
         s->bricks_touched = c[C_BRICKS];
+        s->sweep_path = c[C_SWEEP];
         return VXP_OK;
     }
 
@@ -1763,6 +1769,7 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     }
     cudaGetLastError();  // a refused size is not an error of this context
     ctx->solver_flow = ctx->cluster_size ? VXP_SOLVER_CLUSTER : VXP_SOLVER_EVENTS;
+    ctx->w.spill_rows = true;
     if (ctx->w.init(cache_cap, ctx->grid_blocks, ctx->err)) return bail(VXP_ERR_OOM);
     if (ctx->d_world.reserve(1) != cudaSuccess || ctx->bar.reserve(2) != cudaSuccess) return bail(VXP_ERR_OOM);
     if (ctx->w.ensure_pairs(std::max<uint32_t>(cfg->max_pairs, 1024), ctx->err)) return bail(VXP_ERR_OOM);

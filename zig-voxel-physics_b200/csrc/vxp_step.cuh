@@ -3425,24 +3425,41 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     // points: the packing's tallies when it grouped for this cluster, else
     // four per slot
     const bool tallied = w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
-    uint32_t needp = 0;
+    // point rows that do not fit in shared memory may go to w.crow: a CTA's
+    // last slots (the point offsets are a prefix in slot order, so once a
+    // slot's rows spill every later slot's do), in that CTA's range of w.crow
+    // (its offset: the points of the CTAs before it)
+    uint32_t needp = 0, goff = 0, gtot = 0;
     for (int attempt = 0; attempt < 2; ++attempt) {
         need = 0;
         needp = 0;
+        goff = 0;
+        gtot = 0;
         for (uint32_t cta = 0; cta < C; ++cta) {
             uint32_t n = 0;
             for (uint32_t c = 0; c < ncol; ++c) n += count_of(c, cta);
             need = max(need, n);
-            needp = max(needp, tallied ? w.ocnt[kOwnerPoints + (by_owner ? 0u : kMaxOwnerGroups) + cta] : 4u * n);
+            const uint32_t p = tallied ? w.ocnt[kOwnerPoints + (by_owner ? 0u : kMaxOwnerGroups) + cta] : 4u * n;
+            needp = max(needp, p);
+            if (cta < k) goff += p;
+            gtot += p;
         }
+        const size_t fixed = cluster_smem_bytes(sm.bcap, sm.nrep, max(need, 1u), 0u, ncol);
         if (!by_owner ||
-            cluster_smem_bytes(sm.bcap, sm.nrep, max(need, 1u), max(needp, 1u), ncol) <= smem_bytes)
+            (fixed <= smem_bytes &&
+             (w.crow != nullptr || fixed + (size_t)max(needp, 1u) * CP_NVEL * sizeof(float) <= smem_bytes)))
             break;
         by_owner = false;
     }
     sm.scap = max(need, 1u);
     sm.pcap = max(needp, 1u);
-    if (cluster_smem_bytes(sm.bcap, sm.nrep, sm.scap, sm.pcap, ncol) > smem_bytes) return false;
+    const size_t fixed = cluster_smem_bytes(sm.bcap, sm.nrep, sm.scap, 0u, ncol);
+    if (fixed > smem_bytes) return false;
+    // rows in shared memory (the rest spill)
+    const uint32_t pcap_s = (uint32_t)min((size_t)sm.pcap, (smem_bytes - fixed) / (CP_NVEL * sizeof(float)));
+    const bool spill = pcap_s < sm.pcap;
+    if (spill && (w.crow == nullptr || (size_t)gtot > 4u * (size_t)w.pair_cap)) return false;
+    if (t == 0 && k == 0) w.ctr[C_SWEEP] = spill ? SWEEP_SPILL : SWEEP_SHARED;
     {
         unsigned char* p = smem;
         sm.body = reinterpret_cast<DBody*>(p);
@@ -3454,7 +3471,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         sm.fr = reinterpret_cast<float2*>(p);
         p += (size_t)sm.scap * sizeof(float2);
         sm.row = reinterpret_cast<float*>(p);
-        p += (size_t)sm.pcap * CP_NVEL * sizeof(float);
+        p += (size_t)pcap_s * CP_NVEL * sizeof(float);
         sm.pos = reinterpret_cast<uint32_t*>(p);
         p += (size_t)sm.scap * sizeof(uint32_t);
         sm.po = reinterpret_cast<uint32_t*>(p);
@@ -3545,6 +3562,12 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     const bool points_fit = carry <= sm.pcap;  // the same in every thread of this block
     if (!points_fit && t == 0) atomicOr(&w.ctr[C_ERROR], ERR_BOUNDS);
     __syncthreads();
+    // a slot's first point row: in shared memory, or spilled to this CTA's
+    // range of w.crow
+    auto row_of = [&](uint32_t slot, uint32_t n) -> float* {
+        const uint32_t po = sm.po[slot];
+        return po + n <= pcap_s ? sm.row + (size_t)po * CP_NVEL : w.crow + ((size_t)goff + po) * CP_NVEL;
+    };
     for (uint32_t slot = t; slot < nsl; slot += T) {
         uint4 mv = sm.man[slot];
         if (!points_fit) {
@@ -3555,7 +3578,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
             sm.man[slot] = mv;
             continue;
         }
-        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + (size_t)sm.po[slot] * CP_NVEL, 1u, CP_NVEL};
+        const CPV vg = cpv_global(w, sm.pos[slot]), vs{row_of(slot, mv.z), 1u, CP_NVEL};
         for (uint32_t i = 0; i < mv.z; ++i) {
             st3(vs, CP_NX, i, ld3(vg, CP_NX, i));
             cpr(vs, CP_NI, i) = cpr(vg, CP_NI, i);
@@ -3593,7 +3616,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         DBody* pb = body_b(mv);
         const DBody A = *pa, B = *pb;
         BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
-        float* rows = sm.row + (size_t)sm.po[slot] * CP_NVEL;
+        float* rows = row_of(slot, mv.z);
         if (kind == 0u)
             warm_points_rows(rows, mv.z, cf.warm_scale, a, b, sf.friction);
         else
@@ -3638,7 +3661,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
                 const DBody A = *body_a(mv), B = *body_b(mv);
                 const BV a = bv_of(A, (mv.w & CM_WA) != 0u), b = bv_of(B, (mv.w & CM_WB) != 0u);
                 prepare_point_s<false>(sf, cpv_global(w, sm.pos[slot]),
-                                       CPV{sm.row + (size_t)sm.po[slot] * CP_NVEL, 1u, CP_NVEL},
+                                       CPV{row_of(slot, mv.z), 1u, CP_NVEL},
                                        sm.fr[slot].y, i,
                                        soft, hinv, a, qof(A.q), b, qof(B.q));
             }
@@ -3714,7 +3737,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     }
     for (uint32_t slot = t; slot < nslot; slot += T) {
         const uint4 mv = sm.man[slot];
-        const CPV vg = cpv_global(w, sm.pos[slot]), vs{sm.row + (size_t)sm.po[slot] * CP_NVEL, 1u, CP_NVEL};
+        const CPV vg = cpv_global(w, sm.pos[slot]), vs{row_of(slot, mv.z), 1u, CP_NVEL};
         for (uint32_t i = 0; i < mv.z; ++i) {
             cpr(vg, CP_NM, i) = cpr(vs, CP_NM, i);
             cpr(vg, CP_TM0, i) = cpr(vs, CP_TM0, i);
@@ -3948,7 +3971,10 @@ __device__ __forceinline__ void world_step_sweeps(ClusterGroup& g, WorldDev& w, 
         g.sync();
     }
     const bool solved = w.cfg.dt > 0.0f;
-    if (solved && !phase_solve_cluster(g, w, M, ncol, smem, smem_bytes)) phase_solve(g, w, M, ncol);
+    if (solved && !phase_solve_cluster(g, w, M, ncol, smem, smem_bytes)) {
+        if (g.rank() == 0) w.ctr[C_SWEEP] = SWEEP_L2;
+        phase_solve(g, w, M, ncol);
+    }
     g.sync();
     stamp(g, w, TS_SOLVE);
     phase_store(g, w, cur, M, solved);

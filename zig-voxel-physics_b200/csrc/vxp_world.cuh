@@ -200,6 +200,7 @@ enum : uint32_t {
     C_HWORK,         // work counter over that list
     C_CONS_M,        // constraint manifolds of the step (solve part split in two kernels)
     C_CONS_NCOL,     // their colours
+    C_SWEEP,         // how the cluster sweeps ran (SWEEP_*)
     C_ERROR = 31,    // sticky error bits (not cleared per step)
     C_NCTR = 32
 };
@@ -207,6 +208,11 @@ enum : uint32_t {
 enum : uint32_t {
     TS_START, TS_BEGIN, TS_PAIRS, TS_CACHE, TS_PROBE, TS_FINALIZE, TS_CONSTRAINTS, TS_SOLVE, TS_END, TS_N = 16
 };
+// C_SWEEP: the cluster kernel's sweeps with every constraint row in shared
+// memory, with the rows that did not fit in global memory, or with all
+// state in L2 (colour barriers); 0 when no cluster kernel ran.
+enum : uint32_t { SWEEP_SHARED = 1u, SWEEP_SPILL = 2u, SWEEP_L2 = 3u };
+static_assert(C_SWEEP < C_ERROR, "C_SWEEP is cleared with the per-step counters");
 enum : uint32_t { ERR_TIMEOUT = 1u, ERR_CAP = 2u, ERR_COLOURS = 4u, ERR_OVERFLOW = 8u, ERR_BOUNDS = 16u };
 
 // A brick-pair cache lookup of the step: the pair, its key and the start of
@@ -278,6 +284,8 @@ struct WorldDev {
     float* subrec;                // per substep and body: position, rotation, v, w (13 floats)
     // packed constraint data, slot-major [slot][M]; see CP_* field ids
     float* cp;                    // CP_NFIELDS * 4 * pair_cap floats
+    float* crow;                  // CP_NVEL * 4 * pair_cap floats or null: the cluster sweeps'
+                                  // point rows that do not fit in shared memory
     uint4* cm;                    // per packed manifold: ia, ib, n, pair
     float2* cfr;                  // per packed manifold: friction, restitution
     // scratch
