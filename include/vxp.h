@@ -275,6 +275,35 @@ int vxp_invalidate_cache_for_body(vxp_ctx* ctx, uint32_t body_id, uint32_t* n_in
 int vxp_bodies_set(vxp_ctx* ctx, const vxp_body* bodies, uint32_t n);
 int vxp_bodies_get(vxp_ctx* ctx, vxp_body* bodies, uint32_t n);
 
+/* Bulk state export for a renderer or another CUDA consumer: the per-handle
+ * getters getPosition, getRotation, getLinearVelocity, getAngularVelocity,
+ * getWorldAABB and isSleeping (src/system.zig:963-1017; getWorldAABB is the
+ * collider's local AABB through AABB.transform, src/body.zig:430-435,
+ * src/collider.zig:341-343, src/math.zig:686-693) for bodies
+ * [first, first + n) in vxp_bodies_set order, one array per field.  Every
+ * null pointer is skipped.  Layouts: 3 floats a body (x, y, z) for vectors,
+ * 4 for the rotation (x, y, z, w), one byte for sleeping (1 = asleep). */
+typedef struct {
+    float* position;
+    float* rotation;
+    float* linear_velocity;
+    float* angular_velocity;
+    float* aabb_min;
+    float* aabb_max;
+    uint8_t* sleeping;
+} vxp_state_view;
+
+/* device_memory = 0: the pointers are host memory (pinned is faster); the
+ * call returns once they are filled.
+ * device_memory = 1: every pointer is device memory of the context's device
+ * (checked; anything else is VXP_ERR_ARG), e.g. an instance buffer that a
+ * renderer maps for CUDA.  One kernel writes them on the context's stream
+ * after the work already queued there, and the call returns without waiting.
+ * When consumer_stream (a cudaStream_t) is not null, that stream waits for
+ * the export, so whatever the caller launches there next reads the state. */
+int vxp_bodies_export(vxp_ctx* ctx, const vxp_state_view* dst, uint32_t first, uint32_t n, int device_memory,
+                      void* consumer_stream);
+
 /* Host-side computeMassProperties (src/body.zig:462-519) over a brick list in
  * the order given; the inertia sum runs brick by brick, voxel index order. */
 int vxp_mass_properties(float voxel_size, const vxp_brick* bricks, uint32_t n_bricks,
@@ -463,6 +492,9 @@ int vxp_batch_world_clear(vxp_batch* b, uint32_t world);
 /* Empties the slot and frees its device memory (which waits for the device). */
 int vxp_batch_world_release(vxp_batch* b, uint32_t world);
 int vxp_batch_world_get(vxp_batch* b, uint32_t world, vxp_body* bodies, uint32_t n);
+/* vxp_bodies_export for one world of a batch, on the batch's stream. */
+int vxp_batch_world_export(vxp_batch* b, uint32_t world, const vxp_state_view* dst, uint32_t first, uint32_t n,
+                           int device_memory, void* consumer_stream);
 int vxp_batch_world_stats(vxp_batch* b, uint32_t world, vxp_stats* out);
 /* Device bytes held by a world slot, occupied or cleared (admission
  * accounting). */

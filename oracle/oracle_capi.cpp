@@ -388,6 +388,29 @@ int vxo_candidates_get(void* p, vxp_candidate* out, uint32_t cap, uint32_t* n_ou
     return 0;
 }
 
+// VoxelBody.getWorldAABB (body.zig:430-435) of every body, 3 floats each.
+int vxo_world_aabbs(void* p, float* mn, float* mx, uint32_t cap) {
+    int rc = 0;
+    DISPATCH(p, {
+        const auto& bodies = h->w.bodies;
+        if (bodies.size() > cap) {
+            rc = VXP_ERR_CAP;
+        } else {
+            for (size_t i = 0; i < bodies.size(); ++i) {
+                const auto& b = bodies[i];
+                using R = std::remove_reference_t<decltype(b.inv_mass)>;
+                Aabb<R> bx;  // a body without a collider: its position (no comma: this is a macro argument)
+                bx.mn = b.pos;
+                bx.mx = b.pos;
+                if (b.collider >= 0) bx = aabbTransform(h->w.colliders[(size_t)b.collider].local_aabb, b.xf());
+                mn[3 * i] = (float)bx.mn.x; mn[3 * i + 1] = (float)bx.mn.y; mn[3 * i + 2] = (float)bx.mn.z;
+                mx[3 * i] = (float)bx.mx.x; mx[3 * i + 1] = (float)bx.mx.y; mx[3 * i + 2] = (float)bx.mx.z;
+            }
+        }
+    });
+    return rc;
+}
+
 int vxo_pairs_find(void* p, float margin, vxp_pair* out, uint32_t cap, uint32_t* n_out) {
     int rc = 0;
     DISPATCH(p, {

@@ -48,6 +48,7 @@ for name, res, args in [
     ("vxo_substeps_get", _I, [_VP, _VP, _U32, _PU32]),
     ("vxo_candidates_get", _I, [_VP, _VP, _U32, _PU32]),
     ("vxo_pairs_find", _I, [_VP, _F, _VP, _U32, _PU32]),
+    ("vxo_world_aabbs", _I, [_VP, _VP, _VP, _U32]),
     ("vxo_narrow_phase_threaded", _I, [_VP, _VP, _U32, _I]),
     ("vxo_step_threaded", _I, [_VP, _F, _VP, _U32, _I]),
     ("vxo_mass_properties", _I, [_F, _VP, _U32, _F, ctypes.POINTER(_F), _VP]),
@@ -167,6 +168,13 @@ class OracleWorld:
         out = np.zeros(n.value, dtype=abi.PAIR_DTYPE)
         assert L.vxo_pairs_find(self.h, np.float32(m), abi.ptr(out), len(out), ctypes.byref(n)) == 0
         return out
+
+    def world_aabbs(self):
+        """VoxelBody.getWorldAABB of every body: (min, max), each (n, 3) float32."""
+        mn = np.zeros((self.n_bodies, 3), dtype=np.float32)
+        mx = np.zeros((self.n_bodies, 3), dtype=np.float32)
+        assert L.vxo_world_aabbs(self.h, abi.ptr(mn), abi.ptr(mx), self.n_bodies) == 0
+        return mn, mx
 
     def step(self, dt, pairs=None):
         if pairs is None:

@@ -163,6 +163,27 @@ class Stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class StateView(ctypes.Structure):
+    """vxp_state_view: one pointer per exported field (null = skipped)."""
+    _fields_ = [
+        ("position", ctypes.c_void_p),
+        ("rotation", ctypes.c_void_p),
+        ("linear_velocity", ctypes.c_void_p),
+        ("angular_velocity", ctypes.c_void_p),
+        ("aabb_min", ctypes.c_void_p),
+        ("aabb_max", ctypes.c_void_p),
+        ("sleeping", ctypes.c_void_p),
+    ]
+
+
+# Exported fields and their per-body shape and type (vxp_bodies_export).
+EXPORT_FIELDS = {
+    "position": (3, np.float32), "rotation": (4, np.float32), "linear_velocity": (3, np.float32),
+    "angular_velocity": (3, np.float32), "aabb_min": (3, np.float32), "aabb_max": (3, np.float32),
+    "sleeping": (1, np.uint8),
+}
+
+
 def default_config(**overrides) -> Config:
     """The reference defaults: PhysicsConfig{} + SolverConfig{} + NarrowPhaseConfig{}
     (system.zig:47-88, solver.zig:75-119, narrow_phase.zig:1325-1343)."""
@@ -221,6 +242,7 @@ SIGNATURES = {
     "vxp_invalidate_cache_for_body": (_I, [_VP, _U32, _VP]),
     "vxp_bodies_set": (_I, [_VP, _VP, _U32]),
     "vxp_bodies_get": (_I, [_VP, _VP, _U32]),
+    "vxp_bodies_export": (_I, [_VP, _VP, _U32, _U32, _I, _VP]),
     "vxp_mass_properties": (_I, [_F, _VP, _U32, _F, ctypes.POINTER(_F), _VP]),
     "vxp_step": (_I, [_VP, _F, _VP, _U32]),
     "vxp_step_device_pairs": (_I, [_VP, _F, _F]),
@@ -260,6 +282,7 @@ SIGNATURES = {
     "vxp_batch_world_set": (_I, [_VP, _U32, _VP, _U32, _U32]),
     "vxp_batch_world_clear": (_I, [_VP, _U32]),
     "vxp_batch_world_release": (_I, [_VP, _U32]),
+    "vxp_batch_world_export": (_I, [_VP, _U32, _VP, _U32, _U32, _I, _VP]),
     "vxp_batch_world_get": (_I, [_VP, _U32, _VP, _U32]),
     "vxp_batch_world_stats": (_I, [_VP, _U32, _VP]),
     "vxp_batch_world_bytes": (ctypes.c_uint64, [_VP, _U32]),

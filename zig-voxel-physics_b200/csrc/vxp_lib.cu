@@ -90,16 +90,15 @@ __global__ void __launch_bounds__(256, 1) k_solve_cluster(const WorldDev* world,
 
 // Pair source: world AABB of each body's collider (AABB.transform,
 // math.zig:686-693) inflated by margin.
-__global__ void k_body_aabbs(const DBody* body, const DBodyProp* prop, uint32_t n, ColliderSet cs, float margin,
-                             float4* mn, float4* mx) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const DBody b = body[i];
+// VoxelBody.getWorldAABB (body.zig:430-435): the collider's local AABB
+// through AABB.transform (math.zig:686-693), or the position for a body
+// without a collider.
+__device__ __forceinline__ void body_world_aabb(const DBody& b, const DBodyProp& pr, const ColliderSet& cs, F3& lo,
+                                                F3& hi) {
     const F3 x = f3of(b.p);
     const Qt q = qof(b.q);
-    F3 lo, hi;
-    if (prop[i].collider < cs.n) {
-        const DCollider& c = cs.c[prop[i].collider];
+    if (pr.collider < cs.n) {
+        const DCollider& c = cs.c[pr.collider];
         const float inf = __int_as_float(0x7f800000);
         lo = F3{inf, inf, inf};
         hi = F3{-inf, -inf, -inf};
@@ -114,10 +113,64 @@ __global__ void k_body_aabbs(const DBody* body, const DBodyProp* prop, uint32_t 
         lo = x;
         hi = x;
     }
+}
+
+__global__ void k_body_aabbs(const DBody* body, const DBodyProp* prop, uint32_t n, ColliderSet cs, float margin,
+                             float4* mn, float4* mx) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    F3 lo, hi;
+    body_world_aabb(body[i], prop[i], cs, lo, hi);
     lo = lo - F3{margin, margin, margin};
     hi = hi + F3{margin, margin, margin};
     mn[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
     mx[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
+}
+
+// Bulk state export of bodies [first, first + n): one thread a body, each
+// requested field into its own array (vxp_bodies_export).
+__global__ void k_export(const DBody* body, const DBodyProp* prop, uint32_t first, uint32_t n, ColliderSet cs,
+                         vxp_state_view d) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t i = first + j;
+    const DBody b = body[i];
+    if (d.position) {
+        d.position[3u * j] = b.p.x;
+        d.position[3u * j + 1u] = b.p.y;
+        d.position[3u * j + 2u] = b.p.z;
+    }
+    if (d.rotation) {  // scalar stores: the caller's array need only be 4-byte aligned
+        d.rotation[4u * j] = b.q.x;
+        d.rotation[4u * j + 1u] = b.q.y;
+        d.rotation[4u * j + 2u] = b.q.z;
+        d.rotation[4u * j + 3u] = b.q.w;
+    }
+    if (d.linear_velocity) {
+        d.linear_velocity[3u * j] = b.v.x;
+        d.linear_velocity[3u * j + 1u] = b.v.y;
+        d.linear_velocity[3u * j + 2u] = b.v.z;
+    }
+    if (d.angular_velocity) {
+        d.angular_velocity[3u * j] = b.w.x;
+        d.angular_velocity[3u * j + 1u] = b.w.y;
+        d.angular_velocity[3u * j + 2u] = b.w.z;
+    }
+    if (d.aabb_min || d.aabb_max) {
+        F3 lo, hi;
+        body_world_aabb(b, prop[i], cs, lo, hi);
+        if (d.aabb_min) {
+            d.aabb_min[3u * j] = lo.x;
+            d.aabb_min[3u * j + 1u] = lo.y;
+            d.aabb_min[3u * j + 2u] = lo.z;
+        }
+        if (d.aabb_max) {
+            d.aabb_max[3u * j] = hi.x;
+            d.aabb_max[3u * j + 1u] = hi.y;
+            d.aabb_max[3u * j + 2u] = hi.z;
+        }
+    }
+    if (d.sleeping) d.sleeping[j] = prop[i].sleeping ? 1u : 0u;
 }
 
 // Pairs (s < t in id order) whose inflated AABBs overlap and that are not
@@ -935,6 +988,7 @@ struct WorldBuffers {
     DBuf<CacheKeyRec> ckey;
     DBuf<CacheValRec> cval;
     DBuf<WorldDev::Cand> dump;
+    DBuf<unsigned char> export_stage;  // host-memory exports land here first
 
     int init(uint32_t cache, uint32_t blocks, std::string& err) {
         cache_cap = cache;
@@ -1839,6 +1893,103 @@ int vxp_bodies_set(vxp_ctx* ctx, const vxp_body* b, uint32_t n) {
     return ctx->w.set_bodies(b, n, ctx->cols, ctx->err);
 }
 
+// vxp_bodies_export / vxp_batch_world_export on one world's buffers.
+static int export_world(WorldBuffers& w, const ColliderSet& cs, const vxp_state_view* dst, uint32_t first,
+                        uint32_t n, int device_memory, void* consumer, cudaStream_t stream, int device,
+                        std::string& err) {
+    if (!dst) {
+        err = "null state view";
+        return VXP_ERR_ARG;
+    }
+    if (first > w.n_bodies || n > w.n_bodies - first) {
+        err = fmt("bodies [%u, %u + %u) outside the %u bodies", first, first, n, w.n_bodies);
+        return VXP_ERR_ARG;
+    }
+    // per field: the caller's pointer and its bytes
+    void* ptr[7] = {dst->position, dst->rotation, dst->linear_velocity, dst->angular_velocity,
+                    dst->aabb_min, dst->aabb_max, dst->sleeping};
+    const size_t per[7] = {12, 16, 12, 12, 12, 12, 1};
+    if (n == 0) return VXP_OK;
+    const dim3 grid((n + 255u) / 256u);
+    if (device_memory) {
+        for (int f = 0; f < 7; ++f) {
+            if (!ptr[f]) continue;
+            cudaPointerAttributes at{};
+            if (cudaPointerGetAttributes(&at, ptr[f]) != cudaSuccess ||
+                (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != device) {
+                cudaGetLastError();  // an unregistered host pointer can leave this call's error behind
+                err = fmt("state view field %d is not device memory of device %d", f, device);
+                return VXP_ERR_ARG;
+            }
+        }
+        k_export<<<grid, 256, 0, stream>>>(w.body.p, w.prop.p, first, n, cs, *dst);
+        if (cudaPeekAtLastError() != cudaSuccess) {
+            err = fmt("export launch: %s", cudaGetErrorString(cudaGetLastError()));
+            return VXP_ERR_CUDA;
+        }
+        if (consumer) {
+            cudaEvent_t ev = nullptr;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventRecord(ev, stream) != cudaSuccess ||
+                cudaStreamWaitEvent((cudaStream_t)consumer, ev, 0) != cudaSuccess) {
+                if (ev) cudaEventDestroy(ev);
+                err = "export: consumer stream wait failed";
+                return VXP_ERR_CUDA;
+            }
+            cudaEventDestroy(ev);  // released once the recorded work completes
+        }
+        return VXP_OK;
+    }
+    // host memory: every requested field into the staging buffer, then copied out
+    size_t off[7], total = 0;
+    for (int f = 0; f < 7; ++f) {
+        off[f] = total;
+        if (ptr[f]) total += (per[f] * n + 15u) & ~(size_t)15u;
+    }
+    if (total == 0) return VXP_OK;
+    if (w.export_stage.reserve(total) != cudaSuccess) {
+        err = "export staging: device allocation failed";
+        return VXP_ERR_OOM;
+    }
+    unsigned char* st = w.export_stage.p;
+    vxp_state_view dv{};
+    dv.position = dst->position ? reinterpret_cast<float*>(st + off[0]) : nullptr;
+    dv.rotation = dst->rotation ? reinterpret_cast<float*>(st + off[1]) : nullptr;
+    dv.linear_velocity = dst->linear_velocity ? reinterpret_cast<float*>(st + off[2]) : nullptr;
+    dv.angular_velocity = dst->angular_velocity ? reinterpret_cast<float*>(st + off[3]) : nullptr;
+    dv.aabb_min = dst->aabb_min ? reinterpret_cast<float*>(st + off[4]) : nullptr;
+    dv.aabb_max = dst->aabb_max ? reinterpret_cast<float*>(st + off[5]) : nullptr;
+    dv.sleeping = dst->sleeping ? st + off[6] : nullptr;
+    k_export<<<grid, 256, 0, stream>>>(w.body.p, w.prop.p, first, n, cs, dv);
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        err = fmt("export launch: %s", cudaGetErrorString(cudaGetLastError()));
+        return VXP_ERR_CUDA;
+    }
+    for (int f = 0; f < 7; ++f) {
+        if (!ptr[f]) continue;
+        if (cudaMemcpyAsync(ptr[f], st + off[f], per[f] * n, cudaMemcpyDeviceToHost, stream) != cudaSuccess) {
+            err = "export: copy to host failed";
+            return VXP_ERR_CUDA;
+        }
+    }
+    if (cudaStreamSynchronize(stream) != cudaSuccess) {
+        err = "export: stream synchronize failed";
+        return VXP_ERR_CUDA;
+    }
+    return VXP_OK;
+}
+
+int vxp_bodies_export(vxp_ctx* ctx, const vxp_state_view* dst, uint32_t first, uint32_t n, int device_memory,
+                      void* consumer_stream) {
+    if (!ctx) return VXP_ERR_ARG;
+    if (!device_memory) {
+        if (int rc = check_device_error(ctx)) return rc;
+    }
+    if (int rc = ctx->cols.sync(ctx->stream, ctx->err)) return rc;
+    return export_world(ctx->w, ctx->cols.set(), dst, first, n, device_memory, consumer_stream, ctx->stream,
+                        ctx->device, ctx->err);
+}
+
 int vxp_bodies_get(vxp_ctx* ctx, vxp_body* b, uint32_t n) {
     if (!ctx || (!b && n)) return fail(ctx, VXP_ERR_ARG, "null argument");
     if (int rc = check_device_error(ctx)) return rc;
@@ -2490,6 +2641,16 @@ int vxp_batch_world_get(vxp_batch* bt, uint32_t world, vxp_body* bodies, uint32_
         return bfail(bt, VXP_ERR_ARG, "no such world");
     BK(cudaStreamSynchronize(bt->stream));
     return bt->slots[world]->get_bodies(bodies, n, bt->stream, bt->err);
+}
+
+int vxp_batch_world_export(vxp_batch* bt, uint32_t world, const vxp_state_view* dst, uint32_t first, uint32_t n,
+                           int device_memory, void* consumer_stream) {
+    if (!bt || world >= bt->slots.size() || !bt->slots[world] || !bt->slots[world]->live)
+        return bfail(bt, VXP_ERR_ARG, "no such world");
+    if (!device_memory) BK(cudaStreamSynchronize(bt->stream));
+    if (int rc = bt->cols.sync(bt->stream, bt->err)) return rc;
+    return export_world(*bt->slots[world], bt->cols.set(), dst, first, n, device_memory, consumer_stream, bt->stream,
+                        bt->device, bt->err);
 }
 
 int vxp_batch_world_stats(vxp_batch* bt, uint32_t world, vxp_stats* s) {

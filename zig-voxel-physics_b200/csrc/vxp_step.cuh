@@ -2371,10 +2371,14 @@ __device__ __forceinline__ BV load_bv(const WorldDev& w, uint32_t i) {
     return r;
 }
 __device__ __forceinline__ F3 point_vel(const BV& b, F3 wp) { return b.v + cross3(b.w, wp - b.p); }
+// A body the solver does not write keeps its velocities: selects, not a
+// branch, so the compiler can interleave both bodies' updates (the sweeps'
+// latency chain; 0.97 -> 0.94 ms for the cluster kernel on the pile).
 __device__ __forceinline__ void apply_impulse(BV& b, F3 imp, F3 r) {  // BodyState.applyImpulseAtPoint
-    if (!b.wr) return;
-    b.v = b.v + imp * b.im;
-    b.w = b.w + mat3_mul_vec(b.I, cross3(r, imp));
+    const F3 v2 = b.v + imp * b.im;
+    const F3 w2 = b.w + mat3_mul_vec(b.I, cross3(r, imp));
+    b.v = F3{b.wr ? v2.x : b.v.x, b.wr ? v2.y : b.v.y, b.wr ? v2.z : b.v.z};
+    b.w = F3{b.wr ? w2.x : b.w.x, b.wr ? w2.y : b.w.y, b.wr ? w2.z : b.w.z};
 }
 __device__ __forceinline__ void store_bv(WorldDev& w, uint32_t i, const BV& b) {
     if (!b.wr) return;

@@ -131,6 +131,27 @@ class VoxelPhysicsSystem:
         self._check(self.lib.vxp_bodies_get(self.ctx, abi.ptr(out), self.n_bodies))
         return out
 
+    def export_state(self, fields=None, first: int = 0, n: int | None = None) -> dict:
+        """Bulk state for a renderer (vxp_bodies_export into host arrays):
+        {field: array of shape (n, k)} for the fields asked (default all of
+        position, rotation, linear_velocity, angular_velocity, aabb_min,
+        aabb_max, sleeping), bodies [first, first + n) in set_bodies order."""
+        n = self.n_bodies - first if n is None else n
+        out, view = _export_arrays(fields, n)
+        self._check(self.lib.vxp_bodies_export(self.ctx, ctypes.byref(view), int(first), int(n), 0, None))
+        return out
+
+    def export_state_to_device(self, pointers: dict, first: int = 0, n: int | None = None,
+                               consumer_stream: int = 0) -> None:
+        """vxp_bodies_export into caller-owned device memory: pointers maps
+        field names to device addresses (ints) of arrays laid out as in
+        export_state.  Returns without waiting; consumer_stream (a
+        cudaStream_t as an int, 0 for none) waits for the export."""
+        n = self.n_bodies - first if n is None else n
+        view = _device_view(pointers)
+        self._check(self.lib.vxp_bodies_export(self.ctx, ctypes.byref(view), int(first), int(n), 1,
+                                               ctypes.c_void_p(consumer_stream or None)))
+
     def load_scene(self, scene) -> None:
         for c in scene.colliders:
             self.add_collider(c.id, c.voxel_size, c.bricks)
@@ -360,6 +381,14 @@ class VoxelWorldBatch:
         self._check(self.lib.vxp_batch_world_get(self.b, int(world), abi.ptr(out), len(out)))
         return out
 
+    def export_world(self, world: int, fields=None, first: int = 0, n: int | None = None) -> dict:
+        """export_state for one world of the batch (vxp_batch_world_export)."""
+        n = self.sizes[int(world)] - first if n is None else n
+        out, view = _export_arrays(fields, n)
+        self._check(self.lib.vxp_batch_world_export(self.b, int(world), ctypes.byref(view), int(first), int(n), 0,
+                                                    None))
+        return out
+
     def world_stats(self, world: int) -> dict:
         s = abi.Stats()
         self._check(self.lib.vxp_batch_world_stats(self.b, int(world), ctypes.byref(s)))
@@ -389,3 +418,24 @@ class VoxelWorldBatch:
         self._check(self.lib.vxp_batch_autotune(self.b, np.float32(dt), int(trial_steps), abi.ptr(ms),
                                                 ctypes.byref(choice)))
         return int(choice.value), ms
+
+
+def _export_arrays(fields, n: int):
+    """Host arrays for an export of n bodies and the state view over them."""
+    names = list(abi.EXPORT_FIELDS) if fields is None else list(fields)
+    out, view = {}, abi.StateView()
+    for name in names:
+        k, dt = abi.EXPORT_FIELDS[name]
+        a = np.zeros((n, k) if k > 1 else n, dtype=dt)
+        out[name] = a
+        setattr(view, name, a.ctypes.data if a.size else None)
+    return out, view
+
+
+def _device_view(pointers: dict):
+    view = abi.StateView()
+    for name, addr in pointers.items():
+        if name not in abi.EXPORT_FIELDS:
+            raise KeyError(f"unknown export field {name!r}")
+        setattr(view, name, int(addr) or None)
+    return view
