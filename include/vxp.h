@@ -152,6 +152,8 @@ typedef struct {
     uint32_t reference_caps;     /* 1: keep the reference's 512-pair cap
                                     (src/system.zig:594,612); 0: uncapped   */
     uint32_t colouring;          /* VXP_COLOUR_*                           */
+    uint32_t enable_islands;     /* PhysicsConfig.enable_islands: IslandManager
+                                    statistics each solve (system.zig:705-760) */
     /* capacities (device buffers are sized from these; 0 = grow on demand) */
     uint32_t max_bodies;
     uint32_t max_pairs;
@@ -186,6 +188,13 @@ typedef struct {
                                         row in shared memory, 2 the rows that did
                                         not fit in global memory, 3 all state in
                                         L2; 0 no cluster sweep this step      */
+    /* PhysicsStats island fields (src/system.zig:119-122), from the
+     * IslandManager after this step's build and sleep update; 0 when islands
+     * are off or the step was skipped */
+    uint32_t island_count;
+    uint32_t active_islands;
+    uint32_t sleeping_islands;
+    uint32_t largest_island_size;
 } vxp_stats;
 
 /* One candidate voxel pair of the narrow phase, for parity checks of the
@@ -453,7 +462,8 @@ int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]);
 
 /* Diagnostics: ns from the start of the last step kernel to the end of each
  * of its phases: [start, begin, pairs, cache, probe, finalize, constraints,
- * solve, end]. */
+ * solve, end, islands] (islands: the IslandManager pass that opens the
+ * constraint phase). */
 int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n);
 
 /* ---------------------------------------------------------------------------

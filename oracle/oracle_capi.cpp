@@ -84,6 +84,7 @@ WorldConfig toWorldCfg(const vxp_config* c) {
     w.cache_size = c->brick_pair_cache_size ? c->brick_pair_cache_size : 1024;
     w.reference_caps = c->reference_caps != 0;
     w.colouring = c->colouring;
+    w.enable_islands = c->enable_islands != 0;
     return w;
 }
 template <class R> SolverConfig<R> toSolverCfg(const vxp_config* c) {
@@ -264,6 +265,7 @@ int vxo_bodies_set(void* p, const vxp_body* b, uint32_t n) {
             h->body_collider_id[i] = b[i].collider_id;
         }
         h->w.reindex();
+        h->w.islands.markDirty();  // the bodies were replaced: rebuild at the next solve
     });
     return 0;
 }
@@ -337,6 +339,10 @@ int vxo_stats_get(void* p, vxp_stats* s) {
         s->step_skipped = t.step_skipped;
         s->max_penetration = t.max_penetration;
         s->candidates = t.candidates;
+        s->island_count = t.island_count;
+        s->active_islands = t.active_islands;
+        s->sleeping_islands = t.sleeping_islands;
+        s->largest_island_size = t.largest_island_size;
     });
     return 0;
 }
@@ -385,6 +391,31 @@ int vxo_candidates_get(void* p, vxp_candidate* out, uint32_t cap, uint32_t* n_ou
         }
         *n_out = (uint32_t)c.size();
     });
+    return 0;
+}
+
+// IslandManager.buildIslands / buildIslandsWithBodyTypes over n manifolds
+// given as (body_a, body_b) pairs (the reference's own island tests,
+// islands.zig:785-816 and 857-888).  types: BodyType per body id (ntypes of
+// them), or null for buildIslands.  island_of[id] (n_ids entries): the
+// island index of body id, -1 for a body in no island.
+int vxo_islands_kat(const vxp_pair* ms, uint32_t n, uint32_t body_count, const uint32_t* types, uint32_t ntypes,
+                    int32_t* island_of, uint32_t n_ids, uint32_t* total_islands, uint32_t* largest) {
+    IslandManager<float> m(body_count);
+    std::vector<Manifold<float>> v(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        v[i].a = ms[i].body_a;
+        v[i].b = ms[i].body_b;
+    }
+    std::vector<uint32_t> t;
+    if (types) t.assign(types, types + ntypes);
+    m.build(v, body_count, t);
+    for (uint32_t id = 0; id < n_ids; ++id) {
+        auto it = m.body_to_island.find(id);
+        island_of[id] = it == m.body_to_island.end() ? -1 : (int32_t)it->second;
+    }
+    *total_islands = (uint32_t)m.total_islands;
+    *largest = (uint32_t)m.largest_island_size;
     return 0;
 }
 

@@ -1521,6 +1521,192 @@ inline std::vector<uint8_t> graphColouring(const std::vector<Manifold<R>>& ms, u
 }
 
 // ---------------------------------------------------------------------------
+// islands.zig: UnionFind (25-137) and IslandManager (194-495), as
+// system.solve drives it (system.zig:705-760).  Only its statistics leave it:
+// updateSleepStates reads copies of the bodies and writes none of them.
+// ---------------------------------------------------------------------------
+struct UnionFind {  // islands.zig:25-137
+    std::vector<uint32_t> parent, rank;
+    size_t count = 0, set_count = 0;
+    explicit UnionFind(size_t n = 0) { resize(n); }
+    void reset() {
+        for (size_t i = 0; i < count; ++i) {
+            parent[i] = (uint32_t)i;
+            rank[i] = 0;
+        }
+        set_count = count;
+    }
+    void resize(size_t n) {
+        if (n > parent.size()) {
+            parent.resize(n);
+            rank.resize(n);
+        }
+        count = n;
+        reset();
+    }
+    uint32_t find(uint32_t x) {  // with path compression
+        if (x >= count) return x;
+        uint32_t root = x;
+        while (parent[root] != root) root = parent[root];
+        uint32_t cur = x;
+        while (cur != root) {
+            const uint32_t next = parent[cur];
+            parent[cur] = root;
+            cur = next;
+        }
+        return root;
+    }
+    void unite(uint32_t x, uint32_t y) {  // union by rank
+        const uint32_t rx = find(x), ry = find(y);
+        if (rx == ry) return;
+        if (rank[rx] < rank[ry]) {
+            parent[rx] = ry;
+        } else if (rank[rx] > rank[ry]) {
+            parent[ry] = rx;
+        } else {
+            parent[ry] = rx;
+            rank[rx] += 1;
+        }
+        set_count -= 1;
+    }
+    bool connected(uint32_t x, uint32_t y) { return find(x) == find(y); }
+};
+
+template <class R> struct IslandManager {
+    struct Island {
+        std::vector<uint32_t> bodies, manifolds;
+        uint32_t id = 0;
+        bool is_sleeping = false;
+        R sleep_timer = 0;
+        bool needs_solving = true;
+    };
+    UnionFind uf;
+    std::vector<Island> islands;
+    std::unordered_map<uint32_t, uint32_t> body_to_island;
+    uint64_t previous_graph_hash = 0;
+    bool needs_rebuild = true;
+    uint32_t rebuilds_skipped = 0, rebuilds_performed = 0;
+    size_t total_islands = 0, active_islands = 0, sleeping_islands = 0, largest_island_size = 0, total_bodies = 0,
+           total_contacts = 0;
+
+    explicit IslandManager(size_t max_bodies = 1024) : uf(max_bodies) {}
+
+    // computeGraphHash (islands.zig:277-296): every manifold is active
+    static uint64_t graphHash(const std::vector<Manifold<R>>& ms) {
+        uint64_t hash = 0;
+        const uint64_t prime = 0x100000001b3ull;
+        for (const auto& m : ms) {
+            const uint32_t a = std::min(m.a, m.b), b = std::max(m.a, m.b);
+            hash ^= ((uint64_t)a << 32) | (uint64_t)b;
+            hash *= prime;
+        }
+        hash ^= (uint64_t)ms.size();
+        hash *= prime;
+        return hash;
+    }
+    void markDirty() { needs_rebuild = true; }  // islands.zig:299-302
+
+    // buildIslandsWithBodyTypes (islands.zig:318-423); types[id] for ids
+    // below types.size(), as the reference's body_types slice
+    void build(const std::vector<Manifold<R>>& ms, size_t body_count, const std::vector<uint32_t>& types) {
+        const uint64_t h = graphHash(ms);
+        if (!needs_rebuild && h == previous_graph_hash && total_islands > 0) {
+            ++rebuilds_skipped;
+            return;
+        }
+        previous_graph_hash = h;
+        needs_rebuild = false;
+        ++rebuilds_performed;
+        for (auto& isl : islands) isl = Island{};
+        body_to_island.clear();
+        total_islands = active_islands = sleeping_islands = largest_island_size = total_bodies = total_contacts = 0;
+        if (ms.empty()) return;
+        // the body ids the manifolds name; the reference walks a hash set, so
+        // its island numbering follows hash order: no statistic depends on it
+        std::vector<uint32_t> body_ids;
+        for (const auto& m : ms) {
+            body_ids.push_back(m.a);
+            body_ids.push_back(m.b);
+        }
+        std::sort(body_ids.begin(), body_ids.end());
+        body_ids.erase(std::unique(body_ids.begin(), body_ids.end()), body_ids.end());
+        const uint32_t max_id = body_ids.back();
+        const size_t required = std::max(body_count, (size_t)max_id + 1);
+        if (required > uf.count) uf.resize(required);
+        else uf.reset();
+        for (const auto& m : ms) {
+            const bool as = m.a < types.size() && types[m.a] == B_STATIC;
+            const bool bs = m.b < types.size() && types[m.b] == B_STATIC;
+            if (as || bs) continue;
+            uf.unite(m.a, m.b);
+        }
+        total_contacts = ms.size();
+        std::unordered_map<uint32_t, uint32_t> root_to_island;
+        uint32_t count = 0;
+        for (uint32_t id : body_ids) {
+            const uint32_t root = uf.find(id);
+            if (!root_to_island.count(root)) {
+                root_to_island[root] = count;
+                while (islands.size() <= count) islands.emplace_back();
+                islands[count].id = root;
+                ++count;
+            }
+            const uint32_t idx = root_to_island[root];
+            body_to_island[id] = idx;
+            auto& bl = islands[idx].bodies;
+            if (std::find(bl.begin(), bl.end(), id) == bl.end()) bl.push_back(id);
+        }
+        for (uint32_t mi = 0; mi < ms.size(); ++mi) {
+            auto it = root_to_island.find(uf.find(ms[mi].a));
+            if (it != root_to_island.end()) islands[it->second].manifolds.push_back(mi);
+        }
+        total_islands = count;
+        for (uint32_t k = 0; k < count; ++k) {
+            const size_t size = islands[k].bodies.size();
+            total_bodies += size;
+            largest_island_size = std::max(largest_island_size, size);
+            if (islands[k].is_sleeping) ++sleeping_islands;
+            else ++active_islands;
+        }
+    }
+
+    // updateSleepStates (islands.zig:426-472).  bodies: the body table, read
+    // at index body id, as the reference reads its copies (islands.zig:437-440).
+    void updateSleepStates(const std::vector<Body<R>>& bodies, R dt) {
+        const R thr = (R)(0.1f * 0.1f);  // ISLAND_SLEEP_{LINEAR,ANGULAR}_THRESHOLD squared, in f32
+        for (auto& isl : islands) {
+            if (isl.bodies.empty()) continue;
+            bool all_still = true;
+            for (uint32_t id : isl.bodies) {
+                if (id >= bodies.size()) continue;
+                const Body<R>& b = bodies[id];
+                if (b.type != B_DYNAMIC) continue;
+                if (dot(b.v, b.v) > thr || dot(b.w, b.w) > thr) {
+                    all_still = false;
+                    break;
+                }
+            }
+            if (all_still) {
+                isl.sleep_timer += dt;
+                if (isl.sleep_timer >= (R)0.5f) {  // ISLAND_SLEEP_TIME_THRESHOLD
+                    isl.is_sleeping = true;
+                    isl.needs_solving = false;
+                }
+            } else {
+                isl.sleep_timer = 0;
+                isl.is_sleeping = false;
+                isl.needs_solving = true;
+            }
+        }
+        sleeping_islands = active_islands = 0;
+        for (size_t k = 0; k < total_islands; ++k) {
+            if (islands[k].is_sleeping) ++sleeping_islands;
+            else ++active_islands;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
 // system.zig: step / narrowPhase / solve / updateSleepStates
 // ---------------------------------------------------------------------------
 struct Stats {
@@ -1530,6 +1716,8 @@ struct Stats {
              position_iterations_run = 0, step_skipped = 0;
     float max_penetration = 0;
     uint32_t candidates = 0;
+    // PhysicsStats island fields (system.zig:119-122)
+    uint32_t island_count = 0, active_islands = 0, sleeping_islands = 0, largest_island_size = 0;
 };
 
 struct WorldConfig {
@@ -1540,6 +1728,7 @@ struct WorldConfig {
     uint32_t cache_size = 1024;
     bool reference_caps = false;
     uint32_t colouring = COLOUR_PROJECT;
+    bool enable_islands = true;
 };
 
 template <class R> struct World {
@@ -1552,6 +1741,7 @@ template <class R> struct World {
     BrickPairCache<R> cache;
     ContactSolver<R> solver;
     Stats stats;
+    IslandManager<R> islands;
     bool dump = false;
     std::vector<CandRec> candidates;
     std::vector<uint32_t> last_colours;  // per constraint in addManifold order
@@ -1713,6 +1903,18 @@ template <class R> struct World {
             if (wcfg.colouring == COLOUR_REFERENCE) ref_colour_of_cons.push_back(ref_colours[mi]);
         }
         stats.constraints = (uint32_t)solver.cons.size();
+        if (wcfg.enable_islands) {  // system.zig:705-760
+            uint32_t max_id = 0;
+            for (const auto& b : bodies) max_id = std::max(max_id, b.id);
+            std::vector<uint32_t> types((size_t)max_id + 1, B_STATIC);
+            for (const auto& b : bodies) types[b.id] = b.type;
+            islands.build(cm.cur, bodies.size(), types);
+            islands.updateSleepStates(bodies, dt);
+            stats.island_count = (uint32_t)islands.total_islands;
+            stats.active_islands = (uint32_t)islands.active_islands;
+            stats.sleeping_islands = (uint32_t)islands.sleeping_islands;
+            stats.largest_island_size = (uint32_t)islands.largest_island_size;
+        }
         uint32_t pts = 0;
         for (auto& c : solver.cons) pts += c.n;
         stats.contact_points = pts;

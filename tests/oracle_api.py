@@ -49,6 +49,7 @@ for name, res, args in [
     ("vxo_candidates_get", _I, [_VP, _VP, _U32, _PU32]),
     ("vxo_pairs_find", _I, [_VP, _F, _VP, _U32, _PU32]),
     ("vxo_world_aabbs", _I, [_VP, _VP, _VP, _U32]),
+    ("vxo_islands_kat", _I, [_VP, _U32, _U32, _VP, _U32, _VP, _U32, _PU32, _PU32]),
     ("vxo_narrow_phase_threaded", _I, [_VP, _VP, _U32, _I]),
     ("vxo_step_threaded", _I, [_VP, _F, _VP, _U32, _I]),
     ("vxo_mass_properties", _I, [_F, _VP, _U32, _F, ctypes.POINTER(_F), _VP]),
@@ -106,6 +107,19 @@ def mass_fn(vs, bricks, density):
                                abi.ptr(inv))
     assert rc == 0
     return np.float32(im.value), inv
+
+
+def islands_kat(manifolds, body_count, types=None, n_ids=None):
+    """The oracle's IslandManager over (a, b) manifolds: (island index per body
+    id or -1, total islands, largest island size)."""
+    ms = np.ascontiguousarray(np.array(manifolds, dtype=np.uint32).reshape(-1, 2)).view(abi.PAIR_DTYPE).reshape(-1)
+    n_ids = body_count if n_ids is None else n_ids
+    out = np.zeros(n_ids, dtype=np.int32)
+    tot, lg = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    t = None if types is None else np.ascontiguousarray(types, dtype=np.uint32)
+    assert L.vxo_islands_kat(abi.ptr(ms), len(ms), int(body_count), abi.ptr(t) if t is not None else None,
+                             0 if t is None else len(t), abi.ptr(out), n_ids, ctypes.byref(tot), ctypes.byref(lg)) == 0
+    return out, tot.value, lg.value
 
 
 class OracleWorld:

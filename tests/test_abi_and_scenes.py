@@ -35,8 +35,8 @@ def test_struct_sizes(vxp):
     assert a.BRICK_DTYPE.itemsize == 524
     assert a.MANIFOLD_DTYPE.itemsize == 376
     assert a.CONTACT_DTYPE.itemsize == 88
-    assert ctypes.sizeof(a.Config) == 4 * 26
-    assert ctypes.sizeof(a.Stats) == 4 * 20
+    assert ctypes.sizeof(a.Config) == 4 * 27
+    assert ctypes.sizeof(a.Stats) == 4 * 24
 
 
 def test_classification_matches_reference(vxp):

@@ -6,9 +6,8 @@ sequential CPU oracle (the reference's own order of work).
   those bodies and step 5 steps together: bodies, every manifold and the
   narrow-phase / solver counters compared after each.
 * The narrow-phase stress scene at full size (config 4: 512 bodies of 64^3
-  voxels, 10 % overlap): 2 steps from the start, where every probe runs the
-  27-lookup path (the colliders exceed the probe-table pool) over ~2.6e8
-  voxel probes a step.
+  voxels, 10 % overlap): 2 steps from the start, ~2.6e8 voxel probes a step,
+  with the neighbourhood-mask tables and with the 27-lookup path.
 * The 256-world batch (config 3): all 256 worlds in one batch for the
   configuration's 300 steps; the three largest worlds (>= 1024 bodies each,
   9 columns of boxes whose lower layers have landed by then) equal the oracle
@@ -69,20 +68,30 @@ def test_full_pile_from_the_benchmarked_state(vxp):
 
 
 def test_stress_scene_full_size(vxp):
+    """Both probe paths at full size: one context builds the neighbourhood-mask
+    tables (2.4 GB for the 512 colliders), the other probes with 27 voxel
+    lookups per centre; each equals the oracle."""
     sc = vxp.scenes.config4(mass_fn=O.mass_fn)
     cfg = dict(substeps=4, reference_caps=0)
     dt = np.float32(sc.dt)
-    g = vxp.VoxelPhysicsSystem(**cfg)
-    g.load_scene(sc)
+    gs = []
+    for tables in (True, False):
+        g = vxp.VoxelPhysicsSystem(**cfg)
+        g.set_probe_tables(tables)
+        g.load_scene(sc)
+        gs.append(g)
     r = O.OracleWorld(**cfg)
     r.load_scene(sc)
     probes = []
     for s in range(2):
         pairs = r.pairs()
-        g.step(dt, pairs)
+        for g in gs:
+            g.step(dt, pairs)
         r.step(dt, pairs)
-        probes.append(_compare(g, r, s)["voxels_checked"])
-    g.close()
+        for g in gs:
+            probes.append(_compare(g, r, s)["voxels_checked"])
+    for g in gs:
+        g.close()
     r.close()
     assert min(probes) > 10 ** 8, probes
 

@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 
 STAT_KEYS = ("pairs_tested", "pairs_colliding", "voxels_checked", "contacts_generated", "pairs_skipped_sleeping",
              "cache_hits", "cache_misses", "cache_evictions", "manifolds", "constraints", "contact_points", "colours",
-             "position_iterations_run", "step_skipped", "max_penetration", "candidates")
+             "position_iterations_run", "step_skipped", "max_penetration", "candidates", "island_count",
+             "active_islands", "sleeping_islands", "largest_island_size")
 
 
 def _first_diff(g, r):
@@ -72,6 +73,18 @@ def lockstep(vxp, scene, steps, mode=-1, own_pairs=False, check_every=1, solver=
     # a run of 20 steps or more must have compared some contacts, not only free fall
     assert steps < 20 or touching >= 5, f"only {touching} of {steps} steps had a manifold"
     return g
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_islands_sleep_like_the_oracle(vxp, mode):
+    """IslandManager statistics (system.zig:705-760) on the reference's
+    example scene: islands appear when the box lands and one sleeps once the
+    contact graph has not changed for 0.5 s; the lockstep compares every
+    statistic each step, in block and grid launch."""
+    sc = vxp.scenes.basic_example(O.mass_fn)
+    g = lockstep(vxp, sc, 78, mode=mode)  # the body itself sleeps after step 78: later steps are skipped
+    assert g.stats()["sleeping_islands"] >= 1
+    g.close()
 
 
 @pytest.mark.parametrize("mode", [0, 1])

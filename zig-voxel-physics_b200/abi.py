@@ -128,6 +128,7 @@ class Config(ctypes.Structure):
         ("brick_pair_cache_size", ctypes.c_uint32),
         ("reference_caps", ctypes.c_uint32),
         ("colouring", ctypes.c_uint32),
+        ("enable_islands", ctypes.c_uint32),
         ("max_bodies", ctypes.c_uint32),
         ("max_pairs", ctypes.c_uint32),
     ]
@@ -157,6 +158,10 @@ class Stats(ctypes.Structure):
         ("candidates", ctypes.c_uint32),
         ("bricks_touched", ctypes.c_uint32),
         ("sweep_path", ctypes.c_uint32),
+        ("island_count", ctypes.c_uint32),
+        ("active_islands", ctypes.c_uint32),
+        ("sleeping_islands", ctypes.c_uint32),
+        ("largest_island_size", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -210,6 +215,7 @@ def default_config(**overrides) -> Config:
     c.brick_pair_cache_size = 1024
     c.reference_caps = 0
     c.colouring = COLOUR_PROJECT
+    c.enable_islands = 1
     c.max_bodies = 0
     c.max_pairs = 0
     for k, v in overrides.items():

@@ -422,8 +422,9 @@ struct ColliderStore {
     bool dirty = false;    // colliders wait for placement
     bool replace = false;  // every collider is placed again (tables switched)
     // neighbourhood-mask tables: colliders with at most kNbMaxCentres probe
-    // centres get one, while the pool stays within kNbMaxTotal entries
-    static constexpr uint64_t kNbMaxCentres = 1ull << 23, kNbMaxTotal = 1ull << 25;
+    // centres get one, while the pool stays within kNbMaxTotal entries (16 B
+    // each: 4 GiB at most, e.g. 2.4 GB for 512 colliders of 64^3 voxels)
+    static constexpr uint64_t kNbMaxCentres = 1ull << 23, kNbMaxTotal = 1ull << 28;
     static constexpr size_t kMaxGridCells = (size_t)1 << 28;
     bool tables = true;  // build neighbourhood-mask tables at all
     // pinned staging of edit lists, two in turn, each free again once the
@@ -947,6 +948,7 @@ StepCfg step_cfg(const vxp_config& c, float dt, uint32_t dump, uint32_t phases) 
     s.heavy_voxels = 1024;  // batches of small worlds: one CTA per world
     s.count_bricks = 0;
     s.owner_groups = 1;
+    s.islands_on = c.enable_islands;
     return s;
 }
 
@@ -977,6 +979,10 @@ struct WorldBuffers {
     DBuf<uint32_t> cons, colour, pos_of, packed_pair, adj, flag;
     DBuf<CacheLook> clist;
     DBuf<float> cp, crow;
+    // islands: per body, per pair slot (two builds' keys), kept state words
+    DBuf<uint32_t> isl_parent, isl_flag, isl_size, isl_state;
+    DBuf<float> isl_timer;
+    DBuf<unsigned long long> isl_keys0, isl_keys1;
     DBuf<uint4> cm, rk;
     DBuf<float2> cfr;
     DBuf<uint32_t> ev;
@@ -1007,6 +1013,8 @@ struct WorldBuffers {
         ok &= cval.reserve(cache) == cudaSuccess;
         ok &= cwriter.reserve(cache) == cudaSuccess;
         ok &= cframe.reserve(1) == cudaSuccess;
+        ok &= isl_state.reserve(IS_N) == cudaSuccess;
+        if (ok) mark_islands_dirty();
         if (!ok) {
             err = "world buffers: device allocation failed";
             return VXP_ERR_OOM;
@@ -1036,6 +1044,8 @@ struct WorldBuffers {
         ok &= clist.reserve(cap) == cudaSuccess;
         ok &= cp.reserve((size_t)CP_NFIELDS * 4 * cap) == cudaSuccess;
         if (spill_rows) ok &= crow.reserve((size_t)CP_NVEL * 4 * cap) == cudaSuccess;
+        ok &= isl_keys0.reserve(cap, true) == cudaSuccess;
+        ok &= isl_keys1.reserve(cap, true) == cudaSuccess;
         ok &= cm.reserve(cap) == cudaSuccess;
         ok &= rk.reserve(cap) == cudaSuccess;
         ok &= chunk.reserve((size_t)cap / 32 + 257) == cudaSuccess;
@@ -1102,6 +1112,10 @@ struct WorldBuffers {
         }
         ok &= ev.reserve(cap) == cudaSuccess;
         ok &= snap.reserve((size_t)cap * 2) == cudaSuccess;
+        ok &= isl_parent.reserve(cap) == cudaSuccess;
+        ok &= isl_flag.reserve(cap) == cudaSuccess;
+        ok &= isl_size.reserve(cap) == cudaSuccess;
+        ok &= isl_timer.reserve(cap) == cudaSuccess;
         if (!ok) {
             err = fmt("body buffers: device allocation of %u bodies failed", cap);
             return VXP_ERR_OOM;
@@ -1170,6 +1184,7 @@ struct WorldBuffers {
         }
         n_static = (uint32_t)st.size();
         n_bodies = n;
+        mark_islands_dirty();  // the island roots are body indices
         return VXP_OK;
     }
 
@@ -1266,6 +1281,13 @@ struct WorldBuffers {
         w.bmask = bmask.p;
         w.cp = cp.p;
         w.crow = crow.p;
+        w.isl_parent = isl_parent.p;
+        w.isl_flag = isl_flag.p;
+        w.isl_size = isl_size.p;
+        w.isl_timer = isl_timer.p;
+        w.isl_keys[0] = isl_keys0.p;
+        w.isl_keys[1] = isl_keys1.p;
+        w.isl_state = isl_state.p;
         w.cm = cm.p;
         w.rk = rk.p;
         w.ev = ev.p;
@@ -1303,7 +1325,16 @@ struct WorldBuffers {
                clist.bytes() + cp.bytes() + cm.bytes() + rk.bytes() + ev.bytes() + snap.bytes() + chunk.bytes() + cfr.bytes() +
                ckey.bytes() + cval.bytes() +
                cwriter.bytes() + scan.bytes() + ctr.bytes() + ts.bytes() + dump.bytes() + ocnt.bytes() + ocur.bytes() +
-               stat.bytes() + bpmask.bytes();
+               stat.bytes() + bpmask.bytes() + crow.bytes() + isl_parent.bytes() + isl_flag.bytes() +
+               isl_size.bytes() + isl_timer.bytes() + isl_keys0.bytes() + isl_keys1.bytes() + isl_state.bytes() +
+               export_stage.bytes();
+    }
+
+    // The next solve rebuilds its islands (IslandManager.markDirty,
+    // islands.zig:301-303): at creation and whenever the bodies are replaced.
+    void mark_islands_dirty() {
+        const uint32_t st[IS_N] = {1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        cudaMemcpy(isl_state.p, st, sizeof(st), cudaMemcpyHostToDevice);
     }
 
     // Counters -> vxp_stats.
@@ -1337,6 +1368,10 @@ struct WorldBuffers {
         s->candidates = c[C_CANDIDATES];
         s->bricks_touched = c[C_BRICKS];
         s->sweep_path = c[C_SWEEP];
+        s->island_count = c[C_ISLANDS];
+        s->sleeping_islands = c[C_ISL_SLEEPING];
+        s->active_islands = c[C_ISLANDS] - c[C_ISL_SLEEPING];
+        s->largest_island_size = c[C_ISL_LARGEST];
         return VXP_OK;
     }
 
@@ -1742,6 +1777,7 @@ void vxp_config_default(vxp_config* c) {
     c->brick_pair_cache_size = 1024;
     c->reference_caps = 0;
     c->colouring = VXP_COLOUR_PROJECT;
+    c->enable_islands = 1;
     c->max_bodies = 0;
     c->max_pairs = 0;
 }

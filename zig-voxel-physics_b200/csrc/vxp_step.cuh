@@ -1978,8 +1978,173 @@ __device__ __forceinline__ size_t cpi(const WorldDev& w, uint32_t field, uint32_
     return ((size_t)(field * 4u + slot)) * w.pair_cap + pos;
 }
 
+// ---------------------------------------------------------------------------
+// Phase: islands (IslandManager.buildIslandsWithBodyTypes + updateSleepStates,
+// islands.zig:318-495, run by system.solve before the solver, system.zig:705-760)
+// ---------------------------------------------------------------------------
+// The reference keeps only statistics from it (updateSleepStates reads copies
+// of the bodies): islands, active and sleeping islands, the largest island.
+// Islands are rebuilt when the frame's contact graph differs from the last
+// build's.  The reference compares a 64-bit fold of the manifolds' pair keys
+// in iteration order (computeGraphHash, islands.zig:277-296); here the key
+// sequences themselves are compared, which differs only where two different
+// sequences fold to the same hash.
+// Build: union-find over the manifolds whose bodies are both non-static.  It
+// is lock-free: a root is linked under the smaller root by CAS, so parents
+// only point to smaller indices and an island's root is its smallest body
+// index.  Every body a manifold names is in one island (a static body alone).
+// Sleep: an island whose bodies are all still (|v|^2 and |w|^2 at most 0.1^2)
+// for 0.5 s sleeps; for island body id k the k-th body of the table is read,
+// as the reference indexes its body copies by id (islands.zig:437-440).
+
+// The root of body i, halving the path on the way: each visited body is
+// pointed at its grandparent, an ancestor in the same tree, so the trees stay
+// valid while other threads link roots (a body that is no root never becomes
+// one again, and only roots are linked).  Parents point to smaller indices,
+// so the walk ends within i + 1 links.
+__device__ __forceinline__ uint32_t isl_root(uint32_t* parent, uint32_t i) {
+    uint32_t x = i;
+    for (uint32_t k = 0; k <= i; ++k) {
+        const uint32_t p = *(volatile uint32_t*)&parent[x];
+        if (p == x) break;
+        const uint32_t gp = *(volatile uint32_t*)&parent[p];
+        if (gp != p) *(volatile uint32_t*)&parent[x] = gp;
+        x = gp;
+    }
+    return x;
+}
+// UnionFind.unite: link the larger root under the smaller.  A failed CAS
+// means another thread linked that root meanwhile; every link removes a
+// root, so the retries are bounded by the body count.
+__device__ __forceinline__ bool isl_unite(uint32_t* parent, uint32_t a, uint32_t b, uint32_t n) {
+    for (uint32_t k = 0; k <= n; ++k) {
+        a = isl_root(parent, a);
+        b = isl_root(parent, b);
+        if (a == b) return true;
+        if (a < b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(&parent[a], a, b) == a) return true;
+    }
+    return false;
+}
+
+template <class G>
+__device__ bool phase_islands(G& g, WorldDev& w, uint32_t cur) {
+    if (!w.cfg.islands_on || !w.isl_state) return true;
+    const uint32_t P = w.n_pairs, N = w.n_bodies;
+    uint32_t* st = w.isl_state;
+    const uint32_t buf = *(volatile uint32_t*)&st[IS_BUF] & 1u, nprev = *(volatile uint32_t*)&st[IS_NKEYS];
+    const unsigned long long* kp = w.isl_keys[buf];
+    unsigned long long* kc = w.isl_keys[buf ^ 1u];
+    const ManifoldRec* man = w.man[cur];
+    // 1. the frame's manifold keys in iteration order (pair order), against
+    // the last build's
+    uint32_t nm = 0;
+    if (!group_scan(
+            g, P, [&](uint32_t p) { return man[p].n > 0u ? 1u : 0u; },
+            [&](uint32_t p, uint32_t q) {
+                if (man[p].n == 0u) return;
+                const unsigned long long k = pair_key(man[p].a, man[p].b);
+                kc[q] = k;
+                if (q >= nprev || kp[q] != k) atomicOr(&w.ctr[C_ISL_DIFF], 1u);
+            },
+            w.scan, &nm))
+        return false;
+    const bool rebuild = *(volatile uint32_t*)&st[IS_DIRTY] != 0u || nm != nprev ||
+                         *(volatile uint32_t*)&w.ctr[C_ISL_DIFF] != 0u || *(volatile uint32_t*)&st[IS_TOTAL] == 0u;
+    if (!g.sync()) return false;  // every thread has decided before the state changes
+    if (rebuild) {
+        // 2. singletons, timers cleared (Island.clear)
+        for (uint32_t i = g.rank(); i < N; i += g.size()) {
+            w.isl_parent[i] = i;
+            w.isl_flag[i] = 0u;
+            w.isl_size[i] = 0u;
+            w.isl_timer[i] = 0.0f;
+        }
+        if (g.rank() == 0) {
+            st[IS_DIRTY] = 0u;
+            st[IS_BUF] = buf ^ 1u;
+            st[IS_NKEYS] = nm;
+            st[IS_BUILDS] += 1u;
+            st[IS_TOTAL] = 0u;
+            st[IS_LARGEST] = 0u;
+        }
+        if (!g.sync()) return false;
+        // 3. every body a manifold names; unions over non-static pairs
+        bool ok = true;
+        for (uint32_t p = g.rank(); p < P; p += g.size()) {
+            if (man[p].n == 0u) continue;
+            const uint32_t ia = w.pinfo[p].ia, ib = w.pinfo[p].ib;
+            if (ia >= N || ib >= N) continue;
+            atomicOr(&w.isl_flag[ia], ISL_TOUCHED);
+            atomicOr(&w.isl_flag[ib], ISL_TOUCHED);
+            if (w.prop[ia].type != 0u && w.prop[ib].type != 0u) ok &= isl_unite(w.isl_parent, ia, ib, N);
+        }
+        if (!ok) atomicOr(&w.ctr[C_ERROR], ERR_BOUNDS);
+        if (!g.sync()) return false;
+        // 4. each body's root, island sizes
+        for (uint32_t i = g.rank(); i < N; i += g.size()) {
+            if (!(w.isl_flag[i] & ISL_TOUCHED)) continue;
+            const uint32_t r = isl_root(w.isl_parent, i);
+            w.isl_parent[i] = r;
+            atomicAdd(&w.isl_size[r], 1u);
+        }
+        if (!g.sync()) return false;
+        // 5. the island count and the largest island
+        uint32_t cnt = 0;
+        for (uint32_t i = g.rank(); i < N; i += g.size()) {
+            if ((w.isl_flag[i] & ISL_TOUCHED) && w.isl_parent[i] == i) {
+                ++cnt;
+                atomicMax(&st[IS_LARGEST], w.isl_size[i]);
+            }
+        }
+        cnt = warp_sum(cnt);
+        if ((threadIdx.x & 31u) == 0u && cnt) atomicAdd(&st[IS_TOTAL], cnt);
+    } else if (g.rank() == 0) {
+        st[IS_SKIPS] += 1u;
+    }
+    // 6. updateSleepStates: is every body of each island still?
+    const float thr = 0.1f * 0.1f;  // ISLAND_SLEEP_{LINEAR,ANGULAR}_THRESHOLD squared
+    for (uint32_t i = g.rank(); i < N; i += g.size()) {
+        if (!(w.isl_flag[i] & ISL_TOUCHED)) continue;
+        const uint32_t j = w.prop[i].id;
+        if (j >= N || w.prop[j].type != 2u) continue;
+        const DBody& b = w.body[j];
+        if (lensq3(f3of(b.v)) > thr || lensq3(f3of(b.w)) > thr) atomicOr(&w.isl_flag[w.isl_parent[i]], ISL_MOVING);
+    }
+    if (!g.sync()) return false;
+    // 7. per island: its timer and sleep flag
+    uint32_t asleep = 0;
+    for (uint32_t i = g.rank(); i < N; i += g.size()) {
+        uint32_t f = w.isl_flag[i];
+        if (!(f & ISL_TOUCHED) || w.isl_parent[i] != i) continue;
+        if (!(f & ISL_MOVING)) {
+            const float t = w.isl_timer[i] + w.cfg.dt;
+            w.isl_timer[i] = t;
+            if (t >= 0.5f) f |= ISL_ASLEEP;  // ISLAND_SLEEP_TIME_THRESHOLD
+        } else {
+            w.isl_timer[i] = 0.0f;
+            f &= ~ISL_ASLEEP;
+        }
+        w.isl_flag[i] = f & ~ISL_MOVING;
+        asleep += (f & ISL_ASLEEP) ? 1u : 0u;
+    }
+    asleep = warp_sum(asleep);
+    if ((threadIdx.x & 31u) == 0u && asleep) atomicAdd(&w.ctr[C_ISL_SLEEPING], asleep);
+    if (g.rank() == 0) {
+        w.ctr[C_ISLANDS] = *(volatile uint32_t*)&st[IS_TOTAL];
+        w.ctr[C_ISL_LARGEST] = *(volatile uint32_t*)&st[IS_LARGEST];
+        if (w.ts) w.ts[TS_ISLANDS] = global_ns();
+    }
+    return g.sync();
+}
+
 template <class G>
 __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_out, uint32_t* ncol_out) {
+    if (!phase_islands(g, w, cur)) return false;
     const uint32_t P = w.n_pairs, N = w.n_bodies;
     // 1. solver constraint list: manifolds that are not both-sleeping, pair order
     for (uint32_t p = g.rank(); p < P; p += g.size()) {

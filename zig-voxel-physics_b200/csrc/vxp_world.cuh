@@ -165,6 +165,7 @@ struct StepCfg {
     uint32_t heavy_voxels;      // overlap regions of at least this many voxels are probed by a CTA (0: never)
     uint32_t count_bricks;      // count the bricks each probed pair touches (C_BRICKS; traffic accounting only)
     uint32_t owner_groups;      // > 1: pack each colour by owner group (home body mod this; the sweep cluster's size)
+    uint32_t islands_on;        // IslandManager statistics each solve (PhysicsConfig.enable_islands)
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 
@@ -201,18 +202,26 @@ enum : uint32_t {
     C_CONS_M,        // constraint manifolds of the step (solve part split in two kernels)
     C_CONS_NCOL,     // their colours
     C_SWEEP,         // how the cluster sweeps ran (SWEEP_*)
-    C_ERROR = 31,    // sticky error bits (not cleared per step)
-    C_NCTR = 32
+    C_ISL_DIFF,      // the frame's contact graph differs from the last island build's
+    C_ISLANDS,       // IslandManager stats of this step: islands,
+    C_ISL_SLEEPING,  // sleeping islands,
+    C_ISL_LARGEST,   // bodies in the largest island
+    C_ERROR = 47,    // sticky error bits (not cleared per step)
+    C_NCTR = 48
 };
 // Phase boundaries recorded in WorldDev::ts by rank 0 (diagnostics).
 enum : uint32_t {
-    TS_START, TS_BEGIN, TS_PAIRS, TS_CACHE, TS_PROBE, TS_FINALIZE, TS_CONSTRAINTS, TS_SOLVE, TS_END, TS_N = 16
+    TS_START, TS_BEGIN, TS_PAIRS, TS_CACHE, TS_PROBE, TS_FINALIZE, TS_CONSTRAINTS, TS_SOLVE, TS_END, TS_ISLANDS,
+    TS_N = 16
 };
 // C_SWEEP: the cluster kernel's sweeps with every constraint row in shared
 // memory, with the rows that did not fit in global memory, or with all
 // state in L2 (colour barriers); 0 when no cluster kernel ran.
 enum : uint32_t { SWEEP_SHARED = 1u, SWEEP_SPILL = 2u, SWEEP_L2 = 3u };
-static_assert(C_SWEEP < C_ERROR, "C_SWEEP is cleared with the per-step counters");
+static_assert(C_ISL_LARGEST < C_ERROR, "every counter below C_ERROR is cleared each step");
+// Island flags (WorldDev::isl_flag) and kept state words (WorldDev::isl_state).
+enum : uint32_t { ISL_TOUCHED = 1u, ISL_MOVING = 2u, ISL_ASLEEP = 4u };
+enum : uint32_t { IS_DIRTY, IS_TOTAL, IS_LARGEST, IS_NKEYS, IS_BUF, IS_BUILDS, IS_SKIPS, IS_N = 8 };
 enum : uint32_t { ERR_TIMEOUT = 1u, ERR_CAP = 2u, ERR_COLOURS = 4u, ERR_OVERFLOW = 8u, ERR_BOUNDS = 16u };
 
 // A brick-pair cache lookup of the step: the pair, its key and the start of
@@ -284,6 +293,17 @@ struct WorldDev {
     float* subrec;                // per substep and body: position, rotation, v, w (13 floats)
     // packed constraint data, slot-major [slot][M]; see CP_* field ids
     float* cp;                    // CP_NFIELDS * 4 * pair_cap floats
+    // islands (IslandManager): per body the union-find parent (the island's
+    // root, its smallest body index, after a build), ISL_* flags and, per
+    // root, its size and sleep timer; the pair keys of the manifolds of two
+    // builds (the last one in isl_keys[state[IS_BUF]]); IS_* words kept
+    // across steps
+    uint32_t* isl_parent;
+    uint32_t* isl_flag;
+    uint32_t* isl_size;
+    float* isl_timer;
+    unsigned long long* isl_keys[2];
+    uint32_t* isl_state;
     float* crow;                  // CP_NVEL * 4 * pair_cap floats or null: the cluster sweeps'
                                   // point rows that do not fit in shared memory
     uint4* cm;                    // per packed manifold: ia, ib, n, pair
