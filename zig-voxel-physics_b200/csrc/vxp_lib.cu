@@ -1013,7 +1013,7 @@ struct WorldBuffers {
         ok &= cval.reserve(cache) == cudaSuccess;
         ok &= cwriter.reserve(cache) == cudaSuccess;
         ok &= cframe.reserve(1) == cudaSuccess;
-        ok &= isl_state.reserve(IS_N) == cudaSuccess;
+        ok &= isl_state.reserve(IS_N + (size_t)blocks) == cudaSuccess;  // + the island pass's scan partials
         if (ok) mark_islands_dirty();
         if (!ok) {
             err = "world buffers: device allocation failed";
@@ -1503,7 +1503,7 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
     const ColliderSet cs = ctx->cols.set();
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (grid) {
-        CK(cudaMemsetAsync(ctx->bar.p, 0, 2 * sizeof(GridBar), ctx->stream));
+        CK(cudaMemsetAsync(ctx->bar.p, 0, 3 * sizeof(GridBar), ctx->stream));
         const WorldDev* wp = ctx->d_world.p;
         GridBar* bp = ctx->bar.p;
         const unsigned long long timeout = ctx->wait_limit_ns ? ctx->wait_limit_ns : kGridWaitNs;
@@ -1861,7 +1861,7 @@ int vxp_create(const vxp_config* cfg, int device, vxp_ctx** out) {
     ctx->solver_flow = ctx->cluster_size ? VXP_SOLVER_CLUSTER : VXP_SOLVER_EVENTS;
     ctx->w.spill_rows = true;
     if (ctx->w.init(cache_cap, ctx->grid_blocks, ctx->err)) return bail(VXP_ERR_OOM);
-    if (ctx->d_world.reserve(1) != cudaSuccess || ctx->bar.reserve(2) != cudaSuccess) return bail(VXP_ERR_OOM);
+    if (ctx->d_world.reserve(1) != cudaSuccess || ctx->bar.reserve(3) != cudaSuccess) return bail(VXP_ERR_OOM);
     if (ctx->w.ensure_pairs(std::max<uint32_t>(cfg->max_pairs, 1024), ctx->err)) return bail(VXP_ERR_OOM);
     if (ctx->w.ensure_bodies(std::max<uint32_t>(cfg->max_bodies, 256), ctx->err)) return bail(VXP_ERR_OOM);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(VXP_ERR_CUDA);

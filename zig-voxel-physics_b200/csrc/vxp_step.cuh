@@ -62,16 +62,20 @@ struct GridGroup {
     GridBar* bar;
     uint32_t* err;
     unsigned long long timeout_ns;
-    uint32_t nb;  // participating blocks: 0 .. nb-1
-    __device__ uint32_t rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+    uint32_t nb;        // participating blocks: base .. base + nb - 1
+    uint32_t base = 0;
+    __device__ uint32_t rank() const { return (blockIdx.x - base) * blockDim.x + threadIdx.x; }
     __device__ uint32_t size() const { return nb * blockDim.x; }
-    __device__ uint32_t block() const { return blockIdx.x; }
+    __device__ uint32_t block() const { return blockIdx.x - base; }
     __device__ uint32_t nblocks() const { return nb; }
-    __device__ bool member() const { return blockIdx.x < nb; }
+    __device__ bool member() const { return blockIdx.x - base < nb; }
     // The first k blocks, with their own barrier word (bar + 1): the solver's
     // colour batches are small, and a barrier over a few blocks costs far less
-    // than one over the whole grid.  The other blocks leave the kernel.
-    __device__ GridGroup subgroup(uint32_t k) const { return GridGroup{bar + 1, err, timeout_ns, k}; }
+    // than one over the whole grid.  The other blocks leave the kernel, or
+    // run as tail(k).
+    __device__ GridGroup subgroup(uint32_t k) const { return GridGroup{bar + 1, err, timeout_ns, k, base}; }
+    // The blocks after the first k, with the third barrier word (bar + 2).
+    __device__ GridGroup tail(uint32_t k) const { return GridGroup{bar + 2, err, timeout_ns, nb - k, base + k}; }
     // Bounded grid barrier: a waiting block gives up after timeout_ns, sets
     // ERR_TIMEOUT and every later sync() of every block returns false.  The
     // block's threads meet at __syncthreads, then thread 0 arrives with an
@@ -2032,7 +2036,7 @@ __device__ __forceinline__ bool isl_unite(uint32_t* parent, uint32_t a, uint32_t
 }
 
 template <class G>
-__device__ bool phase_islands(G& g, WorldDev& w, uint32_t cur) {
+__device__ bool phase_islands(G& g, WorldDev& w, uint32_t cur, uint32_t* scratch) {
     if (!w.cfg.islands_on || !w.isl_state) return true;
     const uint32_t P = w.n_pairs, N = w.n_bodies;
     uint32_t* st = w.isl_state;
@@ -2051,7 +2055,7 @@ __device__ bool phase_islands(G& g, WorldDev& w, uint32_t cur) {
                 kc[q] = k;
                 if (q >= nprev || kp[q] != k) atomicOr(&w.ctr[C_ISL_DIFF], 1u);
             },
-            w.scan, &nm))
+            scratch, &nm))
         return false;
     const bool rebuild = *(volatile uint32_t*)&st[IS_DIRTY] != 0u || nm != nprev ||
                          *(volatile uint32_t*)&w.ctr[C_ISL_DIFF] != 0u || *(volatile uint32_t*)&st[IS_TOTAL] == 0u;
@@ -2143,8 +2147,9 @@ __device__ bool phase_islands(G& g, WorldDev& w, uint32_t cur) {
 }
 
 template <class G>
-__device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_out, uint32_t* ncol_out) {
-    if (!phase_islands(g, w, cur)) return false;
+__device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_out, uint32_t* ncol_out,
+                                  bool islands = true) {
+    if (islands && !phase_islands(g, w, cur, w.scan)) return false;
     const uint32_t P = w.n_pairs, N = w.n_bodies;
     // 1. solver constraint list: manifolds that are not both-sleeping, pair order
     for (uint32_t p = g.rank(); p < P; p += g.size()) {
@@ -4076,9 +4081,23 @@ __device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go, u
     if (G::kEventSweeps && w.cfg.solver_flow && w.cfg.flow_smem_chunks)
         want = max(want, (nman / 32u + 64u + w.cfg.flow_smem_chunks - 1u) / w.cfg.flow_smem_chunks);
     G s = g.subgroup(min(want, g.nblocks()));
+    // The island pass only reads (manifolds, velocities before the solve) and
+    // writes statistics, so while the constraint table is built the blocks
+    // that phase leaves idle run it, when the sweeps follow in another kernel.
+    bool islands_here = true;
+    if constexpr (G::kEventSweeps) {
+        if (part == SOLVE_CONSTRAINTS && w.cfg.islands_on && want + 2u <= g.nblocks()) {
+            islands_here = false;
+            if (!s.member()) {
+                G r = g.tail(want);
+                phase_islands(r, w, cur, w.isl_state + IS_N);
+                return;
+            }
+        }
+    }
     if (!s.member()) return;
     uint32_t M = 0, ncol = 0;
-    if (!phase_constraints(s, w, cur, &M, &ncol)) return;
+    if (!phase_constraints(s, w, cur, &M, &ncol, islands_here)) return;
     stamp(s, w, TS_CONSTRAINTS);
     if (part == SOLVE_CONSTRAINTS) {
         if (s.rank() == 0) {
