@@ -462,8 +462,9 @@ int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]);
 
 /* Diagnostics: ns from the start of the last step kernel to the end of each
  * of its phases: [start, begin, pairs, cache, probe, finalize, constraints,
- * solve, end, islands] (islands: the IslandManager pass that opens the
- * constraint phase). */
+ * solve, end, islands, broad phase] (islands: the IslandManager pass beside
+ * the constraint phase; broad phase: the device pair list, when the step
+ * builds it). */
 int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n);
 
 /* ---------------------------------------------------------------------------

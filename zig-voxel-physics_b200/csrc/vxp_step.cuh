@@ -3827,7 +3827,9 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
         }
         g.sync();
         if (has) {
-            // prepareConstraints: one thread per (slot, point)
+            // prepareConstraints: one thread per (slot, point).  (One thread
+            // per slot, its bodies read once and its points' inputs loaded
+            // together, was slower: 0.960 against 0.939 ms on the pile.)
             for (uint32_t it = t; it < 4u * nslot; it += T) {
                 const uint32_t slot = it >> 2, i = it & 3u;
                 const uint4 mv = sm.man[slot];
@@ -4021,6 +4023,7 @@ __device__ bool world_step_narrow(G& g, WorldDev& w, const ColliderSet& cs, Warp
     if ((ph & PH_NARROW) && w.cfg.device_pairs) {
         bool overflow = false;
         if (!phase_broadphase(g, w, cs, &overflow)) return false;
+        stamp(g, w, TS_BROAD);
         if (overflow) {
             if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_CAP);
             return false;
