@@ -574,7 +574,9 @@ def batched(args, steps=None, warmup=None, emit=True, dist_ctx=(1, 0, 0, None)):
     # after another, from the state the batch reached
     plain_ms = 0.0
     for sc, st in zip(scenes, states):
-        s = vxp.VoxelPhysicsSystem(substeps=4, device=local)
+        # pair buffers sized up front: a fresh context's first device pair
+        # list would otherwise overflow its default capacity on a settled world
+        s = vxp.VoxelPhysicsSystem(substeps=4, device=local, max_pairs=max(1024, 16 * sc.dynamic_count))
         s.load_scene(sc)
         s.set_bodies(st)
         for _ in range(2):
@@ -609,7 +611,7 @@ def batched(args, steps=None, warmup=None, emit=True, dist_ctx=(1, 0, 0, None)):
                    "settle_steps": args.batch_settle,
                    "parallelism": f"worlds sharded over {ws} GPUs by estimated cost" if ws > 1 else "one GPU",
                    "substeps": 4, "dt": "1/60", "l2": "flushed (256 MiB write) between timed steps",
-                   "schedule": {"choice": ["256/slot", "256/longest-first", "512/slot", "512/longest-first"][choice],
+                   "schedule": {"choice": vxp.VoxelWorldBatch.schedule_name(choice),
                                 "autotune_ms": [float(x) for x in tune_ms]}},
         "plain_single_world": {"value": plain_value, "ms_per_batch_step": plain_ms,
                                "method": "each world alone from the batch's state, its own launches, "

@@ -522,8 +522,16 @@ int vxp_batch_times(vxp_batch* b, float* total_ms, float* world_ms, uint32_t n);
 /* Schedule: CTA size 256 or 512; launch order 0 = slot order, 1 = longest
  * measured world first. */
 int vxp_batch_set_schedule(vxp_batch* b, uint32_t threads, uint32_t order_mode);
+/* Per-world tiles: worlds of at least min_bodies_512 bodies step as
+ * 512-thread CTAs, the others as 256-thread CTAs; the two launches run side
+ * by side (one graph, two streams).  order_mode as above, within each group.
+ * No counterpart in the reference (it steps one world). */
+int vxp_batch_set_tiles(vxp_batch* b, uint32_t min_bodies_512, uint32_t order_mode);
 /* Autotuner: runs trial_steps real steps under each schedule, keeps the
- * fastest; ms_out[4] = mean step ms of (256,0), (256,1), (512,0), (512,1). */
+ * fastest; ms_out[VXP_BATCH_SCHEDULES] = mean step ms of (256,0), (256,1),
+ * (512,0), (512,1), then per-world tiles with the 512-thread threshold at
+ * 128, 256, 512 and 1024 bodies (longest first).  *choice: the index kept. */
+#define VXP_BATCH_SCHEDULES 8
 int vxp_batch_autotune(vxp_batch* b, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice);
 
 /* ---------------------------------------------------------------------------

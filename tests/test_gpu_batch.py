@@ -55,14 +55,20 @@ def test_batch_equals_alone_and_oracle(vxp):
     b.close()
 
 
-@pytest.mark.parametrize("threads,order", [(256, 0), (256, 1), (512, 0), (512, 1)])
+@pytest.mark.parametrize("threads,order", [(256, 0), (256, 1), (512, 0), (512, 1), ("tiles", 30), ("tiles", 50)])
 def test_schedule_does_not_change_results(vxp, threads, order):
+    """Every schedule, per-world tiles included (order = the body count from
+    which a world steps as a 512-thread CTA), gives each world its results
+    alone."""
     scenes = small_mix(vxp, [40, 12, 70], seed=8)
     dt = np.float32(1.0 / 60.0)
     b = vxp.VoxelWorldBatch(3, substeps=4)
     for i, sc in enumerate(scenes):
         b.load_scene(i, sc, collider_offset=1000 * (i + 1))
-    b.set_schedule(threads, order)
+    if threads == "tiles":
+        b.set_tiles(order)
+    else:
+        b.set_schedule(threads, order)
     b.step(dt, 40)
     b.synchronize()
     for i, sc in enumerate(scenes):
@@ -78,14 +84,15 @@ def test_autotune_keeps_results(vxp):
     b = vxp.VoxelWorldBatch(4, substeps=4)
     for i, sc in enumerate(scenes):
         b.load_scene(i, sc, collider_offset=1000 * (i + 1))
-    choice, ms = b.autotune(dt, trial_steps=2)  # 4 x (1 + 2) real steps
-    assert 0 <= choice < 4 and np.all(ms > 0)
+    choice, ms = b.autotune(dt, trial_steps=2)  # every schedule: 1 + 2 real steps
+    assert 0 <= choice < vxp.abi.BATCH_SCHEDULES and len(ms) == vxp.abi.BATCH_SCHEDULES and np.all(ms > 0)
     b.step(dt, 8)
     b.synchronize()
+    steps = vxp.abi.BATCH_SCHEDULES * 3 + 8
     for i, sc in enumerate(scenes):
         got = b.get_world(i)
         got["collider_id"] -= 1000 * (i + 1)
-        assert got.tobytes() == run_alone(vxp, sc, 20, dt).tobytes()
+        assert got.tobytes() == run_alone(vxp, sc, steps, dt).tobytes()
     b.close()
 
 

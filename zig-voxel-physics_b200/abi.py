@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 VXP_OK = 0
 VXP_ERR_ARG = -1
+BATCH_SCHEDULES = 8  # VXP_BATCH_SCHEDULES
 VXP_ERR_OOM = -2
 VXP_ERR_CUDA = -3
 VXP_ERR_TIMEOUT = -4
@@ -297,6 +298,7 @@ SIGNATURES = {
     "vxp_batch_times": (_I, [_VP, _VP, _VP, _U32]),
     "vxp_batch_set_schedule": (_I, [_VP, _U32, _U32]),
     "vxp_batch_autotune": (_I, [_VP, _F, _U32, _VP, _VP]),
+    "vxp_batch_set_tiles": (_I, [_VP, _U32, _U32]),
 }
 
 _LIB = None

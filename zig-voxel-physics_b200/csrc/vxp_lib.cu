@@ -2435,6 +2435,14 @@ struct vxp_batch {
     DBuf<uint32_t> d_status;          // per launch position: [error word, pair count]
     uint32_t threads = 256;           // CTA size
     uint32_t order_mode = 1;          // 0: slot order, 1: longest measured / largest first
+    // per-world tiles: > 0, worlds of at least this many bodies step as
+    // 512-thread CTAs (launch positions [0, n_big)) and the rest as 256-thread
+    // CTAs, two launches side by side in the graph (second stream)
+    uint32_t tile_min_bodies = 0;
+    uint32_t n_big = 0;
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    uint32_t graph_tile = 0, graph_nbig = 0;
     float margin = 0.1f;
     float built_dt = -1.0f;
     bool rebuild = true;
@@ -2498,6 +2506,15 @@ int batch_prepare(vxp_batch* bt, float dt) {
                 return ea > ec;
             });
         }
+        if (bt->tile_min_bodies) {
+            // the 512-thread worlds first, each group in the order above
+            const auto mid = std::stable_partition(ord.begin(), ord.end(), [&](uint32_t x) {
+                return bt->slots[x]->n_bodies >= bt->tile_min_bodies;
+            });
+            bt->n_big = (uint32_t)(mid - ord.begin());
+        } else {
+            bt->n_big = bt->threads == 512 ? (uint32_t)ord.size() : 0u;
+        }
         bt->order = ord;
         std::vector<WorldDev> wd(ord.size());
         for (size_t i = 0; i < ord.size(); ++i)
@@ -2517,7 +2534,8 @@ int batch_prepare(vxp_batch* bt, float dt) {
     const uint32_t n = (uint32_t)bt->order.size();
     if (bt->exec && bt->d_worlds.p == bt->graph_worlds && cs.c == bt->graph_cs.c &&
         cs.grid == bt->graph_cs.grid && cs.vox == bt->graph_cs.vox && cs.n == bt->graph_cs.n && cs.nb == bt->graph_cs.nb &&
-        n == bt->graph_n && bt->threads == bt->graph_threads)
+        n == bt->graph_n && bt->threads == bt->graph_threads && bt->tile_min_bodies == bt->graph_tile &&
+        bt->n_big == bt->graph_nbig)
         return VXP_OK;
     if (bt->exec) {
         cudaGraphExecDestroy(bt->exec);
@@ -2530,8 +2548,29 @@ int batch_prepare(vxp_batch* bt, float dt) {
     if (n == 0) return VXP_OK;
     const size_t smem = step_smem(bt->threads, bt->cache_cap);
     BK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
-    if (bt->threads == 512) k_step_block<512><<<n, 512, smem, bt->stream>>>(bt->d_worlds.p, cs);
-    else k_step_block<256><<<n, 256, smem, bt->stream>>>(bt->d_worlds.p, cs);
+    if (bt->tile_min_bodies) {
+        // 512-thread worlds on the batch stream, 256-thread worlds on the
+        // second stream, forked from and joined back into the first
+        const uint32_t nb = bt->n_big, ns = n - bt->n_big;
+        const bool both = nb > 0 && ns > 0;
+        if (both) {
+            cudaEventRecord(bt->ev_fork, bt->stream);
+            cudaStreamWaitEvent(bt->stream2, bt->ev_fork, 0);
+        }
+        if (nb)
+            k_step_block<512><<<nb, 512, step_smem(512, bt->cache_cap), bt->stream>>>(bt->d_worlds.p, cs);
+        if (ns)
+            k_step_block<256><<<ns, 256, step_smem(256, bt->cache_cap), both ? bt->stream2 : bt->stream>>>(
+                bt->d_worlds.p + nb, cs);
+        if (both) {
+            cudaEventRecord(bt->ev_join, bt->stream2);
+            cudaStreamWaitEvent(bt->stream, bt->ev_join, 0);
+        }
+    } else if (bt->threads == 512) {
+        k_step_block<512><<<n, 512, smem, bt->stream>>>(bt->d_worlds.p, cs);
+    } else {
+        k_step_block<256><<<n, 256, smem, bt->stream>>>(bt->d_worlds.p, cs);
+    }
     const cudaError_t le = cudaGetLastError();
     cudaGraph_t g = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(bt->stream, &g);
@@ -2543,6 +2582,8 @@ int batch_prepare(vxp_batch* bt, float dt) {
     bt->graph_cs = cs;
     bt->graph_n = n;
     bt->graph_threads = bt->threads;
+    bt->graph_tile = bt->tile_min_bodies;
+    bt->graph_nbig = bt->n_big;
     return VXP_OK;
 }
 
@@ -2568,8 +2609,11 @@ int vxp_batch_create(const vxp_config* cfg, int device, uint32_t max_worlds, vxp
     };
     if (cudaSetDevice(device) != cudaSuccess) return bail(VXP_ERR_CUDA);
     // blocking, for the same reason as a context's stream (vxp_create)
-    if (cudaStreamCreate(&bt->stream) != cudaSuccess) return bail(VXP_ERR_CUDA);
-    if (cudaEventCreate(&bt->ev0) != cudaSuccess || cudaEventCreate(&bt->ev1) != cudaSuccess)
+    if (cudaStreamCreate(&bt->stream) != cudaSuccess || cudaStreamCreate(&bt->stream2) != cudaSuccess)
+        return bail(VXP_ERR_CUDA);
+    if (cudaEventCreate(&bt->ev0) != cudaSuccess || cudaEventCreate(&bt->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&bt->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&bt->ev_join, cudaEventDisableTiming) != cudaSuccess)
         return bail(VXP_ERR_CUDA);
     if (set_kernel_smem(bt->cache_cap)) return bail(VXP_ERR_CUDA);
     *out = bt;
@@ -2583,6 +2627,9 @@ void vxp_batch_destroy(vxp_batch* bt) {
     if (bt->graph) cudaGraphDestroy(bt->graph);
     if (bt->ev0) cudaEventDestroy(bt->ev0);
     if (bt->ev1) cudaEventDestroy(bt->ev1);
+    if (bt->ev_fork) cudaEventDestroy(bt->ev_fork);
+    if (bt->ev_join) cudaEventDestroy(bt->ev_join);
+    if (bt->stream2) cudaStreamDestroy(bt->stream2);
     if (bt->stream) cudaStreamDestroy(bt->stream);
     delete bt;
 }
@@ -2794,20 +2841,38 @@ int vxp_batch_set_schedule(vxp_batch* bt, uint32_t threads, uint32_t order_mode)
     if (!bt || (threads != 256 && threads != 512) || order_mode > 1) return VXP_ERR_ARG;
     bt->threads = threads;
     bt->order_mode = order_mode;
+    bt->tile_min_bodies = 0;
     bt->rebuild = true;
     return VXP_OK;
 }
 
+int vxp_batch_set_tiles(vxp_batch* bt, uint32_t min_bodies_512, uint32_t order_mode) {
+    if (!bt || min_bodies_512 == 0 || order_mode > 1) return VXP_ERR_ARG;
+    bt->tile_min_bodies = min_bodies_512;
+    bt->order_mode = order_mode;
+    bt->rebuild = true;
+    return VXP_OK;
+}
+
+// Schedule i of the autotuner: 0-3 one CTA size for every world, (256, slot
+// order), (256, longest first), (512, slot order), (512, longest first);
+// 4-7 per-world tiles, worlds of at least 128 / 256 / 512 / 1024 bodies as
+// 512-thread CTAs and the rest as 256-thread CTAs, longest first.
+static int batch_schedule(vxp_batch* bt, uint32_t i) {
+    if (i < 4) return vxp_batch_set_schedule(bt, i < 2 ? 256u : 512u, i & 1u);
+    return vxp_batch_set_tiles(bt, 128u << (i - 4u), 1u);
+}
+
 // Tries each schedule for trial_steps real steps (each world's results do
-// not depend on the schedule) and keeps the fastest.  ms_out[4] receives the
-// mean step time of (256, slot order), (256, longest first), (512, slot
-// order), (512, longest first); *choice the index kept.
+// not depend on the schedule) and keeps the fastest.  ms_out receives the
+// mean step time of each of the VXP_BATCH_SCHEDULES schedules; *choice the
+// index kept.
 int vxp_batch_autotune(vxp_batch* bt, float dt, uint32_t trial_steps, float* ms_out, uint32_t* choice) {
     if (!bt || trial_steps == 0) return VXP_ERR_ARG;
     float best = 1e30f;
     uint32_t best_i = 0;
-    for (uint32_t i = 0; i < 4; ++i) {
-        if (int rc = vxp_batch_set_schedule(bt, i < 2 ? 256u : 512u, i & 1u)) return rc;
+    for (uint32_t i = 0; i < VXP_BATCH_SCHEDULES; ++i) {
+        if (int rc = batch_schedule(bt, i)) return rc;
         if (int rc = vxp_batch_step(bt, dt, 1)) return rc;  // measures world times, builds the graph
         if (int rc = vxp_batch_synchronize(bt)) return rc;
         if (int rc = vxp_batch_times(bt, nullptr, nullptr, 0)) return rc;
@@ -2824,7 +2889,7 @@ int vxp_batch_autotune(vxp_batch* bt, float dt, uint32_t trial_steps, float* ms_
         }
     }
     if (choice) *choice = best_i;
-    return vxp_batch_set_schedule(bt, best_i < 2 ? 256u : 512u, best_i & 1u);
+    return batch_schedule(bt, best_i);
 }
 
 }  // extern "C"

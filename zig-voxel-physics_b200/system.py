@@ -410,10 +410,23 @@ class VoxelWorldBatch:
         return float(total.value), per
 
     def set_schedule(self, threads: int, order_mode: int) -> None:
+        """One CTA size (256 or 512) for every world; order 0 slot order, 1 longest first."""
         self._check(self.lib.vxp_batch_set_schedule(self.b, int(threads), int(order_mode)))
 
+    def set_tiles(self, min_bodies_512: int, order_mode: int = 1) -> None:
+        """Per-world tiles: worlds of at least min_bodies_512 bodies as 512-thread
+        CTAs, the rest as 256-thread CTAs, the two launches side by side."""
+        self._check(self.lib.vxp_batch_set_tiles(self.b, int(min_bodies_512), int(order_mode)))
+
+    @staticmethod
+    def schedule_name(choice: int) -> str:
+        """The autotuner's schedule index as text."""
+        if choice < 4:
+            return f"{256 if choice < 2 else 512}/{'longest-first' if choice & 1 else 'slot-order'}"
+        return f"tiles: >= {128 << (choice - 4)} bodies 512, else 256/longest-first"
+
     def autotune(self, dt: float, trial_steps: int = 3) -> tuple:
-        ms = np.zeros(4, dtype=np.float32)
+        ms = np.zeros(abi.BATCH_SCHEDULES, dtype=np.float32)
         choice = ctypes.c_uint32(0)
         self._check(self.lib.vxp_batch_autotune(self.b, np.float32(dt), int(trial_steps), abi.ptr(ms),
                                                 ctypes.byref(choice)))
