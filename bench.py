@@ -305,7 +305,7 @@ def ours(args):
     n_dyn = scene.dynamic_count
     n_nonstatic = int((scene.bodies["body_type"] != abi.BODY_STATIC).sum())
     sysm = vxp.VoxelPhysicsSystem(device=local, substeps=substeps, fixed_timestep=np.float32(scene.dt),
-                                  reference_caps=0, max_pairs=max(65536, 16 * n_dyn), max_bodies=len(scene.bodies))
+                                  reference_caps=0, max_pairs=max(1024, 16 * n_dyn), max_bodies=len(scene.bodies))
     sysm.load_scene(scene)
     sysm.set_launch_mode(args.launch_mode)
     if args.solver >= 0:
@@ -403,7 +403,7 @@ def ours(args):
                              "achieved": achieved, "frac": achieved / peak}
 
     # ---- e2e through the public API with pinned host buffers
-    cap = max(65536, 16 * n_dyn)
+    cap = max(1024, 16 * n_dyn)
     pin_pairs = torch.empty(cap * 8, dtype=torch.uint8).pin_memory().numpy().view(abi.PAIR_DTYPE)
     pin_bodies = torch.empty(len(scene.bodies) * 128, dtype=torch.uint8).pin_memory().numpy().view(abi.BODY_DTYPE)
     h2d = d2h = 0

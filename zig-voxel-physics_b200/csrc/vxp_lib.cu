@@ -313,6 +313,12 @@ size_t step_smem(uint32_t threads, uint32_t cache_cap) {
 // of constraint rows per block in shared memory.
 constexpr uint32_t kGridFlowChunks = 4;
 size_t grid_smem(uint32_t cache_cap) { return step_smem(kGridThreads, cache_cap); }
+// Dynamic shared memory of a one-CTA world's launch (either CTA size): the
+// narrow part's warp scratch and cache table, then room for the sweeps' state
+// of a small world (bodies, manifold slots, point rows); two 256-thread CTAs
+// still fit on one SM.
+constexpr size_t kBlockSolveSmem = 96 * 1024;
+size_t block_smem(uint32_t cache_cap) { return std::max(step_smem(512, cache_cap), kBlockSolveSmem); }
 size_t solve_smem() { return (size_t)kGridFlowChunks * kChunkFloats * sizeof(float); }
 uint32_t flow_chunks(size_t smem) { return (uint32_t)(smem / (kChunkFloats * sizeof(float))); }
 
@@ -1488,7 +1494,8 @@ int launch_step(vxp_ctx* ctx, float dt, uint32_t phases, bool device_pairs, floa
     const bool cluster = grid && ctx->solver_flow == VXP_SOLVER_CLUSTER && ctx->cluster_size > 0;
     const uint32_t flow = ctx->solver_flow == VXP_SOLVER_EVENTS ? 1u : 0u;
     WorldDev w = ctx->w.make(ctx->cfg, dt, phases, ctx->solver_div, device_pairs, margin, flow);
-    const size_t smem = grid ? grid_smem(w.cache_cap) : step_smem(kBlockThreads, w.cache_cap);
+    const size_t smem = grid ? grid_smem(w.cache_cap) : block_smem(w.cache_cap);
+    if (!grid) w.cfg.block_smem = (uint32_t)smem;
     w.cfg.flow_smem_chunks = grid ? flow_chunks(solve_smem()) : 0u;
     w.cfg.heavy_voxels = ctx->heavy_voxels;
     w.cfg.count_bricks = ctx->count_bricks ? 1u : 0u;
@@ -1784,9 +1791,9 @@ void vxp_config_default(vxp_config* c) {
 
 static int set_kernel_smem(uint32_t cache_cap) {
     if (cudaFuncSetAttribute(k_step_block<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)step_smem(256, cache_cap)) != cudaSuccess ||
+                             (int)block_smem(kMaxCacheSmem)) != cudaSuccess ||
         cudaFuncSetAttribute(k_step_block<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)step_smem(512, cache_cap)) != cudaSuccess ||
+                             (int)block_smem(kMaxCacheSmem)) != cudaSuccess ||
         cudaFuncSetAttribute(k_step_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)grid_smem(cache_cap)) != cudaSuccess ||
         cudaFuncSetAttribute(k_solve_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem()) !=
@@ -2518,7 +2525,10 @@ int batch_prepare(vxp_batch* bt, float dt) {
         bt->order = ord;
         std::vector<WorldDev> wd(ord.size());
         for (size_t i = 0; i < ord.size(); ++i)
+        {
             wd[i] = bt->slots[ord[i]]->make(bt->cfg, dt, PH_STEP, 128, true, bt->margin, 0u);
+            wd[i].cfg.block_smem = (uint32_t)block_smem(bt->cache_cap);
+        }
         if (bt->d_worlds.reserve(std::max<size_t>(wd.size(), 1)) != cudaSuccess ||
             bt->d_ts.reserve(2 * std::max<size_t>(wd.size(), 1)) != cudaSuccess ||
             bt->d_status.reserve(2 * std::max<size_t>(wd.size(), 1)) != cudaSuccess)
@@ -2546,7 +2556,7 @@ int batch_prepare(vxp_batch* bt, float dt) {
         bt->graph = nullptr;
     }
     if (n == 0) return VXP_OK;
-    const size_t smem = step_smem(bt->threads, bt->cache_cap);
+    const size_t smem = block_smem(bt->cache_cap);
     BK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
     if (bt->tile_min_bodies) {
         // 512-thread worlds on the batch stream, 256-thread worlds on the
@@ -2558,9 +2568,9 @@ int batch_prepare(vxp_batch* bt, float dt) {
             cudaStreamWaitEvent(bt->stream2, bt->ev_fork, 0);
         }
         if (nb)
-            k_step_block<512><<<nb, 512, step_smem(512, bt->cache_cap), bt->stream>>>(bt->d_worlds.p, cs);
+            k_step_block<512><<<nb, 512, smem, bt->stream>>>(bt->d_worlds.p, cs);
         if (ns)
-            k_step_block<256><<<ns, 256, step_smem(256, bt->cache_cap), both ? bt->stream2 : bt->stream>>>(
+            k_step_block<256><<<ns, 256, smem, both ? bt->stream2 : bt->stream>>>(
                 bt->d_worlds.p + nb, cs);
         if (both) {
             cudaEventRecord(bt->ev_join, bt->stream2);

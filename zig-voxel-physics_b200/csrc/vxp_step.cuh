@@ -39,6 +39,7 @@ struct BlockGroup {
     // One CTA's barriers are cheap: the solver sweeps colour batch by colour
     // batch (the event-ordered sweeps are not compiled for this group).
     static constexpr bool kEventSweeps = false;
+    static constexpr bool kDistributed = false;  // shared memory is the CTA's own
     __device__ uint32_t rank() const { return threadIdx.x; }
     __device__ uint32_t size() const { return blockDim.x; }
     __device__ uint32_t block() const { return 0; }
@@ -59,6 +60,7 @@ struct GridBar {
 
 struct GridGroup {
     static constexpr bool kEventSweeps = true;
+    static constexpr bool kDistributed = false;
     GridBar* bar;
     uint32_t* err;
     unsigned long long timeout_ns;
@@ -130,6 +132,7 @@ struct GridGroup {
 // world_step_sweeps).  sync() never fails.
 struct ClusterGroup {
     static constexpr bool kEventSweeps = false;
+    static constexpr bool kDistributed = true;  // other CTAs' shared memory through mapa
     __device__ uint32_t rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
     __device__ uint32_t size() const { return gridDim.x * blockDim.x; }
     __device__ uint32_t block() const { return blockIdx.x; }
@@ -3542,6 +3545,14 @@ __device__ __forceinline__ T* cluster_map(T* p, uint32_t rank) {
     return reinterpret_cast<T*>(r);
 }
 
+// Another CTA's copy of a shared-memory object: through the cluster's
+// distributed shared memory, or the object itself for a one-CTA group.
+template <class G, class T>
+__device__ __forceinline__ T* group_map(T* p, uint32_t rank) {
+    if constexpr (G::kDistributed) return cluster_map(p, rank);
+    else return p;
+}
+
 constexpr uint32_t kMaxStaticReplicas = 32;
 
 struct ClusterSolveSmem {
@@ -3570,7 +3581,8 @@ __device__ __forceinline__ size_t cluster_smem_bytes(uint32_t bcap, uint32_t nre
            (size_t)kMaxStaticReplicas * sizeof(uint32_t);
 }
 
-__device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, uint32_t ncol, unsigned char* smem,
+template <class G>
+__device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol, unsigned char* smem,
                                     uint32_t smem_bytes) {
     const StepCfg& cf = w.cfg;
     const uint32_t C = g.nblocks(), k = g.block(), t = threadIdx.x, T = blockDim.x;
@@ -3579,7 +3591,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     // by owner when the packing is grouped so and the fullest CTA's share
     // fits; else round-robin over the same positions (any order inside a
     // colour will do), which balances the CTAs exactly
-    bool by_owner = w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
+    bool by_owner = C > 1u && w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
     // this CTA's manifolds of colour c: positions [first(c), first(c) + count(c))
     // by owner, else every C-th from lo + k
     auto count_of = [&](uint32_t c, uint32_t cta) -> uint32_t {
@@ -3598,7 +3610,7 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     sm.nrep = w.n_static <= kMaxStaticReplicas ? w.n_static : 0u;
     // points: the packing's tallies when it grouped for this cluster, else
     // four per slot
-    const bool tallied = w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
+    const bool tallied = C > 1u && w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
     // point rows that do not fit in shared memory may go to w.crow: a CTA's
     // last slots (the point offsets are a prefix in slot order, so once a
     // slot's rows spill every later slot's do), in that CTA's range of w.crow
@@ -3613,7 +3625,10 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
             uint32_t n = 0;
             for (uint32_t c = 0; c < ncol; ++c) n += count_of(c, cta);
             need = max(need, n);
-            const uint32_t p = tallied ? w.ocnt[kOwnerPoints + (by_owner ? 0u : kMaxOwnerGroups) + cta] : 4u * n;
+            // one CTA holds every point of the constraint set
+            const uint32_t p = tallied ? w.ocnt[kOwnerPoints + (by_owner ? 0u : kMaxOwnerGroups) + cta]
+                               : C == 1u ? *(volatile uint32_t*)&w.ctr[C_POINTS]
+                                         : 4u * n;
             needp = max(needp, p);
             if (cta < k) goff += p;
             gtot += p;
@@ -3776,10 +3791,10 @@ __device__ bool phase_solve_cluster(ClusterGroup& g, WorldDev& w, uint32_t M, ui
     auto home_slot = [&](uint32_t i) { return csh < 32u ? i >> csh : i / C; };
     // body a (or b) of a manifold: its static copy here, else its home CTA's record
     auto body_a = [&](const uint4& mv) {
-        return (mv.w & CM_RA) ? sm.rep + ((mv.w >> 8) & 0xFFu) : cluster_map(sm.body + home_slot(mv.x), home(mv.x));
+        return (mv.w & CM_RA) ? sm.rep + ((mv.w >> 8) & 0xFFu) : group_map<G>(sm.body + home_slot(mv.x), home(mv.x));
     };
     auto body_b = [&](const uint4& mv) {
-        return (mv.w & CM_RB) ? sm.rep + ((mv.w >> 16) & 0xFFu) : cluster_map(sm.body + home_slot(mv.y), home(mv.y));
+        return (mv.w & CM_RB) ? sm.rep + ((mv.w >> 16) & 0xFFu) : group_map<G>(sm.body + home_slot(mv.y), home(mv.y));
     };
     // one manifold of a velocity-type sweep: 0 warm start, 1 velocity, 2 relax
     auto vel_item = [&](uint32_t slot, uint32_t kind) {
@@ -4123,7 +4138,11 @@ __device__ void world_step_solve(G& g, WorldDev& w, float* fsm, bool check_go, u
                               (*(volatile uint32_t*)&w.ctr[C_ERROR] & ERR_COLOURS) == 0u;
             ok = flow ? phase_solve_flow(s, w, fsm, M, ncol) : phase_solve(s, w, M, ncol);
         } else {
-            ok = phase_solve(s, w, M, ncol);
+            // a one-CTA world: the sweeps keep their state in the block's
+            // shared memory when it fits (the narrow part is done with it)
+            ok = (w.cfg.block_smem && phase_solve_cluster(s, w, M, ncol, reinterpret_cast<unsigned char*>(fsm),
+                                                          w.cfg.block_smem)) ||
+                 phase_solve(s, w, M, ncol);
         }
         if (!ok) return;
     }

@@ -166,6 +166,7 @@ struct StepCfg {
     uint32_t count_bricks;      // count the bricks each probed pair touches (C_BRICKS; traffic accounting only)
     uint32_t owner_groups;      // > 1: pack each colour by owner group (home body mod this; the sweep cluster's size)
     uint32_t islands_on;        // IslandManager statistics each solve (PhysicsConfig.enable_islands)
+    uint32_t block_smem;        // one-CTA launch: dynamic shared memory the sweeps may hold their state in (0: L2)
 };
 enum : uint32_t { PH_NARROW = 1u, PH_SOLVE = 2u, PH_SKIP_TEST = 4u, PH_STEP = 7u };
 
