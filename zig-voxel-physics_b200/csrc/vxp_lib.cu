@@ -127,6 +127,33 @@ __global__ void k_body_aabbs(const DBody* body, const DBodyProp* prop, uint32_t 
     mx[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
 }
 
+// The body table as vxp_body records (vxp_bodies_get): one thread a body,
+// packed on the device so that the host reads it back in one copy.
+__global__ void k_pack_bodies(const DBody* body, const DBodyProp* prop, const uint32_t* pub_cid, uint32_t n,
+                              vxp_body* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DBody d = body[i];
+    const DBodyProp& p = prop[i];
+    vxp_body s;
+    s.id = p.id;
+    s.body_type = p.type;
+    s.collider_id = pub_cid[i];
+    s.is_sleeping = p.sleeping;
+    s.position[0] = d.p.x; s.position[1] = d.p.y; s.position[2] = d.p.z;
+    s.rotation[0] = d.q.x; s.rotation[1] = d.q.y; s.rotation[2] = d.q.z; s.rotation[3] = d.q.w;
+    s.linear_velocity[0] = d.v.x; s.linear_velocity[1] = d.v.y; s.linear_velocity[2] = d.v.z;
+    s.angular_velocity[0] = d.w.x; s.angular_velocity[1] = d.w.y; s.angular_velocity[2] = d.w.z;
+    s.inv_mass = d.p.w;
+    for (int k = 0; k < 9; ++k) s.inv_inertia_local[k] = p.il[k];
+    s.friction = p.friction;
+    s.restitution = p.restitution;
+    s.linear_damping = p.lin_damp;
+    s.angular_damping = p.ang_damp;
+    s.sleep_timer = p.sleep_timer;
+    out[i] = s;
+}
+
 // Bulk state export of bodies [first, first + n): one thread a body, each
 // requested field into its own array (vxp_bodies_export).
 __global__ void k_export(const DBody* body, const DBodyProp* prop, uint32_t first, uint32_t n, ColliderSet cs,
@@ -1001,6 +1028,8 @@ struct WorldBuffers {
     DBuf<CacheValRec> cval;
     DBuf<WorldDev::Cand> dump;
     DBuf<unsigned char> export_stage;  // host-memory exports land here first
+    DBuf<uint32_t> pub_cid;            // per body: its collider id as the caller named it
+    DBuf<vxp_body> pack;               // vxp_bodies_get's records, packed on the device
 
     int init(uint32_t cache, uint32_t blocks, std::string& err) {
         cache_cap = cache;
@@ -1174,7 +1203,10 @@ struct WorldBuffers {
             }
         if (n && (cudaMemcpy(body.p, db.data(), n * sizeof(DBody), cudaMemcpyHostToDevice) != cudaSuccess ||
                   cudaMemcpy(prop.p, dp.data(), n * sizeof(DBodyProp), cudaMemcpyHostToDevice) != cudaSuccess ||
-                  cudaMemcpy(ids.p, id.data(), n * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess)) {
+                  cudaMemcpy(ids.p, id.data(), n * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess ||
+                  pub_cid.reserve(n) != cudaSuccess || pack.reserve(n) != cudaSuccess ||
+                  cudaMemcpy(pub_cid.p, collider_public.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+                      cudaSuccess)) {
             err = "body upload failed";
             return VXP_ERR_CUDA;
         }
@@ -1199,35 +1231,13 @@ struct WorldBuffers {
             err = fmt("expected %u bodies, got %u", n_bodies, n);
             return VXP_ERR_ARG;
         }
-        std::vector<DBody> db(n);
-        std::vector<DBodyProp> dp(n);
-        if (n && (cudaMemcpyAsync(db.data(), body.p, n * sizeof(DBody), cudaMemcpyDeviceToHost, stream) !=
-                      cudaSuccess ||
-                  cudaMemcpyAsync(dp.data(), prop.p, n * sizeof(DBodyProp), cudaMemcpyDeviceToHost, stream) !=
-                      cudaSuccess ||
-                  cudaStreamSynchronize(stream) != cudaSuccess)) {
+        if (!n) return VXP_OK;
+        k_pack_bodies<<<(n + 255u) / 256u, 256, 0, stream>>>(body.p, prop.p, pub_cid.p, n, pack.p);
+        if (cudaPeekAtLastError() != cudaSuccess ||
+            cudaMemcpyAsync(b, pack.p, n * sizeof(vxp_body), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
             err = "body download failed";
             return VXP_ERR_CUDA;
-        }
-        for (uint32_t i = 0; i < n; ++i) {
-            vxp_body& s = b[i];
-            const DBody& d = db[i];
-            const DBodyProp& p = dp[i];
-            s.id = p.id;
-            s.body_type = p.type;
-            s.collider_id = collider_public[i];
-            s.is_sleeping = p.sleeping;
-            s.position[0] = d.p.x; s.position[1] = d.p.y; s.position[2] = d.p.z;
-            s.rotation[0] = d.q.x; s.rotation[1] = d.q.y; s.rotation[2] = d.q.z; s.rotation[3] = d.q.w;
-            s.linear_velocity[0] = d.v.x; s.linear_velocity[1] = d.v.y; s.linear_velocity[2] = d.v.z;
-            s.angular_velocity[0] = d.w.x; s.angular_velocity[1] = d.w.y; s.angular_velocity[2] = d.w.z;
-            s.inv_mass = d.p.w;
-            for (int k = 0; k < 9; ++k) s.inv_inertia_local[k] = p.il[k];
-            s.friction = p.friction;
-            s.restitution = p.restitution;
-            s.linear_damping = p.lin_damp;
-            s.angular_damping = p.ang_damp;
-            s.sleep_timer = p.sleep_timer;
         }
         return VXP_OK;
     }
@@ -1333,7 +1343,7 @@ struct WorldBuffers {
                cwriter.bytes() + scan.bytes() + ctr.bytes() + ts.bytes() + dump.bytes() + ocnt.bytes() + ocur.bytes() +
                stat.bytes() + bpmask.bytes() + crow.bytes() + isl_parent.bytes() + isl_flag.bytes() +
                isl_size.bytes() + isl_timer.bytes() + isl_keys0.bytes() + isl_keys1.bytes() + isl_state.bytes() +
-               export_stage.bytes();
+               export_stage.bytes() + pub_cid.bytes() + pack.bytes();
     }
 
     // The next solve rebuilds its islands (IslandManager.markDirty,

@@ -46,7 +46,7 @@ class Job:
 
 def estimate_bytes(n_bodies: int, cache_entries: int = 1024) -> int:
     """Device memory a world of n bodies takes (WorldBuffers with the default
-    pair capacity of 16 x n, at least 1024): ~1.4 KB per pair slot, ~320 B
+    pair capacity of 16 x n, at least 1024): ~1.4 KB per pair slot, ~480 B
     per body, the broad phase's hit masks (body capacity^2 / 8 bytes up to
     8192 bodies), ~0.4 MB of brick-pair cache and fixed scratch."""
     pairs = max(1024, 16 * n_bodies)
@@ -56,8 +56,10 @@ def estimate_bytes(n_bodies: int, cache_entries: int = 1024) -> int:
     bcap = 64
     while bcap < n_bodies:
         bcap *= 2
-    per_pair = 8 + 76 + 2 * 376 + 4 * 6 + 24 + 4 * 31 * 4 + 16 + 8 + 2 * 16 * 2
-    per_body = 112 + 64 + 4 * 16 + 8 + 4 * 4 + 4 * 10
+    # + two island key buffers per pair slot
+    per_pair = 8 + 76 + 2 * 376 + 4 * 6 + 24 + 4 * 31 * 4 + 16 + 8 + 2 * 16 * 2 + 2 * 8
+    # + the island arrays, the public collider id and the packed readback record
+    per_body = 112 + 64 + 4 * 16 + 8 + 4 * 4 + 4 * 10 + 16 + 4 + 128
     masks = bcap * ((bcap + 31) // 32) * 4 if bcap <= 8192 else 0
     return (cap * per_pair + max(64, n_bodies) * per_body + masks + cache_entries * (24 + 368 + 4) +
             (64 << 10))
