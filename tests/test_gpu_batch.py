@@ -34,6 +34,39 @@ def run_oracle(scene, steps, dt):
     return out
 
 
+ISLAND_KEYS = ("island_count", "active_islands", "sleeping_islands", "largest_island_size")
+
+
+def test_batch_world_islands_equal_the_oracle(vxp):
+    """The island pass runs in every batch world (one CTA): after each of 200
+    steps every world's IslandManager statistics equal the oracle's for that
+    world alone.  Islands of the 12-box world sleep from step ~183, those of
+    the reference's example scene from step 76 (its box sleeps soon after and
+    every later step is skipped)."""
+    scenes = small_mix(vxp, [12, 40, 25], seed=21) + [vxp.scenes.basic_example(O.mass_fn)]
+    dt = np.float32(1.0 / 60.0)
+    b = vxp.VoxelWorldBatch(len(scenes), substeps=4)
+    rs = []
+    for i, sc in enumerate(scenes):
+        b.load_scene(i, sc, collider_offset=1000 * (i + 1))
+        r = O.OracleWorld(substeps=4)
+        r.load_scene(sc)
+        rs.append(r)
+    slept = 0
+    for s in range(200):
+        b.step(dt)
+        b.synchronize()
+        for i, r in enumerate(rs):
+            r.step(dt)
+            got, want = b.world_stats(i), r.stats()
+            assert {k: got[k] for k in ISLAND_KEYS} == {k: want[k] for k in ISLAND_KEYS}, (s, i)
+            slept += want["sleeping_islands"]
+    for r in rs:
+        r.close()
+    b.close()
+    assert slept > 0
+
+
 def test_batch_equals_alone_and_oracle(vxp):
     scenes = small_mix(vxp, [8, 30, 90, 17, 60])
     dt = np.float32(1.0 / 60.0)

@@ -3776,6 +3776,7 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
         }
     }
     g.sync();  // every block's bodies are in place (and every block has started)
+    if (g.rank() == 0 && w.ts) w.ts[TS_SW_SETUP] = global_ns();
     const SolveFlags sf = solve_flags(cf);
     const float h = cf.dt / (float)cf.substeps;
     const Soft soft = soft_params(cf.hertz, cf.damping_ratio, h);
@@ -3887,6 +3888,7 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
             if (g.rank() == 0) w.ctr[C_SUBREC] = s + 1u;
         }
     }
+    if (g.rank() == 0 && w.ts) w.ts[TS_SW_SUBSTEPS] = global_ns();
     if (has) {
         for (uint32_t it = 0; it < cf.pos_iters; ++it) {
             float mn = 0.0f, mx = -__int_as_float(0x7f800000);
@@ -3919,6 +3921,7 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
         }
     }
     g.sync();
+    if (g.rank() == 0 && w.ts) w.ts[TS_SW_POSITION] = global_ns();
     // bodies back to the world, impulses and masses back to the packed rows
     // (storeImpulses reads them)
     for (uint32_t q = t; q < sm.bcap; q += T) {
