@@ -2978,6 +2978,57 @@ __device__ void position_points(const SolveFlags sf, const CPV v, uint32_t n, PB
     B.x = xb;
     B.q = qb;
 }
+// position_points over contiguous point rows that hold, once the velocity
+// sweeps are done, each point's position-sweep inputs: the normal where the
+// velocity rows keep it (CP_NX), local anchor a at CP_PX, local anchor b at
+// CP_RAX, the base separation at CP_RBX.  The same operations in the same
+// order.
+__device__ void position_points_rows(const SolveFlags sf, const float* rows, uint32_t n, PB& A, PB& B,
+                                     float* min_sep, float* max_pen) {
+    F3 xa = A.x, xb = B.x;
+    Qt qa = A.q, qb = B.q;
+    const float ima = A.im, imb = B.im;
+    const M33 Ia = A.I, Ib = B.I;
+    const bool wa_ = A.wr, wb_ = B.wr;
+    const float slop = sf.slop;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float2* q = reinterpret_cast<const float2*>(rows + (size_t)i * CP_NVEL);
+        const float2 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4];
+        const F3 n = F3{q0.x, q0.y, q1.x};
+        const F3 la = F3{q1.y, q2.x, q2.y};
+        const F3 lb = F3{q3.x, q3.y, q4.x};
+        const float base = q4.y;
+        const F3 wa = qrotate(qa, la) + xa;
+        const F3 wb = qrotate(qb, lb) + xb;
+        const F3 ad = wb - wa;
+        const float sep = base + dot3(ad, n);
+        *min_sep = fminf(*min_sep, sep);
+        *max_pen = fmaxf(*max_pen, -sep);
+        if (sep >= -slop) continue;
+        const float corr = fmaxf(sf.pos_rate * (sep + slop), -sf.max_corr);
+        const F3 ra = wa - xa, rb = wb - xb;
+        const F3 rna = cross3(ra, n), rnb = cross3(rb, n);
+        float k = ima + imb;
+        k += dot3(rna, mat3_mul_vec(Ia, rna));
+        k += dot3(rnb, mat3_mul_vec(Ib, rnb));
+        if (k < kEpsilon) continue;
+        const F3 pimp = n * (-corr / k);
+        if (wa_) {
+            xa = xa - pimp * ima;
+            qa = integrate_rotation_small(qa, mat3_mul_vec(Ia, cross3(ra, -pimp)));
+        }
+        if (wb_) {
+            xb = xb + pimp * imb;
+            qb = integrate_rotation_small(qb, mat3_mul_vec(Ib, cross3(rb, pimp)));
+        }
+    }
+    A.x = xa;
+    A.q = qa;
+    B.x = xb;
+    B.q = qb;
+}
+static_assert(CP_NX == 0 && CP_PX == 3 && CP_RAX == 6 && CP_RBX == 9 && CP_NM > CP_RBX,
+              "position rows: normal, anchor a, anchor b, base separation in the first ten floats");
 __device__ void position_manifold(WorldDev& w, uint32_t pos, float* min_sep, float* max_pen) {
     const uint4 cmv = w.cm[pos];
     const DBodyProp& pa = w.prop[cmv.x];
@@ -3889,6 +3940,33 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
         }
     }
     if (g.rank() == 0 && w.ts) w.ts[TS_SW_SUBSTEPS] = global_ns();
+    // the velocity sweeps are done: impulses and masses back to the packed
+    // rows now (storeImpulses reads them), and in their rows each point's
+    // position-sweep inputs, which do not change during the solve (the normal
+    // stays where it is)
+    const bool pos_rows = has && cf.pos_iters > 0u;
+    if (pos_rows) {
+        for (uint32_t slot = t; slot < nslot; slot += T) {
+            const uint4 mv = sm.man[slot];
+            const CPV vg = cpv_global(w, sm.pos[slot]);
+            float* rows = row_of(slot, mv.z);
+            for (uint32_t i = 0; i < mv.z; ++i) {
+                float* r = rows + (size_t)i * CP_NVEL;
+                cpr(vg, CP_NM, i) = r[CP_NM];
+                cpr(vg, CP_TM0, i) = r[CP_TM0];
+                cpr(vg, CP_TM1, i) = r[CP_TM1];
+                cpr(vg, CP_NI, i) = r[CP_NI];
+                cpr(vg, CP_TI0, i) = r[CP_TI0];
+                cpr(vg, CP_TI1, i) = r[CP_TI1];
+                const F3 la = ld3(vg, CP_LAX, i), lb = ld3(vg, CP_LBX, i);
+                const float base = cpr(vg, CP_BASE, i);
+                r[CP_PX] = la.x; r[CP_PX + 1u] = la.y; r[CP_PX + 2u] = la.z;
+                r[CP_RAX] = lb.x; r[CP_RAX + 1u] = lb.y; r[CP_RAX + 2u] = lb.z;
+                r[CP_RBX] = base;
+            }
+        }
+        __syncthreads();  // the rows of this CTA are its own
+    }
     if (has) {
         for (uint32_t it = 0; it < cf.pos_iters; ++it) {
             float mn = 0.0f, mx = -__int_as_float(0x7f800000);
@@ -3903,7 +3981,7 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
                     const DBody A = *pa, B = *pb;
                     PB a = pb_of(A.p, A.q, A.i0, A.i1, A.i2, (mv.w & CM_WA) != 0u);
                     PB b = pb_of(B.p, B.q, B.i0, B.i1, B.i2, (mv.w & CM_WB) != 0u);
-                    position_points(sf, cpv_global(w, sm.pos[slot]), mv.z, a, b, &mn, &mx);
+                    position_points_rows(sf, row_of(slot, mv.z), mv.z, a, b, &mn, &mx);
                     if (a.wr) {
                         pa->p = make_float4(a.x.x, a.x.y, a.x.z, a.im);
                         pa->q = f4of(a.q);
@@ -3929,7 +4007,7 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
         if (i >= N) break;
         if (w.prop[i].type != 0u) w.body[i] = sm.body[q];
     }
-    for (uint32_t slot = t; slot < nslot; slot += T) {
+    for (uint32_t slot = pos_rows ? nslot : t; slot < nslot; slot += T) {  // done above when pos_rows
         const uint4 mv = sm.man[slot];
         const CPV vg = cpv_global(w, sm.pos[slot]), vs{row_of(slot, mv.z), 1u, CP_NVEL};
         for (uint32_t i = 0; i < mv.z; ++i) {
