@@ -59,17 +59,16 @@ SOLVER_V, SOLVER_Q = 1, 2
 
 # DRAM bytes (read + write) per launch of each step kernel, keyed by
 # (workload, kernel), from one ncu capture of the same workload (the pile's
-# state after 360 steps; the stress scene's first steps) with the kernels as
-# of commit d08c536, summarised in the profile file named beside each; to be
-# captured again whenever a kernel changes.  The bench line carries the
-# commit next to the figure.
-PROFILED_TRAFFIC_COMMIT = "d08c536"
+# state after 360 steps; the stress scene's first steps): the bytes, the
+# profile file that summarises the capture, and the commit whose kernel was
+# captured; to be captured again whenever a kernel changes.  The bench line
+# carries the commit next to the figure.
+_PILE_PROFILE = "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"
 PROFILED_TRAFFIC = {
-    ("config2_pile_4096", "k_step_grid"): (54_253_312, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
-    ("config2_pile_4096", "k_solve_grid"): (7_303_680, "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
-    ("config2_pile_4096", "k_solve_cluster"): (4_129_792,
-                                               "profiles/k_step_grid_k_solve_grid_k_solve_cluster_config2_pile.md"),
-    ("config4_stress_512", "k_step_grid"): (755_527_680, "profiles/k_step_grid_config4_stress.md"),
+    ("config2_pile_4096", "k_step_grid"): (54_253_312, _PILE_PROFILE, "d08c536"),
+    ("config2_pile_4096", "k_solve_grid"): (7_303_680, _PILE_PROFILE, "d08c536"),
+    ("config2_pile_4096", "k_solve_cluster"): (4_125_184, _PILE_PROFILE, "8a7312f"),
+    ("config4_stress_512", "k_step_grid"): (755_527_680, "profiles/k_step_grid_config4_stress.md", "d08c536"),
 }
 
 
@@ -485,7 +484,7 @@ def ours(args):
                          "frac": kernels[dominant]["frac"],
                          "traffic": PROFILED_TRAFFIC.get((workload, dominant), (None,))[0],
                          "traffic_source": PROFILED_TRAFFIC.get((workload, dominant), (None, None))[1],
-                         "traffic_captured_at": PROFILED_TRAFFIC_COMMIT,
+                         "traffic_captured_at": PROFILED_TRAFFIC.get((workload, dominant), (None, None, None))[2],
                          "peak_kind": peak_kind, "kernel": dominant,
                          "alg_bytes_per_launch": kernels[dominant]["alg_bytes_per_launch"],
                          "step": {"achieved": achieved, "frac": achieved / peak,
