@@ -463,9 +463,10 @@ int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]);
 /* Diagnostics: ns from the start of the last step kernel to the end of each
  * of its phases: [start, begin, pairs, cache, probe, finalize, constraints,
  * solve, end, islands, broad phase, sweep setup, sweep substeps, position
- * sweeps] (islands: the IslandManager pass beside the constraint phase;
- * broad phase: the device pair list, when the step builds it; the last
- * three: the shared-memory sweeps' setup, substeps and position sweeps). */
+ * sweeps, sweep kernel start] (islands: the IslandManager pass beside the
+ * constraint phase; broad phase: the device pair list, when the step builds
+ * it; the last four: the shared-memory sweeps' setup, substeps and position
+ * sweeps, and the first instruction of the cluster kernel). */
 int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n);
 
 /* ---------------------------------------------------------------------------

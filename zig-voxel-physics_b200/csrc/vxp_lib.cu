@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(256, 1) k_solve_cluster(const WorldDev* world,
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&w.ctr[C_ERROR], ERR_BOUNDS);
         return;
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && w.ts) w.ts[TS_SW_START] = global_ns();
     ClusterGroup g;
     world_step_sweeps(g, w, smem_raw, smem_bytes, whole != 0u);
 }

@@ -3650,18 +3650,42 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
         const uint32_t n = w.colour_cnt[c + 1u] - w.colour_cnt[c];
         return n > cta ? (n - 1u - cta) / C + 1u : 0u;
     };
+    // every CTA's slots and points under both dealings, tallied by every
+    // block at once from the packing's counts (one or two loads a thread,
+    // then shared atomics; the same values, so the same verdicts, in every
+    // block): [0] slots by owner, [1] slots round-robin, [2] points by owner,
+    // [3] points round-robin
+    __shared__ uint32_t s_tally[4][kMaxOwnerGroups];
+    __shared__ int s_bad;
+    if (C > kMaxOwnerGroups) return false;
+    for (uint32_t x = t; x < 4u * kMaxOwnerGroups; x += T) (&s_tally[0][0])[x] = 0u;
+    if (t == 0) s_bad = 0;
+    __syncthreads();
+    const bool owner_ok = by_owner;
+    for (uint32_t x = t; x < ncol * C; x += T) {
+        const uint32_t c = x / C, cta = x - c * C;
+        const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
+        if (cta == 0u && (hi < lo || hi > M)) s_bad = 1;
+        const uint32_t n = hi - lo;
+        const uint32_t rr = n > cta && hi >= lo ? (n - 1u - cta) / C + 1u : 0u;
+        if (rr) atomicAdd(&s_tally[1][cta], rr);
+        if (owner_ok) {
+            const uint32_t o = w.ocnt[c * C + cta + 1u] - w.ocnt[c * C + cta];
+            if (o) atomicAdd(&s_tally[0][cta], o);
+        }
+    }
+    const bool tallied = C > 1u && w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
+    if (tallied && t < C) {
+        s_tally[2][t] = w.ocnt[kOwnerPoints + t];
+        s_tally[3][t] = w.ocnt[kOwnerPoints + kMaxOwnerGroups + t];
+    }
+    __syncthreads();
+    if (s_bad) return false;
     // the most slots any CTA holds (the same verdict in every block)
     uint32_t need = 0;
-    for (uint32_t c = 0; c < ncol; ++c) {
-        const uint32_t lo = w.colour_cnt[c], hi = w.colour_cnt[c + 1u];
-        if (hi < lo || hi > M) return false;
-    }
     ClusterSolveSmem sm;
     sm.bcap = (N + C - 1u) / C;
     sm.nrep = w.n_static <= kMaxStaticReplicas ? w.n_static : 0u;
-    // points: the packing's tallies when it grouped for this cluster, else
-    // four per slot
-    const bool tallied = C > 1u && w.cfg.owner_groups == C && C <= kMaxOwnerGroups;
     // point rows that do not fit in shared memory may go to w.crow: a CTA's
     // last slots (the point offsets are a prefix in slot order, so once a
     // slot's rows spill every later slot's do), in that CTA's range of w.crow
@@ -3673,11 +3697,11 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
         goff = 0;
         gtot = 0;
         for (uint32_t cta = 0; cta < C; ++cta) {
-            uint32_t n = 0;
-            for (uint32_t c = 0; c < ncol; ++c) n += count_of(c, cta);
+            const uint32_t n = s_tally[by_owner ? 0 : 1][cta];
             need = max(need, n);
-            // one CTA holds every point of the constraint set
-            const uint32_t p = tallied ? w.ocnt[kOwnerPoints + (by_owner ? 0u : kMaxOwnerGroups) + cta]
+            // points: the packing's tallies when it grouped for this cluster;
+            // one CTA holds every point of the constraint set; else four a slot
+            const uint32_t p = tallied ? s_tally[by_owner ? 2 : 3][cta]
                                : C == 1u ? *(volatile uint32_t*)&w.ctr[C_POINTS]
                                          : 4u * n;
             needp = max(needp, p);

@@ -213,7 +213,7 @@ enum : uint32_t {
 // Phase boundaries recorded in WorldDev::ts by rank 0 (diagnostics).
 enum : uint32_t {
     TS_START, TS_BEGIN, TS_PAIRS, TS_CACHE, TS_PROBE, TS_FINALIZE, TS_CONSTRAINTS, TS_SOLVE, TS_END, TS_ISLANDS,
-    TS_BROAD, TS_SW_SETUP, TS_SW_SUBSTEPS, TS_SW_POSITION, TS_N = 16
+    TS_BROAD, TS_SW_SETUP, TS_SW_SUBSTEPS, TS_SW_POSITION, TS_SW_START, TS_N = 16
 };
 // C_SWEEP: the cluster kernel's sweeps with every constraint row in shared
 // memory, with the rows that did not fit in global memory, or with all
