@@ -2217,16 +2217,13 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
     if (!g.sync()) return false;
     {
         uint32_t tot;
-        // in-place exclusive scan: read counts into adj_cur, write offsets
-        for (uint32_t i = g.rank(); i < N; i += g.size()) w.adj_cur[i] = w.adj_off[i];
-        if (!g.sync()) return false;
+        // exclusive scan of the counts in place (group_scan reads and writes
+        // each element in the same thread and tile); adj_cur is still zero
         if (!group_scan(
-                g, N, [&](uint32_t i) { return w.adj_cur[i]; }, [&](uint32_t i, uint32_t pre) { w.adj_off[i] = pre; },
+                g, N, [&](uint32_t i) { return w.adj_off[i]; }, [&](uint32_t i, uint32_t pre) { w.adj_off[i] = pre; },
                 w.scan, &tot))
             return false;
         if (g.rank() == 0) w.adj_off[N] = tot;
-        for (uint32_t i = g.rank(); i < N; i += g.size()) w.adj_cur[i] = 0u;
-        if (!g.sync()) return false;
         for (uint32_t k = g.rank(); k < M; k += g.size()) {
             const PairInfo& pi = w.pinfo[w.cons[k]];
             if (writable(w.prop[pi.ia])) w.adj[w.adj_off[pi.ia] + atomicAdd(&w.adj_cur[pi.ia], 1u)] = k;
@@ -2361,29 +2358,53 @@ __device__ bool phase_constraints(G& g, WorldDev& w, uint32_t cur, uint32_t* M_o
     }
     if (!g.sync()) return false;
     if (NG > 1u && g.block() == 0u) {
-        // exclusive scan of the (colour, group) counts, colour-major, by block 0
+        // exclusive scan of the (colour, group) counts, colour-major, by block
+        // 0: each thread's run of at most 16 counts loaded at once (one round
+        // trip, not one per count), scanned, stored
+        constexpr uint32_t kPer = 16;
         const uint32_t E = 256u * NG, per = (E + blockDim.x - 1u) / blockDim.x, lo = threadIdx.x * per;
+        uint32_t v[kPer];
         uint32_t sum = 0;
-        for (uint32_t i = lo; i < min(E, lo + per); ++i) sum += w.ocnt[i];
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; ++j) {
+            const uint32_t i = lo + j;
+            v[j] = j < per && i < E ? w.ocnt[i] : 0u;
+            sum += v[j];
+        }
+        // (blocks of fewer than 256 threads: the rest of each run one by one)
+        for (uint32_t i = lo + kPer; i < min(E, lo + per); ++i) sum += w.ocnt[i];
         uint32_t total = 0;
         uint32_t run = block_excl_scan(sum, &total);
-        for (uint32_t i = lo; i < min(E, lo + per); ++i) {
-            const uint32_t v = w.ocnt[i];
+#pragma unroll
+        for (uint32_t j = 0; j < kPer; ++j) {
+            const uint32_t i = lo + j;
+            if (j < per && i < E) {
+                w.ocnt[i] = run;
+                run += v[j];
+            }
+        }
+        for (uint32_t i = lo + kPer; i < min(E, lo + per); ++i) {
+            const uint32_t x = w.ocnt[i];
             w.ocnt[i] = run;
-            run += v;
+            run += x;
         }
         if (threadIdx.x == 0) w.ocnt[E] = total;
     }
     if (g.rank() < 32u) {
+        // exclusive scan of the 256 colour counts by one warp: all eight
+        // loads first, then the scans
         const uint32_t lane = threadIdx.x & 31;
+        uint32_t v[8];
+#pragma unroll
+        for (uint32_t r = 0; r < 8u; ++r) v[r] = w.colour_cnt[32u * r + lane];
         uint32_t carry = 0, last = 0;
-        for (uint32_t c0 = 0; c0 < 256u; c0 += 32u) {
-            const uint32_t v = w.colour_cnt[c0 + lane];
-            const uint32_t inc = warp_incl_scan(v);
-            const uint32_t nz = __ballot_sync(0xffffffffu, v != 0u);
+#pragma unroll
+        for (uint32_t r = 0; r < 8u; ++r) {
+            const uint32_t c0 = 32u * r;
+            const uint32_t inc = warp_incl_scan(v[r]);
+            const uint32_t nz = __ballot_sync(0xffffffffu, v[r] != 0u);
             if (nz) last = c0 + 32u - __clz(nz);
-            __syncwarp();
-            w.colour_cnt[c0 + lane] = carry + inc - v;
+            w.colour_cnt[c0 + lane] = carry + inc - v[r];
             carry += __shfl_sync(0xffffffffu, inc, 31);
         }
         if (lane == 0) {
