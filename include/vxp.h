@@ -463,10 +463,13 @@ int vxp_last_solve_split_ms(vxp_ctx* ctx, float out[2]);
 /* Diagnostics: ns from the start of the last step kernel to the end of each
  * of its phases: [start, begin, pairs, cache, probe, finalize, constraints,
  * solve, end, islands, broad phase, sweep setup, sweep substeps, position
- * sweeps, sweep kernel start] (islands: the IslandManager pass beside the
- * constraint phase; broad phase: the device pair list, when the step builds
- * it; the last four: the shared-memory sweeps' setup, substeps and position
- * sweeps, and the first instruction of the cluster kernel). */
+ * sweeps, sweep kernel start, broad-phase boxes, broad-phase count pass,
+ * broad-phase scan, pair id lookup, pair SAT and regions, sweep slot records,
+ * sweep rows] (islands: the IslandManager pass beside the constraint phase;
+ * broad phase: the device pair list, when the step builds it; sweep: the
+ * shared-memory sweeps of the cluster kernel or a one-CTA world); at most
+ * 23 entries.  A phase that did not run this step leaves a stale or zero
+ * entry. */
 int vxp_phase_times(vxp_ctx* ctx, uint64_t* out, uint32_t n);
 
 /* ---------------------------------------------------------------------------

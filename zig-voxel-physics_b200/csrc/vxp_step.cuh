@@ -595,13 +595,16 @@ __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool*
     if (!g.sync()) return false;
     const uint32_t lane = threadIdx.x & 31, wid = g.rank() >> 5, nw = g.size() >> 5;
     const bool masks = w.bpmask != nullptr && N <= w.bp_rows;
+    if (g.rank() == 0 && w.ts) w.ts[TS_BP_AABB] = global_ns();
     for (int pass = 0; pass < 2; ++pass) {
         if (pass == 1) {
+            if (g.rank() == 0 && w.ts) w.ts[TS_BP_COUNT] = global_ns();
             uint32_t total = 0;
             if (!group_scan(
                     g, N, [&](uint32_t i) { return w.pcount[i]; }, [&](uint32_t i, uint32_t pre) { w.poff[i] = pre; },
                     w.scan, &total))
                 return false;
+            if (g.rank() == 0 && w.ts) w.ts[TS_BP_SCAN] = global_ns();
             *overflow = total > w.pair_cap;
             w.n_pairs = total;
             if (g.rank() == 0) *w.n_pairs_dev = total;
@@ -702,6 +705,7 @@ __device__ bool phase_pairs(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
         w.flag[p] = (fl & PF_CARRY) ? 0u : 1u;
     }
     if (!g.sync()) return false;
+    if (g.rank() == 0 && w.ts) w.ts[TS_PR_IDS] = global_ns();
     if (w.cfg.reference_caps) {
         uint32_t tot;
         if (!group_scan(
@@ -772,6 +776,7 @@ __device__ bool phase_pairs(G& g, WorldDev& w, const ColliderSet& cs, uint32_t c
     tested = warp_sum(tested);
     if ((threadIdx.x & 31) == 0 && tested) atomicAdd(&w.ctr[C_PAIRS_TESTED], tested);
     if (!g.sync()) return false;
+    if (g.rank() == 0 && w.ts) w.ts[TS_PR_SAT] = global_ns();
     if (w.cfg.use_cache) {
         // the lookups of the pairs consulting the cache, in pair order, for
         // the replay warp (window starts computed here, off its chain)
@@ -3833,6 +3838,7 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
         }
     }
     __syncthreads();
+    if (g.rank() == 0 && w.ts) w.ts[TS_SW_SLOTS] = global_ns();
     // each slot's first point: exclusive scan of the point counts in slot order
     const uint32_t nsl = sm.base[ncol];
     uint32_t carry = 0;
@@ -3864,13 +3870,30 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
             continue;
         }
         const CPV vg = cpv_global(w, sm.pos[slot]), vs{row_of(slot, mv.z), 1u, CP_NVEL};
-        for (uint32_t i = 0; i < mv.z; ++i) {
-            st3(vs, CP_NX, i, ld3(vg, CP_NX, i));
-            cpr(vs, CP_NI, i) = cpr(vg, CP_NI, i);
-            cpr(vs, CP_TI0, i) = cpr(vg, CP_TI0, i);
-            cpr(vs, CP_TI1, i) = cpr(vg, CP_TI1, i);
+        // every point's fields loaded before any is stored (the stores would
+        // otherwise hold each next point's loads back)
+        F3 nn[4];
+        float ni[4], t0[4], t1[4];
+#pragma unroll
+        for (uint32_t i = 0; i < 4u; ++i) {
+            if (i < mv.z) {
+                nn[i] = ld3(vg, CP_NX, i);
+                ni[i] = cpr(vg, CP_NI, i);
+                t0[i] = cpr(vg, CP_TI0, i);
+                t1[i] = cpr(vg, CP_TI1, i);
+            }
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < 4u; ++i) {
+            if (i < mv.z) {
+                st3(vs, CP_NX, i, nn[i]);
+                cpr(vs, CP_NI, i) = ni[i];
+                cpr(vs, CP_TI0, i) = t0[i];
+                cpr(vs, CP_TI1, i) = t1[i];
+            }
         }
     }
+    if (g.rank() == 0 && w.ts) w.ts[TS_SW_ROWS] = global_ns();
     g.sync();  // every block's bodies are in place (and every block has started)
     if (g.rank() == 0 && w.ts) w.ts[TS_SW_SETUP] = global_ns();
     const SolveFlags sf = solve_flags(cf);
@@ -3995,19 +4018,32 @@ __device__ bool phase_solve_cluster(G& g, WorldDev& w, uint32_t M, uint32_t ncol
             const uint4 mv = sm.man[slot];
             const CPV vg = cpv_global(w, sm.pos[slot]);
             float* rows = row_of(slot, mv.z);
-            for (uint32_t i = 0; i < mv.z; ++i) {
-                float* r = rows + (size_t)i * CP_NVEL;
-                cpr(vg, CP_NM, i) = r[CP_NM];
-                cpr(vg, CP_TM0, i) = r[CP_TM0];
-                cpr(vg, CP_TM1, i) = r[CP_TM1];
-                cpr(vg, CP_NI, i) = r[CP_NI];
-                cpr(vg, CP_TI0, i) = r[CP_TI0];
-                cpr(vg, CP_TI1, i) = r[CP_TI1];
-                const F3 la = ld3(vg, CP_LAX, i), lb = ld3(vg, CP_LBX, i);
-                const float base = cpr(vg, CP_BASE, i);
-                r[CP_PX] = la.x; r[CP_PX + 1u] = la.y; r[CP_PX + 2u] = la.z;
-                r[CP_RAX] = lb.x; r[CP_RAX + 1u] = lb.y; r[CP_RAX + 2u] = lb.z;
-                r[CP_RBX] = base;
+            // the packed inputs of every point loaded first, then the rows
+            // rewritten (stores would otherwise hold the next loads back)
+            F3 la[4], lb[4];
+            float base[4];
+#pragma unroll
+            for (uint32_t i = 0; i < 4u; ++i) {
+                if (i < mv.z) {
+                    la[i] = ld3(vg, CP_LAX, i);
+                    lb[i] = ld3(vg, CP_LBX, i);
+                    base[i] = cpr(vg, CP_BASE, i);
+                }
+            }
+#pragma unroll
+            for (uint32_t i = 0; i < 4u; ++i) {
+                if (i < mv.z) {
+                    float* r = rows + (size_t)i * CP_NVEL;
+                    cpr(vg, CP_NM, i) = r[CP_NM];
+                    cpr(vg, CP_TM0, i) = r[CP_TM0];
+                    cpr(vg, CP_TM1, i) = r[CP_TM1];
+                    cpr(vg, CP_NI, i) = r[CP_NI];
+                    cpr(vg, CP_TI0, i) = r[CP_TI0];
+                    cpr(vg, CP_TI1, i) = r[CP_TI1];
+                    r[CP_PX] = la[i].x; r[CP_PX + 1u] = la[i].y; r[CP_PX + 2u] = la[i].z;
+                    r[CP_RAX] = lb[i].x; r[CP_RAX + 1u] = lb[i].y; r[CP_RAX + 2u] = lb[i].z;
+                    r[CP_RBX] = base[i];
+                }
             }
         }
         __syncthreads();  // the rows of this CTA are its own

@@ -213,7 +213,9 @@ enum : uint32_t {
 // Phase boundaries recorded in WorldDev::ts by rank 0 (diagnostics).
 enum : uint32_t {
     TS_START, TS_BEGIN, TS_PAIRS, TS_CACHE, TS_PROBE, TS_FINALIZE, TS_CONSTRAINTS, TS_SOLVE, TS_END, TS_ISLANDS,
-    TS_BROAD, TS_SW_SETUP, TS_SW_SUBSTEPS, TS_SW_POSITION, TS_SW_START, TS_N = 16
+    TS_BROAD, TS_SW_SETUP, TS_SW_SUBSTEPS, TS_SW_POSITION, TS_SW_START,
+    // inside the broad phase, the pair filter and the sweep setup
+    TS_BP_AABB, TS_BP_COUNT, TS_BP_SCAN, TS_PR_IDS, TS_PR_SAT, TS_SW_SLOTS, TS_SW_ROWS, TS_N = 24
 };
 // C_SWEEP: the cluster kernel's sweeps with every constraint row in shared
 // memory, with the rows that did not fit in global memory, or with all
