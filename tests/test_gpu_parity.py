@@ -94,6 +94,14 @@ def test_config1_trajectory_bit_exact(vxp, mode):
     lockstep(vxp, sc, 300 if mode == 0 else 120, mode=mode).close()
 
 
+def test_pile_subset_device_pair_source_on_the_grid(vxp):
+    """The grid step's own broad phase (its count pass tiled through shared
+    memory, two tiles for 217 bodies) on 216 boxes of the pile: every step's
+    results equal the oracle's on the oracle's pair list."""
+    sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
+    lockstep(vxp, sc, 120, mode=1, own_pairs=True, check_every=10, substeps=8).close()
+
+
 def test_config1_device_pair_source(vxp):
     sc = vxp.scenes.config1(mass_fn=O.mass_fn, seed=9)
     lockstep(vxp, sc, 150, own_pairs=True).close()

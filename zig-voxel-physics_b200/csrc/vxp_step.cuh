@@ -559,7 +559,7 @@ __device__ bool phase_begin(G& g, WorldDev& w, bool skip_test, bool* skipped) {
 // the list does not fit pair_cap (nothing is written; the host grows the
 // buffers).
 template <class G>
-__device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool* overflow) {
+__device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool* overflow, unsigned char* smem) {
     const uint32_t N = w.n_bodies;
     const float m = w.cfg.margin;
     // inflated world AABBs in id order (position s holds body ids[s]), w = 1
@@ -596,7 +596,75 @@ __device__ bool phase_broadphase(G& g, WorldDev& w, const ColliderSet& cs, bool*
     const uint32_t lane = threadIdx.x & 31, wid = g.rank() >> 5, nw = g.size() >> 5;
     const bool masks = w.bpmask != nullptr && N <= w.bp_rows;
     if (g.rank() == 0 && w.ts) w.ts[TS_BP_AABB] = global_ns();
-    for (int pass = 0; pass < 2; ++pass) {
+    // The count pass with the boxes staged in shared memory, kBpTile at a
+    // time, when every warp holds at most one row pair and the hit masks are
+    // kept (the grid launch): each warp tests the 32-column chunks of its two
+    // rows that start in the tile (the tile holds 32 boxes more for the
+    // chunks that run past its end).  The same chunks, masks and counts as
+    // the sweep below; its write pass follows.
+    // tiles of up to 512 boxes, as many as the launch's dynamic shared memory
+    // holds (each tile is one round trip to L2 for the block)
+    uint32_t dyn = 0;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    const uint32_t kBpTile = min(512u, (dyn / (2u * (uint32_t)sizeof(float4)) > 32u
+                                            ? dyn / (2u * (uint32_t)sizeof(float4)) - 32u
+                                            : 0u) & ~31u);
+    const uint32_t kBpSpan = kBpTile + 32u;
+    const bool tiled = masks && smem != nullptr && (N + 1u) / 2u <= nw && kBpTile >= 128u;
+    if (tiled) {
+        float4* tmn = reinterpret_cast<float4*>(smem);
+        float4* tmx = tmn + kBpSpan;
+        const uint32_t r = wid;
+        const bool rows = r < (N + 1u) / 2u;
+        const uint32_t s2[2] = {r, N - 1u - r};
+        bool act[2], si[2];
+        float4 a0[2], a1[2];
+        uint32_t cnt[2] = {0u, 0u};
+#pragma unroll
+        for (uint32_t h = 0; h < 2u; ++h) {
+            act[h] = rows && !(h && s2[1] == r);
+            a0[h] = act[h] ? w.aabb_mn[s2[h]] : make_float4(0.f, 0.f, 0.f, 0.f);
+            a1[h] = act[h] ? w.aabb_mx[s2[h]] : make_float4(0.f, 0.f, 0.f, 0.f);
+            si[h] = a0[h].w != 0.f;
+        }
+        for (uint32_t tile0 = 0; tile0 < N; tile0 += kBpTile) {
+            __syncthreads();
+            for (uint32_t x = threadIdx.x; x < kBpSpan; x += blockDim.x) {
+                const uint32_t t = tile0 + x;
+                if (t < N) {
+                    tmn[x] = w.aabb_mn[t];
+                    tmx[x] = w.aabb_mx[t];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (uint32_t h = 0; h < 2u; ++h) {
+                if (!act[h]) continue;
+                const uint32_t s = s2[h];
+                // this row's chunks c = s + 1 + 32 j that start in the tile
+                uint32_t c = s + 1u;
+                if (c < tile0) c += (tile0 - c + 31u) / 32u * 32u;
+                for (; c < tile0 + kBpTile && c < N; c += 32u) {
+                    const uint32_t t = c + lane;
+                    bool hit = false;
+                    if (t < N) {
+                        const float4 b0 = tmn[t - tile0], b1 = tmx[t - tile0];
+                        hit = !(si[h] && b0.w != 0.f) && a0[h].x <= b1.x && a1[h].x >= b0.x && a0[h].y <= b1.y &&
+                              a1[h].y >= b0.y && a0[h].z <= b1.z && a1[h].z >= b0.z;
+                    }
+                    const uint32_t mk = __ballot_sync(0xffffffffu, hit);
+                    if (lane == 0) w.bpmask[(size_t)s * w.bp_stride + (c - s - 1u) / 32u] = mk;
+                    cnt[h] += (uint32_t)__popc(mk);
+                }
+            }
+        }
+        if (lane == 0) {
+            if (act[0]) w.pcount[s2[0]] = cnt[0];
+            if (act[1]) w.pcount[s2[1]] = cnt[1];
+        }
+        if (!g.sync()) return false;
+    }
+    for (int pass = tiled ? 1 : 0; pass < 2; ++pass) {
         if (pass == 1) {
             if (g.rank() == 0 && w.ts) w.ts[TS_BP_COUNT] = global_ns();
             uint32_t total = 0;
@@ -4199,7 +4267,7 @@ __device__ bool world_step_narrow(G& g, WorldDev& w, const ColliderSet& cs, Warp
     if (skipped) return false;
     if ((ph & PH_NARROW) && w.cfg.device_pairs) {
         bool overflow = false;
-        if (!phase_broadphase(g, w, cs, &overflow)) return false;
+        if (!phase_broadphase(g, w, cs, &overflow, reinterpret_cast<unsigned char*>(warp_sm))) return false;
         stamp(g, w, TS_BROAD);
         if (overflow) {
             if (g.rank() == 0) atomicOr(&w.ctr[C_ERROR], ERR_CAP);
