@@ -96,10 +96,11 @@ def test_config1_trajectory_bit_exact(vxp, mode):
 
 def test_pile_subset_device_pair_source_on_the_grid(vxp):
     """The grid step's own broad phase (its count pass tiled through shared
-    memory, two tiles for 217 bodies) on 216 boxes of the pile: every step's
-    results equal the oracle's on the oracle's pair list."""
-    sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=6, seed=2)
-    lockstep(vxp, sc, 120, mode=1, own_pairs=True, check_every=10, substeps=8).close()
+    memory, 512 boxes a tile: two tiles for the 514 bodies here) on 512 boxes
+    of the pile: every step's results equal the oracle's on the oracle's pair
+    list."""
+    sc = vxp.scenes.config2(mass_fn=O.mass_fn, n_side=8, seed=2)
+    lockstep(vxp, sc, 100, mode=1, own_pairs=True, check_every=10, substeps=8).close()
 
 
 def test_config1_device_pair_source(vxp):
