@@ -16,7 +16,7 @@ memory: every step copies the pair list host->device (vxp_step) and reads the
 pair list and the body table back (vxp_pairs_from_bodies, vxp_bodies_get),
 timed by the host clock.
 
-The pile's line also carries compact runs of the other two north-star
+The pile's line also carries compact runs of the batched and served
 comparisons, on the same box: "batched" (the 256-world mix under the
 autotuned schedule against the plain single-world path, 10 timed steps) and
 "serving" (150 Poisson-arriving jobs through the continuous-batching server,
@@ -450,7 +450,7 @@ def ours(args):
     sysm.close()
     extras = {}
     if rank == 0 and ws == 1 and args.workload == "pile" and not args.no_extras:
-        # the north-star comparisons, measured on the same box in the same run
+        # the batched and served comparisons, measured on the same box in the same run
         # (compact versions of --workload batched / serving)
         bl = batched(args, steps=10, warmup=3, emit=False)
         extras["batched"] = {k: bl[k] for k in ("value", "unit", "ms_per_step", "plain_single_world",
